@@ -1,0 +1,155 @@
+/*
+ * rsdft_b200.h -- C ABI of the B200 (sm_100a) band-update library for RSDFT.
+ *
+ * The library replaces the four module procedures of RSDFT_DEVELOP's band
+ * update with CUDA implementations that keep the wavefunctions resident in HBM:
+ *
+ *   hamiltonian(tpsi, htpsi, n, k, s)            src/hamiltonian_module.f90:44-46,118-172
+ *   conjugate_gradient(n1, n2, k, s, unk, esp, res)
+ *                                                src/conjugate_gradient/cg_module.f90:53-109
+ *   gram_schmidt(n0, n1, k, s)                   src/gram_schmidt/gram_schmidt_module.f90:35-79
+ *   subspace_diag(k, s, unk, esp)                src/subspace_diag/subspace_diag_module.f90:17-32
+ *
+ * plus the sweep driver order of calc_sweep (src/sweep_module.f90:148-215).
+ *
+ * Conventions (chosen so a Fortran ISO_C_BINDING shim can pass its arrays as is):
+ *  - k, s, band and grid indices are 1-based, as in the reference;
+ *  - wavefunction blocks are Fortran column-major unk(ML0, nb): band-major,
+ *    grid index j = 1 + i1 + i2*N1 + i3*N1*N2 (x fastest,
+ *    src/kinetic/d_kinetic_sol_module.f90:129);
+ *  - complex16 arrays are interleaved (re, im) pairs, i.e. Fortran complex(8);
+ *  - every entry returns RSDFT_OK (0) or a negative status; it never aborts.
+ *    rsdft_gpu_last_error() gives the message of the last failure (the
+ *    reference instead calls stop_program, e.g. src/hamiltonian_module.f90:396).
+ *  - single-threaded host use: one implicit context per process, one CUDA
+ *    stream; not re-entrant (the reference calls these from the serial part of
+ *    its OpenMP code, src/hamiltonian_module.f90:123-140).
+ */
+#ifndef RSDFT_B200_H
+#define RSDFT_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define RSDFT_OK               0
+#define RSDFT_ERR_ARG         -1   /* invalid argument / size */
+#define RSDFT_ERR_OOM         -2   /* device allocation failed */
+#define RSDFT_ERR_CUDA        -3   /* CUDA runtime / library error */
+#define RSDFT_ERR_NOT_SPD     -4   /* overlap matrix not positive definite (Cholesky) */
+#define RSDFT_ERR_EIG         -5   /* dense eigensolver failed */
+#define RSDFT_ERR_TIMEOUT     -6   /* a bounded device-side wait gave up */
+#define RSDFT_ERR_STATE       -7   /* call order (init/set_* missing) */
+#define RSDFT_ERR_UNSUPPORTED -8   /* configuration not built in */
+#define RSDFT_ERR_NUMERIC     -9   /* NaN/Inf detected in inputs or results */
+
+/* ---- precision modes ---- */
+#define RSDFT_PREC_FP64   0  /* all FP64 (the plain GPU drop-in) */
+#define RSDFT_PREC_MIXED  1  /* FP32 stencils/CG, split-BF16 GEMMs, FP64 dense solves + residuals */
+
+/* ---- preconditioner modes (SWPC in the reference, src/conjugate_gradient/cg_module.f90:27) ---- */
+#define RSDFT_PC_NONE      0
+#define RSDFT_PC_HPRSDFT   4   /* precond_hprsdft: mloop CG steps on the 7-point -1/2 Laplacian */
+#define RSDFT_PC_LEARNED 100   /* learned 3-D conv preconditioner, hprsdft fallback */
+
+/* ---- memory spaces for pointer arguments ---- */
+#define RSDFT_MEM_HOST    0
+#define RSDFT_MEM_DEVICE  1
+
+#define RSDFT_MDMAX 12
+
+/* Operator/grid description; mirrors init_kinetic + rgrid_module state
+ * (src/kinetic/kinetic_module.f90:28-162, src/rgrid_sol_module.f90:25-38). */
+typedef struct rsdft_gpu_params {
+  int n1, n2, n3;                 /* Ngrid(1:3) */
+  int md;                         /* FD half order Md (4 or 6 built in) */
+  double hgrid[3];                /* Hgrid(1:3) */
+  double dv;                      /* dV */
+  double coef_lap[3][RSDFT_MDMAX];/* coef_lap(d, m), m = 1..Md */
+  double coef_lap0;               /* coef_lap0 */
+  double ggg[3];                  /* ggg(1:3); preconditioner c0 = sum ggg/H^2 */
+  int nk;                         /* k-points held by this context */
+  int nspin;                      /* spins held by this context */
+  int mb;                         /* bands per (k, s) (maximum) */
+  int is_complex;                 /* 0: real8/Gamma build, 1: complex16 build */
+  int precision;                  /* RSDFT_PREC_* */
+  int pc_mode;                    /* RSDFT_PC_* */
+  int ncg;                        /* Ncg (default 3) */
+  int mloop;                      /* preconditioner inner steps (default 3) */
+  int cg_block;                   /* MB_d bands per batched CG block (0: automatic) */
+} rsdft_gpu_params;
+
+/* ---- context ---- */
+int rsdft_gpu_init(const rsdft_gpu_params* p);
+int rsdft_gpu_finalize(void);
+const char* rsdft_gpu_last_error(void);
+int rsdft_gpu_get_stream(void** stream);              /* the library's cudaStream_t */
+int rsdft_gpu_synchronize(void);
+
+/* ---- operator set-up ---- */
+/* k-dependent kinetic terms (coef_nabk(3,Md,k), const_k2(k); kinetic_module.f90:141-162)
+ * and the active band count of this k-point. */
+int rsdft_gpu_set_kpoint(int k, const double coef_nabk[3][RSDFT_MDMAX], double const_k2, int nband);
+/* Vloc(ML0, s) (src/localpot_module.f90:40-87). */
+int rsdft_gpu_set_vloc(const double* vloc, int ml, int s);
+/* Projector tables in the reference layout: MJJ(nzlma), JJP(MAXMJJ,nzlma) (1-based grid
+ * indices), amap(nzlma) atom of each projector, and the coupling in nzqr_pair(2,npair) /
+ * Dij00(npair) form (src/ps_nloc_mr_module.f90:852-897).  The KB form of
+ * src/d_ps_nloc2_op_module.f90 is npair = nzlma with pairs (p,p) and Dij00 = iuV(p).
+ * Pairs must couple projectors of the same atom. */
+int rsdft_gpu_set_projectors(int nzlma, int maxmjj, const int* mjj, const int* jjp,
+                             const int* amap, int npair, const int* pairs, const double* dij00);
+/* d_uVk(MAXMJJ, nzlma, k) / z_uVk(MAXMJJ, nzlma, k) for one k (ps_nloc2_module.f90:1070-1167). */
+int rsdft_gpu_set_uvk_d(int k, const double* uvk);
+int rsdft_gpu_set_uvk_z(int k, const double* uvk_interleaved);
+
+/* ---- wavefunctions (resident on the device between calls) ---- */
+int rsdft_gpu_set_wf_d(int k, int s, const double* unk, int ld, int nb);
+int rsdft_gpu_get_wf_d(int k, int s, double* unk, int ld, int nb);
+int rsdft_gpu_set_wf_z(int k, int s, const double* unk, int ld, int nb);
+int rsdft_gpu_get_wf_z(int k, int s, double* unk, int ld, int nb);
+/* Seeded device-side initial wavefunctions (replaces random_initial_wf,
+ * src/wf_module.f90:161-191): element e = ((k0*2^20 + band0)*ML0 + j)*2 + reim holds
+ * sum_{t<12} u(e,t) - 6, u = (splitmix64(seed*2^40 + 12e + t) >> 11) * 2^-53. */
+int rsdft_gpu_random_wf(int k, int s, uint64_t seed);
+
+/* ---- the four module procedures ---- */
+/* hamiltonian: htpsi(:,1:nb) = H tpsi(:,1:nb) (overwrites htpsi).  mem selects host or device
+ * pointers; _f is the FP32 variant on FP32 arrays. */
+int rsdft_gpu_hamiltonian_d(int k, int s, const double* tpsi, double* htpsi, int ld, int nb, int mem);
+int rsdft_gpu_hamiltonian_z(int k, int s, const double* tpsi, double* htpsi, int ld, int nb, int mem);
+int rsdft_gpu_hamiltonian_f(int k, int s, const float* tpsi, float* htpsi, int ld, int nb, int mem);
+int rsdft_gpu_hamiltonian_c(int k, int s, const float* tpsi, float* htpsi, int ld, int nb, int mem);
+/* conjugate_gradient on the resident unk(:,:,k,s); esp/res (host, length nband) as the
+ * reference's esp(:,k,s)/res(:,k,s), res = dV |H psi - e psi|^2 (cg_module.f90:231,556). */
+int rsdft_gpu_conjugate_gradient(int k, int s, double* esp, double* res);
+/* gram_schmidt(1, nband, k, s) on the resident unk (Cholesky-QR on the device). */
+int rsdft_gpu_gram_schmidt(int k, int s);
+/* subspace_diag(k, s, unk, esp): Rayleigh-Ritz on the resident unk; esp may be NULL. */
+int rsdft_gpu_subspace_diag(int k, int s, double* esp);
+/* FP64 residual check of the resident unk: esp = <x|Hx>/<x|x>, res = dV|Hx-esp x|^2/<x|x>dV. */
+int rsdft_gpu_residual(int k, int s, double* esp, double* res);
+/* Preconditioner alone (precond_hprsdft): pgk = P gk; test entry. */
+int rsdft_gpu_precond_d(int k, const double* gk, double* pgk, int ld, int nb, int mem);
+
+/* calc_sweep: up to nsweep iterations of CG -> GS -> SD over all (k, s); stops early when the
+ * FP64 residual max over bands <= tol (tol <= 0: never).  iters receives the sweeps done;
+ * esp/res (host, nband*nk*nspin, k-major after band) receive the final FP64 values. */
+int rsdft_gpu_sweep(int nsweep, double tol, int* iters, double* esp, double* res);
+
+/* ---- measurement ---- */
+/* Per-kernel CUDA-event timing of the library's own launches (off by default). */
+int rsdft_gpu_profile(int on);
+/* total device time (ms) and launch count recorded for kernel family `name`
+ * ("hpsi_stencil", "nl_gather", "gemm", "cg", "pc", ...). */
+int rsdft_gpu_profile_get(const char* name, double* total_ms, long long* launches);
+/* Launch count of all library kernels since init (for launch accounting). */
+long long rsdft_gpu_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RSDFT_B200_H */

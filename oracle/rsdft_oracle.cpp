@@ -1,0 +1,546 @@
+// CPU FP64 oracle for the RSDFT band-update hot path.
+//
+// TEST INFRASTRUCTURE ONLY.  This file restates the reference's CPU algorithms
+// loop for loop so the CUDA library can be checked against it; nothing in the
+// product (rsdft_develop_b200/) links, imports or calls it.  Parity is pinned
+// by exact known answers (FD rationals, plane-wave dispersion, dense-matrix
+// eigenvalues) in tests/, because the reference ships no golden vectors for
+// this path.
+//
+// Restated reference routines (paths relative to the RSDFT_DEVELOP tree):
+//   kinetic stencil + V_loc   src/kinetic/d_kinetic_sol_module.f90:29-292 (and the
+//                             complex flag_nab branch :144-200, z_kinetic_sol_module.f90)
+//   periodic halo             src/bc/bcset_3_module.f90:15-151 (one rank: wrap)
+//   nonlocal gather/Dij/scatter src/ps_nloc_mr_module.f90:1159-1359
+//                             (KB form src/d_ps_nloc2_op_module.f90:146-288 is the
+//                              diagonal-Dij special case)
+//   preconditioner            src/conjugate_gradient/cgpc_hprsdft_module.f90:133-361
+//   CG band update            src/conjugate_gradient/cg_module.f90:112-431 (real),
+//                             :434-754 (complex)
+//   Gram-Schmidt              src/gram_schmidt/gram_schmidt_t_module.f90:85-308
+//   subspace diagonalisation  src/subspace_diag/subspace_diag_la_module.f90:18-223
+//   sweep order               src/sweep_module.f90:158-167
+// Dense BLAS/LAPACK calls go to the OpenBLAS bundled with scipy (scipy_ prefix).
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+#include <type_traits>
+#include <omp.h>
+
+typedef std::complex<double> cplx;
+
+extern "C" {
+void scipy_dgemm_(const char*, const char*, const int*, const int*, const int*, const double*,
+                  const double*, const int*, const double*, const int*, const double*, double*,
+                  const int*);
+void scipy_zgemm_(const char*, const char*, const int*, const int*, const int*, const cplx*,
+                  const cplx*, const int*, const cplx*, const int*, const cplx*, cplx*, const int*);
+void scipy_dgemv_(const char*, const int*, const int*, const double*, const double*, const int*,
+                  const double*, const int*, const double*, double*, const int*);
+void scipy_zgemv_(const char*, const int*, const int*, const cplx*, const cplx*, const int*,
+                  const cplx*, const int*, const cplx*, cplx*, const int*);
+void scipy_dsyr2k_(const char*, const char*, const int*, const int*, const double*, const double*,
+                   const int*, const double*, const int*, const double*, double*, const int*);
+void scipy_zher2k_(const char*, const char*, const int*, const int*, const cplx*, const cplx*,
+                   const int*, const cplx*, const int*, const double*, cplx*, const int*);
+void scipy_dsyev_(const char*, const char*, const int*, double*, const int*, double*, double*,
+                  const int*, int*);
+void scipy_zheevd_(const char*, const char*, const int*, cplx*, const int*, double*, cplx*,
+                   const int*, double*, const int*, int*, const int*, int*);
+void scipy_dsygv_(const int*, const char*, const char*, const int*, double*, const int*, double*,
+                  const int*, double*, double*, const int*, int*);
+void scipy_zhegv_(const int*, const char*, const char*, const int*, cplx*, const int*, cplx*,
+                  const int*, double*, cplx*, const int*, double*, int*);
+void scipy_openblas_set_num_threads(int);
+}
+
+#define ORC_MDMAX 12
+
+// Operator description for one k-point (filled by oracle/oracle.py).
+struct OrcProb {
+  int n1, n2, n3, md;
+  double dV;
+  double coef_lap[3][ORC_MDMAX];   // coef_lap(d, m), m = 1..md
+  double coef_lap0;
+  double const_k2;
+  double zc_re[3][2 * ORC_MDMAX + 1];  // zcoef_kin(d, m) at index m + md
+  double zc_im[3][2 * ORC_MDMAX + 1];
+  double pc_c0, pc_c[3];           // precond_hprsdft coefficients (c0, c1..c3)
+  const double* vloc;
+  int nzlma, maxmjj;
+  const int* mjj;
+  const int* jjp;                  // 1-based, [nzlma][maxmjj]
+  const double* uv_re;             // [nzlma][maxmjj]
+  const double* uv_im;             // null for real8
+  int npair;
+  const int* pairs;                // [npair][2] 1-based (lma1, lma2)
+  const double* dij;               // [npair]
+  int ncg, mloop;
+  int is_complex;
+};
+
+static inline double conj_(double x) { return x; }
+static inline cplx conj_(cplx x) { return std::conj(x); }
+static inline double re_(double x) { return x; }
+static inline double re_(cplx x) { return x.real(); }
+static inline double abs2_(double x) { return x * x; }
+static inline double abs2_(cplx x) { return std::norm(x); }
+
+// ---------------------------------------------------------------------------
+// hpsi: kinetic (+V_loc) then nonlocal, one band at a time.
+// ---------------------------------------------------------------------------
+template <typename T>
+static void kinetic_band(const OrcProb* P, const T* tpsi, T* htpsi, std::vector<T>& www) {
+  const int n1 = P->n1, n2 = P->n2, n3 = P->n3, md = P->md;
+  const int p1 = n1 + 2 * md, p2 = n2 + 2 * md, p3 = n3 + 2 * md;
+  www.resize((size_t)p1 * p2 * p3);
+  // copy into the padded array and fill the periodic halo (bcset_3 on one rank)
+  for (int i3 = -md; i3 < n3 + md; ++i3)
+    for (int i2 = -md; i2 < n2 + md; ++i2)
+      for (int i1 = -md; i1 < n1 + md; ++i1) {
+        int j1 = ((i1 % n1) + n1) % n1, j2 = ((i2 % n2) + n2) % n2, j3 = ((i3 % n3) + n3) % n3;
+        www[(size_t)(i1 + md) + (size_t)p1 * ((i2 + md) + (size_t)p2 * (i3 + md))] =
+            tpsi[j1 + (size_t)n1 * (j2 + (size_t)n2 * j3)];
+      }
+  auto W = [&](int i1, int i2, int i3) -> T {
+    return www[(size_t)(i1 + md) + (size_t)p1 * ((i2 + md) + (size_t)p2 * (i3 + md))];
+  };
+  const double c = P->coef_lap0 + P->const_k2;
+  for (int i3 = 0; i3 < n3; ++i3)
+    for (int i2 = 0; i2 < n2; ++i2)
+      for (int i1 = 0; i1 < n1; ++i1) {
+        size_t j = i1 + (size_t)n1 * (i2 + (size_t)n2 * i3);
+        T acc = (c + P->vloc[j]) * W(i1, i2, i3);
+        if constexpr (std::is_same<T, double>::value) {
+          for (int m = 1; m <= md; ++m) {
+            acc += P->coef_lap[0][m - 1] * (W(i1 - m, i2, i3) + W(i1 + m, i2, i3));
+            acc += P->coef_lap[1][m - 1] * (W(i1, i2 - m, i3) + W(i1, i2 + m, i3));
+            acc += P->coef_lap[2][m - 1] * (W(i1, i2, i3 - m) + W(i1, i2, i3 + m));
+          }
+        } else {
+          for (int m = 1; m <= md; ++m) {
+            cplx zp[3], zm[3];
+            for (int d = 0; d < 3; ++d) {
+              zp[d] = cplx(P->zc_re[d][md + m], P->zc_im[d][md + m]);
+              zm[d] = std::conj(zp[d]);
+            }
+            acc += zp[0] * W(i1 + m, i2, i3) + zm[0] * W(i1 - m, i2, i3) +
+                   zp[1] * W(i1, i2 + m, i3) + zm[1] * W(i1, i2 - m, i3) +
+                   zp[2] * W(i1, i2, i3 + m) + zm[2] * W(i1, i2, i3 - m);
+          }
+        }
+        htpsi[j] = acc;
+      }
+}
+
+template <typename T> static T uv_at(const OrcProb* P, size_t idx);
+template <> double uv_at<double>(const OrcProb* P, size_t idx) { return P->uv_re[idx]; }
+template <> cplx uv_at<cplx>(const OrcProb* P, size_t idx) {
+  return cplx(P->uv_re[idx], P->uv_im ? P->uv_im[idx] : 0.0);
+}
+
+template <typename T>
+static void nonlocal_band(const OrcProb* P, const T* tpsi, T* htpsi, std::vector<T>& uvunk) {
+  uvunk.assign(P->nzlma, T(0));
+  for (int lma = 0; lma < P->nzlma; ++lma) {
+    T s = T(0);
+    for (int j = 0; j < P->mjj[lma]; ++j) {
+      size_t e = (size_t)lma * P->maxmjj + j;
+      s += conj_(uv_at<T>(P, e)) * tpsi[P->jjp[e] - 1];
+    }
+    uvunk[lma] = s * P->dV;
+  }
+  for (int m = 0; m < P->npair; ++m) {
+    int l1 = P->pairs[2 * m] - 1, l2 = P->pairs[2 * m + 1] - 1;
+    T cf = P->dij[m] * uvunk[l2];
+    for (int j = 0; j < P->mjj[l1]; ++j) {
+      size_t e = (size_t)l1 * P->maxmjj + j;
+      htpsi[P->jjp[e] - 1] += uv_at<T>(P, e) * cf;
+    }
+  }
+}
+
+template <typename T>
+static void hpsi_band(const OrcProb* P, const T* tpsi, T* htpsi) {
+  thread_local std::vector<T> www, uvunk;
+  kinetic_band(P, tpsi, htpsi, www);
+  nonlocal_band(P, tpsi, htpsi, uvunk);
+}
+
+template <typename T>
+static void hpsi_all(const OrcProb* P, const T* tpsi, T* htpsi, int nb) {
+  const size_t ng = (size_t)P->n1 * P->n2 * P->n3;
+#pragma omp parallel for schedule(dynamic)
+  for (int b = 0; b < nb; ++b) hpsi_band(P, tpsi + b * ng, htpsi + b * ng);
+}
+
+// ---------------------------------------------------------------------------
+// preconditioner: mloop CG iterations on the 7-point -1/2 Laplacian
+// (precond_hprsdft, E0 = 0), one band.
+// ---------------------------------------------------------------------------
+template <typename T>
+static void pc_mat(const OrcProb* P, const T* g, T* f) {
+  const int n1 = P->n1, n2 = P->n2, n3 = P->n3;
+  const double d = P->pc_c0;  // c0 - E0, E0 = 0
+  for (int i3 = 0; i3 < n3; ++i3)
+    for (int i2 = 0; i2 < n2; ++i2)
+      for (int i1 = 0; i1 < n1; ++i1) {
+        auto at = [&](int a, int b, int c) {
+          a = (a + n1) % n1; b = (b + n2) % n2; c = (c + n3) % n3;
+          return g[a + (size_t)n1 * (b + (size_t)n2 * c)];
+        };
+        f[i1 + (size_t)n1 * (i2 + (size_t)n2 * i3)] =
+            d * at(i1, i2, i3) + P->pc_c[0] * (at(i1 + 1, i2, i3) + at(i1 - 1, i2, i3)) +
+            P->pc_c[1] * (at(i1, i2 + 1, i3) + at(i1, i2 - 1, i3)) +
+            P->pc_c[2] * (at(i1, i2, i3 + 1) + at(i1, i2, i3 - 1));
+      }
+}
+
+template <typename T>
+static void precond_band(const OrcProb* P, const T* gk, T* Pgk) {
+  const size_t ng = (size_t)P->n1 * P->n2 * P->n3;
+  if (P->mloop <= 0) return;
+  thread_local std::vector<T> f, r, p;
+  f.resize(ng); r.resize(ng); p.resize(ng);
+  pc_mat(P, gk, f.data());
+  double rr1 = 0, rr0, pAp;
+  for (size_t i = 0; i < ng; ++i) { r[i] = gk[i] - f[i]; p[i] = r[i]; rr1 += abs2_(r[i]); }
+  if (rr1 < 1.0e-24) return;
+  for (int it = 1; it <= P->mloop; ++it) {
+    pc_mat(P, p.data(), f.data());
+    pAp = 0;
+    for (size_t i = 0; i < ng; ++i) pAp += re_(conj_(p[i]) * f[i]);
+    rr0 = rr1;
+    double a = rr0 / pAp;
+    for (size_t i = 0; i < ng; ++i) Pgk[i] += a * p[i];
+    if (it == P->mloop) break;
+    rr1 = 0;
+    for (size_t i = 0; i < ng; ++i) { r[i] -= a * f[i]; rr1 += abs2_(r[i]); }
+    double b = rr1 / rr0;
+    for (size_t i = 0; i < ng; ++i) p[i] = r[i] + b * p[i];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 2x2 generalised eigenproblem of the CG line minimisation (dsygv / zhegv)
+// ---------------------------------------------------------------------------
+static int sygv2(double A[4], double B[4], double W[2]) {
+  int itype = 1, n = 2, lw = 9, info = 0;
+  double work[9];
+  scipy_dsygv_(&itype, "V", "U", &n, A, &n, B, &n, W, work, &lw, &info);
+  return info;
+}
+static int sygv2(cplx A[4], cplx B[4], double W[2]) {
+  int itype = 1, n = 2, lw = 9, info = 0;
+  cplx work[9];
+  double rwork[9];
+  scipy_zhegv_(&itype, "V", "U", &n, A, &n, B, &n, W, work, &lw, rwork, &info);
+  return info;
+}
+
+// One band of d/z_conjugate_gradient_1 with MB_d = 1.
+template <typename T>
+static void cg_band(const OrcProb* P, T* unk, double* esp, double* res) {
+  const size_t ng = (size_t)P->n1 * P->n2 * P->n3;
+  const double dV = P->dV;
+  const bool cpx = P->is_complex;
+  const double gfac = cpx ? -1.0 : -2.0;   // g = -2(Hx - Ex) real, -(Hx - Ex) complex
+  const double c1sq = cpx ? 1.0 : 4.0;     // res = rb / c1^2
+  thread_local std::vector<T> hxk, hpk, gk, Pgk, pk;
+  hxk.assign(ng, T(0)); hpk.resize(ng); gk.resize(ng); Pgk.resize(ng); pk.resize(ng);
+  double E1 = 1.0e10, E, rb, gkgk = 0.0;
+  hpsi_band(P, unk, hxk.data());
+  double s = 0;
+  for (size_t i = 0; i < ng; ++i) s += re_(conj_(unk[i]) * hxk[i]);
+  E = s * dV;
+  s = 0;
+  for (size_t i = 0; i < ng; ++i) { gk[i] = gfac * (hxk[i] - E * unk[i]); s += abs2_(gk[i]); }
+  rb = s * dV;
+  double resv = 0;
+  for (int icg = 1; icg <= P->ncg + 1; ++icg) {
+    for (size_t i = 0; i < ng; ++i) Pgk[i] = gk[i];
+    resv = rb / c1sq;
+    if (rb < 0.0) break;
+    if (std::fabs(E - E1) < 1.0e-15) break;
+    if (icg == P->ncg + 1) break;
+    precond_band(P, gk.data(), Pgk.data());
+    s = 0;
+    for (size_t i = 0; i < ng; ++i) s += re_(conj_(Pgk[i]) * gk[i]);
+    rb = s * dV;
+    if (icg == 1) {
+      for (size_t i = 0; i < ng; ++i) pk[i] = Pgk[i];
+    } else {
+      double bk = rb / gkgk;
+      for (size_t i = 0; i < ng; ++i) pk[i] = Pgk[i] + bk * pk[i];
+    }
+    gkgk = rb;
+    std::fill(hpk.begin(), hpk.end(), T(0));
+    hpsi_band(P, pk.data(), hpk.data());
+    double v1 = 0, v3 = 0, v4 = 0, v6 = 0;
+    T v2 = T(0), v5 = T(0);
+    for (size_t i = 0; i < ng; ++i) {
+      v1 += abs2_(unk[i]);
+      v2 += conj_(pk[i]) * unk[i];
+      v3 += abs2_(pk[i]);
+      v4 += re_(conj_(unk[i]) * hxk[i]);
+      v5 += conj_(pk[i]) * hxk[i];
+      v6 += re_(conj_(pk[i]) * hpk[i]);
+    }
+    T B[4] = {T(v1 * dV), v2 * dV, conj_(v2 * dV), T(v3 * dV)};   // column major
+    T A[4] = {T(v4 * dV), v5 * dV, conj_(v5 * dV), T(v6 * dV)};
+    double W[2];
+    sygv2(A, B, W);
+    if (std::fabs(W[0] - E) > 1.0e-1 && std::fabs(W[1] - E) <= 1.0e-1) {
+      A[0] = A[2]; A[1] = A[3]; W[0] = W[1];
+    }
+    T u1 = A[0], u2 = A[1];
+    if (!cpx) {
+      if (re_(u1) < 0.0) { u1 = -u1; u2 = -u2; }
+    } else {
+      double r = std::sqrt(abs2_(u1));
+      T ph = conj_(u1) / r;
+      u1 = u1 * ph; u2 = u2 * ph;
+    }
+    E1 = E; E = W[0];
+    s = 0;
+    for (size_t i = 0; i < ng; ++i) {
+      hxk[i] = u1 * hxk[i] + u2 * hpk[i];
+      gk[i] = gfac * (hxk[i] - W[0] * (u1 * unk[i] + u2 * pk[i]));
+      s += abs2_(gk[i]);
+    }
+    rb = s * dV;
+    if (rb / resv > 1.0e8) { E = E1; continue; }
+    for (size_t i = 0; i < ng; ++i) unk[i] = u1 * unk[i] + u2 * pk[i];
+  }
+  *res = resv;
+  *esp = E;
+}
+
+template <typename T>
+static void cg_all(const OrcProb* P, T* unk, int nb, double* esp, double* res) {
+  const size_t ng = (size_t)P->n1 * P->n2 * P->n3;
+#pragma omp parallel for schedule(dynamic)
+  for (int b = 0; b < nb; ++b) cg_band(P, unk + b * ng, esp + b, res + b);
+}
+
+// ---------------------------------------------------------------------------
+// Gram-Schmidt: gram_schmidt_t / gram_schmidt_sub with one band rank
+// (NBLK = MB, NBLK1 = 4).
+// ---------------------------------------------------------------------------
+static void gemm_(const char* ta, const char* tb, int m, int n, int k, double al, const double* A,
+                  int lda, const double* B, int ldb, double be, double* C, int ldc) {
+  scipy_dgemm_(ta, tb, &m, &n, &k, &al, A, &lda, B, &ldb, &be, C, &ldc);
+}
+static void gemm_(const char* ta, const char* tb, int m, int n, int k, cplx al, const cplx* A,
+                  int lda, const cplx* B, int ldb, cplx be, cplx* C, int ldc) {
+  scipy_zgemm_(ta, tb, &m, &n, &k, &al, A, &lda, B, &ldb, &be, C, &ldc);
+}
+static void gemv_(const char* t, int m, int n, double al, const double* A, int lda,
+                  const double* x, double be, double* y) {
+  int one = 1;
+  scipy_dgemv_(t, &m, &n, &al, A, &lda, x, &one, &be, y, &one);
+}
+static void gemv_(const char* t, int m, int n, cplx al, const cplx* A, int lda, const cplx* x,
+                  cplx be, cplx* y) {
+  int one = 1;
+  scipy_zgemv_(t, &m, &n, &al, A, &lda, x, &one, &be, y, &one);
+}
+
+template <typename T>
+struct GS {
+  const OrcProb* P;
+  T* unk;
+  int ML0, NBLK1 = 4;
+  const char* TA;
+  T* col(int n) { return unk + (size_t)(n - 1) * ML0; }   // 1-based band index
+  void normalize(int m) {
+    double c = 0;
+    T* u = col(m);
+    for (int i = 0; i < ML0; ++i) c += abs2_(u[i]);
+    c = 1.0 / std::sqrt(c * P->dV);
+    for (int i = 0; i < ML0; ++i) u[i] *= c;
+  }
+  void sub(int mm1, int mm2, int nn1, int nn2, int MBLK) {
+    for (int ms = mm1; ms <= mm2; ms += MBLK) {
+      int me = std::min(ms + MBLK - 1, mm2);
+      int mm = me - ms + 1;
+      for (int ns = nn1; ns <= nn2; ns += MBLK) {
+        int ne = std::min(ns + MBLK - 1, nn2);
+        ne = std::min(ne, me - 1);
+        int nn = ne - ns + 1;
+        if (nn <= 0) continue;
+        if (ms >= ne + 1) {
+          std::vector<T> ut((size_t)nn * mm);
+          gemm_(TA, "N", nn, mm, ML0, T(-P->dV), col(ns), ML0, col(ms), ML0, T(0), ut.data(), nn);
+          gemm_("N", "N", ML0, mm, nn, T(1), col(ns), ML0, ut.data(), nn, T(1), col(ms), ML0);
+          if (ms == ne + 1) normalize(ms);
+        } else if (mm <= NBLK1) {
+          std::vector<T> ut(NBLK1);
+          for (int m = ms; m <= me; ++m) {
+            int n = std::min(m - 1, ne);
+            if (n - ns + 1 > 0) {
+              gemv_(TA, ML0, n - ns + 1, T(-P->dV), col(ns), ML0, col(m), T(0), ut.data());
+              gemv_("N", ML0, n - ns + 1, T(1), col(ns), ML0, ut.data(), T(1), col(m));
+            }
+            if (m == 1 || (n == m - 1 && m != ns)) normalize(m);
+          }
+        } else {
+          int MBLKH = std::max(MBLK / 2, NBLK1);
+          sub(ms, me, ns, ne, MBLKH);
+        }
+      }
+    }
+  }
+};
+
+template <typename T>
+static void gs_all(const OrcProb* P, T* unk, int nb) {
+  GS<T> g;
+  g.P = P; g.unk = unk; g.ML0 = P->n1 * P->n2 * P->n3;
+  g.TA = P->is_complex ? "C" : "T";
+  int NBLK = nb;
+  g.sub(1, nb, 1, nb, NBLK);
+}
+
+// ---------------------------------------------------------------------------
+// subspace diagonalisation (subspace_diag_la)
+// ---------------------------------------------------------------------------
+static int sd_solve(int MB, double* H, double* w) {
+  int lw = 3 * MB - 1, info = 0;
+  std::vector<double> work(std::max(1, lw));
+  scipy_dsyev_("V", "U", &MB, H, &MB, w, work.data(), &lw, &info);
+  return info;
+}
+static int sd_solve(int MB, cplx* H, double* w) {
+  int lw = 2 * MB + MB * MB, lrw = 1 + 5 * MB + 2 * MB * MB, liw = 3 + 5 * MB, info = 0;
+  std::vector<cplx> work(lw);
+  std::vector<double> rwork(lrw);
+  std::vector<int> iwork(liw);
+  scipy_zheevd_("V", "U", &MB, H, &MB, w, work.data(), &lw, rwork.data(), &lrw, iwork.data(),
+                &liw, &info);
+  return info;
+}
+static void syr2k_(int MB, int ML0, double zz, const double* A, const double* B, double* C) {
+  double zero = 0.0;
+  scipy_dsyr2k_("U", "T", &MB, &ML0, &zz, A, &ML0, B, &ML0, &zero, C, &MB);
+}
+static void syr2k_(int MB, int ML0, cplx zz, const cplx* A, const cplx* B, cplx* C) {
+  double zero = 0.0;
+  scipy_zher2k_("U", "C", &MB, &ML0, &zz, A, &ML0, B, &ML0, &zero, C, &MB);
+}
+
+template <typename T>
+static int sd_all(const OrcProb* P, T* unk, int nb, double* esp) {
+  const int ML0 = P->n1 * P->n2 * P->n3;
+  std::vector<T> psit((size_t)ML0 * nb), H((size_t)nb * nb, T(0));
+  hpsi_all(P, unk, psit.data(), nb);
+  syr2k_(nb, ML0, T(0.5 * P->dV), unk, psit.data(), H.data());
+  int info = sd_solve(nb, H.data(), esp);
+  if (info != 0) return info;
+  gemm_("N", "N", ML0, nb, nb, T(1), unk, ML0, H.data(), nb, T(0), psit.data(), ML0);
+  std::memcpy(unk, psit.data(), sizeof(T) * (size_t)ML0 * nb);
+  return 0;
+}
+
+// FP64 residual of each band: e = <x|Hx>/<x|x>, res = dV |Hx - e x|^2 / <x|x>.
+template <typename T>
+static void residual_all(const OrcProb* P, const T* unk, int nb, double* esp, double* res) {
+  const size_t ng = (size_t)P->n1 * P->n2 * P->n3;
+#pragma omp parallel for schedule(dynamic)
+  for (int b = 0; b < nb; ++b) {
+    std::vector<T> h(ng);
+    hpsi_band(P, unk + b * ng, h.data());
+    const T* x = unk + b * ng;
+    double xx = 0, xh = 0;
+    for (size_t i = 0; i < ng; ++i) { xx += abs2_(x[i]); xh += re_(conj_(x[i]) * h[i]); }
+    double e = xh / xx, r = 0;
+    for (size_t i = 0; i < ng; ++i) r += abs2_(h[i] - e * x[i]);
+    esp[b] = e;
+    res[b] = r * P->dV / (xx * P->dV);
+  }
+}
+
+extern "C" {
+
+void orc_set_threads(int n) {
+  omp_set_num_threads(n);
+  scipy_openblas_set_num_threads(n);
+}
+
+void orc_hpsi_d(const OrcProb* P, const double* t, double* h, int nb) { hpsi_all(P, t, h, nb); }
+void orc_hpsi_z(const OrcProb* P, const cplx* t, cplx* h, int nb) { hpsi_all(P, t, h, nb); }
+
+void orc_precond_d(const OrcProb* P, const double* g, double* pg, int nb) {
+  const size_t ng = (size_t)P->n1 * P->n2 * P->n3;
+#pragma omp parallel for schedule(dynamic)
+  for (int b = 0; b < nb; ++b) precond_band(P, g + b * ng, pg + b * ng);
+}
+void orc_precond_z(const OrcProb* P, const cplx* g, cplx* pg, int nb) {
+  const size_t ng = (size_t)P->n1 * P->n2 * P->n3;
+#pragma omp parallel for schedule(dynamic)
+  for (int b = 0; b < nb; ++b) precond_band(P, g + b * ng, pg + b * ng);
+}
+
+void orc_cg_d(const OrcProb* P, double* u, int nb, double* esp, double* res) {
+  cg_all(P, u, nb, esp, res);
+}
+void orc_cg_z(const OrcProb* P, cplx* u, int nb, double* esp, double* res) {
+  cg_all(P, u, nb, esp, res);
+}
+void orc_gs_d(const OrcProb* P, double* u, int nb) { gs_all(P, u, nb); }
+void orc_gs_z(const OrcProb* P, cplx* u, int nb) { gs_all(P, u, nb); }
+int orc_sd_d(const OrcProb* P, double* u, int nb, double* esp) { return sd_all(P, u, nb, esp); }
+int orc_sd_z(const OrcProb* P, cplx* u, int nb, double* esp) { return sd_all(P, u, nb, esp); }
+void orc_residual_d(const OrcProb* P, const double* u, int nb, double* esp, double* res) {
+  residual_all(P, u, nb, esp, res);
+}
+void orc_residual_z(const OrcProb* P, const cplx* u, int nb, double* esp, double* res) {
+  residual_all(P, u, nb, esp, res);
+}
+
+// calc_sweep for one (k, s): CG -> GS -> SD, nsweep times (src/sweep_module.f90:158-167).
+int orc_sweep_d(const OrcProb* P, double* u, int nb, int nsweep, double* esp, double* res) {
+  for (int it = 0; it < nsweep; ++it) {
+    cg_all(P, u, nb, esp, res);
+    gs_all(P, u, nb);
+    int info = sd_all(P, u, nb, esp);
+    if (info) return info;
+  }
+  return 0;
+}
+int orc_sweep_z(const OrcProb* P, cplx* u, int nb, int nsweep, double* esp, double* res) {
+  for (int it = 0; it < nsweep; ++it) {
+    cg_all(P, u, nb, esp, res);
+    gs_all(P, u, nb);
+    int info = sd_all(P, u, nb, esp);
+    if (info) return info;
+  }
+  return 0;
+}
+
+// Dense kinetic matrix of the periodic FD operator (d_construct_matrix_kinetic_sol,
+// src/kinetic/d_kinetic_sol_module.f90:540-770): H[i][j] = coefficient of psi_j in (T psi)_i.
+void orc_dense_kinetic_d(const OrcProb* P, double* H) {
+  const int n1 = P->n1, n2 = P->n2, n3 = P->n3, md = P->md;
+  const size_t ng = (size_t)n1 * n2 * n3;
+  std::memset(H, 0, sizeof(double) * ng * ng);
+  for (int i3 = 0; i3 < n3; ++i3)
+    for (int i2 = 0; i2 < n2; ++i2)
+      for (int i1 = 0; i1 < n1; ++i1) {
+        size_t i = i1 + (size_t)n1 * (i2 + (size_t)n2 * i3);
+        H[i * ng + i] += P->coef_lap0;
+        for (int m = 1; m <= md; ++m)
+          for (int s = -1; s <= 1; s += 2) {
+            int a = ((i1 + s * m) % n1 + n1) % n1, b = ((i2 + s * m) % n2 + n2) % n2,
+                c = ((i3 + s * m) % n3 + n3) % n3;
+            H[i * ng + (a + (size_t)n1 * (i2 + (size_t)n2 * i3))] += P->coef_lap[0][m - 1];
+            H[i * ng + (i1 + (size_t)n1 * (b + (size_t)n2 * i3))] += P->coef_lap[1][m - 1];
+            H[i * ng + (i1 + (size_t)n1 * (i2 + (size_t)n2 * c))] += P->coef_lap[2][m - 1];
+          }
+      }
+}
+
+}  // extern "C"

@@ -1,0 +1,311 @@
+"""Python host mirror of RSDFT's band-update module interfaces over the C ABI.
+
+The reference's Fortran procedures and their counterparts here:
+
+=====================================================  ===================================
+reference (RSDFT_DEVELOP)                              this module
+=====================================================  ===================================
+``hamiltonian(tpsi, htpsi, n, k, s)``                  :meth:`BandUpdate.hamiltonian`
+(src/hamiltonian_module.f90:44-46,118-172)
+``conjugate_gradient(n1, n2, k, s, unk, esp, res)``    :meth:`BandUpdate.conjugate_gradient`
+(src/conjugate_gradient/cg_module.f90:53-109)
+``gram_schmidt(n0, n1, k, s)``                         :meth:`BandUpdate.gram_schmidt`
+(src/gram_schmidt/gram_schmidt_module.f90:35-79)
+``subspace_diag(k, s, unk, esp)``                      :meth:`BandUpdate.subspace_diag`
+(src/subspace_diag/subspace_diag_module.f90:17-32)
+``calc_sweep`` (src/sweep_module.f90:64-248)           :meth:`BandUpdate.calc_sweep`
+=====================================================  ===================================
+
+k and s are 1-based as in the reference.  Every call goes to ``librsdft_b200.so``;
+there is no CPU fallback: a missing or unloadable library raises immediately.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import synth
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "librsdft_b200.so")
+
+PREC_FP64, PREC_MIXED = 0, 1
+PC_NONE, PC_HPRSDFT, PC_LEARNED = 0, 4, 100
+MEM_HOST, MEM_DEVICE = 0, 1
+MDMAX = 12
+
+ERRORS = {
+    -1: "RSDFT_ERR_ARG", -2: "RSDFT_ERR_OOM", -3: "RSDFT_ERR_CUDA", -4: "RSDFT_ERR_NOT_SPD",
+    -5: "RSDFT_ERR_EIG", -6: "RSDFT_ERR_TIMEOUT", -7: "RSDFT_ERR_STATE", -8: "RSDFT_ERR_UNSUPPORTED",
+    -9: "RSDFT_ERR_NUMERIC",
+}
+
+# Every symbol declared in include/rsdft_b200.h (checked by tests).
+EXPORTS = [
+    "rsdft_gpu_init", "rsdft_gpu_finalize", "rsdft_gpu_last_error", "rsdft_gpu_get_stream",
+    "rsdft_gpu_synchronize", "rsdft_gpu_set_kpoint", "rsdft_gpu_set_vloc", "rsdft_gpu_set_projectors",
+    "rsdft_gpu_set_uvk_d", "rsdft_gpu_set_uvk_z", "rsdft_gpu_set_wf_d", "rsdft_gpu_get_wf_d",
+    "rsdft_gpu_set_wf_z", "rsdft_gpu_get_wf_z", "rsdft_gpu_random_wf", "rsdft_gpu_hamiltonian_d",
+    "rsdft_gpu_hamiltonian_z", "rsdft_gpu_hamiltonian_f", "rsdft_gpu_hamiltonian_c",
+    "rsdft_gpu_conjugate_gradient", "rsdft_gpu_gram_schmidt", "rsdft_gpu_subspace_diag",
+    "rsdft_gpu_residual", "rsdft_gpu_precond_d", "rsdft_gpu_sweep", "rsdft_gpu_profile",
+    "rsdft_gpu_profile_get", "rsdft_gpu_kernel_launches",
+]
+
+
+class RsdftError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("n1", C.c_int), ("n2", C.c_int), ("n3", C.c_int), ("md", C.c_int),
+        ("hgrid", C.c_double * 3), ("dv", C.c_double),
+        ("coef_lap", (C.c_double * MDMAX) * 3), ("coef_lap0", C.c_double),
+        ("ggg", C.c_double * 3),
+        ("nk", C.c_int), ("nspin", C.c_int), ("mb", C.c_int), ("is_complex", C.c_int),
+        ("precision", C.c_int), ("pc_mode", C.c_int), ("ncg", C.c_int), ("mloop", C.c_int),
+        ("cg_block", C.c_int),
+    ]
+
+
+_LIB = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load librsdft_b200.so (build it in place first if absent); never falls back."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        from . import build as _build
+        _build.build()
+    lib = C.CDLL(path)
+    vp, i, d = C.c_void_p, C.c_int, C.c_double
+    sig = {
+        "rsdft_gpu_init": [C.POINTER(Params)], "rsdft_gpu_finalize": [],
+        "rsdft_gpu_get_stream": [C.POINTER(C.c_void_p)], "rsdft_gpu_synchronize": [],
+        "rsdft_gpu_set_kpoint": [vp, d, i], "rsdft_gpu_set_vloc": [vp, i, i],
+        "rsdft_gpu_set_projectors": [i, i, vp, vp, vp, i, vp, vp],
+        "rsdft_gpu_set_uvk_d": [i, vp], "rsdft_gpu_set_uvk_z": [i, vp],
+        "rsdft_gpu_set_wf_d": [i, i, vp, i, i], "rsdft_gpu_get_wf_d": [i, i, vp, i, i],
+        "rsdft_gpu_set_wf_z": [i, i, vp, i, i], "rsdft_gpu_get_wf_z": [i, i, vp, i, i],
+        "rsdft_gpu_random_wf": [i, i, C.c_uint64],
+        "rsdft_gpu_hamiltonian_d": [i, i, vp, vp, i, i, i], "rsdft_gpu_hamiltonian_z": [i, i, vp, vp, i, i, i],
+        "rsdft_gpu_hamiltonian_f": [i, i, vp, vp, i, i, i], "rsdft_gpu_hamiltonian_c": [i, i, vp, vp, i, i, i],
+        "rsdft_gpu_conjugate_gradient": [i, i, vp, vp], "rsdft_gpu_gram_schmidt": [i, i],
+        "rsdft_gpu_subspace_diag": [i, i, vp], "rsdft_gpu_residual": [i, i, vp, vp],
+        "rsdft_gpu_precond_d": [i, vp, vp, i, i, i],
+        "rsdft_gpu_sweep": [i, d, C.POINTER(C.c_int), vp, vp],
+        "rsdft_gpu_profile": [i], "rsdft_gpu_profile_get": [C.c_char_p, C.POINTER(C.c_double),
+                                                            C.POINTER(C.c_longlong)],
+    }
+    for name, args in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = C.c_int
+    lib.rsdft_gpu_last_error.restype = C.c_char_p
+    lib.rsdft_gpu_last_error.argtypes = []
+    lib.rsdft_gpu_kernel_launches.restype = C.c_longlong
+    lib.rsdft_gpu_kernel_launches.argtypes = []
+    _LIB = lib
+    return lib
+
+
+def _call(fn, *args):
+    r = fn(*args)
+    if r != 0:
+        raise RsdftError(r, load_library().rsdft_gpu_last_error().decode())
+    return r
+
+
+def _ptr(a: np.ndarray):
+    return C.c_void_p(a.ctypes.data)
+
+
+class BandUpdate:
+    """One library context holding the operator of a synthetic problem and its wavefunctions."""
+
+    def __init__(self, prob: "synth.Problem", precision: int = PREC_FP64, pc_mode: int = PC_HPRSDFT,
+                 ncg: int = 3, mloop: int = 3, cg_block: int = 0, nonlocal_on: bool = True,
+                 nspin: int = 1):
+        self.lib = load_library()
+        self.prob = prob
+        self.cplx = prob.is_complex
+        p = Params()
+        p.n1, p.n2, p.n3 = prob.n
+        p.md = prob.md
+        for d in range(3):
+            p.hgrid[d] = prob.h
+            p.ggg[d] = prob.kin["ggg"][d]
+            for m in range(prob.md):
+                p.coef_lap[d][m] = prob.kin["coef_lap"][d, m]
+        p.dv = prob.dV
+        p.coef_lap0 = prob.kin["coef_lap0"]
+        p.nk = prob.nk
+        p.nspin = nspin
+        p.mb = prob.nband
+        p.is_complex = 1 if self.cplx else 0
+        p.precision = precision
+        p.pc_mode = pc_mode
+        p.ncg, p.mloop, p.cg_block = ncg, mloop, cg_block
+        self.params = p
+        self.precision = precision
+        _call(self.lib.rsdft_gpu_init, C.byref(p))
+        self._open = True
+        for k in range(prob.nk):
+            nabk = np.zeros((3, MDMAX))
+            nabk[:, :prob.md] = prob.kin["coef_nabk"][k]
+            _call(self.lib.rsdft_gpu_set_kpoint, _ptr(nabk), float(prob.kin["const_k2"][k]), int(prob.nband_k[k]))
+        for s in range(1, nspin + 1):
+            v = np.ascontiguousarray(prob.vloc, dtype=np.float64)
+            _call(self.lib.rsdft_gpu_set_vloc, _ptr(v), prob.ng, s)
+        if nonlocal_on and prob.nzlma > 0:
+            self._set_projectors()
+        else:
+            _call(self.lib.rsdft_gpu_set_projectors, 0, 0, None, None, None, 0, None, None)
+
+    def _set_projectors(self):
+        pr = self.prob
+        mjj = np.ascontiguousarray(pr.mjj, np.int32)
+        jjp = np.ascontiguousarray(pr.jjp, np.int32)
+        amap = np.ascontiguousarray(pr.amap, np.int32)
+        pairs = np.ascontiguousarray(pr.pairs, np.int32)
+        dij = np.ascontiguousarray(pr.dij, np.float64)
+        _call(self.lib.rsdft_gpu_set_projectors, pr.nzlma, pr.maxmjj, _ptr(mjj), _ptr(jjp), _ptr(amap),
+              pairs.shape[0], _ptr(pairs), _ptr(dij))
+        for k in range(pr.nk):
+            if self.cplx:
+                u = np.ascontiguousarray(pr.uvk[k], np.complex128)
+                _call(self.lib.rsdft_gpu_set_uvk_z, k + 1, _ptr(u))
+            else:
+                u = np.ascontiguousarray(pr.uvk[k], np.float64)
+                _call(self.lib.rsdft_gpu_set_uvk_d, k + 1, _ptr(u))
+
+    # ---- context ----
+    def close(self):
+        if getattr(self, "_open", False):
+            self.lib.rsdft_gpu_finalize()
+            self._open = False
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def synchronize(self):
+        _call(self.lib.rsdft_gpu_synchronize)
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        _call(self.lib.rsdft_gpu_get_stream, C.byref(s))
+        return s.value or 0
+
+    # ---- wavefunctions ----
+    def nband(self, k: int = 1) -> int:
+        return int(self.prob.nband_k[k - 1])
+
+    def set_wf(self, unk: np.ndarray, k: int = 1, s: int = 1):
+        nb = unk.shape[0]
+        if self.cplx:
+            a = np.ascontiguousarray(unk, np.complex128)
+            _call(self.lib.rsdft_gpu_set_wf_z, k, s, _ptr(a), self.prob.ng, nb)
+        else:
+            a = np.ascontiguousarray(unk, np.float64)
+            _call(self.lib.rsdft_gpu_set_wf_d, k, s, _ptr(a), self.prob.ng, nb)
+
+    def get_wf(self, k: int = 1, s: int = 1) -> np.ndarray:
+        nb = self.nband(k)
+        if self.cplx:
+            a = np.zeros((nb, self.prob.ng), np.complex128)
+            _call(self.lib.rsdft_gpu_get_wf_z, k, s, _ptr(a), self.prob.ng, nb)
+        else:
+            a = np.zeros((nb, self.prob.ng), np.float64)
+            _call(self.lib.rsdft_gpu_get_wf_d, k, s, _ptr(a), self.prob.ng, nb)
+        return a
+
+    def random_wf(self, seed: int, k: int = 1, s: int = 1):
+        _call(self.lib.rsdft_gpu_random_wf, k, s, C.c_uint64(seed))
+
+    # ---- the four module procedures ----
+    def hamiltonian(self, tpsi: np.ndarray, k: int = 1, s: int = 1, fp32: bool = False) -> np.ndarray:
+        """htpsi = H tpsi for a host block tpsi[nb][ML0] (hamiltonian(tpsi,htpsi,n,k,s))."""
+        tpsi = np.atleast_2d(tpsi)
+        nb = tpsi.shape[0]
+        ng = self.prob.ng
+        if self.cplx:
+            dt = np.complex64 if fp32 else np.complex128
+            fn = self.lib.rsdft_gpu_hamiltonian_c if fp32 else self.lib.rsdft_gpu_hamiltonian_z
+        else:
+            dt = np.float32 if fp32 else np.float64
+            fn = self.lib.rsdft_gpu_hamiltonian_f if fp32 else self.lib.rsdft_gpu_hamiltonian_d
+        a = np.ascontiguousarray(tpsi, dt)
+        out = np.zeros_like(a)
+        _call(fn, k, s, _ptr(a), _ptr(out), ng, nb, MEM_HOST)
+        return out
+
+    def hamiltonian_device(self, tpsi_ptr: int, htpsi_ptr: int, nb: int, k: int = 1, s: int = 1,
+                           fp32: bool = False):
+        """Device-pointer form (both pointers from the caller's CUDA allocation)."""
+        if self.cplx:
+            fn = self.lib.rsdft_gpu_hamiltonian_c if fp32 else self.lib.rsdft_gpu_hamiltonian_z
+        else:
+            fn = self.lib.rsdft_gpu_hamiltonian_f if fp32 else self.lib.rsdft_gpu_hamiltonian_d
+        _call(fn, k, s, C.c_void_p(tpsi_ptr), C.c_void_p(htpsi_ptr), self.prob.ng, nb, MEM_DEVICE)
+
+    def precond(self, gk: np.ndarray, k: int = 1) -> np.ndarray:
+        g = np.ascontiguousarray(np.atleast_2d(gk), np.float64)
+        out = np.zeros_like(g)
+        _call(self.lib.rsdft_gpu_precond_d, k, _ptr(g), _ptr(out), self.prob.ng, g.shape[0], MEM_HOST)
+        return out
+
+    def conjugate_gradient(self, k: int = 1, s: int = 1):
+        nb = self.nband(k)
+        esp = np.zeros(nb)
+        res = np.zeros(nb)
+        _call(self.lib.rsdft_gpu_conjugate_gradient, k, s, _ptr(esp), _ptr(res))
+        return esp, res
+
+    def gram_schmidt(self, n0: int = 1, n1: int | None = None, k: int = 1, s: int = 1):
+        if n0 != 1 or (n1 is not None and n1 != self.nband(k)):
+            raise RsdftError(-1, "gram_schmidt orthonormalises bands 1..nband")
+        _call(self.lib.rsdft_gpu_gram_schmidt, k, s)
+
+    def subspace_diag(self, k: int = 1, s: int = 1) -> np.ndarray:
+        esp = np.zeros(self.nband(k))
+        _call(self.lib.rsdft_gpu_subspace_diag, k, s, _ptr(esp))
+        return esp
+
+    def residual(self, k: int = 1, s: int = 1):
+        nb = self.nband(k)
+        esp = np.zeros(nb)
+        res = np.zeros(nb)
+        _call(self.lib.rsdft_gpu_residual, k, s, _ptr(esp), _ptr(res))
+        return esp, res
+
+    def calc_sweep(self, nsweep: int, tol: float = 0.0):
+        """CG -> GS -> SD sweeps over all (k, s) until max FP64 residual <= tol."""
+        nk, mb = self.prob.nk, self.prob.nband
+        esp = np.zeros((self.params.nspin, nk, mb))
+        res = np.zeros((self.params.nspin, nk, mb))
+        it = C.c_int(0)
+        _call(self.lib.rsdft_gpu_sweep, nsweep, float(tol), C.byref(it), _ptr(esp), _ptr(res))
+        return it.value, esp, res
+
+    # ---- measurement ----
+    def profile(self, on: bool):
+        _call(self.lib.rsdft_gpu_profile, 1 if on else 0)
+
+    def profile_get(self, name: str):
+        ms = C.c_double(0.0)
+        n = C.c_longlong(0)
+        _call(self.lib.rsdft_gpu_profile_get, name.encode(), C.byref(ms), C.byref(n))
+        return ms.value, n.value
+
+    def kernel_launches(self) -> int:
+        return int(self.lib.rsdft_gpu_kernel_launches())

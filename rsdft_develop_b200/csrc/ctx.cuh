@@ -1,0 +1,135 @@
+// Library context: operator tables, resident wavefunctions and workspaces.
+#pragma once
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+#include <algorithm>
+#include <map>
+#include <type_traits>
+#include <string>
+
+#include "common.cuh"
+
+namespace rsdft {
+
+// Nonlocal projectors grouped by atom (footprint union), for the gather kernel,
+// plus the per-point CSR used by the scatter fused into the stencil kernel.
+struct NonlocalTables {
+  int nproj = 0;          // nzlma
+  int ngroups = 0;        // atoms
+  int pg = 0;             // padded projectors per group (1, 4, 9, 16)
+  int ftotal = 0;         // total footprint entries over groups
+  std::vector<int> h_gofs, h_gplist;         // host copies (group layout)
+  DBuf gofs, gjj, gplist, gD;                // int / int / int[ngroups*PG] / double[ngroups*PG*PG]
+  DBuf rowptr, col;                          // CSR (ng+1), (nnz)
+  int nnz = 0;
+  // per k: weights in both precisions (gather: conj(uVk) for complex), CSR values
+  struct PerK {
+    DBuf gw64, gw32;      // [ftotal][PG] real (T) or complex (T2)
+    DBuf val64, val32;    // [nnz] scatter values
+    bool ready = false;
+  };
+  std::vector<PerK> perk;
+  // host-side copies needed to build per-k tables
+  std::vector<int> h_mjj, h_jjp;  // reference layout
+  int maxmjj = 0;
+  std::vector<int> h_slot;        // for each (lma, j): footprint slot in its group
+  std::vector<int> h_csr_src;     // for each CSR entry: flat (lma*maxmjj + j)
+};
+
+struct KPoint {
+  double coef_nabk[3][MDMAX] = {};
+  double const_k2 = 0.0;
+  int nband = 0;
+  bool set = false;
+};
+
+struct WaveFns {
+  DBuf psi;        // resident unk: FP64 (double / double2) or FP32 (float / float2)
+  bool valid = false;
+};
+
+struct ProfEntry {
+  double ms = 0.0;
+  long long launches = 0;
+};
+
+struct Ctx {
+  rsdft_gpu_params p{};
+  size_t ng = 0;
+  bool cplx = false;
+  bool mixed = false;
+  cudaStream_t stream = nullptr;
+  cublasHandle_t cublas = nullptr;
+  cusolverDnHandle_t cusolver = nullptr;
+  unsigned* d_status = nullptr;
+  long long launches = 0;
+
+  std::vector<KPoint> kp;
+  DBuf vloc64, vloc32;             // [nspin][ng]
+  std::vector<bool> vloc_set;
+  NonlocalTables nl;
+  std::vector<WaveFns> wf;         // [k][s]
+
+  // workspaces
+  DBuf ws_coef;                    // nonlocal coefficients [nb][nproj]
+  DBuf ws_io_a, ws_io_b;           // staging for host-pointer hamiltonian calls
+  DBuf ws_cg;                      // CG / PC block vectors
+  DBuf ws_red;                     // reduction partials
+  DBuf ws_scal;                    // per-band scalars (double)
+  DBuf ws_dense;                   // M x M matrices
+  DBuf ws_hpsi;                    // H psi for subspace diag (nb x ng)
+  DBuf ws_rot;                     // rotation / GS temporaries
+  DBuf ws_solver;                  // cusolver workspace
+  DBuf ws_info;                    // cusolver info
+  DBuf ws_gemm;                    // split-BF16 operands
+  DBuf ws_out;                     // small per-band outputs (esp/res) handed to callers
+  DBuf ws_f64;                     // FP64 copy of FP32-resident bands (mixed mode dense ops)
+
+  // profiling
+  bool profiling = false;
+  std::map<std::string, ProfEntry> prof;
+  std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+  std::vector<cudaEvent_t> event_pool;
+
+  WaveFns& wfn(int k, int s) { return wf[(size_t)k * p.nspin + s]; }
+  size_t elem_bytes() const { return (mixed ? 4 : 8) * (cplx ? 2 : 1); }
+};
+
+Ctx* ctx();   // the process-wide context (null before init)
+
+// profiling helpers: bracket a launch sequence with events on the library stream
+struct ProfScope {
+  Ctx& c;
+  const char* name;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  ProfScope(Ctx& c_, const char* n);
+  ~ProfScope();
+};
+void prof_flush(Ctx& c);
+
+// error check after a launch
+int check_launch(const char* what);
+
+// ---- hpsi ----
+template <typename T>
+int hpsi_real(Ctx& c, int k, int s, const T* psi, T* hpsi, size_t ld, int nb);
+template <typename T>
+int hpsi_cplx(Ctx& c, int k, int s, const T* psi, T* hpsi, size_t ld, int nb);  // T = float / double (interleaved)
+int nl_prepare_k(Ctx& c, int k);
+
+// ---- preconditioner / CG ----
+int cg_run(Ctx& c, int k, int s, double* h_esp, double* h_res);
+template <typename T>
+int precond_real(Ctx& c, const T* g, T* pg, size_t ld, int nb);
+
+// ---- dense ----
+int gs_run(Ctx& c, int k, int s, int passes);
+int sd_run(Ctx& c, int k, int s, double* h_esp);
+int residual_run(Ctx& c, int k, int s, double* d_esp, double* d_res);
+
+// ---- util ----
+int random_wf(Ctx& c, int k, int s, uint64_t seed);
+int convert_d2f(Ctx& c, const double* src, float* dst, size_t n);
+int convert_f2d(Ctx& c, const float* src, double* dst, size_t n);
+
+}  // namespace rsdft
