@@ -143,9 +143,10 @@ int rsdft_gpu_sweep(int nsweep, double tol, int* iters, double* esp, double* res
 /* ---- measurement ---- */
 /* Per-kernel CUDA-event timing of the library's own launches (off by default). */
 int rsdft_gpu_profile(int on);
-/* total device time (ms) and launch count recorded for kernel family `name`
- * ("hpsi_stencil", "nl_gather", "gemm", "cg", "pc", ...). */
-int rsdft_gpu_profile_get(const char* name, double* total_ms, long long* launches);
+/* total device time (ms), launch count, algorithmic bytes and flops recorded for kernel
+ * family `name` ("hpsi_stencil", "nl_gather", "gemm", "cg", "pc", ...); any output may be NULL. */
+int rsdft_gpu_profile_get(const char* name, double* total_ms, long long* launches, double* bytes,
+                          double* flops);
 /* Launch count of all library kernels since init (for launch accounting). */
 long long rsdft_gpu_kernel_launches(void);
 

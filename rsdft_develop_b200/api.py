@@ -89,7 +89,7 @@ def load_library(path: str = LIB_PATH):
     sig = {
         "rsdft_gpu_init": [C.POINTER(Params)], "rsdft_gpu_finalize": [],
         "rsdft_gpu_get_stream": [C.POINTER(C.c_void_p)], "rsdft_gpu_synchronize": [],
-        "rsdft_gpu_set_kpoint": [vp, d, i], "rsdft_gpu_set_vloc": [vp, i, i],
+        "rsdft_gpu_set_kpoint": [i, vp, d, i], "rsdft_gpu_set_vloc": [vp, i, i],
         "rsdft_gpu_set_projectors": [i, i, vp, vp, vp, i, vp, vp],
         "rsdft_gpu_set_uvk_d": [i, vp], "rsdft_gpu_set_uvk_z": [i, vp],
         "rsdft_gpu_set_wf_d": [i, i, vp, i, i], "rsdft_gpu_get_wf_d": [i, i, vp, i, i],
@@ -102,7 +102,8 @@ def load_library(path: str = LIB_PATH):
         "rsdft_gpu_precond_d": [i, vp, vp, i, i, i],
         "rsdft_gpu_sweep": [i, d, C.POINTER(C.c_int), vp, vp],
         "rsdft_gpu_profile": [i], "rsdft_gpu_profile_get": [C.c_char_p, C.POINTER(C.c_double),
-                                                            C.POINTER(C.c_longlong)],
+                                                            C.POINTER(C.c_longlong), C.POINTER(C.c_double),
+                                                            C.POINTER(C.c_double)],
     }
     for name, args in sig.items():
         f = getattr(lib, name)
@@ -160,7 +161,7 @@ class BandUpdate:
         for k in range(prob.nk):
             nabk = np.zeros((3, MDMAX))
             nabk[:, :prob.md] = prob.kin["coef_nabk"][k]
-            _call(self.lib.rsdft_gpu_set_kpoint, _ptr(nabk), float(prob.kin["const_k2"][k]), int(prob.nband_k[k]))
+            _call(self.lib.rsdft_gpu_set_kpoint, k + 1, _ptr(nabk), float(prob.kin["const_k2"][k]), int(prob.nband_k[k]))
         for s in range(1, nspin + 1):
             v = np.ascontiguousarray(prob.vloc, dtype=np.float64)
             _call(self.lib.rsdft_gpu_set_vloc, _ptr(v), prob.ng, s)
@@ -302,10 +303,13 @@ class BandUpdate:
         _call(self.lib.rsdft_gpu_profile, 1 if on else 0)
 
     def profile_get(self, name: str):
+        """(total ms, launches, algorithmic bytes, algorithmic flops) of a kernel family."""
         ms = C.c_double(0.0)
         n = C.c_longlong(0)
-        _call(self.lib.rsdft_gpu_profile_get, name.encode(), C.byref(ms), C.byref(n))
-        return ms.value, n.value
+        by = C.c_double(0.0)
+        fl = C.c_double(0.0)
+        _call(self.lib.rsdft_gpu_profile_get, name.encode(), C.byref(ms), C.byref(n), C.byref(by), C.byref(fl))
+        return ms.value, n.value, by.value, fl.value
 
     def kernel_launches(self) -> int:
         return int(self.lib.rsdft_gpu_kernel_launches())

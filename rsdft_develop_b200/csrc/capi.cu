@@ -42,7 +42,8 @@ static cudaEvent_t take_event(Ctx& c) {
   cudaEventCreate(&e);
   return e;
 }
-ProfScope::ProfScope(Ctx& c_, const char* n) : c(c_), name(n) {
+ProfScope::ProfScope(Ctx& c_, const char* n, double bytes_, double flops_)
+    : c(c_), name(n), bytes(bytes_), flops(flops_) {
   if (!c.profiling) return;
   e0 = take_event(c);
   e1 = take_event(c);
@@ -51,7 +52,7 @@ ProfScope::ProfScope(Ctx& c_, const char* n) : c(c_), name(n) {
 ProfScope::~ProfScope() {
   if (!c.profiling || !e0) return;
   cudaEventRecord(e1, c.stream);
-  c.pending.push_back({std::string(name), {e0, e1}});
+  c.pending.push_back({std::string(name), e0, e1, bytes, flops});
   if (c.pending.size() > 4096) prof_flush(c);
 }
 void prof_flush(Ctx& c) {
@@ -59,12 +60,14 @@ void prof_flush(Ctx& c) {
   cudaStreamSynchronize(c.stream);
   for (auto& pe : c.pending) {
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, pe.second.first, pe.second.second);
-    ProfEntry& e = c.prof[pe.first];
+    cudaEventElapsedTime(&ms, pe.e0, pe.e1);
+    ProfEntry& e = c.prof[pe.name];
     e.ms += ms;
     e.launches += 1;
-    c.event_pool.push_back(pe.second.first);
-    c.event_pool.push_back(pe.second.second);
+    e.bytes += pe.bytes;
+    e.flops += pe.flops;
+    c.event_pool.push_back(pe.e0);
+    c.event_pool.push_back(pe.e1);
   }
   c.pending.clear();
 }
@@ -241,8 +244,8 @@ static void destroy(Ctx* c) {
   if (!c) return;
   cudaStreamSynchronize(c->stream);
   for (auto& pe : c->pending) {
-    cudaEventDestroy(pe.second.first);
-    cudaEventDestroy(pe.second.second);
+    cudaEventDestroy(pe.e0);
+    cudaEventDestroy(pe.e1);
   }
   for (auto e : c->event_pool) cudaEventDestroy(e);
   DBuf* bufs[] = {&c->vloc64, &c->vloc32, &c->ws_coef, &c->ws_io_a, &c->ws_io_b, &c->ws_cg, &c->ws_red,
@@ -631,13 +634,16 @@ int rsdft_gpu_profile(int on) {
   return 0;
 }
 
-int rsdft_gpu_profile_get(const char* name, double* total_ms, long long* launches) {
+int rsdft_gpu_profile_get(const char* name, double* total_ms, long long* launches, double* bytes, double* flops) {
   REQUIRE_CTX();
   Ctx& c = *g_ctx;
   prof_flush(c);
   auto it = c.prof.find(name ? name : "");
-  if (total_ms) *total_ms = it == c.prof.end() ? 0.0 : it->second.ms;
-  if (launches) *launches = it == c.prof.end() ? 0 : it->second.launches;
+  const bool f = it != c.prof.end();
+  if (total_ms) *total_ms = f ? it->second.ms : 0.0;
+  if (launches) *launches = f ? it->second.launches : 0;
+  if (bytes) *bytes = f ? it->second.bytes : 0.0;
+  if (flops) *flops = f ? it->second.flops : 0.0;
   return 0;
 }
 

@@ -51,6 +51,8 @@ struct WaveFns {
 struct ProfEntry {
   double ms = 0.0;
   long long launches = 0;
+  double bytes = 0.0;   // algorithmic bytes moved by the bracketed launches
+  double flops = 0.0;   // algorithmic flops of the bracketed launches
 };
 
 struct Ctx {
@@ -88,7 +90,12 @@ struct Ctx {
   // profiling
   bool profiling = false;
   std::map<std::string, ProfEntry> prof;
-  std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+  struct Pending {
+    std::string name;
+    cudaEvent_t e0, e1;
+    double bytes, flops;
+  };
+  std::vector<Pending> pending;
   std::vector<cudaEvent_t> event_pool;
 
   WaveFns& wfn(int k, int s) { return wf[(size_t)k * p.nspin + s]; }
@@ -102,7 +109,8 @@ struct ProfScope {
   Ctx& c;
   const char* name;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
-  ProfScope(Ctx& c_, const char* n);
+  double bytes = 0.0, flops = 0.0;
+  ProfScope(Ctx& c_, const char* n, double bytes_ = 0.0, double flops_ = 0.0);
   ~ProfScope();
 };
 void prof_flush(Ctx& c);

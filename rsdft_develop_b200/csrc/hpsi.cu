@@ -415,7 +415,10 @@ static int launch_stencil(Ctx& c, int k, int s, const T* psi, T* out, size_t ld,
     attr_done = true;
   }
   dim3 grid(ytiles, zch, nb), block(bx, by);
-  ProfScope ps(c, "hpsi_stencil");
+  // algorithmic bytes: read psi + write H psi per band, V_loc and the scatter tables once
+  const double alg_bytes = (double)sizeof(T) * (2.0 * (double)c.ng * nb + (double)c.ng) +
+                           (nl_on ? 4.0 * (double)(c.ng + 1) + (4.0 + sizeof(T)) * c.nl.nnz : 0.0);
+  ProfScope ps(c, "hpsi_stencil", alg_bytes);
   kern<<<grid, block, smem, c.stream>>>(a);
   c.launches++;
   return check_launch("hpsi_stencil");

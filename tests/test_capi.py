@@ -22,6 +22,24 @@ def test_header_matches_exports():
     assert _declared() == sorted(api.EXPORTS)
 
 
+def _declared_arity():
+    src = open(os.path.join(ROOT, "include", "rsdft_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(rsdft_gpu_\w+)\s*\(([^)]*)\)\s*;", src):
+        args = m.group(2).strip()
+        out[m.group(1)] = 0 if args in ("", "void") else len(args.split(","))
+    return out
+
+
+def test_ctypes_signatures_match_header():
+    lib = api.load_library()
+    for name, n in _declared_arity().items():
+        f = getattr(lib, name)
+        assert f.argtypes is not None, name
+        assert len(f.argtypes) == n, (name, len(f.argtypes), n)
+
+
 def test_library_exports_every_declared_symbol():
     lib = api.load_library()
     for name in _declared():
