@@ -139,6 +139,10 @@ int rsdft_gpu_precond_d(int k, const double* gk, double* pgk, int ld, int nb, in
  * FP64 residual max over bands <= tol (tol <= 0: never).  iters receives the sweeps done;
  * esp/res (host, nband*nk*nspin, k-major after band) receive the final FP64 values. */
 int rsdft_gpu_sweep(int nsweep, double tol, int* iters, double* esp, double* res);
+/* Convergence band set of rsdft_gpu_sweep: bands 1..mb_ref are judged (0: all bands), as the
+ * reference's init_sweep(iconv_check, mb_ref, tol) does for its band and DOS drivers
+ * (src/sweep_module.f90:46-60,267-278; src/band_module.f90:207; src/dos_module.f90:64-75). */
+int rsdft_gpu_init_sweep(int mb_ref);
 
 /* ---- measurement ---- */
 /* Per-kernel CUDA-event timing of the library's own launches (off by default). */
@@ -149,6 +153,10 @@ int rsdft_gpu_profile_get(const char* name, double* total_ms, long long* launche
                           double* flops);
 /* Launch count of all library kernels since init (for launch accounting). */
 long long rsdft_gpu_kernel_launches(void);
+/* Diagnostic: the split-BF16 tensor-core GEMM against cuBLAS DGEMM on the same FP32 inputs.
+ * op 0: C = A B^T (A: m x k, B: n x k); op 1: X <- X V (X: m bands x k points, V: m x m).
+ * err receives max|x3 - dgemm| / max|dgemm|.  No counterpart in the reference. */
+int rsdft_gpu_selftest_gemm(int m, int n, long long k, int op, double* err);
 
 #ifdef __cplusplus
 }

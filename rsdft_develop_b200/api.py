@@ -51,7 +51,7 @@ EXPORTS = [
     "rsdft_gpu_hamiltonian_z", "rsdft_gpu_hamiltonian_f", "rsdft_gpu_hamiltonian_c",
     "rsdft_gpu_conjugate_gradient", "rsdft_gpu_gram_schmidt", "rsdft_gpu_subspace_diag",
     "rsdft_gpu_residual", "rsdft_gpu_precond_d", "rsdft_gpu_sweep", "rsdft_gpu_profile",
-    "rsdft_gpu_profile_get", "rsdft_gpu_kernel_launches",
+    "rsdft_gpu_profile_get", "rsdft_gpu_kernel_launches", "rsdft_gpu_selftest_gemm", "rsdft_gpu_init_sweep",
 ]
 
 
@@ -101,6 +101,8 @@ def load_library(path: str = LIB_PATH):
         "rsdft_gpu_subspace_diag": [i, i, vp], "rsdft_gpu_residual": [i, i, vp, vp],
         "rsdft_gpu_precond_d": [i, vp, vp, i, i, i],
         "rsdft_gpu_sweep": [i, d, C.POINTER(C.c_int), vp, vp],
+        "rsdft_gpu_selftest_gemm": [i, i, C.c_longlong, i, C.POINTER(C.c_double)],
+        "rsdft_gpu_init_sweep": [i],
         "rsdft_gpu_profile": [i], "rsdft_gpu_profile_get": [C.c_char_p, C.POINTER(C.c_double),
                                                             C.POINTER(C.c_longlong), C.POINTER(C.c_double),
                                                             C.POINTER(C.c_double)],
@@ -289,6 +291,10 @@ class BandUpdate:
         _call(self.lib.rsdft_gpu_residual, k, s, _ptr(esp), _ptr(res))
         return esp, res
 
+    def init_sweep(self, mb_ref: int = 0):
+        """Judge convergence on bands 1..mb_ref (0: all), as init_sweep(..., mb_ref, ...)."""
+        _call(self.lib.rsdft_gpu_init_sweep, int(mb_ref))
+
     def calc_sweep(self, nsweep: int, tol: float = 0.0):
         """CG -> GS -> SD sweeps over all (k, s) until max FP64 residual <= tol."""
         nk, mb = self.prob.nk, self.prob.nband
@@ -310,6 +316,12 @@ class BandUpdate:
         fl = C.c_double(0.0)
         _call(self.lib.rsdft_gpu_profile_get, name.encode(), C.byref(ms), C.byref(n), C.byref(by), C.byref(fl))
         return ms.value, n.value, by.value, fl.value
+
+    def selftest_gemm(self, m: int, n: int, k: int, op: int) -> float:
+        """Relative error of the split-BF16 tensor-core GEMM against cuBLAS DGEMM."""
+        e = C.c_double(0.0)
+        _call(self.lib.rsdft_gpu_selftest_gemm, m, n, k, op, C.byref(e))
+        return e.value
 
     def kernel_launches(self) -> int:
         return int(self.lib.rsdft_gpu_kernel_launches())

@@ -159,39 +159,40 @@ static int build_nonlocal(Ctx& c, int nzlma, int maxmjj, const int* mjj, const i
     const int g = proj_group[l1];
     D[((size_t)g * PG + proj_slot[l1]) * PG + proj_slot[l2]] += dij[m];
   }
-  // per-point CSR for the scatter (stable counting sort by grid point)
-  std::vector<int> cnt(c.ng + 1, 0);
-  size_t nnz = 0;
-  for (int p = 0; p < nzlma; ++p)
-    for (int j = 0; j < mjj[p]; ++j) {
-      cnt[jjp[(size_t)p * maxmjj + j]]++;  // 1-based -> rowptr index +1
-      ++nnz;
+  // scatter records: one per (group, footprint point), sorted by grid point (stable counting sort)
+  const int nrec = nl.ftotal;
+  std::vector<int> cnt(c.ng + 1, 0), fslot_group(nrec);
+  for (int g = 0; g < nl.ngroups; ++g)
+    for (int f = nl.h_gofs[g]; f < nl.h_gofs[g + 1]; ++f) {
+      cnt[gjj[f] + 1]++;
+      fslot_group[f] = g;
     }
-  RS_CHECK(nnz < (size_t)INT32_MAX, RSDFT_ERR_UNSUPPORTED, "too many projector entries");
-  std::vector<int> rowptr(c.ng + 1, 0);
+  std::vector<int> rowptr(c.ng + 16, 0);
   for (size_t i = 0; i < c.ng; ++i) rowptr[i + 1] = rowptr[i] + cnt[i + 1];
-  std::vector<int> fill(rowptr.begin(), rowptr.end() - 1), col(nnz);
-  nl.h_csr_src.assign(nnz, 0);
-  for (int p = 0; p < nzlma; ++p)
-    for (int j = 0; j < mjj[p]; ++j) {
-      const int pt = jjp[(size_t)p * maxmjj + j] - 1;
-      const int e = fill[pt]++;
-      col[e] = p;
-      nl.h_csr_src[e] = p * maxmjj + j;
-    }
-  nl.nnz = (int)nnz;
+  for (size_t i = c.ng + 1; i < rowptr.size(); ++i) rowptr[i] = rowptr[c.ng];
+  std::vector<int> fill(rowptr.begin(), rowptr.begin() + c.ng), rpt(nrec), rg(nrec);
+  nl.h_rec_src.assign(nrec, 0);
+  for (int f = 0; f < nrec; ++f) {
+    const int e = fill[gjj[f]]++;
+    rpt[e] = gjj[f];
+    rg[e] = fslot_group[f];
+    nl.h_rec_src[e] = f;
+  }
+  nl.nrec = nrec;
   RS_TRY(nl.gofs.ensure(nl.h_gofs.size() * sizeof(int)));
   RS_TRY(nl.gjj.ensure(std::max<size_t>(1, gjj.size()) * sizeof(int)));
   RS_TRY(nl.gplist.ensure(nl.h_gplist.size() * sizeof(int)));
   RS_TRY(nl.gD.ensure(D.size() * sizeof(double)));
-  RS_TRY(nl.rowptr.ensure(rowptr.size() * sizeof(int)));
-  RS_TRY(nl.col.ensure(std::max<size_t>(1, nnz) * sizeof(int)));
+  RS_TRY(nl.rec_rowptr.ensure(rowptr.size() * sizeof(int)));
+  RS_TRY(nl.rec_pt.ensure(std::max(1, nrec) * sizeof(int)));
+  RS_TRY(nl.rec_g.ensure(std::max(1, nrec) * sizeof(int)));
   RS_CUDA(cudaMemcpy(nl.gofs.p, nl.h_gofs.data(), nl.h_gofs.size() * sizeof(int), cudaMemcpyHostToDevice));
   RS_CUDA(cudaMemcpy(nl.gjj.p, gjj.data(), gjj.size() * sizeof(int), cudaMemcpyHostToDevice));
   RS_CUDA(cudaMemcpy(nl.gplist.p, nl.h_gplist.data(), nl.h_gplist.size() * sizeof(int), cudaMemcpyHostToDevice));
   RS_CUDA(cudaMemcpy(nl.gD.p, D.data(), D.size() * sizeof(double), cudaMemcpyHostToDevice));
-  RS_CUDA(cudaMemcpy(nl.rowptr.p, rowptr.data(), rowptr.size() * sizeof(int), cudaMemcpyHostToDevice));
-  RS_CUDA(cudaMemcpy(nl.col.p, col.data(), nnz * sizeof(int), cudaMemcpyHostToDevice));
+  RS_CUDA(cudaMemcpy(nl.rec_rowptr.p, rowptr.data(), rowptr.size() * sizeof(int), cudaMemcpyHostToDevice));
+  RS_CUDA(cudaMemcpy(nl.rec_pt.p, rpt.data(), nrec * sizeof(int), cudaMemcpyHostToDevice));
+  RS_CUDA(cudaMemcpy(nl.rec_g.p, rg.data(), nrec * sizeof(int), cudaMemcpyHostToDevice));
   nl.perk.assign(c.p.nk, NonlocalTables::PerK());
   return 0;
 }
@@ -201,7 +202,8 @@ static int set_uvk(Ctx& c, int k, const double* uvk, bool cplx) {
   NonlocalTables& nl = c.nl;
   RS_CHECK(nl.nproj > 0, RSDFT_ERR_STATE, "set_projectors must precede set_uvk");
   const int PG = nl.pg, nc = cplx ? 2 : 1;
-  std::vector<double> gw((size_t)nl.ftotal * PG * nc, 0.0), val((size_t)nl.nnz * nc);
+  std::vector<double> gw((size_t)nl.ftotal * PG * nc, 0.0), sw((size_t)nl.ftotal * PG * nc, 0.0),
+      ru((size_t)nl.nrec * PG * nc);
   std::vector<int> pslot(nl.nproj, 0);
   for (int g = 0; g < nl.ngroups; ++g)
     for (int i = 0; i < PG; ++i) {
@@ -211,25 +213,28 @@ static int set_uvk(Ctx& c, int k, const double* uvk, bool cplx) {
   for (int p = 0; p < nl.nproj; ++p)
     for (int j = 0; j < nl.h_mjj[p]; ++j) {
       const size_t e = (size_t)p * nl.maxmjj + j;
-      const int f = nl.h_slot[e];
-      // gather weight: conj(uVk) (src/ps_nloc_mr_module.f90:1290); accumulate duplicates
-      gw[((size_t)f * PG + pslot[p]) * nc + 0] += uvk[e * nc + 0];
-      if (cplx) gw[((size_t)f * PG + pslot[p]) * nc + 1] -= uvk[e * nc + 1];
+      const size_t w = ((size_t)nl.h_slot[e] * PG + pslot[p]) * nc;
+      // gather weight conj(uVk) (src/ps_nloc_mr_module.f90:1290), scatter weight uVk (:1341);
+      // duplicate grid points of one projector accumulate
+      gw[w] += uvk[e * nc];
+      sw[w] += uvk[e * nc];
+      if (cplx) {
+        gw[w + 1] -= uvk[e * nc + 1];
+        sw[w + 1] += uvk[e * nc + 1];
+      }
     }
-  for (int e = 0; e < nl.nnz; ++e) {
-    const size_t src = nl.h_csr_src[e];
-    for (int q = 0; q < nc; ++q) val[(size_t)e * nc + q] = uvk[src * nc + q];
-  }
+  for (int r = 0; r < nl.nrec; ++r)
+    for (int q = 0; q < PG * nc; ++q) ru[(size_t)r * PG * nc + q] = sw[(size_t)nl.h_rec_src[r] * PG * nc + q];
   NonlocalTables::PerK& pk = nl.perk[k];
-  std::vector<float> gw32(gw.begin(), gw.end()), val32(val.begin(), val.end());
+  std::vector<float> gw32(gw.begin(), gw.end()), ru32(ru.begin(), ru.end());
   RS_TRY(pk.gw64.ensure(std::max<size_t>(1, gw.size()) * sizeof(double)));
   RS_TRY(pk.gw32.ensure(std::max<size_t>(1, gw.size()) * sizeof(float)));
-  RS_TRY(pk.val64.ensure(std::max<size_t>(1, val.size()) * sizeof(double)));
-  RS_TRY(pk.val32.ensure(std::max<size_t>(1, val.size()) * sizeof(float)));
+  RS_TRY(pk.ru64.ensure(std::max<size_t>(1, ru.size()) * sizeof(double)));
+  RS_TRY(pk.ru32.ensure(std::max<size_t>(1, ru.size()) * sizeof(float)));
   RS_CUDA(cudaMemcpy(pk.gw64.p, gw.data(), gw.size() * sizeof(double), cudaMemcpyHostToDevice));
   RS_CUDA(cudaMemcpy(pk.gw32.p, gw32.data(), gw32.size() * sizeof(float), cudaMemcpyHostToDevice));
-  RS_CUDA(cudaMemcpy(pk.val64.p, val.data(), val.size() * sizeof(double), cudaMemcpyHostToDevice));
-  RS_CUDA(cudaMemcpy(pk.val32.p, val32.data(), val32.size() * sizeof(float), cudaMemcpyHostToDevice));
+  RS_CUDA(cudaMemcpy(pk.ru64.p, ru.data(), ru.size() * sizeof(double), cudaMemcpyHostToDevice));
+  RS_CUDA(cudaMemcpy(pk.ru32.p, ru32.data(), ru32.size() * sizeof(float), cudaMemcpyHostToDevice));
   pk.ready = true;
   return 0;
 }
@@ -250,10 +255,10 @@ static void destroy(Ctx* c) {
   for (auto e : c->event_pool) cudaEventDestroy(e);
   DBuf* bufs[] = {&c->vloc64, &c->vloc32, &c->ws_coef, &c->ws_io_a, &c->ws_io_b, &c->ws_cg, &c->ws_red,
                   &c->ws_scal, &c->ws_dense, &c->ws_hpsi, &c->ws_rot, &c->ws_solver, &c->ws_info, &c->ws_gemm, &c->ws_out, &c->ws_f64,
-                  &c->nl.gofs, &c->nl.gjj, &c->nl.gplist, &c->nl.gD, &c->nl.rowptr, &c->nl.col};
+                  &c->nl.gofs, &c->nl.gjj, &c->nl.gplist, &c->nl.gD, &c->nl.rec_rowptr, &c->nl.rec_pt, &c->nl.rec_g};
   for (DBuf* b : bufs) b->release();
   for (auto& pk : c->nl.perk) {
-    pk.gw64.release(); pk.gw32.release(); pk.val64.release(); pk.val32.release();
+    pk.gw64.release(); pk.gw32.release(); pk.ru64.release(); pk.ru32.release();
   }
   for (auto& w : c->wf) w.psi.release();
   if (c->d_status) cudaFree(c->d_status);
@@ -593,6 +598,13 @@ int rsdft_gpu_residual(int k, int s, double* esp, double* res) {
   return check_status(c);
 }
 
+int rsdft_gpu_init_sweep(int mb_ref) {
+  REQUIRE_CTX();
+  RS_CHECK(mb_ref >= 0, RSDFT_ERR_ARG, "mb_ref must be >= 0");
+  g_ctx->mb_ref = mb_ref;
+  return 0;
+}
+
 int rsdft_gpu_sweep(int nsweep, double tol, int* iters, double* esp, double* res) {
   REQUIRE_CTX();
   Ctx& c = *g_ctx;
@@ -613,7 +625,8 @@ int rsdft_gpu_sweep(int nsweep, double tol, int* iters, double* esp, double* res
         for (int k = 0; k < c.p.nk; ++k) {
           const int nb = c.kp[k].nband;
           RS_TRY(rsdft_gpu_residual(k + 1, s + 1, e.data(), r.data()));
-          for (int n = 0; n < nb; ++n) rmax = std::max(rmax, r[n]);
+          const int nconv = c.mb_ref > 0 ? std::min(c.mb_ref, nb) : nb;
+          for (int n = 0; n < nconv; ++n) rmax = std::max(rmax, r[n]);
           const size_t off = ((size_t)s * c.p.nk + k) * nbmax;
           if (esp) std::memcpy(esp + off, e.data(), sizeof(double) * nb);
           if (res) std::memcpy(res + off, r.data(), sizeof(double) * nb);
@@ -648,5 +661,12 @@ int rsdft_gpu_profile_get(const char* name, double* total_ms, long long* launche
 }
 
 long long rsdft_gpu_kernel_launches(void) { return g_ctx ? g_ctx->launches : 0; }
+
+int rsdft_gpu_selftest_gemm(int m, int n, long long k, int op, double* err) {
+  REQUIRE_CTX();
+  RS_CHECK(m > 0 && n > 0 && k > 0 && err && (op == 0 || op == 1), RSDFT_ERR_ARG, "bad selftest arguments");
+  RS_TRY(selftest_gemm(*g_ctx, m, n, k, op, err));
+  return check_status(*g_ctx);
+}
 
 }  // extern "C"

@@ -1,12 +1,18 @@
-// Batched band-by-band preconditioned CG (real8 build) and the hprsdft preconditioner.
+// Batched band-by-band preconditioned CG and the hprsdft preconditioner, real8 and complex16.
 //
-// Reference: d_conjugate_gradient_1 (src/conjugate_gradient/cg_module.f90:112-431) with
-// MB_d = 1: every band runs its own CG independently, so all bands of a block are advanced
-// together here with per-band state (E, E1, rb, gkgk, res, active flag) kept on the device.
-// A band that leaves the reference's icg loop early (|E-E1| < 1e-15, which follows a
-// rejected step, :233) is masked out for the rest of the call, which reproduces the
+// Reference: d_/z_conjugate_gradient_1 (src/conjugate_gradient/cg_module.f90:112-431 and
+// :434-754) with MB_d = 1: every band runs its own CG independently, so all bands of a block
+// are advanced together here with per-band state (E, E1, rb, gkgk, res, active flag) kept on
+// the device.  A band that leaves the reference's icg loop early (|E-E1| < 1e-15, which
+// follows a rejected step, :233) is masked out for the rest of the call, which reproduces the
 // per-band exits of MB_d = 1 exactly.  precond_hprsdft
 // (src/conjugate_gradient/cgpc_hprsdft_module.f90:133-270) is batched the same way.
+//
+// complex16 arrays are handled through their interleaved real view (2*ML0 reals per band,
+// the same view the reference's dot_product takes with mm = 2*ML0, cg_module.f90:478):
+// every kernel whose coefficients are real works unchanged on that view; only the two
+// complex overlaps <p|psi>, <p|H psi>, the 2x2 Hermitian solve (zhegv) and the updates with
+// complex coefficients have NC = 2 variants.
 //
 // Reductions are deterministic: each CTA writes a per-band partial sum and the scalar
 // kernels add the partials of a band in a fixed order.
@@ -18,18 +24,19 @@ namespace rsdft {
 
 constexpr int kThreads = 256;
 constexpr int kMaxChunks = 128;
+constexpr int kPS = 8;  // partial slots per (band, chunk)
 
 enum Scal {
-  S_E = 0, S_E1, S_RB, S_GKGK, S_RES, S_W, S_U1, S_U2, S_ACT, S_BETA, S_ACC,
+  S_E = 0, S_E1, S_RB, S_GKGK, S_RES, S_W, S_U1, S_U1I, S_U2, S_U2I, S_ACT, S_BETA, S_ACC,
   S_RR0, S_RR1, S_PCA, S_PCB, S_PCACT, S_COUNT
 };
 
 struct Blk {
   int nbb;        // bands in the block
   int nch;        // CTAs (chunks) per band for elementwise/reduction kernels
-  size_t ng;
+  size_t ng;      // reals per band (grid points x components)
   double* sc;     // scalars [S_COUNT][nbb]
-  double* part;   // partials [nbb][nch][6]
+  double* part;   // partials [nbb][nch][kPS]
 };
 
 __device__ __forceinline__ double& SC(const Blk& k, int which, int b) { return k.sc[(size_t)which * k.nbb + b]; }
@@ -50,29 +57,31 @@ __device__ __forceinline__ void block_partials(double (&v)[ND], const Blk& k, in
     double t = 0.0;
 #pragma unroll
     for (int w = 0; w < kThreads / 32; ++w) t += red[w][threadIdx.x];
-    k.part[((size_t)b * k.nch + blockIdx.x) * 6 + threadIdx.x] = t;
+    k.part[((size_t)b * k.nch + blockIdx.x) * kPS + threadIdx.x] = t;
   }
 }
 
 __device__ __forceinline__ double sum_part(const Blk& k, int b, int d) {
   double t = 0.0;
-  for (int c = 0; c < k.nch; ++c) t += k.part[((size_t)b * k.nch + c) * 6 + d];
+  for (int c = 0; c < k.nch; ++c) t += k.part[((size_t)b * k.nch + c) * kPS + d];
   return t;
 }
 
-#define BAND_LOOP(k)                                                        \
+// NC = 2 loops run over complex points (pairs of reals)
+#define BAND_LOOP(k, NC)                                                    \
   const int b = blockIdx.y;                                                 \
   const size_t off = (size_t)b * (k).ng;                                    \
-  const size_t per = ((k).ng + (k).nch - 1) / (k).nch;                      \
-  const size_t i0 = per * blockIdx.x, i1 = min((k).ng, i0 + per);
+  const size_t npt = (k).ng / (NC);                                         \
+  const size_t per = (npt + (k).nch - 1) / (k).nch;                         \
+  const size_t i0 = per * blockIdx.x, i1 = min(npt, i0 + per);
 
 // ---------------------------------------------------------------------------
-// elementwise + reduction kernels
+// elementwise + reduction kernels on the real view
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_dot(Blk k, const T* __restrict__ a, const T* __restrict__ bb,
                                                   int act_idx) {
-  BAND_LOOP(k);
+  BAND_LOOP(k, 1);
   if (act_idx >= 0 && SC(k, act_idx, b) == 0.0) return;
   double v[1] = {0.0};
   for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) v[0] += (double)a[off + i] * (double)bb[off + i];
@@ -83,7 +92,7 @@ __global__ void __launch_bounds__(kThreads) k_dot(Blk k, const T* __restrict__ a
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_make_g(Blk k, const T* __restrict__ x, const T* __restrict__ hx,
                                                      T* __restrict__ g, double gfac) {
-  BAND_LOOP(k);
+  BAND_LOOP(k, 1);
   if (SC(k, S_ACT, b) == 0.0) return;
   const double E = SC(k, S_E, b);
   double v[1] = {0.0};
@@ -97,7 +106,7 @@ __global__ void __launch_bounds__(kThreads) k_make_g(Blk k, const T* __restrict_
 
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_copy(Blk k, const T* __restrict__ src, T* __restrict__ dst) {
-  BAND_LOOP(k);
+  BAND_LOOP(k, 1);
   if (SC(k, S_ACT, b) == 0.0) return;
   for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) dst[off + i] = src[off + i];
 }
@@ -105,7 +114,7 @@ __global__ void __launch_bounds__(kThreads) k_copy(Blk k, const T* __restrict__ 
 // p = Pg + beta p
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_make_p(Blk k, const T* __restrict__ pg, T* __restrict__ p, int first) {
-  BAND_LOOP(k);
+  BAND_LOOP(k, 1);
   if (SC(k, S_ACT, b) == 0.0) return;
   const T beta = (T)SC(k, S_BETA, b);
   if (first) {
@@ -115,53 +124,98 @@ __global__ void __launch_bounds__(kThreads) k_make_p(Blk k, const T* __restrict_
   }
 }
 
-// the six dot products of the line minimisation (cg_module.f90:288-296)
-template <typename T>
+// the six dot products of the line minimisation (cg_module.f90:288-296, :623-630);
+// NC = 2 adds Im<p|x> and Im<p|hx> in slots 6 and 7
+template <typename T, int NC>
 __global__ void __launch_bounds__(kThreads) k_dots6(Blk k, const T* __restrict__ x, const T* __restrict__ p,
                                                     const T* __restrict__ hx, const T* __restrict__ hp) {
-  BAND_LOOP(k);
+  BAND_LOOP(k, NC);
   if (SC(k, S_ACT, b) == 0.0) return;
-  double v[6] = {0, 0, 0, 0, 0, 0};
+  constexpr int ND = NC == 1 ? 6 : 8;
+  double v[ND];
+#pragma unroll
+  for (int d = 0; d < ND; ++d) v[d] = 0.0;
   for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) {
-    const double xi = x[off + i], pi = p[off + i], hxi = hx[off + i], hpi = hp[off + i];
-    v[0] += xi * xi;
-    v[1] += pi * xi;
-    v[2] += pi * pi;
-    v[3] += xi * hxi;
-    v[4] += pi * hxi;
-    v[5] += pi * hpi;
+    if (NC == 1) {
+      const double xi = x[off + i], pi = p[off + i], hxi = hx[off + i], hpi = hp[off + i];
+      v[0] += xi * xi;
+      v[1] += pi * xi;
+      v[2] += pi * pi;
+      v[3] += xi * hxi;
+      v[4] += pi * hxi;
+      v[5] += pi * hpi;
+    } else {
+      const size_t j = off + 2 * i;
+      const double xr = x[j], xm = x[j + 1], pr = p[j], pm = p[j + 1];
+      const double hr = hx[j], hm = hx[j + 1], qr = hp[j], qm = hp[j + 1];
+      v[0] += xr * xr + xm * xm;
+      v[1] += pr * xr + pm * xm;
+      v[2] += pr * pr + pm * pm;
+      v[3] += xr * hr + xm * hm;
+      v[4] += pr * hr + pm * hm;
+      v[5] += pr * qr + pm * qm;
+      v[ND - 2] += pr * xm - pm * xr;
+      v[ND - 1] += pr * hm - pm * hr;
+    }
   }
-  block_partials<6>(v, k, b);
+  block_partials<ND>(v, k, b);
 }
 
 // hx = u1 hx + u2 hp ; g = gfac (hx - W (u1 x + u2 p)) ; partial |g|^2
-template <typename T>
+template <typename T, int NC>
 __global__ void __launch_bounds__(kThreads) k_update_hg(Blk k, const T* __restrict__ x, const T* __restrict__ p,
                                                         T* __restrict__ hx, const T* __restrict__ hp,
                                                         T* __restrict__ g, double gfac) {
-  BAND_LOOP(k);
+  BAND_LOOP(k, NC);
   if (SC(k, S_ACT, b) == 0.0) return;
   const double u1 = SC(k, S_U1, b), u2 = SC(k, S_U2, b), W = SC(k, S_W, b);
+  const double u1i = SC(k, S_U1I, b), u2i = SC(k, S_U2I, b);
   double v[1] = {0.0};
   for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) {
-    const double h = u1 * (double)hx[off + i] + u2 * (double)hp[off + i];
-    const T ht = (T)h;
-    hx[off + i] = ht;
-    const T gi = (T)(gfac * ((double)ht - W * (u1 * (double)x[off + i] + u2 * (double)p[off + i])));
-    g[off + i] = gi;
-    v[0] += (double)gi * (double)gi;
+    if (NC == 1) {
+      const double h = u1 * (double)hx[off + i] + u2 * (double)hp[off + i];
+      const T ht = (T)h;
+      hx[off + i] = ht;
+      const T gi = (T)(gfac * ((double)ht - W * (u1 * (double)x[off + i] + u2 * (double)p[off + i])));
+      g[off + i] = gi;
+      v[0] += (double)gi * (double)gi;
+    } else {
+      const size_t j = off + 2 * i;
+      const double hr = hx[j], hm = hx[j + 1], qr = hp[j], qm = hp[j + 1];
+      const T nr = (T)(u1 * hr - u1i * hm + u2 * qr - u2i * qm);
+      const T nm = (T)(u1 * hm + u1i * hr + u2 * qm + u2i * qr);
+      hx[j] = nr;
+      hx[j + 1] = nm;
+      const double xr = x[j], xm = x[j + 1], pr = p[j], pm = p[j + 1];
+      const double yr = u1 * xr - u1i * xm + u2 * pr - u2i * pm;
+      const double ym = u1 * xm + u1i * xr + u2 * pm + u2i * pr;
+      const T gr = (T)(gfac * ((double)nr - W * yr));
+      const T gm = (T)(gfac * ((double)nm - W * ym));
+      g[j] = gr;
+      g[j + 1] = gm;
+      v[0] += (double)gr * (double)gr + (double)gm * (double)gm;
+    }
   }
   block_partials<1>(v, k, b);
 }
 
 // x = u1 x + u2 p for accepted bands
-template <typename T>
+template <typename T, int NC>
 __global__ void __launch_bounds__(kThreads) k_update_x(Blk k, T* __restrict__ x, const T* __restrict__ p) {
-  BAND_LOOP(k);
+  BAND_LOOP(k, NC);
   if (SC(k, S_ACT, b) == 0.0 || SC(k, S_ACC, b) == 0.0) return;
   const double u1 = SC(k, S_U1, b), u2 = SC(k, S_U2, b);
-  for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads)
-    x[off + i] = (T)(u1 * (double)x[off + i] + u2 * (double)p[off + i]);
+  const double u1i = SC(k, S_U1I, b), u2i = SC(k, S_U2I, b);
+  for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) {
+    if (NC == 1) {
+      x[off + i] = (T)(u1 * (double)x[off + i] + u2 * (double)p[off + i]);
+    } else {
+      const size_t j = off + 2 * i;
+      const double xr = x[j], xm = x[j + 1], pr = p[j], pm = p[j + 1];
+      x[j] = (T)(u1 * xr - u1i * xm + u2 * pr - u2i * pm);
+      x[j + 1] = (T)(u1 * xm + u1i * xr + u2 * pm + u2i * pr);
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -176,14 +230,13 @@ __global__ void k_sc_init(Blk k, double dV) {
   SC(k, S_RES, b) = 0.0;
 }
 
-// rb = dV * sum
 __global__ void k_sc_rb(Blk k, double dV) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= k.nbb || SC(k, S_ACT, b) == 0.0) return;
   SC(k, S_RB, b) = sum_part(k, b, 0) * dV;
 }
 
-// loop head: res = rb / c1^2, exit tests (cg_module.f90:231-237)
+// loop head: res = rb / c1^2, exit tests (cg_module.f90:231-237, :556-562)
 __global__ void k_sc_top(Blk k, double c1sq) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= k.nbb || SC(k, S_ACT, b) == 0.0) return;
@@ -202,62 +255,91 @@ __global__ void k_sc_beta(Blk k, double dV, int first) {
   SC(k, S_GKGK, b) = rb;
 }
 
-// 2x2 generalised symmetric eigenproblem A z = w B z (dsygv itype 1, cg_module.f90:316),
-// root selection (:317-321) and sign fix (:322-327).
+// 2x2 generalised Hermitian eigenproblem A z = w B z (dsygv/zhegv itype 1, cg_module.f90:316,
+// :651) by Cholesky B = U^H U and C = U^-H A U^-1, root selection (:317-321) and phase fix
+// (real: :322-327, complex: :657-662).  B12 = <psi|p>, A12 = <psi|H p> = conj(<p|H psi>).
+template <int NC>
 __global__ void k_sc_solve2(Blk k, double dV) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= k.nbb || SC(k, S_ACT, b) == 0.0) return;
-  const double B11 = sum_part(k, b, 0) * dV, B12 = sum_part(k, b, 1) * dV, B22 = sum_part(k, b, 2) * dV;
-  const double A11 = sum_part(k, b, 3) * dV, A12 = sum_part(k, b, 4) * dV, A22 = sum_part(k, b, 5) * dV;
+  const double B11 = sum_part(k, b, 0) * dV, B22 = sum_part(k, b, 2) * dV;
+  const double A11 = sum_part(k, b, 3) * dV, A22 = sum_part(k, b, 5) * dV;
+  const double B12r = sum_part(k, b, 1) * dV, A12r = sum_part(k, b, 4) * dV;
+  const double B12i = NC == 2 ? -sum_part(k, b, 6) * dV : 0.0;
+  const double A12i = NC == 2 ? -sum_part(k, b, 7) * dV : 0.0;
   const double E = SC(k, S_E, b);
-  double w1, w2, z1[2], z2[2];
   bool ok = B11 > 0.0;
-  double u11 = 0, u12 = 0, u22 = 0;
+  double u11 = 0, u12r = 0, u12i = 0, u22 = 0;
   if (ok) {
     u11 = sqrt(B11);
-    u12 = B12 / u11;
-    const double t = B22 - u12 * u12;
+    u12r = B12r / u11;
+    u12i = B12i / u11;
+    const double t = B22 - (u12r * u12r + u12i * u12i);
     ok = t > 0.0;
     if (ok) u22 = sqrt(t);
   }
-  if (!ok) {
-    // B not positive definite: keep the band unchanged
+  if (!ok) {  // B not positive definite: keep the band unchanged
     SC(k, S_U1, b) = 1.0;
+    SC(k, S_U1I, b) = 0.0;
     SC(k, S_U2, b) = 0.0;
+    SC(k, S_U2I, b) = 0.0;
     SC(k, S_W, b) = E;
     SC(k, S_E1, b) = E;
     return;
   }
-  // C = U^-T A U^-1
-  const double l11 = 1.0 / u11, l21 = -u12 / (u11 * u22), l22 = 1.0 / u22;
-  const double a = l11 * l11 * A11;
-  const double c12 = l11 * (l21 * A11 + l22 * A12);
-  const double d = l21 * l21 * A11 + 2.0 * l21 * l22 * A12 + l22 * l22 * A22;
-  const double mean = 0.5 * (a + d), r = hypot(0.5 * (a - d), c12);
-  w1 = mean - r;
-  w2 = mean + r;
-  double v1, v2;
+  // L = U^-H: l11 = 1/u11, l21 = -conj(u12)/(u11 u22), l22 = 1/u22 ; C = L A L^H
+  const double l11 = 1.0 / u11, l22 = 1.0 / u22;
+  const double l21r = -u12r / (u11 * u22), l21i = u12i / (u11 * u22);
+  const double ca = l11 * l11 * A11;
+  // C12 = l11 (A11 conj(l21) + A12 l22)
+  const double c12r = l11 * (A11 * l21r + A12r * l22);
+  const double c12i = l11 * (-A11 * l21i + A12i * l22);
+  // C22 = |l21|^2 A11 + 2 l22 Re(l21 A12) + l22^2 A22
+  const double cd = (l21r * l21r + l21i * l21i) * A11 + 2.0 * l22 * (l21r * A12r - l21i * A12i) + l22 * l22 * A22;
+  const double mean = 0.5 * (ca + cd), r = sqrt(0.25 * (ca - cd) * (ca - cd) + c12r * c12r + c12i * c12i);
+  const double w1 = mean - r, w2 = mean + r;
+  // eigenvector of w1: (c12, w1 - ca) or (cd - w1, -conj(c12)), the longer one
+  double v1r, v1i, v2r, v2i;
   if (r == 0.0) {
-    v1 = 1.0; v2 = 0.0;
-  } else if (d - w1 >= a - w1) {
-    v1 = d - w1; v2 = -c12;
+    v1r = 1.0; v1i = 0.0; v2r = 0.0; v2i = 0.0;
+  } else if (cd - w1 >= ca - w1) {
+    v1r = cd - w1; v1i = 0.0; v2r = -c12r; v2i = c12i;
   } else {
-    v1 = c12; v2 = w1 - a;
+    v1r = c12r; v1i = c12i; v2r = w1 - ca; v2i = 0.0;
   }
-  const double nv = hypot(v1, v2);
-  v1 /= nv; v2 /= nv;
-  // second eigenvector (-v2, v1); back-transform z = U^-1 v
-  z1[0] = v1 / u11 - u12 * v2 / (u11 * u22);
-  z1[1] = v2 / u22;
-  z2[0] = -v2 / u11 - u12 * v1 / (u11 * u22);
-  z2[1] = v1 / u22;
-  double W = w1, x1 = z1[0], x2 = z1[1];
+  const double nv = sqrt(v1r * v1r + v1i * v1i + v2r * v2r + v2i * v2i);
+  v1r /= nv; v1i /= nv; v2r /= nv; v2i /= nv;
+  // eigenvector of w2: (-conj(v2), conj(v1))
+  const double s1r = -v2r, s1i = v2i, s2r = v1r, s2i = -v1i;
+  // back-transform z = U^-1 v: z1 = v1/u11 - u12 v2/(u11 u22), z2 = v2/u22
+  auto back = [&](double a1r, double a1i, double a2r, double a2i, double& z1r, double& z1i, double& z2r,
+                  double& z2i) {
+    const double f = 1.0 / (u11 * u22);
+    z1r = a1r / u11 - f * (u12r * a2r - u12i * a2i);
+    z1i = a1i / u11 - f * (u12r * a2i + u12i * a2r);
+    z2r = a2r / u22;
+    z2i = a2i / u22;
+  };
+  double z1r, z1i, z2r, z2i, W = w1;
+  back(v1r, v1i, v2r, v2i, z1r, z1i, z2r, z2i);
   if (fabs(w1 - E) > 1.0e-1 && fabs(w2 - E) <= 1.0e-1) {
-    W = w2; x1 = z2[0]; x2 = z2[1];
+    W = w2;
+    back(s1r, s1i, s2r, s2i, z1r, z1i, z2r, z2i);
   }
-  if (x1 < 0.0) { x1 = -x1; x2 = -x2; }
-  SC(k, S_U1, b) = x1;
-  SC(k, S_U2, b) = x2;
+  if (NC == 1) {
+    if (z1r < 0.0) { z1r = -z1r; z2r = -z2r; }
+    z1i = z2i = 0.0;
+  } else {
+    // multiply by conj(z1)/|z1| so that z1 is real and positive
+    const double az = sqrt(z1r * z1r + z1i * z1i);
+    const double pr = z1r / az, pi = -z1i / az;
+    const double t2r = z2r * pr - z2i * pi, t2i = z2r * pi + z2i * pr;
+    z1r = az; z1i = 0.0; z2r = t2r; z2i = t2i;
+  }
+  SC(k, S_U1, b) = z1r;
+  SC(k, S_U1I, b) = z1i;
+  SC(k, S_U2, b) = z2r;
+  SC(k, S_U2I, b) = z2i;
   SC(k, S_W, b) = W;
   SC(k, S_E1, b) = E;
   SC(k, S_E, b) = W;
@@ -278,35 +360,38 @@ __global__ void k_sc_reject(Blk k, double dV) {
 }
 
 // ---------------------------------------------------------------------------
-// preconditioner: 7-point operator A = (c0 - E0) I + sum_d c_d (shift_+ + shift_-), E0 = 0
+// preconditioner: 7-point operator A = (c0 - E0) I + sum_d c_d (shift_+ + shift_-), E0 = 0,
+// applied to each component of the real view (real coefficients)
 // ---------------------------------------------------------------------------
 struct PcCoef {
   double c0, c1, c2, c3;
-  int n1, n2, n3;
+  int n1, n2, n3, nc;
 };
 
 template <typename T>
-__device__ __forceinline__ double apply7(const T* __restrict__ g, size_t i, const PcCoef& q) {
-  const int n1 = q.n1, n2 = q.n2, n3 = q.n3;
+__device__ __forceinline__ double apply7(const T* __restrict__ g, size_t j, const PcCoef& q) {
+  const int n1 = q.n1, n2 = q.n2, n3 = q.n3, nc = q.nc;
+  const size_t i = j / nc;
+  const size_t comp = j - i * nc;
   const int i1 = (int)(i % n1);
   const int i2 = (int)((i / n1) % n2);
   const int i3 = (int)(i / ((size_t)n1 * n2));
   const size_t row = i - i1;
   const size_t pln = (size_t)n1 * n2;
   const size_t xm = row + (i1 == 0 ? n1 - 1 : i1 - 1), xp = row + (i1 == n1 - 1 ? 0 : i1 + 1);
-  const size_t ym = i + (i2 == 0 ? (size_t)(n2 - 1) * n1 : 0) - (i2 == 0 ? 0 : n1);
-  const size_t yp = i - (i2 == n2 - 1 ? (size_t)(n2 - 1) * n1 : 0) + (i2 == n2 - 1 ? 0 : n1);
-  const size_t zm = i + (i3 == 0 ? (size_t)(n3 - 1) * pln : 0) - (i3 == 0 ? 0 : pln);
-  const size_t zp = i - (i3 == n3 - 1 ? (size_t)(n3 - 1) * pln : 0) + (i3 == n3 - 1 ? 0 : pln);
-  return q.c0 * (double)g[i] + q.c1 * ((double)g[xp] + (double)g[xm]) + q.c2 * ((double)g[yp] + (double)g[ym]) +
-         q.c3 * ((double)g[zp] + (double)g[zm]);
+  const size_t ym = i2 == 0 ? i + (size_t)(n2 - 1) * n1 : i - n1;
+  const size_t yp = i2 == n2 - 1 ? i - (size_t)(n2 - 1) * n1 : i + n1;
+  const size_t zm = i3 == 0 ? i + (size_t)(n3 - 1) * pln : i - pln;
+  const size_t zp = i3 == n3 - 1 ? i - (size_t)(n3 - 1) * pln : i + pln;
+  auto G = [&](size_t pt) { return (double)g[pt * nc + comp]; };
+  return q.c0 * (double)g[j] + q.c1 * (G(xp) + G(xm)) + q.c2 * (G(yp) + G(ym)) + q.c3 * (G(zp) + G(zm));
 }
 
 // F = A G ; R = G - F ; Q = R ; PG = G ; partial |R|^2
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_pc_first(Blk k, PcCoef q, const T* __restrict__ G,
                                                        T* __restrict__ R, T* __restrict__ Q, T* __restrict__ PG) {
-  BAND_LOOP(k);
+  BAND_LOOP(k, 1);
   if (SC(k, S_ACT, b) == 0.0) return;
   const T* g = G + off;
   double v[1] = {0.0};
@@ -324,14 +409,14 @@ __global__ void __launch_bounds__(kThreads) k_pc_first(Blk k, PcCoef q, const T*
 // F = A Q ; partial <Q|F>
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_pc_apply(Blk k, PcCoef q, const T* __restrict__ Q, T* __restrict__ F) {
-  BAND_LOOP(k);
+  BAND_LOOP(k, 1);
   if (SC(k, S_PCACT, b) == 0.0) return;
   const T* qq = Q + off;
   double v[1] = {0.0};
   for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) {
-    const double f = apply7(qq, i, q);
-    F[off + i] = (T)f;
-    v[0] += (double)qq[i] * (double)(T)f;
+    const T f = (T)apply7(qq, i, q);
+    F[off + i] = f;
+    v[0] += (double)qq[i] * (double)f;
   }
   block_partials<1>(v, k, b);
 }
@@ -340,7 +425,7 @@ __global__ void __launch_bounds__(kThreads) k_pc_apply(Blk k, PcCoef q, const T*
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_pc_update(Blk k, const T* __restrict__ Q, const T* __restrict__ F,
                                                         T* __restrict__ R, T* __restrict__ PG, int last) {
-  BAND_LOOP(k);
+  BAND_LOOP(k, 1);
   if (SC(k, S_PCACT, b) == 0.0) return;
   const double a = SC(k, S_PCA, b);
   double v[1] = {0.0};
@@ -359,7 +444,7 @@ __global__ void __launch_bounds__(kThreads) k_pc_update(Blk k, const T* __restri
 // Q = R + b Q
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_pc_newdir(Blk k, const T* __restrict__ R, T* __restrict__ Q) {
-  BAND_LOOP(k);
+  BAND_LOOP(k, 1);
   if (SC(k, S_PCACT, b) == 0.0) return;
   const double bb = SC(k, S_PCB, b);
   for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) Q[off + i] = (T)((double)R[off + i] + bb * (double)Q[off + i]);
@@ -368,10 +453,13 @@ __global__ void __launch_bounds__(kThreads) k_pc_newdir(Blk k, const T* __restri
 __global__ void k_pc_sc_first(Blk k) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= k.nbb) return;
-  if (SC(k, S_ACT, b) == 0.0) { SC(k, S_PCACT, b) = 0.0; return; }
+  if (SC(k, S_ACT, b) == 0.0) {
+    SC(k, S_PCACT, b) = 0.0;
+    return;
+  }
   const double rr1 = sum_part(k, b, 0);
   SC(k, S_RR1, b) = rr1;
-  SC(k, S_PCACT, b) = rr1 < 1.0e-24 ? 0.0 : 1.0;   // cgpc_hprsdft_module.f90:181
+  SC(k, S_PCACT, b) = rr1 < 1.0e-24 ? 0.0 : 1.0;  // cgpc_hprsdft_module.f90:181
 }
 __global__ void k_pc_sc_alpha(Blk k) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -417,6 +505,7 @@ static int pc_block(Ctx& c, Blk& k, const T* G, T* PG, T* R, T* Q, T* F) {
   q.c2 = -0.5 * c.p.ggg[1] / (H[1] * H[1]);
   q.c3 = -0.5 * c.p.ggg[2] / (H[2] * H[2]);
   q.n1 = c.p.n1; q.n2 = c.p.n2; q.n3 = c.p.n3;
+  q.nc = c.cplx ? 2 : 1;
   ProfScope ps(c, "pc");
   LAUNCH_E(k_pc_first<T>, q, G, R, Q, PG);
   LAUNCH_S(k_pc_sc_first);
@@ -434,22 +523,23 @@ static int pc_block(Ctx& c, Blk& k, const T* G, T* PG, T* R, T* Q, T* F) {
 
 template <typename T>
 int precond_real(Ctx& c, const T* g, T* pg, size_t ld, int nb) {
-  RS_CHECK(ld == c.ng, RSDFT_ERR_ARG, "precond: ld must equal the grid size");
+  const size_t nreal = c.ng * (c.cplx ? 2 : 1);
+  RS_CHECK(ld == nreal, RSDFT_ERR_ARG, "precond: ld must equal the grid size");
   Blk k;
   k.nbb = nb;
-  k.ng = c.ng;
-  k.nch = pick_nch(c.ng, nb);
+  k.ng = nreal;
+  k.nch = pick_nch(nreal, nb);
   RS_TRY(c.ws_scal.ensure(sizeof(double) * S_COUNT * nb + 64));
-  RS_TRY(c.ws_red.ensure(sizeof(double) * 6 * (size_t)nb * k.nch));
-  RS_TRY(c.ws_cg.ensure(sizeof(T) * 3 * c.ng * (size_t)nb));
+  RS_TRY(c.ws_red.ensure(sizeof(double) * kPS * (size_t)nb * k.nch));
+  RS_TRY(c.ws_cg.ensure(sizeof(T) * 3 * nreal * (size_t)nb));
   k.sc = c.ws_scal.as<double>();
   k.part = c.ws_red.as<double>();
   std::vector<double> act((size_t)nb, 1.0);
   RS_CUDA(cudaMemcpyAsync(k.sc + (size_t)S_ACT * nb, act.data(), sizeof(double) * nb, cudaMemcpyHostToDevice,
                           c.stream));
   T* R = c.ws_cg.as<T>();
-  T* Q = R + c.ng * nb;
-  T* F = Q + c.ng * nb;
+  T* Q = R + nreal * nb;
+  T* F = Q + nreal * nb;
   RS_TRY(pc_block<T>(c, k, g, pg, R, Q, F));
   RS_CUDA(cudaStreamSynchronize(c.stream));
   return 0;
@@ -458,50 +548,50 @@ template int precond_real<double>(Ctx&, const double*, double*, size_t, int);
 template int precond_real<float>(Ctx&, const float*, float*, size_t, int);
 
 template <typename T>
-static int cg_real(Ctx& c, int kk, int s, double* h_esp, double* h_res) {
+static int hpsi_any(Ctx& c, int kk, int s, const T* x, T* hx, size_t ld, int nb) {
+  if (c.cplx) return hpsi_cplx<T>(c, kk, s, x, hx, ld, nb);
+  return hpsi_real<T>(c, kk, s, x, hx, ld, nb);
+}
+
+template <typename T, int NC>
+static int cg_block_run(Ctx& c, int kk, int s, double* h_esp, double* h_res) {
   const int nb = c.kp[kk].nband;
-  const size_t ng = c.ng;
+  const size_t nreal = c.ng * NC;
   int nbb = c.p.cg_block > 0 ? std::min(c.p.cg_block, nb) : nb;
-  // budget: 8 block vectors per band; keep them within ~40% of free memory
   size_t freeb = 0, totb = 0;
   cudaMemGetInfo(&freeb, &totb);
-  const size_t per_band = 8 * ng * sizeof(T);
-  const size_t have = c.ws_cg.bytes;
-  const size_t budget = (size_t)(0.4 * (double)(freeb + have));
-  if (c.p.cg_block <= 0) {
+  const size_t per_band = 8 * nreal * sizeof(T);
+  const size_t budget = (size_t)(0.4 * (double)(freeb + c.ws_cg.bytes));
+  if (c.p.cg_block <= 0)
     while (nbb > 1 && (size_t)nbb * per_band > budget) nbb = (nbb + 1) / 2;
-  }
   RS_TRY(c.ws_cg.ensure(per_band * nbb));
   RS_TRY(c.ws_scal.ensure(sizeof(double) * S_COUNT * nbb + 64));
   Blk k;
-  k.nbb = nbb;
-  k.ng = ng;
-  k.nch = pick_nch(ng, nbb);
-  RS_TRY(c.ws_red.ensure(sizeof(double) * 6 * (size_t)nbb * k.nch));
+  k.ng = nreal;
+  k.nch = pick_nch(nreal, nbb);
+  RS_TRY(c.ws_red.ensure(sizeof(double) * kPS * (size_t)nbb * pick_nch(nreal, 1)));
   k.sc = c.ws_scal.as<double>();
   k.part = c.ws_red.as<double>();
   T* base = c.ws_cg.as<T>();
   T* HX = base;
-  T* HP = HX + ng * nbb;
-  T* G = HP + ng * nbb;
-  T* PG = G + ng * nbb;
-  T* P = PG + ng * nbb;
-  T* R = P + ng * nbb;
-  T* Q = R + ng * nbb;
-  T* F = Q + ng * nbb;
+  T* HP = HX + nreal * nbb;
+  T* G = HP + nreal * nbb;
+  T* PG = G + nreal * nbb;
+  T* P = PG + nreal * nbb;
+  T* R = P + nreal * nbb;
+  T* Q = R + nreal * nbb;
+  T* F = Q + nreal * nbb;
   T* psi = c.wfn(kk, s).psi.as<T>();
   const double dV = c.p.dv;
-  const double gfac = -2.0, c1sq = 4.0;  // real build: g = -2(Hx - Ex), res = rb / 2^2
+  // real build: g = -2(Hx - Ex), res = rb/2^2; complex build: g = -(Hx - Ex), res = rb
+  const double gfac = NC == 1 ? -2.0 : -1.0, c1sq = NC == 1 ? 4.0 : 1.0;
   std::vector<double> hE, hR;
   for (int b0 = 0; b0 < nb; b0 += nbb) {
     const int nn = std::min(nbb, nb - b0);
     k.nbb = nn;
-    k.nch = pick_nch(ng, nn);
-    T* X = psi + (size_t)b0 * ng;
-    {
-      ProfScope ps(c, "cg");
-      RS_TRY(hpsi_real<T>(c, kk, s, X, HX, ng, nn));
-    }
+    k.nch = pick_nch(nreal, nn);
+    T* X = psi + (size_t)b0 * nreal;
+    RS_TRY(hpsi_any<T>(c, kk, s, X, HX, nreal, nn));
     {
       ProfScope ps(c, "cg");
       LAUNCH_E(k_dot<T>, X, HX, -1);
@@ -527,21 +617,22 @@ static int cg_real(Ctx& c, int kk, int s, double* h_esp, double* h_res) {
         LAUNCH_S(k_sc_beta, dV, icg == 1 ? 1 : 0);
         LAUNCH_E(k_make_p<T>, PG, P, icg == 1 ? 1 : 0);
       }
-      RS_TRY(hpsi_real<T>(c, kk, s, P, HP, ng, nn));
+      RS_TRY(hpsi_any<T>(c, kk, s, P, HP, nreal, nn));
       {
         ProfScope ps(c, "cg");
-        LAUNCH_E(k_dots6<T>, X, P, HX, HP);
-        LAUNCH_S(k_sc_solve2, dV);
-        LAUNCH_E(k_update_hg<T>, X, P, HX, HP, G, gfac);
+        LAUNCH_E((k_dots6<T, NC>), X, P, HX, HP);
+        LAUNCH_S(k_sc_solve2<NC>, dV);
+        LAUNCH_E((k_update_hg<T, NC>), X, P, HX, HP, G, gfac);
         LAUNCH_S(k_sc_reject, dV);
-        LAUNCH_E(k_update_x<T>, X, P);
+        LAUNCH_E((k_update_x<T, NC>), X, P);
       }
     }
     RS_TRY(check_launch("cg"));
     if (h_esp || h_res) {
       hE.resize(nn);
       hR.resize(nn);
-      RS_CUDA(cudaMemcpyAsync(hE.data(), k.sc + (size_t)S_E * nn, sizeof(double) * nn, cudaMemcpyDeviceToHost, c.stream));
+      RS_CUDA(cudaMemcpyAsync(hE.data(), k.sc + (size_t)S_E * nn, sizeof(double) * nn, cudaMemcpyDeviceToHost,
+                              c.stream));
       RS_CUDA(cudaMemcpyAsync(hR.data(), k.sc + (size_t)S_RES * nn, sizeof(double) * nn, cudaMemcpyDeviceToHost,
                               c.stream));
       RS_CUDA(cudaStreamSynchronize(c.stream));
@@ -553,23 +644,16 @@ static int cg_real(Ctx& c, int kk, int s, double* h_esp, double* h_res) {
 }
 
 int cg_run(Ctx& c, int k, int s, double* h_esp, double* h_res) {
-  if (c.cplx) {
-    RS_CHECK(false, RSDFT_ERR_UNSUPPORTED, "complex16 CG is provided by cg_cplx");
-  }
-  if (c.mixed) return cg_real<float>(c, k, s, h_esp, h_res);
-  return cg_real<double>(c, k, s, h_esp, h_res);
+  if (c.cplx) return c.mixed ? cg_block_run<float, 2>(c, k, s, h_esp, h_res) : cg_block_run<double, 2>(c, k, s, h_esp, h_res);
+  return c.mixed ? cg_block_run<float, 1>(c, k, s, h_esp, h_res) : cg_block_run<double, 1>(c, k, s, h_esp, h_res);
 }
-
-}  // namespace rsdft
-
-namespace rsdft {
 
 // ---------------------------------------------------------------------------
 // FP64 residual check (esp_calc + the CG residual definition, in FP64 for any storage)
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_res_dots(Blk k, const T* __restrict__ x, const double* __restrict__ hx) {
-  BAND_LOOP(k);
+  BAND_LOOP(k, 1);
   double v[2] = {0.0, 0.0};
   for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) {
     const double xi = (double)x[off + i];
@@ -588,7 +672,7 @@ __global__ void k_res_sc1(Blk k, double* esp) {
 }
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_res_norm(Blk k, const T* __restrict__ x, const double* __restrict__ hx) {
-  BAND_LOOP(k);
+  BAND_LOOP(k, 1);
   const double e = SC(k, S_E, b);
   double v[1] = {0.0};
   for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) {
@@ -604,35 +688,36 @@ __global__ void k_res_sc2(Blk k, double* res) {
 }
 
 template <typename T>
-static int residual_real(Ctx& c, int kk, int s, double* d_esp, double* d_res) {
+static int residual_t(Ctx& c, int kk, int s, double* d_esp, double* d_res) {
   const int nb = c.kp[kk].nband;
-  const size_t ng = c.ng;
+  const int nc = c.cplx ? 2 : 1;
+  const size_t nreal = c.ng * nc;
   // band chunk so that the FP64 copies stay around 1 GiB
-  int nbc = (int)std::max<size_t>(1, std::min<size_t>(nb, (size_t)(1u << 30) / (16 * ng)));
+  int nbc = (int)std::max<size_t>(1, std::min<size_t>(nb, (size_t)(1u << 30) / (16 * nreal)));
   const size_t extra = std::is_same<T, double>::value ? 0 : 1;
-  RS_TRY(c.ws_rot.ensure(sizeof(double) * ng * nbc * (1 + extra)));
-  RS_TRY(c.ws_scal.ensure(sizeof(double) * S_COUNT * nbc + sizeof(double) * 2 * nb + 64));
+  RS_TRY(c.ws_rot.ensure(sizeof(double) * nreal * nbc * (1 + extra)));
+  RS_TRY(c.ws_scal.ensure(sizeof(double) * S_COUNT * nbc + 64));
   const T* psi = c.wfn(kk, s).psi.as<T>();
   double* HX = c.ws_rot.as<double>();
-  double* XD = HX + ng * nbc;
+  double* XD = HX + nreal * nbc;
   Blk k;
-  k.ng = ng;
+  k.ng = nreal;
   for (int b0 = 0; b0 < nb; b0 += nbc) {
     const int nn = std::min(nbc, nb - b0);
     k.nbb = nn;
-    k.nch = pick_nch(ng, nn);
-    RS_TRY(c.ws_red.ensure(sizeof(double) * 6 * (size_t)nn * k.nch));
+    k.nch = pick_nch(nreal, nn);
+    RS_TRY(c.ws_red.ensure(sizeof(double) * kPS * (size_t)nn * k.nch));
     k.sc = c.ws_scal.as<double>();
     k.part = c.ws_red.as<double>();
-    const T* X = psi + (size_t)b0 * ng;
+    const T* X = psi + (size_t)b0 * nreal;
     const double* XH;
     if (std::is_same<T, double>::value) {
       XH = reinterpret_cast<const double*>(X);
     } else {
-      RS_TRY(convert_f2d(c, reinterpret_cast<const float*>(X), XD, ng * nn));
+      RS_TRY(convert_f2d(c, reinterpret_cast<const float*>(X), XD, nreal * nn));
       XH = XD;
     }
-    RS_TRY(hpsi_real<double>(c, kk, s, XH, HX, ng, nn));
+    RS_TRY(hpsi_any<double>(c, kk, s, XH, HX, nreal, nn));
     ProfScope ps(c, "residual");
     LAUNCH_E(k_res_dots<T>, X, HX);
     LAUNCH_S(k_res_sc1, d_esp + b0);
@@ -643,9 +728,8 @@ static int residual_real(Ctx& c, int kk, int s, double* d_esp, double* d_res) {
 }
 
 int residual_run(Ctx& c, int k, int s, double* d_esp, double* d_res) {
-  RS_CHECK(!c.cplx, RSDFT_ERR_UNSUPPORTED, "complex16 residual is provided by residual_cplx");
-  if (c.mixed) return residual_real<float>(c, k, s, d_esp, d_res);
-  return residual_real<double>(c, k, s, d_esp, d_res);
+  if (c.mixed) return residual_t<float>(c, k, s, d_esp, d_res);
+  return residual_t<double>(c, k, s, d_esp, d_res);
 }
 
 }  // namespace rsdft

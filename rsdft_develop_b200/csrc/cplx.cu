@@ -58,9 +58,10 @@ struct StArgsC {
   int tile_y, tz, stage_elems;  // stage_elems in S units
   S c0;
   S cc[3][MD], cs[3][MD];       // zcoef_kin(d,+m) = cc - i cs
-  const int* rowptr;
-  const int* col;
-  const S* val;    // interleaved uVk
+  const int* rowptr;  // per point: scatter records [rowptr[i], rowptr[i+1])
+  const int* rec_g;   // record -> atom group
+  const S* val;       // record -> interleaved uVk of the group's projectors [pg]
+  int pg;
   const S* coef;   // interleaved c[b][p]
   int ldc;         // complex elements per band in coef
   unsigned* status;
@@ -261,11 +262,15 @@ __global__ void __launch_bounds__(256) k_stencil_cplx(const StArgsC<S, MD> a) {
                     for (int i = 0; i < V; ++i) {
                       const int ea = __ldg(a.rowptr + g + i), eb = __ldg(a.rowptr + g + i + 1);
                       for (int e = ea; e < eb; ++e) {
-                        const S ur = __ldg(a.val + 2 * e), ui = __ldg(a.val + 2 * e + 1);
-                        const int cl = __ldg(a.col + e);
-                        const S cr = __ldg(coefb + 2 * cl), ci = __ldg(coefb + 2 * cl + 1);
-                        orr[i] += ur * cr - ui * ci;
-                        oi[i] += ur * ci + ui * cr;
+                        // record e: atom group gg with its pg projector values uVk at this point
+                        const int gg = __ldg(a.rec_g + e);
+                        for (int q = 0; q < a.pg; ++q) {
+                          const S ur = __ldg(a.val + 2 * ((size_t)e * a.pg + q));
+                          const S ui = __ldg(a.val + 2 * ((size_t)e * a.pg + q) + 1);
+                          const S cr = __ldg(coefb + 2 * (gg * a.pg + q)), ci = __ldg(coefb + 2 * (gg * a.pg + q) + 1);
+                          orr[i] += ur * cr - ui * ci;
+                          oi[i] += ur * ci + ui * cr;
+                        }
                       }
                     }
                   }
@@ -350,8 +355,8 @@ __global__ void __launch_bounds__(256) k_nl_gather_cplx(const S* __restrict__ ps
   __syncthreads();
   if (threadIdx.x < BB * PG) {
     const int bb = threadIdx.x / PG, p = threadIdx.x % PG;
-    const int lma = gplist[g * PG + p];
-    if (lma >= 0 && b0 + bb < nb) {
+    (void)gplist;
+    if (b0 + bb < nb) {
       double cr = 0.0, ci = 0.0;
 #pragma unroll
       for (int q = 0; q < PG; ++q) {
@@ -359,8 +364,8 @@ __global__ void __launch_bounds__(256) k_nl_gather_cplx(const S* __restrict__ ps
         cr += d * u[2 * (bb * PG + q)];
         ci += d * u[2 * (bb * PG + q) + 1];
       }
-      coef[((long long)(b0 + bb) * ldc + lma) * 2] = (S)cr;
-      coef[((long long)(b0 + bb) * ldc + lma) * 2 + 1] = (S)ci;
+      coef[((long long)(b0 + bb) * ldc + g * PG + p) * 2] = (S)cr;
+      coef[((long long)(b0 + bb) * ldc + g * PG + p) * 2 + 1] = (S)ci;
     }
   }
 }
@@ -371,7 +376,7 @@ static void launch_gather_c(Ctx& c, const S* psi, size_t ld, int nb, S* coef, co
   dim3 grid(nl.ngroups, (nb + BB - 1) / BB);
   k_nl_gather_cplx<S, PG, BB><<<grid, 256, 0, c.stream>>>(psi, (long long)ld, nb, nl.gofs.as<int>(), nl.gjj.as<int>(),
                                                            gw, nl.gplist.as<int>(), nl.gD.as<double>(), c.p.dv, coef,
-                                                           nl.nproj);
+                                                           nl.ngroups * PG);
   c.launches++;
 }
 
@@ -410,13 +415,14 @@ static int launch_stencil_c(Ctx& c, int k, int s, const S* psi, S* out, size_t l
       a.cs[d][m] = (S)c.kp[k].coef_nabk[d][m];
     }
   const bool nl_on = c.nl.nproj > 0 && coef != nullptr;
-  a.rowptr = nl_on ? c.nl.rowptr.as<int>() : nullptr;
-  a.col = nl_on ? c.nl.col.as<int>() : nullptr;
-  a.val = nl_on ? (std::is_same<S, double>::value ? (const S*)c.nl.perk[k].val64.as<double>()
-                                                  : (const S*)c.nl.perk[k].val32.as<float>())
+  a.rowptr = nl_on ? c.nl.rec_rowptr.as<int>() : nullptr;
+  a.rec_g = nl_on ? c.nl.rec_g.as<int>() : nullptr;
+  a.val = nl_on ? (std::is_same<S, double>::value ? (const S*)c.nl.perk[k].ru64.as<double>()
+                                                  : (const S*)c.nl.perk[k].ru32.as<float>())
                 : nullptr;
+  a.pg = c.nl.pg;
   a.coef = coef;
-  a.ldc = c.nl.nproj;
+  a.ldc = c.nl.ngroups * c.nl.pg;
   a.status = c.d_status;
   auto kern = k_stencil_cplx<S, MD, R, SS>;
   static bool attr_done = false;
@@ -425,7 +431,7 @@ static int launch_stencil_c(Ctx& c, int k, int s, const S* psi, S* out, size_t l
     attr_done = true;
   }
   const double alg_bytes = (double)sizeof(S) * (4.0 * (double)c.ng * nb + (double)c.ng) +
-                           (nl_on ? 4.0 * (double)(c.ng + 1) + (4.0 + 2 * sizeof(S)) * c.nl.nnz : 0.0);
+                           (nl_on ? 4.0 * (double)(c.ng + 1) + (8.0 + 2 * sizeof(S) * c.nl.pg) * c.nl.nrec : 0.0);
   ProfScope ps(c, "hpsi_stencil", alg_bytes);
   kern<<<dim3(ytiles, zch, nb), dim3(bx, by), smem, c.stream>>>(a);
   c.launches++;
@@ -442,7 +448,7 @@ int hpsi_cplx(Ctx& c, int k, int s, const S* psi, S* out, size_t ld, int nb) {
   S* coef = nullptr;
   if (c.nl.nproj > 0) {
     RS_TRY(nl_prepare_k(c, k));
-    RS_TRY(c.ws_coef.ensure((size_t)nb * c.nl.nproj * 2 * sizeof(S)));
+    RS_TRY(c.ws_coef.ensure((size_t)nb * c.nl.ngroups * c.nl.pg * 2 * sizeof(S)));
     coef = c.ws_coef.as<S>();
     const S* gw = std::is_same<S, double>::value ? (const S*)c.nl.perk[k].gw64.as<double>()
                                                  : (const S*)c.nl.perk[k].gw32.as<float>();

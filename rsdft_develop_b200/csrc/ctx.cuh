@@ -20,12 +20,13 @@ struct NonlocalTables {
   int ftotal = 0;         // total footprint entries over groups
   std::vector<int> h_gofs, h_gplist;         // host copies (group layout)
   DBuf gofs, gjj, gplist, gD;                // int / int / int[ngroups*PG] / double[ngroups*PG*PG]
-  DBuf rowptr, col;                          // CSR (ng+1), (nnz)
-  int nnz = 0;
-  // per k: weights in both precisions (gather: conj(uVk) for complex), CSR values
+  // scatter records: one per (group, footprint point), sorted by grid point
+  DBuf rec_rowptr, rec_pt, rec_g;            // (ng+1 padded), (nrec), (nrec)
+  int nrec = 0;
+  // per k: gather weights conj(uVk) and scatter weights uVk, both [ftotal|nrec][PG] (T or T2)
   struct PerK {
-    DBuf gw64, gw32;      // [ftotal][PG] real (T) or complex (T2)
-    DBuf val64, val32;    // [nnz] scatter values
+    DBuf gw64, gw32;
+    DBuf ru64, ru32;
     bool ready = false;
   };
   std::vector<PerK> perk;
@@ -33,7 +34,7 @@ struct NonlocalTables {
   std::vector<int> h_mjj, h_jjp;  // reference layout
   int maxmjj = 0;
   std::vector<int> h_slot;        // for each (lma, j): footprint slot in its group
-  std::vector<int> h_csr_src;     // for each CSR entry: flat (lma*maxmjj + j)
+  std::vector<int> h_rec_src;     // for each record: its footprint slot
 };
 
 struct KPoint {
@@ -65,6 +66,7 @@ struct Ctx {
   cusolverDnHandle_t cusolver = nullptr;
   unsigned* d_status = nullptr;
   long long launches = 0;
+  int mb_ref = 0;  // bands 1..mb_ref judged for convergence (0: all)
 
   std::vector<KPoint> kp;
   DBuf vloc64, vloc32;             // [nspin][ng]
@@ -134,6 +136,12 @@ int precond_real(Ctx& c, const T* g, T* pg, size_t ld, int nb);
 int gs_run(Ctx& c, int k, int s, int passes);
 int sd_run(Ctx& c, int k, int s, double* h_esp);
 int residual_run(Ctx& c, int k, int s, double* d_esp, double* d_res);
+
+// ---- split-BF16 tensor-core GEMMs (gemm_x3.cu) ----
+int gemm_tn_x3(Ctx& c, const float* A, long long lda, int M, const float* B, long long ldb, int N, long long K,
+               double alpha, double* C, long long ldc, int swapB);
+int gemm_rotate_x3(Ctx& c, float* X, long long ldx, int nb, long long G, const double* V, int ldv);
+int selftest_gemm(Ctx& c, int m, int n, long long k, int op, double* err);
 
 // ---- util ----
 int random_wf(Ctx& c, int k, int s, uint64_t seed);

@@ -4,11 +4,12 @@
 //   gram_schmidt_t (src/gram_schmidt/gram_schmidt_t_module.f90:85-308) orthonormalises the
 //   bands in order with the dV inner product; its result is the Q factor of Psi = Q R with
 //   R upper triangular and positive diagonal.  Cholesky QR (the reference's GS=4 variant,
-//   src/gram_schmidt/gram_schmidt_lusl_module.f90:241-328: S = dV Psi^T Psi, potrf, trtri,
+//   src/gram_schmidt/gram_schmidt_lusl_module.f90:241-328: S = dV Psi^H Psi, potrf, trtri,
 //   Psi <- Psi R^-1) produces the same Q, with O(N M^2) GEMM work instead of a recursion.
 //   subspace_diag_la (src/subspace_diag/subspace_diag_la_module.f90:18-223):
-//   Hsub = 1/2 dV (Psi^T H Psi + (H Psi)^T Psi) (dsyr2k), dsyev, Psi <- Psi V.
-// FP64 path: cuBLAS dsyrk/dsyr2k/dtrsm/dgemm and cuSOLVER dpotrf/dsyevd.
+//   Hsub = 1/2 dV (Psi^H H Psi + (H Psi)^H Psi) (dsyr2k / zher2k), dsyev / zheevd, Psi <- Psi V.
+// FP64 path: cuBLAS syrk/herk, syr2k/her2k, trsm, gemm and cuSOLVER potrf, syevd/heevd.
+// Mixed mode keeps psi in FP32; the split-BF16 tensor-core path lives in gemm_bf16x3.cu.
 #include <cstring>
 
 #include "ctx.cuh"
@@ -40,24 +41,24 @@ struct F64View {
   bool converted = false;
 };
 
-static int f64_view(Ctx& c, int k, int s, F64View& v, DBuf& tmp) {
+static size_t nreal(const Ctx& c) { return c.ng * (c.cplx ? 2 : 1); }
+
+static int f64_view(Ctx& c, int k, int s, F64View& v) {
   const int nb = c.kp[k].nband;
   if (!c.mixed) {
     v.x = c.wfn(k, s).psi.as<double>();
     return 0;
   }
-  RS_TRY(tmp.ensure(sizeof(double) * c.ng * nb));
-  RS_TRY(convert_f2d(c, c.wfn(k, s).psi.as<float>(), tmp.as<double>(), c.ng * nb));
-  v.x = tmp.as<double>();
+  RS_TRY(c.ws_f64.ensure(sizeof(double) * nreal(c) * nb));
+  RS_TRY(convert_f2d(c, c.wfn(k, s).psi.as<float>(), c.ws_f64.as<double>(), nreal(c) * nb));
+  v.x = c.ws_f64.as<double>();
   v.converted = true;
   return 0;
 }
 static int f64_commit(Ctx& c, int k, int s, F64View& v) {
   if (!v.converted) return 0;
-  return convert_d2f(c, v.x, c.wfn(k, s).psi.as<float>(), c.ng * c.kp[k].nband);
+  return convert_d2f(c, v.x, c.wfn(k, s).psi.as<float>(), nreal(c) * c.kp[k].nband);
 }
-
-
 
 static int read_info(Ctx& c, int* d_info, int* h_info) {
   RS_CUDA(cudaMemcpyAsync(h_info, d_info, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
@@ -65,72 +66,200 @@ static int read_info(Ctx& c, int* d_info, int* h_info) {
   return 0;
 }
 
-int gs_run(Ctx& c, int k, int s, int passes) {
-  RS_CHECK(!c.cplx, RSDFT_ERR_UNSUPPORTED, "complex16 GS is provided by gs_cplx");
+// ---------------------------------------------------------------------------
+// mixed precision (real8): psi stays FP32; S, Hsub and the rotations run as split-BF16
+// tensor-core GEMMs with FP64 results; Cholesky, R^-1 and the eigensolve stay FP64.
+// ---------------------------------------------------------------------------
+__global__ void k_symmetrize(double* H, int n) {
+  // H <- (H + H^T)/2, full matrix, column-major
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)n * n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % n), j = (int)(t / n);
+    if (i < j) {
+      const double a = 0.5 * (H[i + (long long)j * n] + H[j + (long long)i * n]);
+      H[i + (long long)j * n] = a;
+      H[j + (long long)i * n] = a;
+    }
+  }
+}
+__global__ void k_identity(double* I, int n) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)n * n;
+       t += (long long)gridDim.x * blockDim.x)
+    I[t] = (t % n) == (t / n) ? 1.0 : 0.0;
+}
+
+static int gs_mixed_real(Ctx& c, int k, int s, int passes) {
   const int nb = c.kp[k].nband;
-  const int ng = (int)c.ng;
-  F64View v;
-  RS_TRY(f64_view(c, k, s, v, c.ws_f64));
-  RS_TRY(c.ws_dense.ensure(sizeof(double) * (size_t)nb * nb));
+  float* X = c.wfn(k, s).psi.as<float>();
+  RS_TRY(c.ws_dense.ensure(sizeof(double) * 2 * (size_t)nb * nb));
   RS_TRY(c.ws_info.ensure(sizeof(int) * 4));
   double* S = c.ws_dense.as<double>();
+  double* Ri = S + (size_t)nb * nb;
   int lwork = 0;
   RS_CUSOLVER(cusolverDnDpotrf_bufferSize(c.cusolver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, &lwork));
   RS_TRY(c.ws_solver.ensure(sizeof(double) * (size_t)std::max(lwork, 1)));
-  const double dV = c.p.dv, zero = 0.0, one = 1.0;
-  ProfScope ps(c, "gs");
+  const double one = 1.0;
   for (int pass = 0; pass < std::max(1, passes); ++pass) {
-    RS_CUBLAS(cublasDsyrk(c.cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, nb, ng, &dV, v.x, ng, &zero, S, nb));
-    RS_CUSOLVER(cusolverDnDpotrf(c.cusolver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, c.ws_solver.as<double>(), lwork,
-                                 c.ws_info.as<int>()));
-    int info = 0;
+    RS_CUDA(cudaMemsetAsync(S, 0, sizeof(double) * (size_t)nb * nb, c.stream));
+    // S[m][n] = dV sum_g X[m][g] X[n][g] (symmetric, row/column major alike)
+    RS_TRY(gemm_tn_x3(c, X, (long long)c.ng, nb, X, (long long)c.ng, nb, (long long)c.ng, c.p.dv, S, nb, 0));
+    {
+      ProfScope ps(c, "gs");
+      RS_CUSOLVER(cusolverDnDpotrf(c.cusolver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, c.ws_solver.as<double>(), lwork,
+                                   c.ws_info.as<int>()));
+      int info = 0;
+      RS_TRY(read_info(c, c.ws_info.as<int>(), &info));
+      RS_CHECK(info == 0, RSDFT_ERR_NOT_SPD, "overlap matrix not positive definite (potrf info=%d)", info);
+      k_identity<<<64, 256, 0, c.stream>>>(Ri, nb);
+      c.launches++;
+      RS_CUBLAS(cublasDtrsm(c.cublas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, nb,
+                            nb, &one, S, nb, Ri, nb));
+    }
+    // X <- X R^-1
+    RS_TRY(gemm_rotate_x3(c, X, (long long)c.ng, nb, (long long)c.ng, Ri, nb));
+  }
+  return 0;
+}
+
+static int sd_mixed_real(Ctx& c, int k, int s, double* h_esp) {
+  const int nb = c.kp[k].nband;
+  float* X = c.wfn(k, s).psi.as<float>();
+  RS_TRY(c.ws_hpsi.ensure(sizeof(float) * c.ng * nb));
+  float* HX = c.ws_hpsi.as<float>();
+  RS_TRY(hpsi_real<float>(c, k, s, X, HX, c.ng, nb));
+  RS_TRY(c.ws_dense.ensure(sizeof(double) * ((size_t)nb * nb + nb)));
+  RS_TRY(c.ws_info.ensure(sizeof(int) * 4));
+  double* H = c.ws_dense.as<double>();
+  double* W = H + (size_t)nb * nb;
+  RS_CUDA(cudaMemsetAsync(H, 0, sizeof(double) * (size_t)nb * nb, c.stream));
+  // H[m][n] = dV sum_g X[m][g] (HX)[n][g]; Hsub = (H + H^T)/2 = 1/2 dV (X^T HX + HX^T X)
+  RS_TRY(gemm_tn_x3(c, X, (long long)c.ng, nb, HX, (long long)c.ng, nb, (long long)c.ng, c.p.dv, H, nb, 0));
+  {
+    ProfScope ps(c, "sd");
+    k_symmetrize<<<64, 256, 0, c.stream>>>(H, nb);
+    c.launches++;
+    int lwork = 0, info = 0;
+    RS_CUSOLVER(cusolverDnDsyevd_bufferSize(c.cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb, H, nb, W,
+                                            &lwork));
+    RS_TRY(c.ws_solver.ensure(sizeof(double) * (size_t)std::max(lwork, 1)));
+    RS_CUSOLVER(cusolverDnDsyevd(c.cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb, H, nb, W,
+                                 c.ws_solver.as<double>(), lwork, c.ws_info.as<int>()));
     RS_TRY(read_info(c, c.ws_info.as<int>(), &info));
-    RS_CHECK(info == 0, RSDFT_ERR_NOT_SPD, "overlap matrix not positive definite (potrf info=%d)", info);
-    RS_CUBLAS(cublasDtrsm(c.cublas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, ng,
-                          nb, &one, S, nb, v.x, ng));
-    c.launches += 3;
+    RS_CHECK(info == 0, RSDFT_ERR_EIG, "subspace eigensolver failed (syevd info=%d)", info);
+  }
+  RS_TRY(gemm_rotate_x3(c, X, (long long)c.ng, nb, (long long)c.ng, H, nb));
+  if (h_esp) {
+    RS_CUDA(cudaMemcpyAsync(h_esp, W, sizeof(double) * nb, cudaMemcpyDeviceToHost, c.stream));
+    RS_CUDA(cudaStreamSynchronize(c.stream));
+  }
+  return 0;
+}
+
+int gs_run(Ctx& c, int k, int s, int passes) {
+  if (c.mixed && !c.cplx) return gs_mixed_real(c, k, s, passes);
+  const int nb = c.kp[k].nband;
+  const int ng = (int)c.ng;
+  const size_t es = c.cplx ? sizeof(cuDoubleComplex) : sizeof(double);
+  F64View v;
+  RS_TRY(f64_view(c, k, s, v));
+  RS_TRY(c.ws_dense.ensure(es * (size_t)nb * nb));
+  RS_TRY(c.ws_info.ensure(sizeof(int) * 4));
+  int lwork = 0;
+  if (c.cplx)
+    RS_CUSOLVER(cusolverDnZpotrf_bufferSize(c.cusolver, CUBLAS_FILL_MODE_UPPER, nb, c.ws_dense.as<cuDoubleComplex>(),
+                                            nb, &lwork));
+  else
+    RS_CUSOLVER(cusolverDnDpotrf_bufferSize(c.cusolver, CUBLAS_FILL_MODE_UPPER, nb, c.ws_dense.as<double>(), nb,
+                                            &lwork));
+  RS_TRY(c.ws_solver.ensure(es * (size_t)std::max(lwork, 1)));
+  const double dV = c.p.dv, zero = 0.0, one = 1.0;
+  const cuDoubleComplex zone = make_cuDoubleComplex(1.0, 0.0);
+  ProfScope ps(c, "gs", 0.0, 2.0 * 2.0 * c.ng * (double)nb * nb * (c.cplx ? 4 : 1));
+  for (int pass = 0; pass < std::max(1, passes); ++pass) {
+    int info = 0;
+    if (c.cplx) {
+      cuDoubleComplex* S = c.ws_dense.as<cuDoubleComplex>();
+      cuDoubleComplex* X = reinterpret_cast<cuDoubleComplex*>(v.x);
+      RS_CUBLAS(cublasZherk(c.cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C, nb, ng, &dV, X, ng, &zero, S, nb));
+      RS_CUSOLVER(cusolverDnZpotrf(c.cusolver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, c.ws_solver.as<cuDoubleComplex>(),
+                                   lwork, c.ws_info.as<int>()));
+      RS_TRY(read_info(c, c.ws_info.as<int>(), &info));
+      RS_CHECK(info == 0, RSDFT_ERR_NOT_SPD, "overlap matrix not positive definite (zpotrf info=%d)", info);
+      RS_CUBLAS(cublasZtrsm(c.cublas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, ng,
+                            nb, &zone, S, nb, X, ng));
+    } else {
+      double* S = c.ws_dense.as<double>();
+      RS_CUBLAS(cublasDsyrk(c.cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, nb, ng, &dV, v.x, ng, &zero, S, nb));
+      RS_CUSOLVER(cusolverDnDpotrf(c.cusolver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, c.ws_solver.as<double>(), lwork,
+                                   c.ws_info.as<int>()));
+      RS_TRY(read_info(c, c.ws_info.as<int>(), &info));
+      RS_CHECK(info == 0, RSDFT_ERR_NOT_SPD, "overlap matrix not positive definite (potrf info=%d)", info);
+      RS_CUBLAS(cublasDtrsm(c.cublas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, ng,
+                            nb, &one, S, nb, v.x, ng));
+    }
   }
   return f64_commit(c, k, s, v);
 }
 
 int sd_run(Ctx& c, int k, int s, double* h_esp) {
-  RS_CHECK(!c.cplx, RSDFT_ERR_UNSUPPORTED, "complex16 SD is provided by sd_cplx");
+  if (c.mixed && !c.cplx) return sd_mixed_real(c, k, s, h_esp);
   const int nb = c.kp[k].nband;
   const int ng = (int)c.ng;
+  const size_t es = c.cplx ? sizeof(cuDoubleComplex) : sizeof(double);
   F64View v;
-  RS_TRY(f64_view(c, k, s, v, c.ws_f64));
-  RS_TRY(c.ws_hpsi.ensure(sizeof(double) * c.ng * nb));
+  RS_TRY(f64_view(c, k, s, v));
+  RS_TRY(c.ws_hpsi.ensure(sizeof(double) * nreal(c) * nb));
   double* HX = c.ws_hpsi.as<double>();
-  RS_TRY(hpsi_real<double>(c, k, s, v.x, HX, c.ng, nb));
-  RS_TRY(c.ws_dense.ensure(sizeof(double) * ((size_t)nb * nb + nb)));
+  if (c.cplx)
+    RS_TRY(hpsi_cplx<double>(c, k, s, v.x, HX, nreal(c), nb));
+  else
+    RS_TRY(hpsi_real<double>(c, k, s, v.x, HX, c.ng, nb));
+  RS_TRY(c.ws_dense.ensure(es * (size_t)nb * nb + sizeof(double) * nb));
   RS_TRY(c.ws_info.ensure(sizeof(int) * 4));
-  double* H = c.ws_dense.as<double>();
-  double* W = H + (size_t)nb * nb;
+  double* W = reinterpret_cast<double*>(c.ws_dense.as<char>() + es * (size_t)nb * nb);
   const double hdV = 0.5 * c.p.dv, zero = 0.0, one = 1.0;
-  ProfScope ps(c, "sd");
-  RS_CUBLAS(cublasDsyr2k(c.cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, nb, ng, &hdV, v.x, ng, HX, ng, &zero, H, nb));
-  int lwork = 0;
-  RS_CUSOLVER(cusolverDnDsyevd_bufferSize(c.cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb, H, nb, W,
-                                          &lwork));
-  RS_TRY(c.ws_solver.ensure(sizeof(double) * (size_t)std::max(lwork, 1)));
-  RS_CUSOLVER(cusolverDnDsyevd(c.cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb, H, nb, W,
-                               c.ws_solver.as<double>(), lwork, c.ws_info.as<int>()));
-  int info = 0;
+  const cuDoubleComplex zhdV = make_cuDoubleComplex(hdV, 0.0), zone = make_cuDoubleComplex(1.0, 0.0),
+                        zzero = make_cuDoubleComplex(0.0, 0.0);
+  ProfScope ps(c, "sd", 0.0, 2.0 * 2.0 * c.ng * (double)nb * nb * (c.cplx ? 4 : 1));
+  int lwork = 0, info = 0;
+  if (c.cplx) {
+    cuDoubleComplex* H = c.ws_dense.as<cuDoubleComplex>();
+    cuDoubleComplex* X = reinterpret_cast<cuDoubleComplex*>(v.x);
+    cuDoubleComplex* ZHX = reinterpret_cast<cuDoubleComplex*>(HX);
+    RS_CUBLAS(cublasZher2k(c.cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C, nb, ng, &zhdV, X, ng, ZHX, ng, &zero, H, nb));
+    RS_CUSOLVER(cusolverDnZheevd_bufferSize(c.cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb, H, nb, W,
+                                            &lwork));
+    RS_TRY(c.ws_solver.ensure(sizeof(cuDoubleComplex) * (size_t)std::max(lwork, 1)));
+    RS_CUSOLVER(cusolverDnZheevd(c.cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb, H, nb, W,
+                                 c.ws_solver.as<cuDoubleComplex>(), lwork, c.ws_info.as<int>()));
+  } else {
+    double* H = c.ws_dense.as<double>();
+    RS_CUBLAS(cublasDsyr2k(c.cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, nb, ng, &hdV, v.x, ng, HX, ng, &zero, H, nb));
+    RS_CUSOLVER(cusolverDnDsyevd_bufferSize(c.cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb, H, nb, W,
+                                            &lwork));
+    RS_TRY(c.ws_solver.ensure(sizeof(double) * (size_t)std::max(lwork, 1)));
+    RS_CUSOLVER(cusolverDnDsyevd(c.cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb, H, nb, W,
+                                 c.ws_solver.as<double>(), lwork, c.ws_info.as<int>()));
+  }
   RS_TRY(read_info(c, c.ws_info.as<int>(), &info));
-  RS_CHECK(info == 0, RSDFT_ERR_EIG, "subspace eigensolver failed (syevd info=%d)", info);
+  RS_CHECK(info == 0, RSDFT_ERR_EIG, "subspace eigensolver failed (syevd/heevd info=%d)", info);
   // rotation Psi <- Psi V in grid chunks (out of place per chunk, then copied back)
-  size_t ch = std::max<size_t>(1024, (size_t)(256u << 20) / (sizeof(double) * (size_t)nb));
+  size_t ch = std::max<size_t>(1024, (size_t)(256u << 20) / (es * (size_t)nb));
   ch = std::min<size_t>(ch, c.ng);
-  RS_TRY(c.ws_rot.ensure(sizeof(double) * ch * nb));
-  double* tmp = c.ws_rot.as<double>();
+  RS_TRY(c.ws_rot.ensure(es * ch * nb));
   for (size_t g0 = 0; g0 < c.ng; g0 += ch) {
     const int m = (int)std::min(ch, c.ng - g0);
-    RS_CUBLAS(cublasDgemm(c.cublas, CUBLAS_OP_N, CUBLAS_OP_N, m, nb, nb, &one, v.x + g0, ng, H, nb, &zero, tmp, m));
-    RS_CUDA(cudaMemcpy2DAsync(v.x + g0, sizeof(double) * c.ng, tmp, sizeof(double) * m, sizeof(double) * m, nb,
-                              cudaMemcpyDeviceToDevice, c.stream));
-    c.launches += 2;
+    if (c.cplx) {
+      cuDoubleComplex* X = reinterpret_cast<cuDoubleComplex*>(v.x);
+      RS_CUBLAS(cublasZgemm(c.cublas, CUBLAS_OP_N, CUBLAS_OP_N, m, nb, nb, &zone, X + g0, ng,
+                            c.ws_dense.as<cuDoubleComplex>(), nb, &zzero, c.ws_rot.as<cuDoubleComplex>(), m));
+      RS_CUDA(cudaMemcpy2DAsync(X + g0, es * c.ng, c.ws_rot.p, es * m, es * m, nb, cudaMemcpyDeviceToDevice, c.stream));
+    } else {
+      RS_CUBLAS(cublasDgemm(c.cublas, CUBLAS_OP_N, CUBLAS_OP_N, m, nb, nb, &one, v.x + g0, ng, c.ws_dense.as<double>(),
+                            nb, &zero, c.ws_rot.as<double>(), m));
+      RS_CUDA(cudaMemcpy2DAsync(v.x + g0, es * c.ng, c.ws_rot.p, es * m, es * m, nb, cudaMemcpyDeviceToDevice, c.stream));
+    }
   }
-  c.launches += 3;
   if (h_esp) {
     RS_CUDA(cudaMemcpyAsync(h_esp, W, sizeof(double) * nb, cudaMemcpyDeviceToHost, c.stream));
     RS_CUDA(cudaStreamSynchronize(c.stream));

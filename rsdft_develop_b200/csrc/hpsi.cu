@@ -7,15 +7,20 @@
 //                   Dij pairs, scatter psi(JJP) += uVk * sum Dij uVunk); the KB form
 //                   src/d_ps_nloc2_op_module.f90:146-288 is the diagonal-Dij case.
 //
-// Design (B200): one pass over psi per band.  A CTA owns an (N1 x TY) column of the
-// grid for one band and streams it along z.  Each xy-plane of the column (with a
-// Md-deep y halo, periodic rows wrapped) is staged into shared memory by the bulk-copy
-// (TMA) engine through an S-deep mbarrier ring; x taps wrap inside the staged row (the
-// CTA holds full rows), y taps read neighbouring staged rows, and z taps are applied
-// "push" style into 2*Md+1 rotating register accumulators, so no plane is read twice
-// from memory.  The finished plane gets V_loc and the nonlocal scatter (a per-point
-// CSR over the projector footprints) before one vector store.  The projector gather
-// + Dij runs before, in an atom-centred kernel.
+// Design (B200): one pass over psi per band.  A CTA owns an (N1 x TY) column of the grid for
+// one band and streams it along z.
+//  * Each xy-plane of the column (with an Md-deep y halo, periodic rows wrapped) and the
+//    matching V_loc tile are staged into shared memory by the bulk-copy (TMA) engine through an
+//    S-deep mbarrier ring issued S-1 planes ahead.
+//  * Compute warps: x taps wrap inside the staged row (the CTA holds full rows), y taps read
+//    neighbouring staged rows, z taps are pushed into 2*Md+1 rotating register accumulators,
+//    so every plane is read once from memory; all operands of a step come from shared memory.
+//  * One nonlocal warp runs ahead of the compute warps: for each plane it evaluates the
+//    projector scatter sum_a sum_p uV_a,p(r) c_b[a,p] from per-(point, atom) records and the
+//    band's coefficient row (staged once in shared memory), accumulates it into a plane
+//    buffer and hands it over through a second mbarrier ring.
+// The projector gather + Dij runs before, in an atom-centred kernel that writes the
+// coefficient rows c_b (atom-major, PG-padded).
 #include "ctx.cuh"
 #include "ptx.cuh"
 
@@ -29,14 +34,6 @@ template <typename T, int V>
 __device__ __forceinline__ void ldv(const T* p, T (&v)[V]) {
   using VT = typename VecT<T>::type;
   VT t = *reinterpret_cast<const VT*>(p);
-  const T* tt = reinterpret_cast<const T*>(&t);
-#pragma unroll
-  for (int i = 0; i < V; ++i) v[i] = tt[i];
-}
-template <typename T, int V>
-__device__ __forceinline__ void ldv_g(const T* p, T (&v)[V]) {
-  using VT = typename VecT<T>::type;
-  VT t = __ldg(reinterpret_cast<const VT*>(p));
   const T* tt = reinterpret_cast<const T*>(&t);
 #pragma unroll
   for (int i = 0; i < V; ++i) v[i] = tt[i];
@@ -56,6 +53,21 @@ __device__ __forceinline__ int pmod(int a, int n) {
   return r < 0 ? r + n : r;
 }
 
+// named barrier over the compute threads, OR-reducing a flag
+__device__ __forceinline__ bool bar_or(int flag, int nthreads) {
+  uint32_t r;
+  asm volatile(
+      "{\n .reg .pred p, q;\n setp.ne.u32 q, %1, 0;\n bar.red.or.pred p, 1, %2, q;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(r)
+      : "r"((uint32_t)flag), "r"((uint32_t)nthreads)
+      : "memory");
+  return r != 0;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 template <typename T, int MD>
 struct StArgs {
   const T* psi;
@@ -63,69 +75,131 @@ struct StArgs {
   long long ld;
   const T* vloc;
   int n1, n2, n3;
-  int tile_y, tz, stage_elems;
+  int tile_y, tz;
+  int bx, nact, nthr_c;      // threads along x; active compute threads; compute threads (x32)
+  int stage_elems, vl_elems, nl_elems;
   T c0;
   T cx[MD], cy[MD], cz[MD];
-  const int* rowptr;
-  const int* col;
-  const T* val;
-  const T* coef;
+  const int* rec_rowptr;     // per point: records [rowptr[i], rowptr[i+1])
+  const int* rec_pt;         // record -> grid point
+  const int* rec_g;          // record -> atom group
+  const T* rec_u;            // record -> uV values of the group's projectors [pg]
+  int pg;
+  const T* coef;             // c_b[g*pg + p], band stride ldc
   int ldc;
   unsigned* status;
 };
 
 constexpr uint32_t kWaitPolls = 1u << 22;
 
-template <typename T, int MD, int R, int S>
-__global__ void __launch_bounds__(256) k_stencil_real(const StArgs<T, MD> a) {
+template <typename T, int MD, int R, int S, int S2>
+__global__ void __launch_bounds__(288, 1) k_stencil_real(const StArgs<T, MD> a) {
   constexpr int V = VecT<T>::V;
   constexpr int NQ = 2 * MD + 1;
   constexpr int NCH = (MD + V - 1) / V;
   extern __shared__ __align__(128) unsigned char smem[];
-  T* stages = reinterpret_cast<T*>(smem);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + (size_t)S * a.stage_elems * sizeof(T));
-
-  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   const int n1 = a.n1, n2 = a.n2, n3 = a.n3;
-  const int x0 = threadIdx.x * V;
-  const int yl = threadIdx.y * R;
+  T* stages = reinterpret_cast<T*>(smem);
+  const int sstride = a.stage_elems + a.vl_elems;
+  T* nlbuf = stages + (size_t)S * sstride;
+  T* coef_s = nlbuf + (size_t)S2 * a.nl_elems;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(coef_s + ((a.ldc + 15) / 16) * 16);
+  uint64_t* nlfull = bar + S;
+  uint64_t* nlempty = nlfull + S2;
+
+  const int tid = threadIdx.x;
+  const int nthr_c = a.nthr_c;
+  const bool compute = tid < nthr_c;
+  const bool active = tid < a.nact;
+  const int tx = tid % a.bx, ty = tid / a.bx;
+  const int x0 = tx * V;
+  const int yl = ty * R;
   const int y0 = blockIdx.x * a.tile_y;
   const int z0 = blockIdx.y * a.tz;
   const int zend = min(z0 + a.tz, n3);
   const int rows = a.tile_y + 2 * MD;
   const int nplanes = (zend - z0) + 2 * MD;
-  const T* src = a.psi + (long long)blockIdx.z * a.ld;
-  T* dst = a.out + (long long)blockIdx.z * a.ld;
-  const T* coefb = a.coef ? a.coef + (long long)blockIdx.z * a.ldc : nullptr;
+  const int ty_valid = min(a.tile_y, n2 - y0);
+  const long long band = blockIdx.z;
+  const T* src = a.psi + band * a.ld;
+  T* dst = a.out + band * a.ld;
+  const bool nl_on = a.rec_rowptr != nullptr;
 
   if (tid == 0) {
 #pragma unroll
     for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
+#pragma unroll
+    for (int s = 0; s < S2; ++s) {
+      mbar_init(&nlfull[s], 1);
+      mbar_init(&nlempty[s], nthr_c);
+    }
     fence_mbar_init();
   }
+  if (nl_on)
+    for (int i = tid; i < a.ldc; i += blockDim.x) coef_s[i] = a.coef[band * a.ldc + i];
   __syncthreads();
 
+  if (!compute) {
+    // ---------------- nonlocal warp ----------------
+    if (!nl_on) return;
+    const int lane = tid - nthr_c;
+    const int npl = zend - z0;
+    const int npts = ty_valid * n1;
+    for (int pi = 0; pi < npl; ++pi) {
+      const int slot = pi % S2;
+      if (pi >= S2) {
+        const bool ok = mbar_wait_bounded(&nlempty[slot], (uint32_t)(((pi / S2) - 1) & 1), kWaitPolls);
+        if (!ok) {
+          if (lane == 0) atomicOr(a.status, DEV_WAIT_TIMEOUT);
+          return;
+        }
+      }
+      T* nl = nlbuf + (size_t)slot * a.nl_elems;
+      for (int e = lane; e < npts; e += 32) nl[e] = T(0);
+      __syncwarp();
+      const int p = z0 + pi;
+      const int base = (p * n2 + y0) * n1;
+      const int rs = __ldg(a.rec_rowptr + base), re = __ldg(a.rec_rowptr + base + npts);
+      for (int r = rs + lane; r < re; r += 32) {
+        const int pt = __ldg(a.rec_pt + r) - base;
+        const int g = __ldg(a.rec_g + r);
+        const T* u = a.rec_u + (size_t)r * a.pg;
+        const T* cg = coef_s + g * a.pg;
+        T v = T(0);
+        for (int q = 0; q < a.pg; ++q) v += __ldg(u + q) * cg[q];
+        atomicAdd(nl + pt, v);
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&nlfull[slot]);
+    }
+    return;
+  }
+
+  // ---------------- compute warps ----------------
   auto issue = [&](int q) {
     const int zg = pmod(z0 - MD + q, n3);
-    T* st = stages + (size_t)(q % S) * a.stage_elems;
+    T* st = stages + (size_t)(q % S) * sstride;
     uint64_t* br = &bar[q % S];
-    mbar_arrive_expect_tx(br, (uint32_t)((size_t)rows * n1 * sizeof(T)));
+    const int p = z0 - MD + q;
+    const bool inch = p >= z0 && p < zend;
+    const uint32_t bytes = (uint32_t)((size_t)rows * n1 * sizeof(T)) + (inch ? (uint32_t)((size_t)ty_valid * n1 * sizeof(T)) : 0u);
+    mbar_arrive_expect_tx(br, bytes);
     int r = 0;
     while (r < rows) {
       const int gy = pmod(y0 - MD + r, n2);
       const int len = min(rows - r, n2 - gy);
-      bulk_g2s(st + (size_t)r * n1, src + ((size_t)zg * n2 + gy) * n1,
-               (uint32_t)((size_t)len * n1 * sizeof(T)), br);
+      bulk_g2s(st + (size_t)r * n1, src + ((size_t)zg * n2 + gy) * n1, (uint32_t)((size_t)len * n1 * sizeof(T)), br);
       r += len;
     }
+    if (inch)
+      bulk_g2s(st + a.stage_elems, a.vloc + ((size_t)p * n2 + y0) * n1, (uint32_t)((size_t)ty_valid * n1 * sizeof(T)), br);
   };
-  if (tid == 0) {
+  if (tid == 0)
     for (int q = 0; q < S - 1 && q < nplanes; ++q) issue(q);
-  }
 
   bool rowok[R];
 #pragma unroll
-  for (int r = 0; r < R; ++r) rowok[r] = (y0 + yl + r) < n2;
+  for (int r = 0; r < R; ++r) rowok[r] = active && (yl + r) < ty_valid;
 
   T acc[NQ][R][V];
 #pragma unroll
@@ -135,7 +209,7 @@ __global__ void __launch_bounds__(256) k_stencil_real(const StArgs<T, MD> a) {
 #pragma unroll
       for (int i = 0; i < V; ++i) acc[q][r][i] = T(0);
 
-  int issued_upto = min(S - 1, nplanes);  // planes [0, issued_upto) issued (thread 0's view)
+  int issued_upto = min(S - 1, nplanes);
   bool aborted = false;
   for (int qb = 0; qb < nplanes && !aborted; qb += NQ) {
 #pragma unroll
@@ -148,74 +222,89 @@ __global__ void __launch_bounds__(256) k_stencil_real(const StArgs<T, MD> a) {
           issued_upto = q + S;
         }
         bool ok = mbar_wait_bounded(&bar[q % S], (uint32_t)((q / S) & 1), kWaitPolls);
-        if (__syncthreads_or(!ok)) {
-          aborted = true;
-          if (tid == 0) atomicOr(a.status, DEV_WAIT_TIMEOUT);
-          break;
-        }
-        const T* pl = stages + (size_t)(q % S) * a.stage_elems;
+        const T* pl = stages + (size_t)(q % S) * sstride;
         const int p = z0 - MD + q;
+        const bool inch = p >= z0 && p < zend;
         T v[R][V];
+        if (active) {
 #pragma unroll
-        for (int r = 0; r < R; ++r) ldv<T, V>(pl + (size_t)(yl + r + MD) * n1 + x0, v[r]);
-
-        if (p >= z0 && p < zend) {
-          T t[R][V];
-#pragma unroll
-          for (int r = 0; r < R; ++r) {
-            T vl[V];
-            if (rowok[r]) {
-              ldv_g<T, V>(a.vloc + ((size_t)p * n2 + (y0 + yl + r)) * n1 + x0, vl);
-            } else {
-#pragma unroll
-              for (int i = 0; i < V; ++i) vl[i] = T(0);
-            }
-#pragma unroll
-            for (int i = 0; i < V; ++i) t[r][i] = (a.c0 + vl[i]) * v[r][i];
-            // x taps: full periodic row is staged; chunks wrap modulo N1
-            T w[(2 * NCH + 1) * V];
-#pragma unroll
-            for (int i = 0; i < V; ++i) w[NCH * V + i] = v[r][i];
-#pragma unroll
-            for (int ch = 1; ch <= NCH; ++ch) {
-              T lf[V], rt[V];
-              ldv<T, V>(pl + (size_t)(yl + r + MD) * n1 + pmod(x0 - ch * V, n1), lf);
-              ldv<T, V>(pl + (size_t)(yl + r + MD) * n1 + pmod(x0 + ch * V, n1), rt);
-#pragma unroll
-              for (int i = 0; i < V; ++i) {
-                w[(NCH - ch) * V + i] = lf[i];
-                w[(NCH + ch) * V + i] = rt[i];
-              }
-            }
-#pragma unroll
-            for (int i = 0; i < V; ++i)
-#pragma unroll
-              for (int m = 1; m <= MD; ++m)
-                t[r][i] += a.cx[m - 1] * (w[NCH * V + i - m] + w[NCH * V + i + m]);
-          }
-          // y taps
-#pragma unroll
-          for (int dy = -MD; dy < R + MD; ++dy) {
-            T rv[V];
-            if (dy >= 0 && dy < R) {
-#pragma unroll
-              for (int i = 0; i < V; ++i) rv[i] = v[dy >= 0 && dy < R ? dy : 0][i];
-            } else {
-              ldv<T, V>(pl + (size_t)(yl + dy + MD) * n1 + x0, rv);
-            }
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-              const int m = dy > r ? dy - r : r - dy;
-              if (m >= 1 && m <= MD) {
-#pragma unroll
-                for (int i = 0; i < V; ++i) t[r][i] += a.cy[(m >= 1 ? m : 1) - 1] * rv[i];
-              }
-            }
-          }
+          for (int r = 0; r < R; ++r) ldv<T, V>(pl + (size_t)(yl + r + MD) * n1 + x0, v[r]);
+        } else {
 #pragma unroll
           for (int r = 0; r < R; ++r)
 #pragma unroll
-            for (int i = 0; i < V; ++i) acc[s][r][i] += t[r][i];
+            for (int i = 0; i < V; ++i) v[r][i] = T(0);
+        }
+        if (inch) {
+          // nonlocal plane buffer for p (filled by the nonlocal warp)
+          const int pi = p - z0;
+          const int slot = pi % S2;
+          const T* nl = nlbuf + (size_t)slot * a.nl_elems;
+          if (nl_on) ok = mbar_wait_bounded(&nlfull[slot], (uint32_t)((pi / S2) & 1), kWaitPolls) && ok;
+          if (active) {
+            T t[R][V];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+              T vl[V], nv[V];
+              if (rowok[r]) {
+                ldv<T, V>(pl + a.stage_elems + (size_t)(yl + r) * n1 + x0, vl);
+                if (nl_on) {
+                  ldv<T, V>(nl + (size_t)(yl + r) * n1 + x0, nv);
+                } else {
+#pragma unroll
+                  for (int i = 0; i < V; ++i) nv[i] = T(0);
+                }
+              } else {
+#pragma unroll
+                for (int i = 0; i < V; ++i) vl[i] = nv[i] = T(0);
+              }
+#pragma unroll
+              for (int i = 0; i < V; ++i) t[r][i] = (a.c0 + vl[i]) * v[r][i] + nv[i];
+              // x taps: the full periodic row is staged; chunks wrap modulo N1
+              T w[(2 * NCH + 1) * V];
+#pragma unroll
+              for (int i = 0; i < V; ++i) w[NCH * V + i] = v[r][i];
+#pragma unroll
+              for (int ch = 1; ch <= NCH; ++ch) {
+                T lf[V], rt[V];
+                ldv<T, V>(pl + (size_t)(yl + r + MD) * n1 + pmod(x0 - ch * V, n1), lf);
+                ldv<T, V>(pl + (size_t)(yl + r + MD) * n1 + pmod(x0 + ch * V, n1), rt);
+#pragma unroll
+                for (int i = 0; i < V; ++i) {
+                  w[(NCH - ch) * V + i] = lf[i];
+                  w[(NCH + ch) * V + i] = rt[i];
+                }
+              }
+#pragma unroll
+              for (int i = 0; i < V; ++i)
+#pragma unroll
+                for (int m = 1; m <= MD; ++m) t[r][i] += a.cx[m - 1] * (w[NCH * V + i - m] + w[NCH * V + i + m]);
+            }
+            // y taps
+#pragma unroll
+            for (int dy = -MD; dy < R + MD; ++dy) {
+              T rv[V];
+              if (dy >= 0 && dy < R) {
+#pragma unroll
+                for (int i = 0; i < V; ++i) rv[i] = v[dy >= 0 && dy < R ? dy : 0][i];
+              } else {
+                ldv<T, V>(pl + (size_t)(yl + dy + MD) * n1 + x0, rv);
+              }
+#pragma unroll
+              for (int r = 0; r < R; ++r) {
+                const int m = dy > r ? dy - r : r - dy;
+                if (m >= 1 && m <= MD) {
+#pragma unroll
+                  for (int i = 0; i < V; ++i) t[r][i] += a.cy[(m >= 1 ? m : 1) - 1] * rv[i];
+                }
+              }
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+#pragma unroll
+              for (int i = 0; i < V; ++i) acc[s][r][i] += t[r][i];
+          }
+          if (nl_on) mbar_arrive(&nlempty[slot]);
         }
         // z taps, pushed into the accumulators of planes p-m and p+m
 #pragma unroll
@@ -230,8 +319,6 @@ __global__ void __launch_bounds__(256) k_stencil_real(const StArgs<T, MD> a) {
         }
         // plane p - MD is complete
         {
-          constexpr int fs_dummy = 0;
-          (void)fs_dummy;
           const int zo = p - MD;
           const int fs = (s + NQ - MD) % NQ;
           if (zo >= z0 && zo < zend) {
@@ -241,18 +328,7 @@ __global__ void __launch_bounds__(256) k_stencil_real(const StArgs<T, MD> a) {
                 T o[V];
 #pragma unroll
                 for (int i = 0; i < V; ++i) o[i] = acc[fs][r][i];
-                const size_t g = ((size_t)zo * n2 + (y0 + yl + r)) * n1 + x0;
-                if (a.rowptr) {
-                  const int e0 = __ldg(a.rowptr + g), eV = __ldg(a.rowptr + g + V);
-                  if (e0 != eV) {
-#pragma unroll
-                    for (int i = 0; i < V; ++i) {
-                      const int ea = __ldg(a.rowptr + g + i), eb = __ldg(a.rowptr + g + i + 1);
-                      for (int e = ea; e < eb; ++e) o[i] += __ldg(a.val + e) * __ldg(coefb + __ldg(a.col + e));
-                    }
-                  }
-                }
-                stv<T, V>(dst + g, o);
+                stv<T, V>(dst + ((size_t)zo * n2 + (y0 + yl + r)) * n1 + x0, o);
               }
             }
           }
@@ -261,7 +337,11 @@ __global__ void __launch_bounds__(256) k_stencil_real(const StArgs<T, MD> a) {
 #pragma unroll
             for (int i = 0; i < V; ++i) acc[fs][r][i] = T(0);
         }
-        __syncthreads();
+        if (bar_or(!ok, nthr_c)) {
+          aborted = true;
+          if (tid == 0) atomicOr(a.status, DEV_WAIT_TIMEOUT);
+          break;
+        }
       }
     }
   }
@@ -272,14 +352,14 @@ __global__ void __launch_bounds__(256) k_stencil_real(const StArgs<T, MD> a) {
 }
 
 // ---------------------------------------------------------------------------
-// nonlocal gather + Dij (atom-centred): coef[b][lma] = sum_q D[lma][q] dV sum_j uV(j,q) psi_b(JJ(j))
+// nonlocal gather + Dij (atom-centred):
+//   c_b[g*PG + p] = sum_q D_g[p][q] dV sum_j uV_g(j,q) psi_b(JJ_g(j))
 // ---------------------------------------------------------------------------
 template <typename T, int PG, int BB>
 __global__ void __launch_bounds__(256) k_nl_gather_real(const T* __restrict__ psi, long long ld, int nb,
                                                         const int* __restrict__ gofs, const int* __restrict__ gjj,
-                                                        const T* __restrict__ gw, const int* __restrict__ gplist,
-                                                        const double* __restrict__ gD, double dV, T* coef,
-                                                        int ldc) {
+                                                        const T* __restrict__ gw, const double* __restrict__ gD,
+                                                        double dV, T* coef, int ldc) {
   const int g = blockIdx.x;
   const int b0 = blockIdx.y * BB;
   const int f0 = gofs[g], f1 = gofs[g + 1];
@@ -324,12 +404,11 @@ __global__ void __launch_bounds__(256) k_nl_gather_real(const T* __restrict__ ps
   __syncthreads();
   if (threadIdx.x < BB * PG) {
     const int bb = threadIdx.x / PG, p = threadIdx.x % PG;
-    const int lma = gplist[g * PG + p];
-    if (lma >= 0 && b0 + bb < nb) {
+    if (b0 + bb < nb) {
       double cfs = 0.0;
 #pragma unroll
       for (int q = 0; q < PG; ++q) cfs += gD[((size_t)g * PG + p) * PG + q] * u[bb * PG + q];
-      coef[(long long)(b0 + bb) * ldc + lma] = (T)cfs;
+      coef[(long long)(b0 + bb) * ldc + g * PG + p] = (T)cfs;
     }
   }
 }
@@ -341,9 +420,8 @@ template <typename T, int PG, int BB>
 static void launch_gather(Ctx& c, const T* psi, size_t ld, int nb, T* coef, const T* gw) {
   NonlocalTables& nl = c.nl;
   dim3 grid(nl.ngroups, (nb + BB - 1) / BB);
-  k_nl_gather_real<T, PG, BB><<<grid, 256, 0, c.stream>>>(psi, (long long)ld, nb, nl.gofs.as<int>(),
-                                                           nl.gjj.as<int>(), gw, nl.gplist.as<int>(),
-                                                           nl.gD.as<double>(), c.p.dv, coef, nl.nproj);
+  k_nl_gather_real<T, PG, BB><<<grid, 256, 0, c.stream>>>(psi, (long long)ld, nb, nl.gofs.as<int>(), nl.gjj.as<int>(),
+                                                           gw, nl.gD.as<double>(), c.p.dv, coef, nl.ngroups * PG);
   c.launches++;
 }
 
@@ -351,7 +429,8 @@ template <typename T>
 static int nl_gather(Ctx& c, int k, const T* psi, size_t ld, int nb, T* coef) {
   NonlocalTables& nl = c.nl;
   const T* gw = std::is_same<T, double>::value ? nl.perk[k].gw64.as<T>() : nl.perk[k].gw32.as<T>();
-  ProfScope ps(c, "nl_gather");
+  const double bytes = (double)sizeof(T) * nl.ftotal * ((double)nb + nl.pg) + 4.0 * nl.ftotal;
+  ProfScope ps(c, "nl_gather", bytes);
   switch (nl.pg) {
     case 1: launch_gather<T, 1, 8>(c, psi, ld, nb, coef, gw); break;
     case 4: launch_gather<T, 4, 8>(c, psi, ld, nb, coef, gw); break;
@@ -366,7 +445,8 @@ template <typename T, int MD>
 static int launch_stencil(Ctx& c, int k, int s, const T* psi, T* out, size_t ld, int nb, const T* coef) {
   constexpr int V = VecT<T>::V;
   constexpr int R = 2;
-  constexpr int S = 4;
+  constexpr int S = sizeof(T) == 4 ? 6 : 5;
+  constexpr int S2 = 3;
   const int n1 = c.p.n1, n2 = c.p.n2, n3 = c.p.n3;
   RS_CHECK(n1 % V == 0 && n1 / V <= 256, RSDFT_ERR_UNSUPPORTED, "N1=%d must be a multiple of %d (<= %d)", n1, V,
            256 * V);
@@ -374,14 +454,19 @@ static int launch_stencil(Ctx& c, int k, int s, const T* psi, T* out, size_t ld,
   const int bx = n1 / V;
   int by = std::max(1, 256 / bx);
   by = std::min(by, (n2 + R - 1) / R);
+  const int nthr_c = ((bx * by + 31) / 32) * 32;
   const int tile_y = by * R;
   const int rows = tile_y + 2 * MD;
   const int align_el = 128 / (int)sizeof(T);
-  const int stage_elems = ((rows * n1 + align_el - 1) / align_el) * align_el;
-  const size_t smem = (size_t)S * stage_elems * sizeof(T) + S * sizeof(uint64_t);
-  RS_CHECK(smem <= 220 * 1024, RSDFT_ERR_UNSUPPORTED, "stencil stage (%zu B) exceeds shared memory", smem);
+  auto rnd = [&](int e) { return ((e + align_el - 1) / align_el) * align_el; };
+  const int stage_elems = rnd(rows * n1), vl_elems = rnd(tile_y * n1), nl_elems = rnd(tile_y * n1);
+  const bool nl_on = c.nl.nproj > 0 && coef != nullptr;
+  const int ldc = nl_on ? c.nl.ngroups * c.nl.pg : 0;
+  const size_t smem = sizeof(T) * ((size_t)S * (stage_elems + vl_elems) + (size_t)S2 * nl_elems +
+                                   (size_t)((ldc + 15) / 16) * 16) +
+                      (S + 2 * S2) * sizeof(uint64_t);
+  RS_CHECK(smem <= 225 * 1024, RSDFT_ERR_UNSUPPORTED, "stencil stages (%zu B) exceed shared memory", smem);
   const int ytiles = (n2 + tile_y - 1) / tile_y;
-  // z chunks: enough CTAs to fill the machine several times
   int zch = 1;
   while ((long long)ytiles * zch * nb < 4 * 148 && n3 / (zch * 2) >= 16) zch *= 2;
   const int tz = (n3 + zch - 1) / zch;
@@ -393,31 +478,33 @@ static int launch_stencil(Ctx& c, int k, int s, const T* psi, T* out, size_t ld,
   a.ld = (long long)ld;
   a.vloc = (std::is_same<T, double>::value ? c.vloc64.as<T>() : c.vloc32.as<T>()) + (size_t)s * c.ng;
   a.n1 = n1; a.n2 = n2; a.n3 = n3;
-  a.tile_y = tile_y; a.tz = tz; a.stage_elems = stage_elems;
+  a.tile_y = tile_y; a.tz = tz;
+  a.bx = bx; a.nact = bx * by; a.nthr_c = nthr_c;
+  a.stage_elems = stage_elems; a.vl_elems = vl_elems; a.nl_elems = nl_elems;
   a.c0 = (T)(c.p.coef_lap0 + c.kp[k].const_k2);
   for (int m = 0; m < MD; ++m) {
     a.cx[m] = (T)c.p.coef_lap[0][m];
     a.cy[m] = (T)c.p.coef_lap[1][m];
     a.cz[m] = (T)c.p.coef_lap[2][m];
   }
-  const bool nl_on = c.nl.nproj > 0 && coef != nullptr;
-  a.rowptr = nl_on ? c.nl.rowptr.as<int>() : nullptr;
-  a.col = nl_on ? c.nl.col.as<int>() : nullptr;
-  a.val = nl_on ? (std::is_same<T, double>::value ? c.nl.perk[k].val64.as<T>() : c.nl.perk[k].val32.as<T>())
-                : nullptr;
+  a.rec_rowptr = nl_on ? c.nl.rec_rowptr.as<int>() : nullptr;
+  a.rec_pt = nl_on ? c.nl.rec_pt.as<int>() : nullptr;
+  a.rec_g = nl_on ? c.nl.rec_g.as<int>() : nullptr;
+  a.rec_u = nl_on ? (std::is_same<T, double>::value ? c.nl.perk[k].ru64.as<T>() : c.nl.perk[k].ru32.as<T>()) : nullptr;
+  a.pg = c.nl.pg;
   a.coef = coef;
-  a.ldc = c.nl.nproj;
+  a.ldc = ldc;
   a.status = c.d_status;
-  auto kern = k_stencil_real<T, MD, R, S>;
+  auto kern = k_stencil_real<T, MD, R, S, S2>;
   static bool attr_done = false;  // one per template instantiation
   if (!attr_done) {
-    RS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+    RS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 225 * 1024));
     attr_done = true;
   }
-  dim3 grid(ytiles, zch, nb), block(bx, by);
-  // algorithmic bytes: read psi + write H psi per band, V_loc and the scatter tables once
+  dim3 grid(ytiles, zch, nb), block(nthr_c + 32);
+  // algorithmic bytes: read psi + write H psi per band, V_loc and the projector records once
   const double alg_bytes = (double)sizeof(T) * (2.0 * (double)c.ng * nb + (double)c.ng) +
-                           (nl_on ? 4.0 * (double)(c.ng + 1) + (4.0 + sizeof(T)) * c.nl.nnz : 0.0);
+                           (nl_on ? 4.0 * (double)(c.ng + 1) + (8.0 + sizeof(T) * c.nl.pg) * c.nl.ftotal : 0.0);
   ProfScope ps(c, "hpsi_stencil", alg_bytes);
   kern<<<grid, block, smem, c.stream>>>(a);
   c.launches++;
@@ -433,7 +520,7 @@ int hpsi_real(Ctx& c, int k, int s, const T* psi, T* out, size_t ld, int nb) {
   T* coef = nullptr;
   if (c.nl.nproj > 0) {
     RS_TRY(nl_prepare_k(c, k));
-    RS_TRY(c.ws_coef.ensure((size_t)nb * c.nl.nproj * sizeof(T)));
+    RS_TRY(c.ws_coef.ensure((size_t)nb * c.nl.ngroups * c.nl.pg * sizeof(T)));
     coef = c.ws_coef.as<T>();
     RS_TRY(nl_gather<T>(c, k, psi, ld, nb, coef));
   }
