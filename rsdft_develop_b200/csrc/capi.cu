@@ -263,6 +263,7 @@ static void destroy(Ctx* c) {
   for (auto& w : c->wf) w.psi.release();
   if (c->d_status) cudaFree(c->d_status);
   if (c->cublas) cublasDestroy(c->cublas);
+  if (c->syevj) cusolverDnDestroySyevjInfo(c->syevj);
   if (c->cusolver) cusolverDnDestroy(c->cusolver);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -340,6 +341,10 @@ int rsdft_gpu_init(const rsdft_gpu_params* p) {
   c->p = *p;
   c->ng = (size_t)p->n1 * p->n2 * p->n3;
   c->cplx = p->is_complex != 0;
+  {
+    const char* e = getenv("RSDFT_EIG");
+    c->eig_jacobi = e && std::strcmp(e, "syevj") == 0;
+  }
   c->mixed = p->precision == RSDFT_PREC_MIXED;
   if (c->p.ncg <= 0) c->p.ncg = 3;
   if (c->p.mloop <= 0) c->p.mloop = 3;

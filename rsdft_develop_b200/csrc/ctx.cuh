@@ -67,6 +67,8 @@ struct Ctx {
   unsigned* d_status = nullptr;
   long long launches = 0;
   int mb_ref = 0;  // bands 1..mb_ref judged for convergence (0: all)
+  bool eig_jacobi = false;          // subspace eigensolver: Jacobi (syevj) instead of syevd
+  syevjInfo_t syevj = nullptr;
 
   std::vector<KPoint> kp;
   DBuf vloc64, vloc32;             // [nspin][ng]

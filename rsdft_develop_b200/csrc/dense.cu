@@ -88,6 +88,51 @@ __global__ void k_identity(double* I, int n) {
     I[t] = (t % n) == (t / n) ? 1.0 : 0.0;
 }
 
+// Eigen-decomposition of the nb x nb Hermitian matrix in H (upper triangle, column-major):
+// eigenvalues ascending into W, eigenvectors overwrite H.  FP64 cuSOLVER: divide and conquer
+// (syevd/heevd, the reference's dsyev/zheevd role) or Jacobi (syevj/heevj), chosen at init.
+static int eig_solve(Ctx& c, int nb, void* H, double* W) {
+  ProfScope ps(c, "sd_eig");
+  int lwork = 0, info = 0;
+  RS_TRY(c.ws_info.ensure(sizeof(int) * 4));
+  if (c.eig_jacobi) {
+    if (!c.syevj) {
+      RS_CUSOLVER(cusolverDnCreateSyevjInfo(&c.syevj));
+      RS_CUSOLVER(cusolverDnXsyevjSetTolerance(c.syevj, 1.0e-15));
+      RS_CUSOLVER(cusolverDnXsyevjSetMaxSweeps(c.syevj, 30));
+    }
+    if (c.cplx) {
+      RS_CUSOLVER(cusolverDnZheevj_bufferSize(c.cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb,
+                                              (cuDoubleComplex*)H, nb, W, &lwork, c.syevj));
+      RS_TRY(c.ws_solver.ensure(sizeof(cuDoubleComplex) * (size_t)std::max(lwork, 1)));
+      RS_CUSOLVER(cusolverDnZheevj(c.cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb,
+                                   (cuDoubleComplex*)H, nb, W, c.ws_solver.as<cuDoubleComplex>(), lwork,
+                                   c.ws_info.as<int>(), c.syevj));
+    } else {
+      RS_CUSOLVER(cusolverDnDsyevj_bufferSize(c.cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb,
+                                              (double*)H, nb, W, &lwork, c.syevj));
+      RS_TRY(c.ws_solver.ensure(sizeof(double) * (size_t)std::max(lwork, 1)));
+      RS_CUSOLVER(cusolverDnDsyevj(c.cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb, (double*)H, nb, W,
+                                   c.ws_solver.as<double>(), lwork, c.ws_info.as<int>(), c.syevj));
+    }
+  } else if (c.cplx) {
+    RS_CUSOLVER(cusolverDnZheevd_bufferSize(c.cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb,
+                                            (cuDoubleComplex*)H, nb, W, &lwork));
+    RS_TRY(c.ws_solver.ensure(sizeof(cuDoubleComplex) * (size_t)std::max(lwork, 1)));
+    RS_CUSOLVER(cusolverDnZheevd(c.cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb, (cuDoubleComplex*)H,
+                                 nb, W, c.ws_solver.as<cuDoubleComplex>(), lwork, c.ws_info.as<int>()));
+  } else {
+    RS_CUSOLVER(cusolverDnDsyevd_bufferSize(c.cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb, (double*)H,
+                                            nb, W, &lwork));
+    RS_TRY(c.ws_solver.ensure(sizeof(double) * (size_t)std::max(lwork, 1)));
+    RS_CUSOLVER(cusolverDnDsyevd(c.cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb, (double*)H, nb, W,
+                                 c.ws_solver.as<double>(), lwork, c.ws_info.as<int>()));
+  }
+  RS_TRY(read_info(c, c.ws_info.as<int>(), &info));
+  RS_CHECK(info == 0, RSDFT_ERR_EIG, "subspace eigensolver failed (info=%d)", info);
+  return 0;
+}
+
 static int gs_mixed_real(Ctx& c, int k, int s, int passes) {
   const int nb = c.kp[k].nband;
   float* X = c.wfn(k, s).psi.as<float>();
@@ -134,19 +179,9 @@ static int sd_mixed_real(Ctx& c, int k, int s, double* h_esp) {
   RS_CUDA(cudaMemsetAsync(H, 0, sizeof(double) * (size_t)nb * nb, c.stream));
   // H[m][n] = dV sum_g X[m][g] (HX)[n][g]; Hsub = (H + H^T)/2 = 1/2 dV (X^T HX + HX^T X)
   RS_TRY(gemm_tn_x3(c, X, (long long)c.ng, nb, HX, (long long)c.ng, nb, (long long)c.ng, c.p.dv, H, nb, 0));
-  {
-    ProfScope ps(c, "sd");
-    k_symmetrize<<<64, 256, 0, c.stream>>>(H, nb);
-    c.launches++;
-    int lwork = 0, info = 0;
-    RS_CUSOLVER(cusolverDnDsyevd_bufferSize(c.cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb, H, nb, W,
-                                            &lwork));
-    RS_TRY(c.ws_solver.ensure(sizeof(double) * (size_t)std::max(lwork, 1)));
-    RS_CUSOLVER(cusolverDnDsyevd(c.cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb, H, nb, W,
-                                 c.ws_solver.as<double>(), lwork, c.ws_info.as<int>()));
-    RS_TRY(read_info(c, c.ws_info.as<int>(), &info));
-    RS_CHECK(info == 0, RSDFT_ERR_EIG, "subspace eigensolver failed (syevd info=%d)", info);
-  }
+  k_symmetrize<<<64, 256, 0, c.stream>>>(H, nb);
+  c.launches++;
+  RS_TRY(eig_solve(c, nb, H, W));
   RS_TRY(gemm_rotate_x3(c, X, (long long)c.ng, nb, (long long)c.ng, H, nb));
   if (h_esp) {
     RS_CUDA(cudaMemcpyAsync(h_esp, W, sizeof(double) * nb, cudaMemcpyDeviceToHost, c.stream));
@@ -220,29 +255,18 @@ int sd_run(Ctx& c, int k, int s, double* h_esp) {
   const double hdV = 0.5 * c.p.dv, zero = 0.0, one = 1.0;
   const cuDoubleComplex zhdV = make_cuDoubleComplex(hdV, 0.0), zone = make_cuDoubleComplex(1.0, 0.0),
                         zzero = make_cuDoubleComplex(0.0, 0.0);
-  ProfScope ps(c, "sd", 0.0, 2.0 * 2.0 * c.ng * (double)nb * nb * (c.cplx ? 4 : 1));
-  int lwork = 0, info = 0;
-  if (c.cplx) {
-    cuDoubleComplex* H = c.ws_dense.as<cuDoubleComplex>();
-    cuDoubleComplex* X = reinterpret_cast<cuDoubleComplex*>(v.x);
-    cuDoubleComplex* ZHX = reinterpret_cast<cuDoubleComplex*>(HX);
-    RS_CUBLAS(cublasZher2k(c.cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C, nb, ng, &zhdV, X, ng, ZHX, ng, &zero, H, nb));
-    RS_CUSOLVER(cusolverDnZheevd_bufferSize(c.cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb, H, nb, W,
-                                            &lwork));
-    RS_TRY(c.ws_solver.ensure(sizeof(cuDoubleComplex) * (size_t)std::max(lwork, 1)));
-    RS_CUSOLVER(cusolverDnZheevd(c.cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb, H, nb, W,
-                                 c.ws_solver.as<cuDoubleComplex>(), lwork, c.ws_info.as<int>()));
-  } else {
-    double* H = c.ws_dense.as<double>();
-    RS_CUBLAS(cublasDsyr2k(c.cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, nb, ng, &hdV, v.x, ng, HX, ng, &zero, H, nb));
-    RS_CUSOLVER(cusolverDnDsyevd_bufferSize(c.cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb, H, nb, W,
-                                            &lwork));
-    RS_TRY(c.ws_solver.ensure(sizeof(double) * (size_t)std::max(lwork, 1)));
-    RS_CUSOLVER(cusolverDnDsyevd(c.cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb, H, nb, W,
-                                 c.ws_solver.as<double>(), lwork, c.ws_info.as<int>()));
+  {
+    ProfScope ps(c, "sd_gemm", 0.0, 2.0 * c.ng * (double)nb * nb * (c.cplx ? 4 : 1));
+    if (c.cplx)
+      RS_CUBLAS(cublasZher2k(c.cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C, nb, ng, &zhdV,
+                             reinterpret_cast<cuDoubleComplex*>(v.x), ng, reinterpret_cast<cuDoubleComplex*>(HX), ng,
+                             &zero, c.ws_dense.as<cuDoubleComplex>(), nb));
+    else
+      RS_CUBLAS(cublasDsyr2k(c.cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, nb, ng, &hdV, v.x, ng, HX, ng, &zero,
+                             c.ws_dense.as<double>(), nb));
   }
-  RS_TRY(read_info(c, c.ws_info.as<int>(), &info));
-  RS_CHECK(info == 0, RSDFT_ERR_EIG, "subspace eigensolver failed (syevd/heevd info=%d)", info);
+  RS_TRY(eig_solve(c, nb, c.ws_dense.p, W));
+  ProfScope ps(c, "sd_rot", 0.0, 2.0 * c.ng * (double)nb * nb * (c.cplx ? 4 : 1));
   // rotation Psi <- Psi V in grid chunks (out of place per chunk, then copied back)
   size_t ch = std::max<size_t>(1024, (size_t)(256u << 20) / (es * (size_t)nb));
   ch = std::min<size_t>(ch, c.ng);

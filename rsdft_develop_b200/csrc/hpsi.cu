@@ -15,10 +15,11 @@
 //  * Compute warps: x taps wrap inside the staged row (the CTA holds full rows), y taps read
 //    neighbouring staged rows, z taps are pushed into 2*Md+1 rotating register accumulators,
 //    so every plane is read once from memory; all operands of a step come from shared memory.
-//  * One nonlocal warp runs ahead of the compute warps: for each plane it evaluates the
-//    projector scatter sum_a sum_p uV_a,p(r) c_b[a,p] from per-(point, atom) records and the
-//    band's coefficient row (staged once in shared memory), accumulates it into a plane
-//    buffer and hands it over through a second mbarrier ring.
+//  * Four nonlocal warps run ahead of the compute warps: for each plane they evaluate the
+//    projector scatter sum_a sum_p uV_a,p(r) c_b[a,p] from per-(point, atom) records (loads
+//    batched several records deep per thread) and the band's coefficient row (staged once in
+//    shared memory), accumulate it into a plane buffer and hand it over through a second
+//    mbarrier ring.
 // The projector gather + Dij runs before, in an atom-centred kernel that writes the
 // coefficient rows c_b (atom-major, PG-padded).
 #include "ctx.cuh"
@@ -91,9 +92,11 @@ struct StArgs {
 };
 
 constexpr uint32_t kWaitPolls = 1u << 22;
+constexpr int kNLW = 4;  // nonlocal warps per CTA
+constexpr int kRB = 4;   // records in flight per nonlocal thread
 
 template <typename T, int MD, int R, int S, int S2>
-__global__ void __launch_bounds__(288, 1) k_stencil_real(const StArgs<T, MD> a) {
+__global__ void __launch_bounds__(256 + 32 * kNLW, 1) k_stencil_real(const StArgs<T, MD> a) {
   constexpr int V = VecT<T>::V;
   constexpr int NQ = 2 * MD + 1;
   constexpr int NCH = (MD + V - 1) / V;
@@ -130,7 +133,7 @@ __global__ void __launch_bounds__(288, 1) k_stencil_real(const StArgs<T, MD> a) 
     for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
 #pragma unroll
     for (int s = 0; s < S2; ++s) {
-      mbar_init(&nlfull[s], 1);
+      mbar_init(&nlfull[s], kNLW);
       mbar_init(&nlempty[s], nthr_c);
     }
     fence_mbar_init();
@@ -140,9 +143,9 @@ __global__ void __launch_bounds__(288, 1) k_stencil_real(const StArgs<T, MD> a) 
   __syncthreads();
 
   if (!compute) {
-    // ---------------- nonlocal warp ----------------
+    // ---------------- nonlocal warps (kNLW of them) ----------------
     if (!nl_on) return;
-    const int lane = tid - nthr_c;
+    const int lt = tid - nthr_c;  // 0 .. 32*kNLW-1
     const int npl = zend - z0;
     const int npts = ty_valid * n1;
     for (int pi = 0; pi < npl; ++pi) {
@@ -150,27 +153,46 @@ __global__ void __launch_bounds__(288, 1) k_stencil_real(const StArgs<T, MD> a) 
       if (pi >= S2) {
         const bool ok = mbar_wait_bounded(&nlempty[slot], (uint32_t)(((pi / S2) - 1) & 1), kWaitPolls);
         if (!ok) {
-          if (lane == 0) atomicOr(a.status, DEV_WAIT_TIMEOUT);
+          atomicOr(a.status, DEV_WAIT_TIMEOUT);
           return;
         }
       }
       T* nl = nlbuf + (size_t)slot * a.nl_elems;
-      for (int e = lane; e < npts; e += 32) nl[e] = T(0);
-      __syncwarp();
+      for (int e = lt; e < npts; e += 32 * kNLW) nl[e] = T(0);
+      asm volatile("bar.sync 2, %0;" ::"r"(32 * kNLW) : "memory");
       const int p = z0 + pi;
       const int base = (p * n2 + y0) * n1;
       const int rs = __ldg(a.rec_rowptr + base), re = __ldg(a.rec_rowptr + base + npts);
-      for (int r = rs + lane; r < re; r += 32) {
-        const int pt = __ldg(a.rec_pt + r) - base;
-        const int g = __ldg(a.rec_g + r);
-        const T* u = a.rec_u + (size_t)r * a.pg;
-        const T* cg = coef_s + g * a.pg;
-        T v = T(0);
-        for (int q = 0; q < a.pg; ++q) v += __ldg(u + q) * cg[q];
-        atomicAdd(nl + pt, v);
+      // batches of kRB records per thread, all loads issued before use
+      for (int r0 = rs; r0 < re; r0 += 32 * kNLW * kRB) {
+        int pt[kRB], gg[kRB];
+        T u[kRB][4];
+#pragma unroll
+        for (int j = 0; j < kRB; ++j) {
+          const int r = r0 + j * 32 * kNLW + lt;
+          pt[j] = -1;
+          if (r < re) {
+            pt[j] = __ldg(a.rec_pt + r) - base;
+            gg[j] = __ldg(a.rec_g + r);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) u[j][q] = q < a.pg ? __ldg(a.rec_u + (size_t)r * a.pg + q) : T(0);
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < kRB; ++j) {
+          if (pt[j] >= 0) {
+            const T* cg = coef_s + gg[j] * a.pg;
+            T v = T(0);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) v += q < a.pg ? u[j][q] * cg[q] : T(0);
+            const int r = r0 + j * 32 * kNLW + lt;
+            for (int q = 4; q < a.pg; ++q) v += __ldg(a.rec_u + (size_t)r * a.pg + q) * cg[q];
+            atomicAdd(nl + pt[j], v);
+          }
+        }
       }
       __syncwarp();
-      if (lane == 0) mbar_arrive(&nlfull[slot]);
+      if ((lt & 31) == 0) mbar_arrive(&nlfull[slot]);
     }
     return;
   }
@@ -501,7 +523,7 @@ static int launch_stencil(Ctx& c, int k, int s, const T* psi, T* out, size_t ld,
     RS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 225 * 1024));
     attr_done = true;
   }
-  dim3 grid(ytiles, zch, nb), block(nthr_c + 32);
+  dim3 grid(ytiles, zch, nb), block(nthr_c + 32 * kNLW);
   // algorithmic bytes: read psi + write H psi per band, V_loc and the projector records once
   const double alg_bytes = (double)sizeof(T) * (2.0 * (double)c.ng * nb + (double)c.ng) +
                            (nl_on ? 4.0 * (double)(c.ng + 1) + (8.0 + sizeof(T) * c.nl.pg) * c.nl.ftotal : 0.0);
