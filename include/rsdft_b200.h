@@ -144,6 +144,48 @@ int rsdft_gpu_sweep(int nsweep, double tol, int* iters, double* esp, double* res
  * (src/sweep_module.f90:46-60,267-278; src/band_module.f90:207; src/dos_module.f90:64-75). */
 int rsdft_gpu_init_sweep(int mb_ref);
 
+/* ---- learned preconditioner (no counterpart in the reference) ----
+ * A 4-layer 3-D convolutional network, channels 1-16-16-16-1, 3x3x3 kernels, no biases, tanh
+ * between layers, BF16 weights with FP32 accumulation.  With pc_mode RSDFT_PC_LEARNED and
+ * RSDFT_PREC_MIXED it replaces precond_hprsdft (src/conjugate_gradient/cgpc_hprsdft_module.f90:
+ * 133-270) in conjugate_gradient: Pg = rms(g) f(g / rms(g)) per band.  Until weights are
+ * loaded or trained, and in other builds, precond_hprsdft runs instead; rsdft_gpu_sweep also
+ * falls back to it for good when the FP64 residual stalls for 3 sweeps.
+ * Weights are RSDFT_LPC_NWEIGHTS FP32 values, layer by layer, each [cout][cin][kz][ky][kx]. */
+#define RSDFT_LPC_NWEIGHTS 14688
+/* Random initial weights (normal, variance 1/(27 cin)). */
+int rsdft_gpu_lpc_init(unsigned long long seed);
+int rsdft_gpu_lpc_set_weights(const float* w, int n);
+int rsdft_gpu_lpc_get_weights(float* w, int n);
+/* Network output y = f(x) for nb fields of n1 x n2 x n3 (x fastest); periodic (1) or zero (0)
+ * padding; no input scaling. */
+int rsdft_gpu_lpc_forward(const float* x, float* y, int nb, int n1, int n2, int n3, int periodic,
+                          int mem);
+/* Mean squared error over the interior (margin points in from every face) of nb zero-padded
+ * n^3 patches, and its gradient with respect to the FP32 weights (grad: RSDFT_LPC_NWEIGHTS
+ * values, host).  loss/grad may be NULL. */
+int rsdft_gpu_lpc_loss_grad(const float* x, const float* t, int nb, int n, int margin,
+                            double* loss, float* grad, int mem);
+/* Empty device training set for `capacity` pairs of patch^3 points. */
+int rsdft_gpu_lpc_dataset(int capacity, int patch);
+/* Append up to npatch pairs cut (periodic, random corners, random bands) from the resident
+ * bands of (k, s): input = the CG gradient -2(H psi - E psi) scaled to unit RMS; target =
+ * sigma (T + sigma)^-1 of it, T the finite-difference kinetic operator, by `iters` CG steps.
+ * added receives the pairs stored. */
+int rsdft_gpu_lpc_harvest(int k, int s, int npatch, double sigma, int iters,
+                          unsigned long long seed, int* added);
+/* Host copy of harvested pairs [first, first+count); x or t may be NULL. */
+int rsdft_gpu_lpc_dataset_get(int first, int count, float* x, float* t);
+/* Adam training on the harvested set (MSE on the patch interior); losses[epoch] (host, may be
+ * NULL) receives the mean batch loss of each epoch. */
+int rsdft_gpu_lpc_train(int margin, int epochs, int batch, double lr, unsigned long long seed,
+                        double* losses);
+/* The preconditioner on full periodic FP32 bands of the context grid: pg = rms(g) f(g/rms(g)). */
+int rsdft_gpu_lpc_precond_f(const float* g, float* pg, int nb, int mem);
+/* ready: weights loaded; pc_in_use: the PC mode CG uses now; fallbacks: learned-to-plain
+ * switches so far; dataset: harvested pairs.  Any output may be NULL. */
+int rsdft_gpu_lpc_status(int* ready, int* pc_in_use, int* fallbacks, int* dataset);
+
 /* ---- measurement ---- */
 /* Per-kernel CUDA-event timing of the library's own launches (off by default). */
 int rsdft_gpu_profile(int on);

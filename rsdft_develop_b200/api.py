@@ -52,7 +52,11 @@ EXPORTS = [
     "rsdft_gpu_conjugate_gradient", "rsdft_gpu_gram_schmidt", "rsdft_gpu_subspace_diag",
     "rsdft_gpu_residual", "rsdft_gpu_precond_d", "rsdft_gpu_sweep", "rsdft_gpu_profile",
     "rsdft_gpu_profile_get", "rsdft_gpu_kernel_launches", "rsdft_gpu_selftest_gemm", "rsdft_gpu_init_sweep",
+    "rsdft_gpu_lpc_init", "rsdft_gpu_lpc_set_weights", "rsdft_gpu_lpc_get_weights", "rsdft_gpu_lpc_forward",
+    "rsdft_gpu_lpc_loss_grad", "rsdft_gpu_lpc_dataset", "rsdft_gpu_lpc_harvest", "rsdft_gpu_lpc_dataset_get",
+    "rsdft_gpu_lpc_train", "rsdft_gpu_lpc_precond_f", "rsdft_gpu_lpc_status",
 ]
+LPC_NWEIGHTS = 14688
 
 
 class RsdftError(RuntimeError):
@@ -103,6 +107,15 @@ def load_library(path: str = LIB_PATH):
         "rsdft_gpu_sweep": [i, d, C.POINTER(C.c_int), vp, vp],
         "rsdft_gpu_selftest_gemm": [i, i, C.c_longlong, i, C.POINTER(C.c_double)],
         "rsdft_gpu_init_sweep": [i],
+        "rsdft_gpu_lpc_init": [C.c_ulonglong], "rsdft_gpu_lpc_set_weights": [vp, i],
+        "rsdft_gpu_lpc_get_weights": [vp, i], "rsdft_gpu_lpc_forward": [vp, vp, i, i, i, i, i, i],
+        "rsdft_gpu_lpc_loss_grad": [vp, vp, i, i, i, C.POINTER(C.c_double), vp, i],
+        "rsdft_gpu_lpc_dataset": [i, i],
+        "rsdft_gpu_lpc_harvest": [i, i, i, d, i, C.c_ulonglong, C.POINTER(C.c_int)],
+        "rsdft_gpu_lpc_dataset_get": [i, i, vp, vp],
+        "rsdft_gpu_lpc_train": [i, i, i, d, C.c_ulonglong, vp],
+        "rsdft_gpu_lpc_precond_f": [vp, vp, i, i],
+        "rsdft_gpu_lpc_status": [C.POINTER(C.c_int)] * 4,
         "rsdft_gpu_profile": [i], "rsdft_gpu_profile_get": [C.c_char_p, C.POINTER(C.c_double),
                                                             C.POINTER(C.c_longlong), C.POINTER(C.c_double),
                                                             C.POINTER(C.c_double)],
@@ -303,6 +316,73 @@ class BandUpdate:
         it = C.c_int(0)
         _call(self.lib.rsdft_gpu_sweep, nsweep, float(tol), C.byref(it), _ptr(esp), _ptr(res))
         return it.value, esp, res
+
+    # ---- learned preconditioner ----
+    def lpc_init(self, seed: int = 1):
+        _call(self.lib.rsdft_gpu_lpc_init, int(seed))
+
+    def lpc_set_weights(self, w: np.ndarray):
+        w = np.ascontiguousarray(w, np.float32).ravel()
+        _call(self.lib.rsdft_gpu_lpc_set_weights, _ptr(w), w.size)
+
+    def lpc_get_weights(self) -> np.ndarray:
+        w = np.zeros(LPC_NWEIGHTS, np.float32)
+        _call(self.lib.rsdft_gpu_lpc_get_weights, _ptr(w), w.size)
+        return w
+
+    def lpc_forward(self, x: np.ndarray, periodic: bool = False) -> np.ndarray:
+        """Network output for x of shape (nb, n3, n2, n1) (no input scaling)."""
+        x = np.ascontiguousarray(x, np.float32)
+        nb, n3, n2, n1 = x.shape
+        y = np.zeros_like(x)
+        _call(self.lib.rsdft_gpu_lpc_forward, _ptr(x), _ptr(y), nb, n1, n2, n3, 1 if periodic else 0, MEM_HOST)
+        return y
+
+    def lpc_loss_grad(self, x: np.ndarray, t: np.ndarray, margin: int):
+        """(loss, dloss/dw) for patches x, t of shape (nb, n, n, n)."""
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        nb, n = x.shape[0], x.shape[1]
+        loss = C.c_double(0.0)
+        g = np.zeros(LPC_NWEIGHTS, np.float32)
+        _call(self.lib.rsdft_gpu_lpc_loss_grad, _ptr(x), _ptr(t), nb, n, margin, C.byref(loss), _ptr(g), MEM_HOST)
+        return loss.value, g
+
+    def lpc_dataset(self, capacity: int, patch: int = 16):
+        _call(self.lib.rsdft_gpu_lpc_dataset, int(capacity), int(patch))
+
+    def lpc_harvest(self, npatch: int, sigma: float = 2.5, iters: int = 30, seed: int = 1, k: int = 1,
+                    s: int = 1) -> int:
+        """Cut (gradient, screened-kinetic correction) patch pairs from the resident bands."""
+        added = C.c_int(0)
+        _call(self.lib.rsdft_gpu_lpc_harvest, k, s, int(npatch), float(sigma), int(iters), int(seed),
+              C.byref(added))
+        return added.value
+
+    def lpc_dataset_get(self, first: int, count: int, patch: int):
+        x = np.zeros((count, patch, patch, patch), np.float32)
+        t = np.zeros_like(x)
+        _call(self.lib.rsdft_gpu_lpc_dataset_get, first, count, _ptr(x), _ptr(t))
+        return x, t
+
+    def lpc_train(self, epochs: int, batch: int = 32, lr: float = 2e-3, margin: int = 4, seed: int = 1):
+        losses = np.zeros(epochs)
+        _call(self.lib.rsdft_gpu_lpc_train, int(margin), int(epochs), int(batch), float(lr), int(seed),
+              _ptr(losses))
+        return losses
+
+    def lpc_precond(self, g: np.ndarray) -> np.ndarray:
+        """Learned preconditioner on full bands (nb, ng), FP32."""
+        g = np.ascontiguousarray(np.atleast_2d(g), np.float32)
+        out = np.zeros_like(g)
+        _call(self.lib.rsdft_gpu_lpc_precond_f, _ptr(g), _ptr(out), g.shape[0], MEM_HOST)
+        return out
+
+    def lpc_status(self):
+        """(weights ready, PC mode in use by CG, learned-to-plain fallbacks, harvested pairs)."""
+        v = [C.c_int(0) for _ in range(4)]
+        _call(self.lib.rsdft_gpu_lpc_status, *[C.byref(x) for x in v])
+        return tuple(x.value for x in v)
 
     # ---- measurement ----
     def profile(self, on: bool):

@@ -340,6 +340,7 @@ int rsdft_gpu_init(const rsdft_gpu_params* p) {
   Ctx* c = new Ctx();
   c->p = *p;
   c->ng = (size_t)p->n1 * p->n2 * p->n3;
+  c->pc_cur = p->pc_mode;
   c->cplx = p->is_complex != 0;
   {
     const char* e = getenv("RSDFT_EIG");
@@ -377,6 +378,7 @@ int rsdft_gpu_init(const rsdft_gpu_params* p) {
 }
 
 int rsdft_gpu_finalize(void) {
+  lpc_release();
   destroy(g_ctx);
   g_ctx = nullptr;
   return 0;
@@ -615,6 +617,11 @@ int rsdft_gpu_sweep(int nsweep, double tol, int* iters, double* esp, double* res
   Ctx& c = *g_ctx;
   const int nbmax = c.p.mb;
   std::vector<double> e((size_t)nbmax), r((size_t)nbmax);
+  // learned-PC guard: every sweep is judged by the FP64 residual without preconditioning; when
+  // it has not dropped below 0.9x its best value for 3 sweeps running, CG falls back to
+  // precond_hprsdft for the rest of the run
+  double best = 1e300;
+  int stall = 0;
   int it = 0;
   for (it = 1; it <= nsweep; ++it) {
     double rmax = 0.0;
@@ -636,6 +643,15 @@ int rsdft_gpu_sweep(int nsweep, double tol, int* iters, double* esp, double* res
           if (esp) std::memcpy(esp + off, e.data(), sizeof(double) * nb);
           if (res) std::memcpy(res + off, r.data(), sizeof(double) * nb);
         }
+      if (pc_effective(c) == RSDFT_PC_LEARNED) {
+        if (rmax < 0.9 * best) {
+          best = rmax;
+          stall = 0;
+        } else if (++stall >= 3) {
+          c.pc_cur = RSDFT_PC_HPRSDFT;
+          c.lpc_fallbacks++;
+        }
+      }
       if (tol > 0.0 && rmax <= tol) break;
     }
   }

@@ -553,6 +553,13 @@ static int hpsi_any(Ctx& c, int kk, int s, const T* x, T* hx, size_t ld, int nb)
   return hpsi_real<T>(c, kk, s, x, hx, ld, nb);
 }
 
+// Preconditioner CG uses now: the learned one only where it is built (real build, FP32
+// bands) and trained; otherwise precond_hprsdft stands in.
+int pc_effective(const Ctx& c) {
+  if (c.pc_cur == RSDFT_PC_LEARNED && !(lpc_ready() && c.mixed && !c.cplx)) return RSDFT_PC_HPRSDFT;
+  return c.pc_cur;
+}
+
 template <typename T, int NC>
 static int cg_block_run(Ctx& c, int kk, int s, double* h_esp, double* h_res) {
   const int nb = c.kp[kk].nband;
@@ -605,9 +612,12 @@ static int cg_block_run(Ctx& c, int kk, int s, double* h_esp, double* h_res) {
         LAUNCH_S(k_sc_top, c1sq);
       }
       if (icg == c.p.ncg + 1) break;
-      if (c.p.pc_mode == RSDFT_PC_NONE) {
+      const int pcm = pc_effective(c);
+      if (pcm == RSDFT_PC_NONE) {
         ProfScope ps(c, "cg");
         LAUNCH_E(k_copy<T>, G, PG);
+      } else if (pcm == RSDFT_PC_LEARNED && std::is_same<T, float>::value && NC == 1) {
+        RS_TRY(lpc_apply(c, reinterpret_cast<const float*>(G), reinterpret_cast<float*>(PG), nn));
       } else {
         RS_TRY(pc_block<T>(c, k, G, PG, R, Q, F));
       }

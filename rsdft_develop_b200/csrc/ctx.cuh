@@ -90,6 +90,9 @@ struct Ctx {
   DBuf ws_gemm;                    // split-BF16 operands
   DBuf ws_out;                     // small per-band outputs (esp/res) handed to callers
   DBuf ws_f64;                     // FP64 copy of FP32-resident bands (mixed mode dense ops)
+  DBuf vzero;                      // zero potential (kinetic-only operator)
+  int pc_cur = 0;                  // preconditioner in use by CG (pc_mode, or its fallback)
+  int lpc_fallbacks = 0;           // sweeps-level switches from the learned to the plain PC
 
   // profiling
   bool profiling = false;
@@ -128,6 +131,14 @@ int hpsi_real(Ctx& c, int k, int s, const T* psi, T* hpsi, size_t ld, int nb);
 template <typename T>
 int hpsi_cplx(Ctx& c, int k, int s, const T* psi, T* hpsi, size_t ld, int nb);  // T = float / double (interleaved)
 int nl_prepare_k(Ctx& c, int k);
+
+int kinetic_shifted(Ctx& c, const float* x, float* y, size_t ld, int nb, double shift);
+
+// ---- learned preconditioner (lpc.cu) ----
+bool lpc_ready();
+void lpc_release();
+int lpc_apply(Ctx& c, const float* g, float* pg, int nb);
+int pc_effective(const Ctx& c);
 
 // ---- preconditioner / CG ----
 int cg_run(Ctx& c, int k, int s, double* h_esp, double* h_res);

