@@ -123,6 +123,18 @@ int rsdft_gpu_hamiltonian_d(int k, int s, const double* tpsi, double* htpsi, int
 int rsdft_gpu_hamiltonian_z(int k, int s, const double* tpsi, double* htpsi, int ld, int nb, int mem);
 int rsdft_gpu_hamiltonian_f(int k, int s, const float* tpsi, float* htpsi, int ld, int nb, int mem);
 int rsdft_gpu_hamiltonian_c(int k, int s, const float* tpsi, float* htpsi, int ld, int nb, int mem);
+/* hamiltonian on caller-owned DEVICE blocks (FP64, real8 build) that performs no device
+ * allocation.  No counterpart in the reference.  For callers that cannot let a library call
+ * cudaMalloc -- a host code that reserves the whole device memory pool up front, a caller
+ * running inside another framework's pool or stream capture, or a loop where cudaMalloc's
+ * implicit device synchronisation would stall -- the nonlocal coefficient scratch comes from a
+ * fixed 4 MiB array compiled into the library (held on every GPU that loads it until the
+ * process exits): nb x (atoms x padded projectors per atom) must not exceed 524288, larger
+ * requests return RSDFT_ERR_ARG (split the bands into blocks).  The first call on a device
+ * looks the array's device address up (cudaGetSymbolAddress); make that first call before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU race; nothing in
+ * it has to start at zero (every call rewrites what it reads).  Runs on the library stream. */
+int rsdft_gpu_hamiltonian_noalloc_d(int k, int s, const double* tpsi, double* htpsi, int ld, int nb);
 /* conjugate_gradient on the resident unk(:,:,k,s); esp/res (host, length nband) as the
  * reference's esp(:,k,s)/res(:,k,s), res = dV |H psi - e psi|^2 (cg_module.f90:231,556). */
 int rsdft_gpu_conjugate_gradient(int k, int s, double* esp, double* res);

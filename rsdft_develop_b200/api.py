@@ -52,6 +52,7 @@ EXPORTS = [
     "rsdft_gpu_conjugate_gradient", "rsdft_gpu_gram_schmidt", "rsdft_gpu_subspace_diag",
     "rsdft_gpu_residual", "rsdft_gpu_precond_d", "rsdft_gpu_sweep", "rsdft_gpu_profile",
     "rsdft_gpu_profile_get", "rsdft_gpu_kernel_launches", "rsdft_gpu_selftest_gemm", "rsdft_gpu_init_sweep",
+    "rsdft_gpu_hamiltonian_noalloc_d",
     "rsdft_gpu_lpc_init", "rsdft_gpu_lpc_set_weights", "rsdft_gpu_lpc_get_weights", "rsdft_gpu_lpc_forward",
     "rsdft_gpu_lpc_loss_grad", "rsdft_gpu_lpc_dataset", "rsdft_gpu_lpc_harvest", "rsdft_gpu_lpc_dataset_get",
     "rsdft_gpu_lpc_train", "rsdft_gpu_lpc_precond_f", "rsdft_gpu_lpc_status",
@@ -107,6 +108,7 @@ def load_library(path: str = LIB_PATH):
         "rsdft_gpu_sweep": [i, d, C.POINTER(C.c_int), vp, vp],
         "rsdft_gpu_selftest_gemm": [i, i, C.c_longlong, i, C.POINTER(C.c_double)],
         "rsdft_gpu_init_sweep": [i],
+        "rsdft_gpu_hamiltonian_noalloc_d": [i, i, vp, vp, i, i],
         "rsdft_gpu_lpc_init": [C.c_ulonglong], "rsdft_gpu_lpc_set_weights": [vp, i],
         "rsdft_gpu_lpc_get_weights": [vp, i], "rsdft_gpu_lpc_forward": [vp, vp, i, i, i, i, i, i],
         "rsdft_gpu_lpc_loss_grad": [vp, vp, i, i, i, C.POINTER(C.c_double), vp, i],
@@ -273,6 +275,13 @@ class BandUpdate:
         else:
             fn = self.lib.rsdft_gpu_hamiltonian_f if fp32 else self.lib.rsdft_gpu_hamiltonian_d
         _call(fn, k, s, C.c_void_p(tpsi_ptr), C.c_void_p(htpsi_ptr), self.prob.ng, nb, MEM_DEVICE)
+
+    def hamiltonian_noalloc_device(self, tpsi_ptr: int, htpsi_ptr: int, nb: int, k: int = 1, s: int = 1):
+        """hamiltonian on caller-owned device blocks without any device allocation: the nonlocal
+        scratch is a fixed 4 MiB array inside the library (for callers that cannot let a library
+        call cudaMalloc).  nb x projector slots must stay <= 524288; concurrent calls race."""
+        _call(self.lib.rsdft_gpu_hamiltonian_noalloc_d, k, s, C.c_void_p(tpsi_ptr), C.c_void_p(htpsi_ptr),
+              self.prob.ng, nb)
 
     def precond(self, gk: np.ndarray, k: int = 1) -> np.ndarray:
         g = np.ascontiguousarray(np.atleast_2d(gk), np.float64)

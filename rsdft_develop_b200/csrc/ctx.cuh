@@ -131,6 +131,8 @@ int hpsi_real(Ctx& c, int k, int s, const T* psi, T* hpsi, size_t ld, int nb);
 template <typename T>
 int hpsi_cplx(Ctx& c, int k, int s, const T* psi, T* hpsi, size_t ld, int nb);  // T = float / double (interleaved)
 int nl_prepare_k(Ctx& c, int k);
+template <typename T>
+int hpsi_real_scratch(Ctx& c, int k, int s, const T* psi, T* hpsi, size_t ld, int nb, T* coef, size_t coef_cap);
 
 int kinetic_shifted(Ctx& c, const float* x, float* y, size_t ld, int nb, double shift);
 

@@ -584,6 +584,29 @@ int hpsi_real(Ctx& c, int k, int s, const T* psi, T* out, size_t ld, int nb) {
 template int hpsi_real<float>(Ctx&, int, int, const float*, float*, size_t, int);
 template int hpsi_real<double>(Ctx&, int, int, const double*, double*, size_t, int);
 
+// hpsi with caller-provided scratch for the nonlocal coefficient rows (coef_cap elements of
+// T); performs no device allocation.
+template <typename T>
+int hpsi_real_scratch(Ctx& c, int k, int s, const T* psi, T* out, size_t ld, int nb, T* coef, size_t coef_cap) {
+  RS_CHECK(!c.cplx, RSDFT_ERR_STATE, "real hpsi called on a complex16 context");
+  RS_CHECK(c.kp[k].set || c.p.nk == 1, RSDFT_ERR_STATE, "k-point %d not set", k + 1);
+  RS_CHECK(c.vloc_set[s], RSDFT_ERR_STATE, "Vloc for spin %d not set", s + 1);
+  if (nb <= 0) return 0;
+  T* cf = nullptr;
+  if (c.nl.nproj > 0) {
+    RS_TRY(nl_prepare_k(c, k));
+    const size_t need = (size_t)nb * c.nl.ngroups * c.nl.pg;
+    RS_CHECK(coef != nullptr && need <= coef_cap, RSDFT_ERR_ARG,
+             "nonlocal scratch too small: %zu coefficients needed, %zu available", need, coef_cap);
+    cf = coef;
+    RS_TRY(nl_gather<T>(c, k, psi, ld, nb, cf));
+  }
+  if (c.p.md == 6) return launch_stencil<T, 6>(c, k, s, psi, out, ld, nb, cf);
+  if (c.p.md == 4) return launch_stencil<T, 4>(c, k, s, psi, out, ld, nb, cf);
+  RS_CHECK(false, RSDFT_ERR_UNSUPPORTED, "Md=%d not built in (4 and 6 are)", c.p.md);
+}
+template int hpsi_real_scratch<double>(Ctx&, int, int, const double*, double*, size_t, int, double*, size_t);
+
 // y = (T + shift) x with T the finite-difference kinetic operator alone (no V_loc, no
 // projectors), real Gamma build, FP32.
 int kinetic_shifted(Ctx& c, const float* x, float* y, size_t ld, int nb, double shift) {
