@@ -194,7 +194,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c1")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--pc", default="auto", choices=["auto", "learned", "hprsdft", "none"],
+                    help="CG preconditioner; auto = learned when trained weights for the grid spacing exist")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="skip the comparison solves (plain FP64, and mixed with precond_hprsdft)")
     ap.add_argument("--sweeps-to-tol", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -209,9 +213,17 @@ def main():
     from rsdft_develop_b200 import api, synth
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
+    from rsdft_develop_b200 import lpc_train
     prob = synth.make_problem(args.config)
     prec = api.PREC_MIXED if args.precision == "mixed" else api.PREC_FP64
-    g = api.BandUpdate(prob, precision=prec)
+    wpath = lpc_train.default_weights_path(prob.h)
+    pc = args.pc
+    if pc == "auto":
+        pc = "learned" if (prec == api.PREC_MIXED and os.path.exists(wpath)) else "hprsdft"
+    pc_mode = {"learned": api.PC_LEARNED, "hprsdft": api.PC_HPRSDFT, "none": api.PC_NONE}[pc]
+    g = api.BandUpdate(prob, precision=prec, pc_mode=pc_mode)
+    if pc == "learned":
+        g.lpc_set_weights(np.load(wpath))
     mb_ref = mb_ref_of(prob.nband)
     g.init_sweep(mb_ref)
     stream = torch.cuda.ExternalStream(g.stream())
@@ -237,9 +249,10 @@ def main():
     dt_ms = ev0.elapsed_time(ev1)
     launches = g.kernel_launches() - launches0
     st_ms, st_n, st_bytes, _ = g.profile_get("hpsi_stencil")
-    names = ["hpsi_stencil", "nl_gather", "cg", "pc", "gs", "sd", "residual"]
+    names = ["hpsi_stencil", "nl_gather", "cg", "pc", "lpc", "gs", "gemm", "sd_gemm", "sd_eig", "sd_rot", "residual"]
     shares = {n: g.profile_get(n)[0] for n in names}
     g.profile(False)
+    lpc_state = g.lpc_status()
     clocks = clk.summary()
     res_max = float(np.max(res[..., :mb_ref]))
     per_step = dt_ms / args.steps
@@ -265,10 +278,38 @@ def main():
     h2d = int(psi0.nbytes)
     d2h = int(out.nbytes + esp.nbytes + res.nbytes)
 
+    g.close()
+    # comparison solves on the same GPU: the plain FP64 method (the drop-in's FP64 path with
+    # precond_hprsdft) and, when the main arm is learned, mixed precision with precond_hprsdft
+    compare = {}
+    if not args.no_compare:
+        arms = [("fp64_hprsdft", api.PREC_FP64, api.PC_HPRSDFT)]
+        if pc != "hprsdft" and prec == api.PREC_MIXED:
+            arms.append(("mixed_hprsdft", api.PREC_MIXED, api.PC_HPRSDFT))
+        for name, pr, pm in arms:
+            if pr == prec and pm == pc_mode:
+                continue
+            with api.BandUpdate(prob, precision=pr, pc_mode=pm) as h:
+                h.init_sweep(mb_ref)
+                hs = torch.cuda.ExternalStream(h.stream())
+                solve(h, 1, TOL)
+                h.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(hs)
+                itc, _, _ = solve(h, 1, TOL)
+                e1.record(hs)
+                e1.synchronize()
+                tc = _max_over_ranks(dist, e0.elapsed_time(e1) / 1000.0)
+            compare[name] = {"s": round(tc, 4), "sweeps": itc}
+        if "fp64_hprsdft" in compare:
+            compare["speedup_vs_fp64_hprsdft"] = round(compare["fp64_hprsdft"]["s"] / t_solve, 3)
+
     hbm, bf16, peak_kind = _peaks()
     achieved = (st_bytes / st_n) / ((st_ms / st_n) * 1e-3) / 1e9 if st_n else 0.0
     ratio = NCU_TRAFFIC_RATIO.get((args.config, args.precision))
-    roof = {"bound": "hbm", "kernel": "k_stencil_real (hpsi: stencil+Vloc+nonlocal scatter)",
+    kname = "k_stencil_f32" if prec == api.PREC_MIXED else "k_stencil_real<double>"
+    roof = {"bound": "hbm", "kernel": f"{kname} (hpsi: stencil+Vloc+nonlocal scatter)",
             "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
             "frac": round(achieved / hbm, 4), "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
             "traffic": (ratio * st_bytes / st_n) if ratio else None,
@@ -293,17 +334,19 @@ def main():
             "data": "synthetic (seeded Gaussian V_loc, Gaussian s/p projectors, seeded psi0)",
             "config": {"workload": args.config, "grid": list(prob.n), "bands": prob.nband,
                        "atoms": prob.cfg.natom, "projectors": prob.nzlma, "precision": args.precision,
-                       "pc": "hprsdft", "mb_ref": mb_ref, "sweeps_to_tol": iters, "final_res_max": res_max,
+                       "pc": pc, "lpc_fallbacks": lpc_state[2] if pc == "learned" else None,
+                       "lpc_weights": os.path.relpath(wpath, ROOT) if pc == "learned" else None,
+                       "mb_ref": mb_ref, "sweeps_to_tol": iters, "final_res_max": res_max,
                        "l2": "inputs larger than L2 (psi >= 0.5 GB)", "parallelism": f"replicas x{ws}"},
             "gpu_launches": int(launches),
             "roofline": roof,
             "time_shares_ms": {k: round(v, 3) for k, v in shares.items()},
+            "compare": compare,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_val, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
-    g.close()
     if dist is not None:
         dist.destroy_process_group()
 

@@ -188,6 +188,8 @@ int rsdft_gpu_lpc_harvest(int k, int s, int npatch, double sigma, int iters,
                           unsigned long long seed, int* added);
 /* Host copy of harvested pairs [first, first+count); x or t may be NULL. */
 int rsdft_gpu_lpc_dataset_get(int first, int count, float* x, float* t);
+/* Append count host pairs (patch^3 each) to the training set; added receives the pairs stored. */
+int rsdft_gpu_lpc_dataset_add(const float* x, const float* t, int count, int* added);
 /* Adam training on the harvested set (MSE on the patch interior); losses[epoch] (host, may be
  * NULL) receives the mean batch loss of each epoch. */
 int rsdft_gpu_lpc_train(int margin, int epochs, int batch, double lr, unsigned long long seed,

@@ -55,7 +55,7 @@ EXPORTS = [
     "rsdft_gpu_hamiltonian_noalloc_d",
     "rsdft_gpu_lpc_init", "rsdft_gpu_lpc_set_weights", "rsdft_gpu_lpc_get_weights", "rsdft_gpu_lpc_forward",
     "rsdft_gpu_lpc_loss_grad", "rsdft_gpu_lpc_dataset", "rsdft_gpu_lpc_harvest", "rsdft_gpu_lpc_dataset_get",
-    "rsdft_gpu_lpc_train", "rsdft_gpu_lpc_precond_f", "rsdft_gpu_lpc_status",
+    "rsdft_gpu_lpc_dataset_add", "rsdft_gpu_lpc_train", "rsdft_gpu_lpc_precond_f", "rsdft_gpu_lpc_status",
 ]
 LPC_NWEIGHTS = 14688
 
@@ -115,6 +115,7 @@ def load_library(path: str = LIB_PATH):
         "rsdft_gpu_lpc_dataset": [i, i],
         "rsdft_gpu_lpc_harvest": [i, i, i, d, i, C.c_ulonglong, C.POINTER(C.c_int)],
         "rsdft_gpu_lpc_dataset_get": [i, i, vp, vp],
+        "rsdft_gpu_lpc_dataset_add": [vp, vp, i, C.POINTER(C.c_int)],
         "rsdft_gpu_lpc_train": [i, i, i, d, C.c_ulonglong, vp],
         "rsdft_gpu_lpc_precond_f": [vp, vp, i, i],
         "rsdft_gpu_lpc_status": [C.POINTER(C.c_int)] * 4,
@@ -373,6 +374,13 @@ class BandUpdate:
         t = np.zeros_like(x)
         _call(self.lib.rsdft_gpu_lpc_dataset_get, first, count, _ptr(x), _ptr(t))
         return x, t
+
+    def lpc_dataset_add(self, x: np.ndarray, t: np.ndarray) -> int:
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        added = C.c_int(0)
+        _call(self.lib.rsdft_gpu_lpc_dataset_add, _ptr(x), _ptr(t), x.shape[0], C.byref(added))
+        return added.value
 
     def lpc_train(self, epochs: int, batch: int = 32, lr: float = 2e-3, margin: int = 4, seed: int = 1):
         losses = np.zeros(epochs)

@@ -184,8 +184,11 @@ static int build_nonlocal(Ctx& c, int nzlma, int maxmjj, const int* mjj, const i
   RS_TRY(nl.gplist.ensure(nl.h_gplist.size() * sizeof(int)));
   RS_TRY(nl.gD.ensure(D.size() * sizeof(double)));
   RS_TRY(nl.rec_rowptr.ensure(rowptr.size() * sizeof(int)));
-  RS_TRY(nl.rec_pt.ensure(std::max(1, nrec) * sizeof(int)));
-  RS_TRY(nl.rec_g.ensure(std::max(1, nrec) * sizeof(int)));
+  // record tables carry kRecPad spare records: the stencil's bulk copies round segments out to 4
+  RS_TRY(nl.rec_pt.ensure((size_t)(nrec + kRecPad) * sizeof(int)));
+  RS_TRY(nl.rec_g.ensure((size_t)(nrec + kRecPad) * sizeof(int)));
+  RS_CUDA(cudaMemset(nl.rec_pt.p, 0, (size_t)(nrec + kRecPad) * sizeof(int)));
+  RS_CUDA(cudaMemset(nl.rec_g.p, 0, (size_t)(nrec + kRecPad) * sizeof(int)));
   RS_CUDA(cudaMemcpy(nl.gofs.p, nl.h_gofs.data(), nl.h_gofs.size() * sizeof(int), cudaMemcpyHostToDevice));
   RS_CUDA(cudaMemcpy(nl.gjj.p, gjj.data(), gjj.size() * sizeof(int), cudaMemcpyHostToDevice));
   RS_CUDA(cudaMemcpy(nl.gplist.p, nl.h_gplist.data(), nl.h_gplist.size() * sizeof(int), cudaMemcpyHostToDevice));
@@ -194,6 +197,8 @@ static int build_nonlocal(Ctx& c, int nzlma, int maxmjj, const int* mjj, const i
   RS_CUDA(cudaMemcpy(nl.rec_pt.p, rpt.data(), nrec * sizeof(int), cudaMemcpyHostToDevice));
   RS_CUDA(cudaMemcpy(nl.rec_g.p, rg.data(), nrec * sizeof(int), cudaMemcpyHostToDevice));
   nl.perk.assign(c.p.nk, NonlocalTables::PerK());
+  nl.h_rowptr.swap(rowptr);
+  nl.seg_max.clear();
   return 0;
 }
 
@@ -203,7 +208,7 @@ static int set_uvk(Ctx& c, int k, const double* uvk, bool cplx) {
   RS_CHECK(nl.nproj > 0, RSDFT_ERR_STATE, "set_projectors must precede set_uvk");
   const int PG = nl.pg, nc = cplx ? 2 : 1;
   std::vector<double> gw((size_t)nl.ftotal * PG * nc, 0.0), sw((size_t)nl.ftotal * PG * nc, 0.0),
-      ru((size_t)nl.nrec * PG * nc);
+      ru((size_t)(nl.nrec + kRecPad) * PG * nc, 0.0);
   std::vector<int> pslot(nl.nproj, 0);
   for (int g = 0; g < nl.ngroups; ++g)
     for (int i = 0; i < PG; ++i) {

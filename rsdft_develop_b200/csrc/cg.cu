@@ -368,57 +368,75 @@ struct PcCoef {
   int n1, n2, n3, nc;
 };
 
+// Row-structured loop for the 7-point operator: the CTA's chunk of x-rows (rows of n1 * nc
+// reals), 8 rows at a time, 32 consecutive reals per row step; neighbour offsets are formed
+// once per row (y, z) and per element (x) with periodic wrap, in 32/64-bit integer adds.
+#define PC_ROWS_BEGIN(k, q)                                                                      \
+  const int b = blockIdx.y;                                                                      \
+  const size_t off = (size_t)b * (k).ng;                                                         \
+  const int L = (q).n1 * (q).nc;                                                                 \
+  const int nrow = (q).n2 * (q).n3;                                                              \
+  const int per = (nrow + (k).nch - 1) / (k).nch;                                                \
+  const int r0 = per * blockIdx.x, r1 = min(nrow, r0 + per);                                     \
+  const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;                                        \
+  const long long pln = (long long)(q).n2 * L;                                                   \
+  for (int row = r0 + ly; row < r1; row += kThreads / 32) {                                      \
+    const int i2 = row % (q).n2, i3 = row / (q).n2;                                              \
+    const long long rb = (long long)row * L;                                                     \
+    const long long ym = i2 == 0 ? (long long)((q).n2 - 1) * L : -(long long)L;                  \
+    const long long yp = i2 == (q).n2 - 1 ? -(long long)((q).n2 - 1) * L : (long long)L;         \
+    const long long zm = i3 == 0 ? (long long)((q).n3 - 1) * pln : -pln;                         \
+    const long long zp = i3 == (q).n3 - 1 ? -(long long)((q).n3 - 1) * pln : pln;                \
+    for (int x = lx; x < L; x += 32) {                                                           \
+      const int i1 = (q).nc == 1 ? x : (x >> 1);                                                 \
+      const int xm = i1 == 0 ? ((q).n1 - 1) * (q).nc : -(q).nc;                                  \
+      const int xp = i1 == (q).n1 - 1 ? -((q).n1 - 1) * (q).nc : (q).nc;                         \
+      const long long j = rb + x;
+#define PC_ROWS_END \
+  }                 \
+  }
+
 template <typename T>
-__device__ __forceinline__ double apply7(const T* __restrict__ g, size_t j, const PcCoef& q) {
-  const int n1 = q.n1, n2 = q.n2, n3 = q.n3, nc = q.nc;
-  const size_t i = j / nc;
-  const size_t comp = j - i * nc;
-  const int i1 = (int)(i % n1);
-  const int i2 = (int)((i / n1) % n2);
-  const int i3 = (int)(i / ((size_t)n1 * n2));
-  const size_t row = i - i1;
-  const size_t pln = (size_t)n1 * n2;
-  const size_t xm = row + (i1 == 0 ? n1 - 1 : i1 - 1), xp = row + (i1 == n1 - 1 ? 0 : i1 + 1);
-  const size_t ym = i2 == 0 ? i + (size_t)(n2 - 1) * n1 : i - n1;
-  const size_t yp = i2 == n2 - 1 ? i - (size_t)(n2 - 1) * n1 : i + n1;
-  const size_t zm = i3 == 0 ? i + (size_t)(n3 - 1) * pln : i - pln;
-  const size_t zp = i3 == n3 - 1 ? i - (size_t)(n3 - 1) * pln : i + pln;
-  auto G = [&](size_t pt) { return (double)g[pt * nc + comp]; };
-  return q.c0 * (double)g[j] + q.c1 * (G(xp) + G(xm)) + q.c2 * (G(yp) + G(ym)) + q.c3 * (G(zp) + G(zm));
+__device__ __forceinline__ double apply7r(const T* __restrict__ g, long long j, int xm, int xp, long long ym,
+                                          long long yp, long long zm, long long zp, const PcCoef& q) {
+  return q.c0 * (double)g[j] + q.c1 * ((double)g[j + xp] + (double)g[j + xm]) +
+         q.c2 * ((double)g[j + yp] + (double)g[j + ym]) + q.c3 * ((double)g[j + zp] + (double)g[j + zm]);
 }
 
 // F = A G ; R = G - F ; Q = R ; PG = G ; partial |R|^2
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_pc_first(Blk k, PcCoef q, const T* __restrict__ G,
                                                        T* __restrict__ R, T* __restrict__ Q, T* __restrict__ PG) {
-  BAND_LOOP(k, 1);
-  if (SC(k, S_ACT, b) == 0.0) return;
-  const T* g = G + off;
+  if (SC(k, S_ACT, blockIdx.y) == 0.0) return;
   double v[1] = {0.0};
-  for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) {
-    const double f = apply7(g, i, q);
-    const T r = (T)((double)g[i] - f);
-    R[off + i] = r;
-    Q[off + i] = r;
-    PG[off + i] = g[i];
+  {
+    PC_ROWS_BEGIN(k, q)
+    const T* g = G + off;
+    const T gj = g[j];
+    const T r = (T)((double)gj - apply7r(g, j, xm, xp, ym, yp, zm, zp, q));
+    R[off + j] = r;
+    Q[off + j] = r;
+    PG[off + j] = gj;
     v[0] += (double)r * (double)r;
+    PC_ROWS_END
   }
-  block_partials<1>(v, k, b);
+  block_partials<1>(v, k, blockIdx.y);
 }
 
 // F = A Q ; partial <Q|F>
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_pc_apply(Blk k, PcCoef q, const T* __restrict__ Q, T* __restrict__ F) {
-  BAND_LOOP(k, 1);
-  if (SC(k, S_PCACT, b) == 0.0) return;
-  const T* qq = Q + off;
+  if (SC(k, S_PCACT, blockIdx.y) == 0.0) return;
   double v[1] = {0.0};
-  for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) {
-    const T f = (T)apply7(qq, i, q);
-    F[off + i] = f;
-    v[0] += (double)qq[i] * (double)f;
+  {
+    PC_ROWS_BEGIN(k, q)
+    const T* qq = Q + off;
+    const T f = (T)apply7r(qq, j, xm, xp, ym, yp, zm, zp, q);
+    F[off + j] = f;
+    v[0] += (double)qq[j] * (double)f;
+    PC_ROWS_END
   }
-  block_partials<1>(v, k, b);
+  block_partials<1>(v, k, blockIdx.y);
 }
 
 // PG += a Q ; (if !last) R -= a F ; partial |R|^2

@@ -11,6 +11,8 @@
 
 namespace rsdft {
 
+constexpr int kRecPad = 8;  // spare records at the end of the scatter-record tables
+
 // Nonlocal projectors grouped by atom (footprint union), for the gather kernel,
 // plus the per-point CSR used by the scatter fused into the stencil kernel.
 struct NonlocalTables {
@@ -35,6 +37,8 @@ struct NonlocalTables {
   int maxmjj = 0;
   std::vector<int> h_slot;        // for each (lma, j): footprint slot in its group
   std::vector<int> h_rec_src;     // for each record: its footprint slot
+  std::vector<int> h_rowptr;      // host copy of rec_rowptr
+  std::map<int, int> seg_max;     // tile_y -> largest record segment of one (plane, y-tile)
 };
 
 struct KPoint {

@@ -22,74 +22,9 @@
 //    mbarrier ring.
 // The projector gather + Dij runs before, in an atom-centred kernel that writes the
 // coefficient rows c_b (atom-major, PG-padded).
-#include "ctx.cuh"
-#include "ptx.cuh"
+#include "stencil.cuh"
 
 namespace rsdft {
-
-template <typename T> struct VecT;
-template <> struct VecT<float> { static constexpr int V = 4; using type = float4; };
-template <> struct VecT<double> { static constexpr int V = 2; using type = double2; };
-
-template <typename T, int V>
-__device__ __forceinline__ void ldv(const T* p, T (&v)[V]) {
-  using VT = typename VecT<T>::type;
-  VT t = *reinterpret_cast<const VT*>(p);
-  const T* tt = reinterpret_cast<const T*>(&t);
-#pragma unroll
-  for (int i = 0; i < V; ++i) v[i] = tt[i];
-}
-template <typename T, int V>
-__device__ __forceinline__ void stv(T* p, const T (&v)[V]) {
-  using VT = typename VecT<T>::type;
-  VT t;
-  T* tt = reinterpret_cast<T*>(&t);
-#pragma unroll
-  for (int i = 0; i < V; ++i) tt[i] = v[i];
-  *reinterpret_cast<VT*>(p) = t;
-}
-
-__device__ __forceinline__ int pmod(int a, int n) {
-  int r = a % n;
-  return r < 0 ? r + n : r;
-}
-
-// named barrier over the compute threads, OR-reducing a flag
-__device__ __forceinline__ bool bar_or(int flag, int nthreads) {
-  uint32_t r;
-  asm volatile(
-      "{\n .reg .pred p, q;\n setp.ne.u32 q, %1, 0;\n bar.red.or.pred p, 1, %2, q;\n selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(r)
-      : "r"((uint32_t)flag), "r"((uint32_t)nthreads)
-      : "memory");
-  return r != 0;
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
-template <typename T, int MD>
-struct StArgs {
-  const T* psi;
-  T* out;
-  long long ld;
-  const T* vloc;
-  int n1, n2, n3;
-  int tile_y, tz;
-  int bx, nact, nthr_c;      // threads along x; active compute threads; compute threads (x32)
-  int stage_elems, vl_elems, nl_elems;
-  T c0;
-  T cx[MD], cy[MD], cz[MD];
-  const int* rec_rowptr;     // per point: records [rowptr[i], rowptr[i+1])
-  const int* rec_pt;         // record -> grid point
-  const int* rec_g;          // record -> atom group
-  const T* rec_u;            // record -> uV values of the group's projectors [pg]
-  int pg;
-  const T* coef;             // c_b[g*pg + p], band stride ldc
-  int ldc;
-  unsigned* status;
-};
 
 // One plane step of the z-push accumulators for rotation slot S (compile-time): add the plane's
 // xy part into its own slot, push its z taps into slots S-m and S+m, emit slot S-MD (complete)
@@ -135,24 +70,25 @@ __device__ __forceinline__ void rot_case(T (&acc)[2 * MD + 1][R][V], const T (&v
     rot_case<T, MD, R, V, S_>(acc, v, t, a.cz, fin, orow, (size_t)n1, rowok); \
     break;
 
-constexpr uint32_t kWaitPolls = 1u << 22;
-constexpr int kNLW = 2;  // nonlocal warps per CTA
-constexpr int kRB = 8;   // records in flight per nonlocal thread
-
 template <typename T, int MD, int R, int S, int S2>
-__global__ void __maxnreg__(200) k_stencil_real(const StArgs<T, MD> a) {
+__global__ void __launch_bounds__(256, 1) k_stencil_real(const StArgs<T, MD> a) {
   constexpr int V = VecT<T>::V;
   constexpr int NQ = 2 * MD + 1;
   constexpr int NCH = (MD + V - 1) / V;
   extern __shared__ __align__(128) unsigned char smem[];
   const int n1 = a.n1, n2 = a.n2, n3 = a.n3;
+  const StLayout L = smem_layout<T>(S, S2, a.stage_elems, a.vl_elems, a.nl_elems, a.ldc, a.rec_slots,
+                                     a.rec_slot_bytes);
   T* stages = reinterpret_cast<T*>(smem);
   const int sstride = a.stage_elems + a.vl_elems;
-  T* nlbuf = stages + (size_t)S * sstride;
-  T* coef_s = nlbuf + (size_t)S2 * a.nl_elems;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(coef_s + ((a.ldc + 15) / 16) * 16);
+  T* nlbuf = reinterpret_cast<T*>(smem + L.nlbuf);
+  T* coef_s = reinterpret_cast<T*>(smem + L.coef);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + L.bars);
   uint64_t* nlfull = bar + S;
   uint64_t* nlempty = nlfull + S2;
+  uint64_t* recfull = nlempty + S2;
+  int4* rechdr = reinterpret_cast<int4*>(smem + L.hdr);
+  unsigned char* recbuf = smem + L.rec;
 
   const int tid = threadIdx.x;
   const int nthr_c = a.nthr_c;
@@ -180,6 +116,7 @@ __global__ void __maxnreg__(200) k_stencil_real(const StArgs<T, MD> a) {
       mbar_init(&nlfull[s], kNLW);
       mbar_init(&nlempty[s], nthr_c);
     }
+    for (int s = 0; s < a.rec_slots; ++s) mbar_init(&recfull[s], 1);
     fence_mbar_init();
   }
   if (nl_on)
@@ -187,57 +124,7 @@ __global__ void __maxnreg__(200) k_stencil_real(const StArgs<T, MD> a) {
   __syncthreads();
 
   if (!compute) {
-    // ---------------- nonlocal warps (kNLW of them) ----------------
-    if (!nl_on) return;
-    const int lt = tid - nthr_c;  // 0 .. 32*kNLW-1
-    const int npl = zend - z0;
-    const int npts = ty_valid * n1;
-    for (int pi = 0; pi < npl; ++pi) {
-      const int slot = pi % S2;
-      if (pi >= S2) {
-        const bool ok = mbar_wait_bounded(&nlempty[slot], (uint32_t)(((pi / S2) - 1) & 1), kWaitPolls);
-        if (!ok) {
-          atomicOr(a.status, DEV_WAIT_TIMEOUT);
-          return;
-        }
-      }
-      T* nl = nlbuf + (size_t)slot * a.nl_elems;
-      for (int e = lt; e < npts; e += 32 * kNLW) nl[e] = T(0);
-      asm volatile("bar.sync 2, %0;" ::"r"(32 * kNLW) : "memory");
-      const int p = z0 + pi;
-      const int base = (p * n2 + y0) * n1;
-      const int rs = __ldg(a.rec_rowptr + base), re = __ldg(a.rec_rowptr + base + npts);
-      // batches of kRB records per thread, all loads issued before use
-      for (int r0 = rs; r0 < re; r0 += 32 * kNLW * kRB) {
-        int pt[kRB], gg[kRB];
-        T u[kRB][4];
-#pragma unroll
-        for (int j = 0; j < kRB; ++j) {
-          const int r = r0 + j * 32 * kNLW + lt;
-          pt[j] = -1;
-          if (r < re) {
-            pt[j] = __ldg(a.rec_pt + r) - base;
-            gg[j] = __ldg(a.rec_g + r);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) u[j][q] = q < a.pg ? __ldg(a.rec_u + (size_t)r * a.pg + q) : T(0);
-          }
-        }
-#pragma unroll
-        for (int j = 0; j < kRB; ++j) {
-          if (pt[j] >= 0) {
-            const T* cg = coef_s + gg[j] * a.pg;
-            T v = T(0);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) v += q < a.pg ? u[j][q] * cg[q] : T(0);
-            const int r = r0 + j * 32 * kNLW + lt;
-            for (int q = 4; q < a.pg; ++q) v += __ldg(a.rec_u + (size_t)r * a.pg + q) * cg[q];
-            atomicAdd(nl + pt[j], v);
-          }
-        }
-      }
-      __syncwarp();
-      if ((lt & 31) == 0) mbar_arrive(&nlfull[slot]);
-    }
+    if (nl_on) nl_warps<T, MD, S2>(a, nlbuf, coef_s, nlfull, nlempty, recfull, rechdr, recbuf, tid, nthr_c, z0, zend, y0, ty_valid);
     return;
   }
 
@@ -496,9 +383,13 @@ static int launch_stencil(Ctx& c, int k, int s, const T* psi, T* out, size_t ld,
   auto kern = k_stencil_real<T, MD, R, S, S2>;
   static int max_block = 0;  // one per template instantiation: block limit at this register count
   if (!max_block) {
-    cudaFuncAttributes fa{};
-    RS_CUDA(cudaFuncGetAttributes(&fa, kern));
-    max_block = fa.maxThreadsPerBlock;
+    if constexpr (std::is_same<T, float>::value) {
+      RS_TRY((stencil_f32_block_limit<MD, S, S2>(&max_block)));
+    } else {
+      cudaFuncAttributes fa{};
+      RS_CUDA(cudaFuncGetAttributes(&fa, kern));
+      max_block = fa.maxThreadsPerBlock;
+    }
   }
   const int max_c = ((max_block - 32 * kNLW) / 32) * 32;
   const int bx = n1 / V;
@@ -514,9 +405,31 @@ static int launch_stencil(Ctx& c, int k, int s, const T* psi, T* out, size_t ld,
   const int stage_elems = rnd(rows * n1), vl_elems = rnd(tile_y * n1), nl_elems = rnd(tile_y * n1);
   const bool nl_on = c.nl.nproj > 0 && coef != nullptr;
   const int ldc = nl_on ? c.nl.ngroups * c.nl.pg : 0;
-  const size_t smem = sizeof(T) * ((size_t)S * (stage_elems + vl_elems) + (size_t)S2 * nl_elems +
-                                   (size_t)((ldc + 15) / 16) * 16) +
-                      (S + 2 * S2) * sizeof(uint64_t);
+  // record ring: sized for the largest (plane, y-tile) record segment, 3 or 2 slots if they fit
+  int rec_slots = 0, rec_cap = 0, rec_cap_rp = 0, rec_slot_bytes = 0;
+  if (nl_on) {
+    auto it = c.nl.seg_max.find(tile_y);
+    if (it == c.nl.seg_max.end()) {
+      int mx = 0;
+      const std::vector<int>& rp = c.nl.h_rowptr;
+      for (int p = 0; p < n3; ++p)
+        for (int y0 = 0; y0 < n2; y0 += tile_y) {
+          const size_t b0 = ((size_t)p * n2 + y0) * n1, b1 = b0 + (size_t)std::min(tile_y, n2 - y0) * n1;
+          mx = std::max(mx, rp[b1] - rp[b0]);
+        }
+      it = c.nl.seg_max.emplace(tile_y, mx).first;
+    }
+    rec_cap = ((it->second + 6) + 3) / 4 * 4;
+    rec_cap_rp = ((tile_y * n1 + 1 + 6) + 3) / 4 * 4;
+    rec_slot_bytes =
+        (int)(((size_t)rec_cap_rp * 4 + (size_t)rec_cap * (4 + c.nl.pg * sizeof(T)) + 127) / 128 * 128);
+    for (int rs = kRecSlotsMax; rs >= 2; --rs)
+      if (smem_layout<T>(S, S2, stage_elems, vl_elems, nl_elems, ldc, rs, rec_slot_bytes).total <= 225 * 1024) {
+        rec_slots = rs;
+        break;
+      }
+  }
+  const size_t smem = smem_layout<T>(S, S2, stage_elems, vl_elems, nl_elems, ldc, rec_slots, rec_slot_bytes).total;
   RS_CHECK(smem <= 225 * 1024, RSDFT_ERR_UNSUPPORTED, "stencil stages (%zu B) exceed shared memory", smem);
   const int ytiles = (n2 + tile_y - 1) / tile_y;
   int zch = 1;
@@ -548,8 +461,12 @@ static int launch_stencil(Ctx& c, int k, int s, const T* psi, T* out, size_t ld,
   a.coef = coef;
   a.ldc = ldc;
   a.status = c.d_status;
+  a.rec_slots = rec_slots;
+  a.rec_cap = rec_cap;
+  a.rec_cap_rp = rec_cap_rp;
+  a.rec_slot_bytes = rec_slot_bytes;
   static bool attr_done = false;  // one per template instantiation
-  if (!attr_done) {
+  if (!attr_done && !std::is_same<T, float>::value) {
     RS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 225 * 1024));
     attr_done = true;
   }
@@ -558,7 +475,11 @@ static int launch_stencil(Ctx& c, int k, int s, const T* psi, T* out, size_t ld,
   const double alg_bytes = (double)sizeof(T) * (2.0 * (double)c.ng * nb + (double)c.ng) +
                            (nl_on ? 4.0 * (double)(c.ng + 1) + (8.0 + sizeof(T) * c.nl.pg) * c.nl.ftotal : 0.0);
   ProfScope ps(c, "hpsi_stencil", alg_bytes);
-  kern<<<grid, block, smem, c.stream>>>(a);
+  if constexpr (std::is_same<T, float>::value) {
+    RS_TRY((launch_stencil_f32<MD, S, S2>(a, grid, block, smem, c.stream)));
+  } else {
+    kern<<<grid, block, smem, c.stream>>>(a);
+  }
   c.launches++;
   return check_launch("hpsi_stencil");
 }

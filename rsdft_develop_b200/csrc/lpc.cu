@@ -47,7 +47,10 @@ struct Dims {
   int tiles_x, tiles_y, tiles_z;
 };
 
-__device__ __forceinline__ int wrap(int a, int n) { return a < 0 ? a + n : (a >= n ? a - n : a); }
+__device__ __forceinline__ int wrap(int a, int n) {
+  const int r = a % n;
+  return r < 0 ? r + n : r;
+}
 
 constexpr int HX = TX + 2, HY = TY + 2, HZ = TZ + 2;
 constexpr int HVOL = HX * HY * HZ;
@@ -115,6 +118,106 @@ __global__ void __launch_bounds__(NTHR) k_conv_fwd(const float* __restrict__ in,
         r *= (1.f - a * a);
       }
       ob[co * vol + o] = r;
+    }
+  }
+}
+
+// Faster 'same' convolution for COUT a multiple of 2 (same contract as k_conv_fwd): output tile
+// 16 x 8 x 8, each thread 4 consecutive z outputs x COUT channels accumulated as float2 pairs
+// of channels with packed FMAs; input channels staged 8 at a time; weights as [ci][tap][co].
+constexpr int FX = 16, FY = 8, FZ = 8, FCC = 8;
+constexpr int FHX = FX + 2, FHY = FY + 2, FHZ = FZ + 2;
+constexpr int FCS = FHX * FHY * FHZ + 4;  // per-channel stride (keeps float4 alignment)
+
+template <int CIN, int COUT, bool ACT, bool DACT>
+__global__ void __launch_bounds__(256, 1) k_conv_fwd4(const float* __restrict__ in, const __nv_bfloat16* __restrict__ w,
+                                                   float* __restrict__ out, const float* __restrict__ act_in, Dims d,
+                                                   int tiles_x, int tiles_y) {
+  static_assert(COUT % 2 == 0, "pairs of output channels");
+  constexpr int CC = CIN < FCC ? CIN : FCC;
+  extern __shared__ __align__(16) float sm[];
+  float* ws = sm;                 // [CC][27][COUT]
+  float* xs = sm + CC * 27 * COUT;  // [CC][FCS]
+  const int t = blockIdx.x;
+  const int bx = t % tiles_x, by = (t / tiles_x) % tiles_y, bz = t / (tiles_x * tiles_y);
+  const int x0 = bx * FX, y0 = by * FY, z0 = bz * FZ;
+  const size_t plane = (size_t)d.n1 * d.n2, vol = plane * d.n3;
+  const float* inb = in + (size_t)blockIdx.y * CIN * vol;
+  const int tx = threadIdx.x % FX, ty = (threadIdx.x / FX) % FY, tq = threadIdx.x / (FX * FY);  // tq: z quarter 0..1
+  float2 acc[4][COUT / 2];
+#pragma unroll
+  for (int zi = 0; zi < 4; ++zi)
+#pragma unroll
+    for (int c = 0; c < COUT / 2; ++c) acc[zi][c] = make_float2(0.f, 0.f);
+  for (int c0 = 0; c0 < CIN; c0 += CC) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < CC * 27 * COUT; e += 256) {
+      const int co = e % COUT, tap = (e / COUT) % 27, ci = e / (27 * COUT);
+      ws[e] = __bfloat162float(w[(co * CIN + c0 + ci) * 27 + tap]);
+    }
+    for (int e = threadIdx.x; e < CC * FHX * FHY * FHZ; e += 256) {
+      const int hx = e % FHX, hy = (e / FHX) % FHY, hz = (e / (FHX * FHY)) % FHZ, c = e / (FHX * FHY * FHZ);
+      int gx = x0 - 1 + hx, gy = y0 - 1 + hy, gz = z0 - 1 + hz;
+      float v = 0.f;
+      if (d.periodic) {
+        gx = wrap(gx, d.n1); gy = wrap(gy, d.n2); gz = wrap(gz, d.n3);
+        v = __ldg(inb + (size_t)(c0 + c) * vol + gz * plane + (size_t)gy * d.n1 + gx);
+      } else if (gx >= 0 && gx < d.n1 && gy >= 0 && gy < d.n2 && gz >= 0 && gz < d.n3) {
+        v = __ldg(inb + (size_t)(c0 + c) * vol + gz * plane + (size_t)gy * d.n1 + gx);
+      }
+      xs[c * FCS + (e - c * FHX * FHY * FHZ)] = v;
+    }
+    __syncthreads();
+    for (int ci = 0; ci < CC; ++ci) {
+      const float* xc = xs + ci * FCS;
+#pragma unroll
+      for (int ky = 0; ky < 3; ++ky)
+#pragma unroll
+        for (int kx = 0; kx < 3; ++kx) {
+          float xv[6];
+#pragma unroll
+          for (int j = 0; j < 6; ++j) xv[j] = xc[((tq * 4 + j) * FHY + ty + ky) * FHX + tx + kx];
+#pragma unroll
+          for (int kz = 0; kz < 3; ++kz) {
+            const float* wt = ws + (ci * 27 + (kz * 3 + ky) * 3 + kx) * COUT;
+#pragma unroll
+            for (int c4 = 0; c4 < COUT / 4; ++c4) {
+              const float4 w4 = *reinterpret_cast<const float4*>(wt + 4 * c4);
+              const float2 wa = make_float2(w4.x, w4.y), wb = make_float2(w4.z, w4.w);
+#pragma unroll
+              for (int zi = 0; zi < 4; ++zi) {
+                const float2 xx = make_float2(xv[zi + kz], xv[zi + kz]);
+                acc[zi][2 * c4] = __ffma2_rn(wa, xx, acc[zi][2 * c4]);
+                acc[zi][2 * c4 + 1] = __ffma2_rn(wb, xx, acc[zi][2 * c4 + 1]);
+              }
+            }
+            if constexpr (COUT % 4 == 2) {
+              const float2 wa = *reinterpret_cast<const float2*>(wt + COUT - 2);
+#pragma unroll
+              for (int zi = 0; zi < 4; ++zi)
+                acc[zi][COUT / 2 - 1] = __ffma2_rn(wa, make_float2(xv[zi + kz], xv[zi + kz]), acc[zi][COUT / 2 - 1]);
+            }
+          }
+        }
+    }
+  }
+  const int gx = x0 + tx, gy = y0 + ty;
+  if (gx >= d.n1 || gy >= d.n2) return;
+  float* ob = out + (size_t)blockIdx.y * COUT * vol;
+#pragma unroll
+  for (int zi = 0; zi < 4; ++zi) {
+    const int gz = z0 + tq * 4 + zi;
+    if (gz >= d.n3) break;
+    const size_t o = (size_t)gz * plane + (size_t)gy * d.n1 + gx;
+#pragma unroll
+    for (int c = 0; c < COUT; ++c) {
+      float r = (c & 1) ? acc[zi][c / 2].y : acc[zi][c / 2].x;
+      if (ACT) r = tanhf(r);
+      if (DACT) {
+        const float a = act_in[(size_t)blockIdx.y * COUT * vol + c * vol + o];
+        r *= (1.f - a * a);
+      }
+      ob[c * vol + o] = r;
     }
   }
 }
@@ -337,6 +440,22 @@ static lpc::Dims make_dims(int n1, int n2, int n3, int periodic) {
 template <int CIN, int COUT, bool ACT, bool DACT>
 static int conv_fwd(Ctx& c, const float* in, const __nv_bfloat16* w, float* out, const float* act, const lpc::Dims& d,
                     int nbatch) {
+  if constexpr (COUT % 2 == 0) {
+    constexpr int CC = CIN < lpc::FCC ? CIN : lpc::FCC;
+    const size_t smem = sizeof(float) * (CC * 27 * COUT + CC * lpc::FCS);
+    auto kern = lpc::k_conv_fwd4<CIN, COUT, ACT, DACT>;
+    static bool attr4 = false;
+    if (!attr4) {
+      RS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      attr4 = true;
+    }
+    const int tx = (d.n1 + lpc::FX - 1) / lpc::FX, ty = (d.n2 + lpc::FY - 1) / lpc::FY;
+    const int tz = (d.n3 + lpc::FZ - 1) / lpc::FZ;
+    dim3 grid(tx * ty * tz, nbatch);
+    kern<<<grid, 256, smem, c.stream>>>(in, w, out, act, d, tx, ty);
+    c.launches++;
+    return check_launch("lpc_conv_fwd");
+  }
   const size_t smem = sizeof(float) * (COUT * CIN * 27 + CIN * lpc::CS);
   auto kern = lpc::k_conv_fwd<CIN, COUT, ACT, DACT>;
   static bool attr = false;
@@ -794,6 +913,21 @@ int rsdft_gpu_lpc_dataset_get(int first, int count, float* x, float* t) {
     RS_CUDA(cudaMemcpyAsync(t, g_lpc.set_t.as<float>() + pv * first, sizeof(float) * pv * count,
                             cudaMemcpyDeviceToHost, c.stream));
   RS_CUDA(cudaStreamSynchronize(c.stream));
+  return 0;
+}
+
+int rsdft_gpu_lpc_dataset_add(const float* x, const float* t, int count, int* added) {
+  LPC_CTX();
+  RS_CHECK(x && t && count >= 0, RSDFT_ERR_ARG, "bad lpc_dataset_add arguments");
+  RS_CHECK(g_lpc.set_cap > 0, RSDFT_ERR_STATE, "no training set: call lpc_dataset first");
+  const int n = std::min(count, g_lpc.set_cap - g_lpc.set_n);
+  const size_t pv = (size_t)g_lpc.set_pn * g_lpc.set_pn * g_lpc.set_pn;
+  if (n > 0) {
+    RS_CUDA(cudaMemcpy(g_lpc.set_x.as<float>() + pv * g_lpc.set_n, x, sizeof(float) * pv * n, cudaMemcpyHostToDevice));
+    RS_CUDA(cudaMemcpy(g_lpc.set_t.as<float>() + pv * g_lpc.set_n, t, sizeof(float) * pv * n, cudaMemcpyHostToDevice));
+    g_lpc.set_n += n;
+  }
+  if (added) *added = std::max(0, n);
   return 0;
 }
 

@@ -31,7 +31,7 @@ def test_hpsi_fp64_matches_oracle(oracle_mod, name):
     assert _rel(out, ref) < TOL64
 
 
-@pytest.mark.parametrize("name", ["t1", "c0"])
+@pytest.mark.parametrize("name", ["t1", "c0", "c1"])
 def test_hpsi_fp32_matches_oracle(oracle_mod, name):
     prob = synth.make_problem(name)
     o = oracle_mod.Oracle(prob)
