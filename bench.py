@@ -195,7 +195,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c1")
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
-    ap.add_argument("--pc", default="auto", choices=["auto", "learned", "hprsdft", "none"],
+    ap.add_argument("--pc", default="hprsdft", choices=["auto", "learned", "hprsdft", "none"],
                     help="CG preconditioner; auto = learned when trained weights for the grid spacing exist")
     ap.add_argument("--no-compare", action="store_true",
                     help="skip the comparison solves (plain FP64, and mixed with precond_hprsdft)")
@@ -286,10 +286,14 @@ def main():
         arms = [("fp64_hprsdft", api.PREC_FP64, api.PC_HPRSDFT)]
         if pc != "hprsdft" and prec == api.PREC_MIXED:
             arms.append(("mixed_hprsdft", api.PREC_MIXED, api.PC_HPRSDFT))
+        if pc != "learned" and os.path.exists(wpath):
+            arms.append(("mixed_learned", api.PREC_MIXED, api.PC_LEARNED))
         for name, pr, pm in arms:
             if pr == prec and pm == pc_mode:
                 continue
             with api.BandUpdate(prob, precision=pr, pc_mode=pm) as h:
+                if pm == api.PC_LEARNED:
+                    h.lpc_set_weights(np.load(wpath))
                 h.init_sweep(mb_ref)
                 hs = torch.cuda.ExternalStream(h.stream())
                 solve(h, 1, TOL)

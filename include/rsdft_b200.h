@@ -204,7 +204,9 @@ int rsdft_gpu_lpc_status(int* ready, int* pc_in_use, int* fallbacks, int* datase
 /* Per-kernel CUDA-event timing of the library's own launches (off by default). */
 int rsdft_gpu_profile(int on);
 /* total device time (ms), launch count, algorithmic bytes and flops recorded for kernel
- * family `name` ("hpsi_stencil", "nl_gather", "gemm", "cg", "pc", ...); any output may be NULL. */
+ * family `name` ("hpsi_stencil", "nl_gather", "gemm", "cg", "pc", ...); any output may be NULL.
+ * "stencil_tune_r1" / "stencil_tune_r2" ("stencil64_..." for FP64) give the last autotuning
+ * time of each stencil variant (rows per thread). */
 int rsdft_gpu_profile_get(const char* name, double* total_ms, long long* launches, double* bytes,
                           double* flops);
 /* Launch count of all library kernels since init (for launch accounting). */

@@ -679,6 +679,16 @@ int rsdft_gpu_profile_get(const char* name, double* total_ms, long long* launche
   prof_flush(c);
   auto it = c.prof.find(name ? name : "");
   const bool f = it != c.prof.end();
+  if (!f && name) {
+    auto tt = c.tune_ms.find(name);
+    if (tt != c.tune_ms.end()) {
+      if (total_ms) *total_ms = tt->second;
+      if (launches) *launches = 1;
+      if (bytes) *bytes = 0.0;
+      if (flops) *flops = 0.0;
+      return 0;
+    }
+  }
   if (total_ms) *total_ms = f ? it->second.ms : 0.0;
   if (launches) *launches = f ? it->second.launches : 0;
   if (bytes) *bytes = f ? it->second.bytes : 0.0;

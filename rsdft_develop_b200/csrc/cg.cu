@@ -403,21 +403,42 @@ __device__ __forceinline__ double apply7r(const T* __restrict__ g, long long j, 
          q.c2 * ((double)g[j + yp] + (double)g[j + ym]) + q.c3 * ((double)g[j + zp] + (double)g[j + zm]);
 }
 
-// F = A G ; R = G - F ; Q = R ; PG = G ; partial |R|^2
+// R = G - A G (the initial residual for the starting guess PG = G, also the first direction);
+// partial |R|^2
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_pc_first(Blk k, PcCoef q, const T* __restrict__ G,
-                                                       T* __restrict__ R, T* __restrict__ Q, T* __restrict__ PG) {
+                                                       T* __restrict__ R) {
   if (SC(k, S_ACT, blockIdx.y) == 0.0) return;
   double v[1] = {0.0};
   {
     PC_ROWS_BEGIN(k, q)
     const T* g = G + off;
-    const T gj = g[j];
-    const T r = (T)((double)gj - apply7r(g, j, xm, xp, ym, yp, zm, zp, q));
+    const T r = (T)((double)g[j] - apply7r(g, j, xm, xp, ym, yp, zm, zp, q));
     R[off + j] = r;
-    Q[off + j] = r;
-    PG[off + j] = gj;
     v[0] += (double)r * (double)r;
+    PC_ROWS_END
+  }
+  block_partials<1>(v, k, blockIdx.y);
+}
+
+// Qn = R + b Q and F = A Qn = A R + b A Q in one pass (Qn written to a third buffer, since
+// the stencil reads Q's neighbours); partial <Qn|F>
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_pc_dirapply(Blk k, PcCoef q, const T* __restrict__ R,
+                                                          const T* __restrict__ Q, T* __restrict__ Qn,
+                                                          T* __restrict__ F) {
+  if (SC(k, S_PCACT, blockIdx.y) == 0.0) return;
+  const double bb = SC(k, S_PCB, blockIdx.y);
+  double v[1] = {0.0};
+  {
+    PC_ROWS_BEGIN(k, q)
+    const T* rr = R + off;
+    const T* qq = Q + off;
+    const T qn = (T)((double)rr[j] + bb * (double)qq[j]);
+    const T f = (T)(apply7r(rr, j, xm, xp, ym, yp, zm, zp, q) + bb * apply7r(qq, j, xm, xp, ym, yp, zm, zp, q));
+    Qn[off + j] = qn;
+    F[off + j] = f;
+    v[0] += (double)qn * (double)f;
     PC_ROWS_END
   }
   block_partials<1>(v, k, blockIdx.y);
@@ -439,6 +460,30 @@ __global__ void __launch_bounds__(kThreads) k_pc_apply(Blk k, PcCoef q, const T*
   block_partials<1>(v, k, blockIdx.y);
 }
 
+// first step: PG = G + a Q (starting guess G); (if !last) Rn = Q - a F (Q = R0); partial |Rn|^2
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_pc_update1(Blk k, const T* __restrict__ G, const T* __restrict__ Q,
+                                                         const T* __restrict__ F, T* __restrict__ Rn,
+                                                         T* __restrict__ PG, int last) {
+  BAND_LOOP(k, 1);
+  if (SC(k, S_PCACT, b) == 0.0) {
+    for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) PG[off + i] = G[off + i];
+    return;
+  }
+  const double a = SC(k, S_PCA, b);
+  double v[1] = {0.0};
+  for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) {
+    const double qi = Q[off + i];
+    PG[off + i] = (T)((double)G[off + i] + a * qi);
+    if (!last) {
+      const T r = (T)(qi - a * (double)F[off + i]);
+      Rn[off + i] = r;
+      v[0] += (double)r * (double)r;
+    }
+  }
+  if (!last) block_partials<1>(v, k, b);
+}
+
 // PG += a Q ; (if !last) R -= a F ; partial |R|^2
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_pc_update(Blk k, const T* __restrict__ Q, const T* __restrict__ F,
@@ -457,15 +502,6 @@ __global__ void __launch_bounds__(kThreads) k_pc_update(Blk k, const T* __restri
     }
   }
   if (!last) block_partials<1>(v, k, b);
-}
-
-// Q = R + b Q
-template <typename T>
-__global__ void __launch_bounds__(kThreads) k_pc_newdir(Blk k, const T* __restrict__ R, T* __restrict__ Q) {
-  BAND_LOOP(k, 1);
-  if (SC(k, S_PCACT, b) == 0.0) return;
-  const double bb = SC(k, S_PCB, b);
-  for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) Q[off + i] = (T)((double)R[off + i] + bb * (double)Q[off + i]);
 }
 
 __global__ void k_pc_sc_first(Blk k) {
@@ -514,8 +550,11 @@ static int pick_nch(size_t ng, int nbb) {
     c.launches++;                                                            \
   } while (0)
 
+// precond_hprsdft (cgpc_hprsdft_module.f90:133-270) on a band block: PG = G + sum_it a_it Q_it
+// for mloop CG steps on A x = G from x = G.  Buffers: X0 holds R0 = Q1, then X0/X1/X2 rotate
+// between the residual and the current/next directions; F = A Q.
 template <typename T>
-static int pc_block(Ctx& c, Blk& k, const T* G, T* PG, T* R, T* Q, T* F) {
+static int pc_block(Ctx& c, Blk& k, const T* G, T* PG, T* X0, T* X1, T* X2, T* F) {
   PcCoef q;
   const double* H = c.p.hgrid;
   q.c0 = c.p.ggg[0] / (H[0] * H[0]) + c.p.ggg[1] / (H[1] * H[1]) + c.p.ggg[2] / (H[2] * H[2]);
@@ -525,16 +564,25 @@ static int pc_block(Ctx& c, Blk& k, const T* G, T* PG, T* R, T* Q, T* F) {
   q.n1 = c.p.n1; q.n2 = c.p.n2; q.n3 = c.p.n3;
   q.nc = c.cplx ? 2 : 1;
   ProfScope ps(c, "pc");
-  LAUNCH_E(k_pc_first<T>, q, G, R, Q, PG);
+  if (c.p.mloop < 1) {
+    LAUNCH_E(k_copy<T>, G, PG);
+    return check_launch("pc");
+  }
+  LAUNCH_E(k_pc_first<T>, q, G, X0);
   LAUNCH_S(k_pc_sc_first);
-  for (int it = 1; it <= c.p.mloop; ++it) {
-    LAUNCH_E(k_pc_apply<T>, q, Q, F);
+  LAUNCH_E(k_pc_apply<T>, q, X0, F);
+  LAUNCH_S(k_pc_sc_alpha);
+  LAUNCH_E(k_pc_update1<T>, G, X0, F, X1, PG, c.p.mloop == 1 ? 1 : 0);
+  T* r = X1;   // residual
+  T* qo = X0;  // current direction
+  T* qn = X2;  // next direction
+  for (int it = 2; it <= c.p.mloop; ++it) {
+    LAUNCH_S(k_pc_sc_beta);
+    LAUNCH_E(k_pc_dirapply<T>, q, r, qo, qn, F);
     LAUNCH_S(k_pc_sc_alpha);
     const int last = it == c.p.mloop;
-    LAUNCH_E(k_pc_update<T>, Q, F, R, PG, last);
-    if (last) break;
-    LAUNCH_S(k_pc_sc_beta);
-    LAUNCH_E(k_pc_newdir<T>, R, Q);
+    LAUNCH_E(k_pc_update<T>, qn, F, r, PG, last);
+    std::swap(qo, qn);
   }
   return check_launch("pc");
 }
@@ -549,16 +597,17 @@ int precond_real(Ctx& c, const T* g, T* pg, size_t ld, int nb) {
   k.nch = pick_nch(nreal, nb);
   RS_TRY(c.ws_scal.ensure(sizeof(double) * S_COUNT * nb + 64));
   RS_TRY(c.ws_red.ensure(sizeof(double) * kPS * (size_t)nb * k.nch));
-  RS_TRY(c.ws_cg.ensure(sizeof(T) * 3 * nreal * (size_t)nb));
+  RS_TRY(c.ws_cg.ensure(sizeof(T) * 4 * nreal * (size_t)nb));
   k.sc = c.ws_scal.as<double>();
   k.part = c.ws_red.as<double>();
   std::vector<double> act((size_t)nb, 1.0);
   RS_CUDA(cudaMemcpyAsync(k.sc + (size_t)S_ACT * nb, act.data(), sizeof(double) * nb, cudaMemcpyHostToDevice,
                           c.stream));
-  T* R = c.ws_cg.as<T>();
-  T* Q = R + nreal * nb;
-  T* F = Q + nreal * nb;
-  RS_TRY(pc_block<T>(c, k, g, pg, R, Q, F));
+  T* X0 = c.ws_cg.as<T>();
+  T* X1 = X0 + nreal * nb;
+  T* X2 = X1 + nreal * nb;
+  T* F = X2 + nreal * nb;
+  RS_TRY(pc_block<T>(c, k, g, pg, X0, X1, X2, F));
   RS_CUDA(cudaStreamSynchronize(c.stream));
   return 0;
 }
@@ -585,7 +634,7 @@ static int cg_block_run(Ctx& c, int kk, int s, double* h_esp, double* h_res) {
   int nbb = c.p.cg_block > 0 ? std::min(c.p.cg_block, nb) : nb;
   size_t freeb = 0, totb = 0;
   cudaMemGetInfo(&freeb, &totb);
-  const size_t per_band = 8 * nreal * sizeof(T);
+  const size_t per_band = 9 * nreal * sizeof(T);
   const size_t budget = (size_t)(0.4 * (double)(freeb + c.ws_cg.bytes));
   if (c.p.cg_block <= 0)
     while (nbb > 1 && (size_t)nbb * per_band > budget) nbb = (nbb + 1) / 2;
@@ -605,7 +654,8 @@ static int cg_block_run(Ctx& c, int kk, int s, double* h_esp, double* h_res) {
   T* P = PG + nreal * nbb;
   T* R = P + nreal * nbb;
   T* Q = R + nreal * nbb;
-  T* F = Q + nreal * nbb;
+  T* Q2 = Q + nreal * nbb;
+  T* F = Q2 + nreal * nbb;
   T* psi = c.wfn(kk, s).psi.as<T>();
   const double dV = c.p.dv;
   // real build: g = -2(Hx - Ex), res = rb/2^2; complex build: g = -(Hx - Ex), res = rb
@@ -637,7 +687,7 @@ static int cg_block_run(Ctx& c, int kk, int s, double* h_esp, double* h_res) {
       } else if (pcm == RSDFT_PC_LEARNED && std::is_same<T, float>::value && NC == 1) {
         RS_TRY(lpc_apply(c, reinterpret_cast<const float*>(G), reinterpret_cast<float*>(PG), nn));
       } else {
-        RS_TRY(pc_block<T>(c, k, G, PG, R, Q, F));
+        RS_TRY(pc_block<T>(c, k, G, PG, R, Q, Q2, F));
       }
       {
         ProfScope ps(c, "cg");

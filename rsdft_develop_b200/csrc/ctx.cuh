@@ -95,6 +95,8 @@ struct Ctx {
   DBuf ws_out;                     // small per-band outputs (esp/res) handed to callers
   DBuf ws_f64;                     // FP64 copy of FP32-resident bands (mixed mode dense ops)
   DBuf vzero;                      // zero potential (kinetic-only operator)
+  std::map<long long, int> stencil_tune;  // autotuned stencil variant (rows per thread) per shape
+  std::map<std::string, double> tune_ms;   // last autotuning timings (reported by profile_get)
   int pc_cur = 0;                  // preconditioner in use by CG (pc_mode, or its fallback)
   int lpc_fallbacks = 0;           // sweeps-level switches from the learned to the plain PC
 
