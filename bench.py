@@ -201,6 +201,7 @@ def main():
                     help="skip the comparison solves (plain FP64, and mixed with precond_hprsdft)")
     ap.add_argument("--sweeps-to-tol", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer (C ABI) solves (large configs)")
     args = ap.parse_args()
     dist, rank, ws = _dist()
     if args.impl == "reference":
@@ -258,25 +259,27 @@ def main():
     per_step = dt_ms / args.steps
     t_solve = _max_over_ranks(dist, per_step / 1000.0)
 
-    # e2e: the same solve through the C ABI from pinned host buffers
-    psi0 = synth.random_wavefunctions(1, prob.nband, prob.ng)
-    pin = torch.from_numpy(psi0).pin_memory()
-    pin_np = pin.numpy()
-    out = torch.empty_like(pin).pin_memory().numpy()
-    e2e_t = []
-    for i in range(1 + args.steps):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        g.set_wf(pin_np)
-        g.gram_schmidt()
-        it, esp, res = g.calc_sweep(MAX_SWEEPS, tol=TOL)
-        g.lib.rsdft_gpu_get_wf_d(1, 1, out.ctypes.data, prob.ng, prob.nband)
-        torch.cuda.synchronize()
-        if i > 0:
-            e2e_t.append(time.perf_counter() - t0)
-    e2e_val = _max_over_ranks(dist, statistics.median(e2e_t))
-    h2d = int(psi0.nbytes)
-    d2h = int(out.nbytes + esp.nbytes + res.nbytes)
+    e2e_t, h2d, d2h = [], 0, 0
+    if not args.no_e2e:
+        # e2e: the same solve through the C ABI from pinned host buffers
+        psi0 = synth.random_wavefunctions(1, prob.nband, prob.ng)
+        pin = torch.from_numpy(psi0).pin_memory()
+        pin_np = pin.numpy()
+        out = torch.empty_like(pin).pin_memory().numpy()
+        e2e_t = []
+        for i in range(1 + args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            g.set_wf(pin_np)
+            g.gram_schmidt()
+            it, esp, res = g.calc_sweep(MAX_SWEEPS, tol=TOL)
+            g.lib.rsdft_gpu_get_wf_d(1, 1, out.ctypes.data, prob.ng, prob.nband)
+            torch.cuda.synchronize()
+            if i > 0:
+                e2e_t.append(time.perf_counter() - t0)
+        h2d = int(psi0.nbytes)
+        d2h = int(out.nbytes + esp.nbytes + res.nbytes)
+    e2e_val = _max_over_ranks(dist, statistics.median(e2e_t)) if e2e_t else None
 
     g.close()
     # comparison solves on the same GPU: the plain FP64 method (the drop-in's FP64 path with
@@ -312,7 +315,7 @@ def main():
     hbm, bf16, peak_kind = _peaks()
     achieved = (st_bytes / st_n) / ((st_ms / st_n) * 1e-3) / 1e9 if st_n else 0.0
     ratio = NCU_TRAFFIC_RATIO.get((args.config, args.precision))
-    kname = "k_stencil_f32" if prec == api.PREC_MIXED else "k_stencil_real<double>"
+    kname = "k_stencil_stream<float>" if prec == api.PREC_MIXED else "k_stencil_stream<double>"
     roof = {"bound": "hbm", "kernel": f"{kname} (hpsi: stencil+Vloc+nonlocal scatter)",
             "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
             "frac": round(achieved / hbm, 4), "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",

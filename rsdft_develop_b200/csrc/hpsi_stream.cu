@@ -10,14 +10,16 @@
 // N1 x TY column of one band streamed along z.
 //  * Thread 0 bulk-copies (TMA engine, cp.async.bulk + mbarrier) each xy-plane of the column
 //    with an Md-deep periodic y halo and its V_loc tile into an S-deep ring, and each plane's
-//    nonlocal records (row pointers per grid point, atom, uV) into an RS-deep ring, a few planes
+//    nonlocal records (grid point, atom, uV per record) into an RS-deep ring, a few planes
 //    ahead and across work-item boundaries.
 //  * Every thread owns W consecutive x points (one 16-byte shared-memory load) on R rows: x taps
 //    wrap inside the staged full row, y taps read neighbouring staged rows, z taps are pushed
-//    into 2*Md+1 rotating register accumulators (each plane is read once from HBM), and the
-//    nonlocal term of each own point is summed from its staged records and the band's
-//    coefficient row.  FP32 runs on float2 pairs with sm_100's packed FMA/ADD/MUL; FP64 on
-//    scalars with the same pairing.
+//    into 2*Md+1 rotating register accumulators (each plane is read once from HBM).  FP32 runs
+//    on float2 pairs with sm_100's packed FMA/ADD/MUL; FP64 on scalars with the same pairing.
+//  * Nonlocal term: one step ahead, all threads of the CTA share out the next plane's staged
+//    records evenly, each adding uV . c_b[atom] into that plane's buffer with a shared-memory
+//    atomic; on the next step each thread takes its own points' sums with one vector load per
+//    row and clears them (two buffers by plane parity; the per-step barrier orders both).
 //  * R (rows per thread: register blocking against occupancy) is picked per shape by timing
 //    both variants on the first call (autotuning).
 // All waits are bounded; a timeout sets the device status word (RSDFT_ERR_TIMEOUT) and every
@@ -152,7 +154,7 @@ __device__ __forceinline__ Item item_of(const StArgs<T, MD>& a, int w) {
 
 // R rows per thread: R = 2 keeps 2W points per thread (1 CTA of 8 warps per SM, up to 255
 // registers); R = 1 keeps W (2 CTAs per SM at <= 128 registers).
-template <typename T, int MD, int R, int S>
+template <typename T, int MD, int R>
 __global__ void __launch_bounds__(256, 3 - R) k_stencil_stream(const StArgs<T, MD> a) {
   using L = Lanes<T>;
   using P2 = typename L::P2;
@@ -162,9 +164,11 @@ __global__ void __launch_bounds__(256, 3 - R) k_stencil_stream(const StArgs<T, M
   constexpr int NCH = (MD + W - 1) / W;  // W-wide chunks of x halo per side
   extern __shared__ __align__(128) unsigned char smem[];
   const int n1 = a.n1, n2 = a.n2, n3 = a.n3;
+  const int S = a.nst;  // plane stages in the ring
   const StLayout Ly = smem_layout<T>(S, a.stage_elems, a.vl_elems, a.ldc, a.rec_slots, a.rec_slot_bytes);
   T* stages = reinterpret_cast<T*>(smem);
   const int sstride = a.stage_elems + a.vl_elems;
+  T* nlb = reinterpret_cast<T*>(smem + Ly.nlb);  // [2][vl_elems] nonlocal sums of a plane, by parity
   T* coef_s = reinterpret_cast<T*>(smem + Ly.coef);
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + Ly.bars);
   uint64_t* recfull = bar + S;
@@ -181,7 +185,7 @@ __global__ void __launch_bounds__(256, 3 - R) k_stencil_stream(const StArgs<T, M
   const int rows = a.tile_y + 2 * MD;
   const bool nl_on = a.rec_rowptr != nullptr;
   const int RS = a.rec_slots;
-  const int cap = a.rec_cap, capr = a.rec_cap_rp;
+  const int cap = a.rec_cap;
   const int nwork = a.ytiles * a.zch * a.nb;
 
   if (tid == 0) {
@@ -189,6 +193,8 @@ __global__ void __launch_bounds__(256, 3 - R) k_stencil_stream(const StArgs<T, M
     for (int s = 0; s < RS; ++s) mbar_init(&recfull[s], 1);
     fence_mbar_init();
   }
+  if (nl_on)  // the plane buffers start at zero; every reader clears what it has read
+    for (int i = tid; i < 2 * a.vl_elems; i += blockDim.x) nlb[i] = T(0);
   __syncthreads();
 
   // ---- producer state (thread 0): plane stages and record segments, issued ahead ----
@@ -236,20 +242,17 @@ __global__ void __launch_bounds__(256, 3 - R) k_stencil_stream(const StArgs<T, M
       if (pw < nwork) pit = item_of<T, MD>(a, pw);
     }
   };
-  // slot: [row pointers: capr ints][atoms: cap ints][uV: cap * pg values]
-  // header: {direct, row-pointer offset, first staged record, -}
+  // slot: [points: cap ints][atoms: cap ints][uV: cap * pg values]
+  // header: {direct, first record of the segment within the slot, records, -}
   auto issue_rec = [&]() {
     const int slot = (int)(gri % RS);
-    const int base = rec_base();
-    const int npts = rit.ty_valid * n1;
     const int rs = pf_rs, re = pf_re;
     const int a0 = rs & ~3, a1 = (re + 3) & ~3, n = a1 - a0;
-    const int b0 = base & ~3, b1 = (base + npts + 1 + 3) & ~3, nr = b1 - b0;
     int4 h;
     uint32_t bytes = 0;
-    if (n <= cap && nr <= capr) {
-      h = make_int4(0, base - b0, a0, 0);
-      bytes = (uint32_t)nr * 4u + (uint32_t)n * (4u + (uint32_t)(a.pg * sizeof(T)));
+    if (n <= cap) {
+      h = make_int4(0, rs - a0, re - rs, 0);
+      bytes = (uint32_t)n * (8u + (uint32_t)(a.pg * sizeof(T)));
     } else {
       h = make_int4(1, 0, 0, 0);
     }
@@ -257,10 +260,10 @@ __global__ void __launch_bounds__(256, 3 - R) k_stencil_stream(const StArgs<T, M
     mbar_arrive_expect_tx(&recfull[slot], bytes);
     if (bytes) {
       unsigned char* sb = recbuf + (size_t)slot * a.rec_slot_bytes;
-      bulk_g2s(sb, a.rec_rowptr + b0, (uint32_t)nr * 4u, &recfull[slot]);
-      bulk_g2s(sb + (size_t)capr * 4, a.rec_g + a0, (uint32_t)n * 4u, &recfull[slot]);
-      bulk_g2s(sb + (size_t)(capr + cap) * 4, a.rec_u + (size_t)a0 * a.pg,
-               (uint32_t)((size_t)n * a.pg * sizeof(T)), &recfull[slot]);
+      bulk_g2s(sb, a.rec_pt + a0, (uint32_t)n * 4u, &recfull[slot]);
+      bulk_g2s(sb + (size_t)cap * 4, a.rec_g + a0, (uint32_t)n * 4u, &recfull[slot]);
+      bulk_g2s(sb + (size_t)cap * 8, a.rec_u + (size_t)a0 * a.pg, (uint32_t)((size_t)n * a.pg * sizeof(T)),
+               &recfull[slot]);
     }
     ++gri;
     if (++rpi == rit.zend - rit.z0) {
@@ -285,6 +288,14 @@ __global__ void __launch_bounds__(256, 3 - R) k_stencil_stream(const StArgs<T, M
   long long gq = 0;   // plane stages consumed
   long long grc = 0;  // record segments consumed
   bool aborted = false;
+  bool cur_direct = true, next_direct = true;  // nonlocal sums of the current / next plane from global memory
+  typename L::U zero_u;  // a zero vector of W values
+  {
+    P2 zp[P];
+#pragma unroll
+    for (int j = 0; j < P; ++j) zp[j] = L::dup(T(0));
+    zero_u = L::join(zp);
+  }
   P2 acc[NQ][R][P];
   for (int w = blockIdx.x; w < nwork && !aborted; w += gridDim.x) {
     const Item it = item_of<T, MD>(a, w);
@@ -393,54 +404,70 @@ __global__ void __launch_bounds__(256, 3 - R) k_stencil_stream(const StArgs<T, M
             }
           }
         }
-        // nonlocal: sum over the records of each own point of uV . c_b
+        // nonlocal term of the own points: sums prepared one step earlier (or from global
+        // memory when that plane's records did not fit a slot)
         if (nl_on) {
           const int base = (p * n2 + it.y0) * n1;
-          bool direct = RS == 0;
-          const int* srp = nullptr;
-          const int* sg = a.rec_g;
-          const T* su = a.rec_u;
-          int rb = 0;
-          if (RS > 0) {
-            const int rslot = (int)(grc % RS);
-            ok = mbar_wait_bounded(&recfull[rslot], (uint32_t)((grc / RS) & 1), kWaitPolls) && ok;
-            const int4 h = rechdr[rslot];
-            if (h.x == 0) {
-              const unsigned char* sb = recbuf + (size_t)rslot * a.rec_slot_bytes;
-              srp = reinterpret_cast<const int*>(sb) + h.y;
-              sg = reinterpret_cast<const int*>(sb + (size_t)capr * 4);
-              su = reinterpret_cast<const T*>(sb + (size_t)(capr + cap) * 4);
-              rb = h.z;
-            } else {
-              direct = true;
-            }
-          }
+          T* nlp = nlb + (size_t)(p & 1) * a.vl_elems;
 #pragma unroll
           for (int r = 0; r < R; ++r) {
             if (!rowok[r]) continue;
             const int e0 = (yl + r) * n1 + x0;
-            int rp[W + 1];
-#pragma unroll
-            for (int i = 0; i <= W; ++i) rp[i] = direct ? __ldg(a.rec_rowptr + base + e0 + i) : srp[e0 + i];
             T nv[W];
+            if (!cur_direct) {
+              L::split(ldu(nlp + e0), nv);
+              *reinterpret_cast<typename L::U*>(nlp + e0) = zero_u;  // cleared for plane p + 2
+            } else {
+              int rp[W + 1];
 #pragma unroll
-            for (int i = 0; i < W; ++i) {
-              T acc_nl = T(0);
-              for (int k = rp[i] - rb; k < rp[i + 1] - rb; ++k) {
-                const int g = sg[k];
-                if (a.pg == 4) {
-                  acc_nl += L::dot4(su + (size_t)k * 4, coef_s + g * 4);
-                } else {
+              for (int i = 0; i <= W; ++i) rp[i] = __ldg(a.rec_rowptr + base + e0 + i);
+#pragma unroll
+              for (int i = 0; i < W; ++i) {
+                T acc_nl = T(0);
+                for (int k = rp[i]; k < rp[i + 1]; ++k) {
+                  const int g = __ldg(a.rec_g + k);
                   for (int qq = 0; qq < a.pg; ++qq)
-                    acc_nl = ::fma(su[(size_t)k * a.pg + qq], coef_s[g * a.pg + qq], acc_nl);
+                    acc_nl = ::fma(__ldg(a.rec_u + (size_t)k * a.pg + qq), coef_s[g * a.pg + qq], acc_nl);
                 }
+                nv[i] = acc_nl;
               }
-              nv[i] = acc_nl;
             }
 #pragma unroll
             for (int j = 0; j < P; ++j) t[r][j] = L::add(t[r][j], L::mk(nv[2 * j], nv[2 * j + 1]));
           }
         }
+      }
+      // the next plane's nonlocal sums, record by record over all threads, into its buffer
+      bool consumed = false;
+      if (nl_on && p + 1 >= it.z0 && p + 1 < it.zend) {
+        bool nd = true;
+        if (RS > 0) {
+          const int rslot = (int)(grc % RS);
+          ok = mbar_wait_bounded(&recfull[rslot], (uint32_t)((grc / RS) & 1), kWaitPolls) && ok;
+          consumed = true;
+          const int4 h = rechdr[rslot];
+          if (h.x == 0) {
+            nd = false;
+            const unsigned char* sb = recbuf + (size_t)rslot * a.rec_slot_bytes;
+            const int* spt = reinterpret_cast<const int*>(sb) + h.y;
+            const int* sg = reinterpret_cast<const int*>(sb + (size_t)cap * 4) + h.y;
+            const T* su = reinterpret_cast<const T*>(sb + (size_t)cap * 8) + (size_t)h.y * a.pg;
+            T* nln = nlb + (size_t)((p + 1) & 1) * a.vl_elems;
+            const int nbase = ((p + 1) * n2 + it.y0) * n1;
+            for (int e = tid; e < h.z; e += blockDim.x) {
+              const int g = sg[e];
+              T v;
+              if (a.pg == 4) {
+                v = L::dot4(su + (size_t)e * 4, coef_s + g * 4);
+              } else {
+                v = T(0);
+                for (int qq = 0; qq < a.pg; ++qq) v = ::fma(su[(size_t)e * a.pg + qq], coef_s[g * a.pg + qq], v);
+              }
+              atomicAdd(nln + (spt[e] - nbase), v);
+            }
+          }
+        }
+        next_direct = nd;
       }
       const int zo = p - MD;
       const bool fin = zo >= it.z0 && zo < it.zend;
@@ -452,7 +479,8 @@ __global__ void __launch_bounds__(256, 3 - R) k_stencil_stream(const StArgs<T, M
         default: break;
       }
       ++gq;
-      if (inch && nl_on && RS > 0) ++grc;
+      if (consumed) ++grc;
+      cur_direct = next_direct;
       if (bar_or(!ok, nthr)) {
         aborted = true;
         break;
@@ -473,11 +501,11 @@ static int launch_variant(Ctx& c, int k, int s, const T* psi, T* out, size_t ld,
                           const T* vloc_override, double c0_shift) {
   constexpr bool F32 = std::is_same<T, float>::value;
   constexpr int W = Lanes<T>::W;
-  // stages: 1 CTA per SM (R = 2) or 2 (R = 1)
-  constexpr int S = R == 2 ? (F32 ? 6 : 5) : (F32 ? 4 : 3);
+  // stages: 1 CTA per SM (R = 2) or 2 (R = 1); fewer when the record ring needs the room
+  constexpr int SMAX = R == 2 ? (F32 ? 6 : 5) : (F32 ? 4 : 3);
   constexpr int CTAS = 3 - R;  // CTAs per SM
   const size_t budget = CTAS == 1 ? 225 * 1024 : 112 * 1024;
-  auto kern = k_stencil_stream<T, MD, R, S>;
+  auto kern = k_stencil_stream<T, MD, R>;
   static int max_block = 0, nsm = 0;  // one per template instantiation
   if (!max_block) {
     cudaFuncAttributes fa{};
@@ -503,19 +531,26 @@ static int launch_variant(Ctx& c, int k, int s, const T* psi, T* out, size_t ld,
   const int stage_elems = rnd(rows * n1), vl_elems = rnd(tile_y * n1);
   const bool nl_on = c.nl.nproj > 0 && coef != nullptr;
   const int ldc = nl_on ? c.nl.ngroups * c.nl.pg : 0;
-  int rec_slots = 0, rec_cap = 0, rec_cap_rp = 0, rec_slot_bytes = 0;
+  int S = SMAX;
+  int rec_slots = 0, rec_cap = 0, rec_slot_bytes = 0;
   if (nl_on) {
     rec_cap = ((record_segment_max(c, tile_y) + 6) + 3) / 4 * 4;
-    rec_cap_rp = ((tile_y * n1 + 1 + 6) + 3) / 4 * 4;
-    rec_slot_bytes =
-        (int)(((size_t)rec_cap_rp * 4 + (size_t)rec_cap * (4 + c.nl.pg * sizeof(T)) + 127) / 128 * 128);
-    for (int rs = kRecSlotsMax; rs >= 2; --rs)
-      if (smem_layout<T>(S, stage_elems, vl_elems, ldc, rs, rec_slot_bytes).total <= budget) {
-        rec_slots = rs;
-        break;
-      }
+    rec_slot_bytes = (int)(((size_t)rec_cap * (8 + c.nl.pg * sizeof(T)) + 127) / 128 * 128);
+    for (int st = SMAX; st >= 3 && rec_slots == 0; --st)
+      for (int rs = kRecSlotsMax; rs >= 2; --rs)
+        if (smem_layout<T>(st, stage_elems, vl_elems, ldc, rs, rec_slot_bytes).total <= budget) {
+          rec_slots = rs;
+          S = st;
+          break;
+        }
   }
   const size_t smem = smem_layout<T>(S, stage_elems, vl_elems, ldc, rec_slots, rec_slot_bytes).total;
+  {  // configuration of this variant, readable through rsdft_gpu_profile_get
+    const std::string pre = std::string(F32 ? "stencil" : "stencil64") + (R == 1 ? "_r1" : "_r2");
+    c.tune_ms[pre + "_stages"] = S;
+    c.tune_ms[pre + "_rec_slots"] = rec_slots;
+    c.tune_ms[pre + "_smem_kb"] = smem / 1024.0;
+  }
   RS_CHECK(smem <= budget, RSDFT_ERR_UNSUPPORTED, "stencil stages (%zu B) exceed shared memory", smem);
   const int ytiles = (n2 + tile_y - 1) / tile_y;
   int zch = 1;
@@ -540,6 +575,7 @@ static int launch_variant(Ctx& c, int k, int s, const T* psi, T* out, size_t ld,
   a.nthr_c = nthr;
   a.stage_elems = stage_elems;
   a.vl_elems = vl_elems;
+  a.nst = S;
   a.c0 = (T)(c.p.coef_lap0 + c.kp[k].const_k2 + c0_shift);
   for (int m = 0; m < MD; ++m) {
     a.cx[m] = (T)c.p.coef_lap[0][m];
@@ -547,6 +583,7 @@ static int launch_variant(Ctx& c, int k, int s, const T* psi, T* out, size_t ld,
     a.cz[m] = (T)c.p.coef_lap[2][m];
   }
   a.rec_rowptr = nl_on ? c.nl.rec_rowptr.as<int>() : nullptr;
+  a.rec_pt = nl_on ? c.nl.rec_pt.as<int>() : nullptr;
   a.rec_g = nl_on ? c.nl.rec_g.as<int>() : nullptr;
   a.rec_u = nl_on ? (F32 ? (const T*)c.nl.perk[k].ru32.as<float>() : (const T*)c.nl.perk[k].ru64.as<double>())
                   : nullptr;
@@ -556,7 +593,6 @@ static int launch_variant(Ctx& c, int k, int s, const T* psi, T* out, size_t ld,
   a.status = c.d_status;
   a.rec_slots = rec_slots;
   a.rec_cap = rec_cap;
-  a.rec_cap_rp = rec_cap_rp;
   a.rec_slot_bytes = rec_slot_bytes;
   a.ytiles = ytiles;
   a.zch = zch;

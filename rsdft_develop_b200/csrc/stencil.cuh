@@ -57,9 +57,11 @@ struct StArgs {
   int tile_y, tz;
   int bx, nact, nthr_c;      // threads along x; active threads; threads per CTA (x32)
   int stage_elems, vl_elems;
+  int nst;                   // plane stages in the ring
   T c0;
   T cx[MD], cy[MD], cz[MD];
   const int* rec_rowptr;     // per point: records [rowptr[i], rowptr[i+1])
+  const int* rec_pt;         // record -> grid point
   const int* rec_g;          // record -> atom group
   const T* rec_u;            // record -> uV values of the group's projectors [pg]
   int pg;
@@ -68,7 +70,7 @@ struct StArgs {
   unsigned* status;
   // record ring: each plane's record segment is bulk-copied into shared memory ahead of use
   // (rec_slots == 0: records are read from global memory directly)
-  int rec_slots, rec_cap, rec_cap_rp, rec_slot_bytes;
+  int rec_slots, rec_cap, rec_slot_bytes;
   // persistent CTAs: work items (band, y-tile, z-chunk)
   int ytiles, zch, nb;
 };
@@ -76,16 +78,17 @@ struct StArgs {
 constexpr int kRecSlotsMax = 3;
 
 // Shared-memory carve of the streaming stencil (host and device agree through smem_layout):
-// [S stages: plane rows + V_loc tile][coefficient row][barriers: S stage, kRecSlotsMax record]
-// [kRecSlotsMax record headers][record slots]
+// [S stages: plane rows + V_loc tile][2 nonlocal plane buffers][coefficient row]
+// [barriers: S stage, kRecSlotsMax record][kRecSlotsMax record headers][record slots]
 struct StLayout {
-  size_t coef, bars, hdr, rec, total;  // byte offsets
+  size_t nlb, coef, bars, hdr, rec, total;  // byte offsets
 };
 template <typename T>
 __host__ __device__ inline StLayout smem_layout(int S, int stage_elems, int vl_elems, int ldc, int rec_slots,
                                                 int rec_slot_bytes) {
   StLayout L;
-  L.coef = sizeof(T) * (size_t)S * (stage_elems + vl_elems);
+  L.nlb = sizeof(T) * (size_t)S * (stage_elems + vl_elems);
+  L.coef = L.nlb + (ldc > 0 ? sizeof(T) * 2 * (size_t)vl_elems : 0);
   L.bars = L.coef + sizeof(T) * (size_t)((ldc + 15) / 16) * 16;
   L.bars = (L.bars + 15) / 16 * 16;
   L.hdr = L.bars + sizeof(uint64_t) * (size_t)(S + kRecSlotsMax);

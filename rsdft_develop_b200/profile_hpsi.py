@@ -35,8 +35,13 @@ def main(argv=None):
             g.hamiltonian_device(a.data_ptr(), b.data_ptr(), nb, fp32=f32)
             g.synchronize()
             pre = "stencil" if f32 else "stencil64"
-            tune = "  (autotune: rows/thread 1 %.3f ms, 2 %.3f ms)" % (
+            tune = "  (autotune: rows/thread 1 %.3f ms, 2 %.3f ms" % (
                 g.profile_get(pre + "_tune_r1")[0], g.profile_get(pre + "_tune_r2")[0])
+            for r in ("r1", "r2"):
+                tune += "; %s stages %d record slots %d smem %.0f KB" % (
+                    r, g.profile_get(f"{pre}_{r}_stages")[0], g.profile_get(f"{pre}_{r}_rec_slots")[0],
+                    g.profile_get(f"{pre}_{r}_smem_kb")[0])
+            tune += ")"
             g.profile(True)
             for _ in range(reps):
                 g.hamiltonian_device(a.data_ptr(), b.data_ptr(), nb, fp32=f32)
