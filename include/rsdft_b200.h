@@ -196,6 +196,10 @@ int rsdft_gpu_lpc_train(int margin, int epochs, int batch, double lr, unsigned l
                         double* losses);
 /* The preconditioner on full periodic FP32 bands of the context grid: pg = rms(g) f(g/rms(g)). */
 int rsdft_gpu_lpc_precond_f(const float* g, float* pg, int nb, int mem);
+/* How the preconditioner (in CG and in rsdft_gpu_lpc_precond_f) evaluates the network: 0 (the
+ * default) runs the two 16 -> 16 layers on the tensor cores with BF16 activations and FP32
+ * accumulation, 1 runs all layers on CUDA cores with FP32 activations. */
+int rsdft_gpu_lpc_inference(int mode);
 /* ready: weights loaded; pc_in_use: the PC mode CG uses now; fallbacks: learned-to-plain
  * switches so far; dataset: harvested pairs.  Any output may be NULL. */
 int rsdft_gpu_lpc_status(int* ready, int* pc_in_use, int* fallbacks, int* dataset);

@@ -56,6 +56,7 @@ EXPORTS = [
     "rsdft_gpu_lpc_init", "rsdft_gpu_lpc_set_weights", "rsdft_gpu_lpc_get_weights", "rsdft_gpu_lpc_forward",
     "rsdft_gpu_lpc_loss_grad", "rsdft_gpu_lpc_dataset", "rsdft_gpu_lpc_harvest", "rsdft_gpu_lpc_dataset_get",
     "rsdft_gpu_lpc_dataset_add", "rsdft_gpu_lpc_train", "rsdft_gpu_lpc_precond_f", "rsdft_gpu_lpc_status",
+    "rsdft_gpu_lpc_inference",
 ]
 LPC_NWEIGHTS = 14688
 
@@ -117,7 +118,7 @@ def load_library(path: str = LIB_PATH):
         "rsdft_gpu_lpc_dataset_get": [i, i, vp, vp],
         "rsdft_gpu_lpc_dataset_add": [vp, vp, i, C.POINTER(C.c_int)],
         "rsdft_gpu_lpc_train": [i, i, i, d, C.c_ulonglong, vp],
-        "rsdft_gpu_lpc_precond_f": [vp, vp, i, i],
+        "rsdft_gpu_lpc_precond_f": [vp, vp, i, i], "rsdft_gpu_lpc_inference": [i],
         "rsdft_gpu_lpc_status": [C.POINTER(C.c_int)] * 4,
         "rsdft_gpu_profile": [i], "rsdft_gpu_profile_get": [C.c_char_p, C.POINTER(C.c_double),
                                                             C.POINTER(C.c_longlong), C.POINTER(C.c_double),
@@ -394,6 +395,10 @@ class BandUpdate:
         out = np.zeros_like(g)
         _call(self.lib.rsdft_gpu_lpc_precond_f, _ptr(g), _ptr(out), g.shape[0], MEM_HOST)
         return out
+
+    def lpc_inference(self, fp32: bool):
+        """Evaluate the network on CUDA cores in FP32 (True) or on the tensor cores (False, default)."""
+        _call(self.lib.rsdft_gpu_lpc_inference, 1 if fp32 else 0)
 
     def lpc_status(self):
         """(weights ready, PC mode in use by CG, learned-to-plain fallbacks, harvested pairs)."""

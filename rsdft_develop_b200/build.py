@@ -74,12 +74,14 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     objs = [os.path.join(BUILD, os.path.basename(s) + ".o") for s in sources]
     if jobs or _stale(OUT, objs):
         lib64 = os.path.join(cuda, "lib64")
-        cmd = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", OUT, *objs,
+        tmp = OUT + ".tmp"  # linked aside, then moved into place in one step
+        cmd = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", tmp, *objs,
                "-L" + lib64, "-lcublas", "-lcusolver", "-Xlinker", "-rpath," + lib64]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError("link of librsdft_b200.so failed")
+        os.replace(tmp, OUT)
     return OUT
 
 

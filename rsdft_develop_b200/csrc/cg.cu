@@ -396,11 +396,13 @@ struct PcCoef {
   }                 \
   }
 
+// 7-point operator at element j in the storage type's arithmetic (FP32 bands: FP32 math, no
+// per-element conversions)
 template <typename T>
-__device__ __forceinline__ double apply7r(const T* __restrict__ g, long long j, int xm, int xp, long long ym,
-                                          long long yp, long long zm, long long zp, const PcCoef& q) {
-  return q.c0 * (double)g[j] + q.c1 * ((double)g[j + xp] + (double)g[j + xm]) +
-         q.c2 * ((double)g[j + yp] + (double)g[j + ym]) + q.c3 * ((double)g[j + zp] + (double)g[j + zm]);
+__device__ __forceinline__ T apply7r(const T* __restrict__ g, long long j, int xm, int xp, long long ym, long long yp,
+                                     long long zm, long long zp, const PcCoef& q) {
+  return (T)q.c0 * g[j] + (T)q.c1 * (g[j + xp] + g[j + xm]) + (T)q.c2 * (g[j + yp] + g[j + ym]) +
+         (T)q.c3 * (g[j + zp] + g[j + zm]);
 }
 
 // R = G - A G (the initial residual for the starting guess PG = G, also the first direction);
@@ -409,15 +411,16 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads) k_pc_first(Blk k, PcCoef q, const T* __restrict__ G,
                                                        T* __restrict__ R) {
   if (SC(k, S_ACT, blockIdx.y) == 0.0) return;
-  double v[1] = {0.0};
+  T vt = T(0);  // per-thread partial in the storage type, added in FP64 across threads
   {
     PC_ROWS_BEGIN(k, q)
     const T* g = G + off;
-    const T r = (T)((double)g[j] - apply7r(g, j, xm, xp, ym, yp, zm, zp, q));
+    const T r = g[j] - apply7r(g, j, xm, xp, ym, yp, zm, zp, q);
     R[off + j] = r;
-    v[0] += (double)r * (double)r;
+    vt += r * r;
     PC_ROWS_END
   }
+  double v[1] = {(double)vt};
   block_partials<1>(v, k, blockIdx.y);
 }
 
@@ -428,19 +431,20 @@ __global__ void __launch_bounds__(kThreads) k_pc_dirapply(Blk k, PcCoef q, const
                                                           const T* __restrict__ Q, T* __restrict__ Qn,
                                                           T* __restrict__ F) {
   if (SC(k, S_PCACT, blockIdx.y) == 0.0) return;
-  const double bb = SC(k, S_PCB, blockIdx.y);
-  double v[1] = {0.0};
+  const T bb = (T)SC(k, S_PCB, blockIdx.y);
+  T vt = T(0);
   {
     PC_ROWS_BEGIN(k, q)
     const T* rr = R + off;
     const T* qq = Q + off;
-    const T qn = (T)((double)rr[j] + bb * (double)qq[j]);
-    const T f = (T)(apply7r(rr, j, xm, xp, ym, yp, zm, zp, q) + bb * apply7r(qq, j, xm, xp, ym, yp, zm, zp, q));
+    const T qn = rr[j] + bb * qq[j];
+    const T f = apply7r(rr, j, xm, xp, ym, yp, zm, zp, q) + bb * apply7r(qq, j, xm, xp, ym, yp, zm, zp, q);
     Qn[off + j] = qn;
     F[off + j] = f;
-    v[0] += (double)qn * (double)f;
+    vt += qn * f;
     PC_ROWS_END
   }
+  double v[1] = {(double)vt};
   block_partials<1>(v, k, blockIdx.y);
 }
 
@@ -448,15 +452,16 @@ __global__ void __launch_bounds__(kThreads) k_pc_dirapply(Blk k, PcCoef q, const
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_pc_apply(Blk k, PcCoef q, const T* __restrict__ Q, T* __restrict__ F) {
   if (SC(k, S_PCACT, blockIdx.y) == 0.0) return;
-  double v[1] = {0.0};
+  T vt = T(0);
   {
     PC_ROWS_BEGIN(k, q)
     const T* qq = Q + off;
-    const T f = (T)apply7r(qq, j, xm, xp, ym, yp, zm, zp, q);
+    const T f = apply7r(qq, j, xm, xp, ym, yp, zm, zp, q);
     F[off + j] = f;
-    v[0] += (double)qq[j] * (double)f;
+    vt += qq[j] * f;
     PC_ROWS_END
   }
+  double v[1] = {(double)vt};
   block_partials<1>(v, k, blockIdx.y);
 }
 
@@ -470,17 +475,18 @@ __global__ void __launch_bounds__(kThreads) k_pc_update1(Blk k, const T* __restr
     for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) PG[off + i] = G[off + i];
     return;
   }
-  const double a = SC(k, S_PCA, b);
-  double v[1] = {0.0};
+  const T a = (T)SC(k, S_PCA, b);
+  T vt = T(0);
   for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) {
-    const double qi = Q[off + i];
-    PG[off + i] = (T)((double)G[off + i] + a * qi);
+    const T qi = Q[off + i];
+    PG[off + i] = G[off + i] + a * qi;
     if (!last) {
-      const T r = (T)(qi - a * (double)F[off + i]);
+      const T r = qi - a * F[off + i];
       Rn[off + i] = r;
-      v[0] += (double)r * (double)r;
+      vt += r * r;
     }
   }
+  double v[1] = {(double)vt};
   if (!last) block_partials<1>(v, k, b);
 }
 
@@ -490,17 +496,18 @@ __global__ void __launch_bounds__(kThreads) k_pc_update(Blk k, const T* __restri
                                                         T* __restrict__ R, T* __restrict__ PG, int last) {
   BAND_LOOP(k, 1);
   if (SC(k, S_PCACT, b) == 0.0) return;
-  const double a = SC(k, S_PCA, b);
-  double v[1] = {0.0};
+  const T a = (T)SC(k, S_PCA, b);
+  T vt = T(0);
   for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) {
-    const double qi = Q[off + i];
-    PG[off + i] = (T)((double)PG[off + i] + a * qi);
+    const T qi = Q[off + i];
+    PG[off + i] = PG[off + i] + a * qi;
     if (!last) {
-      const T r = (T)((double)R[off + i] - a * (double)F[off + i]);
+      const T r = R[off + i] - a * F[off + i];
       R[off + i] = r;
-      v[0] += (double)r * (double)r;
+      vt += r * r;
     }
   }
+  double v[1] = {(double)vt};
   if (!last) block_partials<1>(v, k, b);
 }
 

@@ -99,6 +99,7 @@ struct Ctx {
   std::map<std::string, double> tune_ms;   // last autotuning timings (reported by profile_get)
   int pc_cur = 0;                  // preconditioner in use by CG (pc_mode, or its fallback)
   int lpc_fallbacks = 0;           // sweeps-level switches from the learned to the plain PC
+  int lpc_fp32 = 0;                // learned PC inference: 0 tensor cores (BF16 activations), 1 FP32 CUDA cores
 
   // profiling
   bool profiling = false;

@@ -24,6 +24,7 @@
 #include <random>
 
 #include "ctx.cuh"
+#include "ptx.cuh"
 
 namespace rsdft {
 namespace lpc {
@@ -411,6 +412,256 @@ __global__ void k_extract(const float* __restrict__ fx, const float* __restrict_
   }
 }
 
+// ---- tensor-core inference path (full periodic grids) ----------------------------------
+// Activations of a band: BF16 in two half-planes of 8 channels, [2][ng][8] (16 bytes per point
+// per half), so that 8 consecutive points of one half form one 128-byte core matrix of the
+// no-swizzle K-major UMMA layout.
+constexpr int TC_TX = 32;                    // output x per tile
+constexpr int TC_HX = TC_TX + 2;             // staged x (periodic halo)
+constexpr int TC_TY = 11;                    // output rows per tile
+constexpr int TC_HY = TC_TY + 2;
+constexpr int TC_NM = (TC_TY * TC_HX + 127) / 128;  // M-tiles (128 rows) per output plane
+constexpr int TC_PB = TC_NM * 128 + 2 * TC_HX + 2;  // staged points per plane (guards included)
+constexpr int TC_SLOTS = 4;                  // plane ring
+constexpr int TC_TZ = 16;                    // output planes per CTA
+constexpr uint32_t TC_POLLS = 1u << 22;
+
+__device__ __forceinline__ uint64_t umma_desc_nosw(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= 1ull << 46;  // descriptor version (sm_100); layout bits 61-63 = 0: no swizzle
+  return d;
+}
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(acc));
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// UMMA B operands of one 16->16 layer: for each tap, [khalf][co 0..15][8 ci] BF16 from the FP32
+// master weights w[co][ci][tap].
+__global__ void k_tc_pack_w(const float* __restrict__ w, __nv_bfloat16* __restrict__ wp) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < 27 * 256; e += gridDim.x * blockDim.x) {
+    const int i = e % 8, co = (e / 8) % 16, kh = (e / 128) % 2, tap = e / 256;
+    wp[e] = __float2bfloat16(w[(co * 16 + kh * 8 + i) * 27 + tap]);
+  }
+}
+
+__device__ __forceinline__ int wrapi(int a, int n) {
+  const int r = a % n;
+  return r < 0 ? r + n : r;
+}
+
+// Layer 1 (1 -> 16, tanh) on CUDA cores: x = g / rms(g) read from the FP32 band, written as
+// BF16 half-planes.  One thread per grid point.
+__global__ void __launch_bounds__(256) k_tc_layer1(const float* __restrict__ g, const double* __restrict__ s2,
+                                                   const __nv_bfloat16* __restrict__ w1, uint4* __restrict__ out,
+                                                   int n1, int n2, int n3) {
+  __shared__ float ws[27 * 16];  // [tap][co]
+  for (int e = threadIdx.x; e < 27 * 16; e += blockDim.x) ws[e] = __bfloat162float(w1[(e % 16) * 27 + e / 16]);
+  __syncthreads();
+  const size_t ng = (size_t)n1 * n2 * n3;
+  const int b = blockIdx.y;
+  const double rms = sqrt(s2[b] / (double)ng);
+  const float sc = rms > 0.0 ? (float)(1.0 / rms) : 0.f;
+  const float* gb = g + (size_t)b * ng;
+  for (size_t pt = blockIdx.x * (size_t)blockDim.x + threadIdx.x; pt < ng; pt += (size_t)gridDim.x * blockDim.x) {
+    const int x = (int)(pt % n1), y = (int)((pt / n1) % n2), z = (int)(pt / ((size_t)n1 * n2));
+    float acc[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) acc[c] = 0.f;
+#pragma unroll
+    for (int kz = 0; kz < 3; ++kz)
+#pragma unroll
+      for (int ky = 0; ky < 3; ++ky)
+#pragma unroll
+        for (int kx = 0; kx < 3; ++kx) {
+          const size_t q = ((size_t)wrapi(z + kz - 1, n3) * n2 + wrapi(y + ky - 1, n2)) * n1 + wrapi(x + kx - 1, n1);
+          const float v = __ldg(gb + q) * sc;
+          const float* wt = ws + ((kz * 3 + ky) * 3 + kx) * 16;
+#pragma unroll
+          for (int c = 0; c < 16; ++c) acc[c] = fmaf(wt[c], v, acc[c]);
+        }
+    __align__(16) __nv_bfloat16 h[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) h[c] = __float2bfloat16(tanhf(acc[c]));
+    uint4* ob = out + (size_t)b * 2 * ng;
+    ob[pt] = *reinterpret_cast<const uint4*>(h);
+    ob[ng + pt] = *reinterpret_cast<const uint4*>(h + 8);
+  }
+}
+
+// Layer 4 (16 -> 1, linear) on CUDA cores from BF16 half-planes, times rms(g): the
+// preconditioned band.  One thread per grid point.
+__global__ void __launch_bounds__(256) k_tc_layer4(const uint4* __restrict__ in, const double* __restrict__ s2,
+                                                   const __nv_bfloat16* __restrict__ w4, float* __restrict__ pg,
+                                                   int n1, int n2, int n3) {
+  __shared__ float ws[27 * 16];  // [tap][ci]
+  for (int e = threadIdx.x; e < 27 * 16; e += blockDim.x) ws[e] = __bfloat162float(w4[(e % 16) * 27 + e / 16]);
+  __syncthreads();
+  const size_t ng = (size_t)n1 * n2 * n3;
+  const int b = blockIdx.y;
+  const float rms = (float)sqrt(s2[b] / (double)ng);
+  const uint4* ib = in + (size_t)b * 2 * ng;
+  for (size_t pt = blockIdx.x * (size_t)blockDim.x + threadIdx.x; pt < ng; pt += (size_t)gridDim.x * blockDim.x) {
+    const int x = (int)(pt % n1), y = (int)((pt / n1) % n2), z = (int)(pt / ((size_t)n1 * n2));
+    float acc = 0.f;
+#pragma unroll
+    for (int kz = 0; kz < 3; ++kz)
+#pragma unroll
+      for (int ky = 0; ky < 3; ++ky)
+#pragma unroll
+        for (int kx = 0; kx < 3; ++kx) {
+          const size_t q = ((size_t)wrapi(z + kz - 1, n3) * n2 + wrapi(y + ky - 1, n2)) * n1 + wrapi(x + kx - 1, n1);
+          const float* wt = ws + ((kz * 3 + ky) * 3 + kx) * 16;
+#pragma unroll
+          for (int hh = 0; hh < 2; ++hh) {
+            const uint4 u = __ldg(ib + (size_t)hh * ng + q);
+            const __nv_bfloat16* hv = reinterpret_cast<const __nv_bfloat16*>(&u);
+#pragma unroll
+            for (int c = 0; c < 8; ++c) acc = fmaf(wt[hh * 8 + c], __bfloat162float(hv[c]), acc);
+          }
+        }
+    pg[(size_t)b * ng + pt] = acc * rms;
+  }
+}
+
+// Layers 2 and 3 (16 -> 16, tanh) on the tensor cores.  A CTA (4 warps) owns a 32 x 11 output
+// tile of x-rows over TC_TZ planes of one band.  Input planes (with a one-point periodic halo)
+// are staged into a ring of TC_SLOTS planes in the half-plane layout; for output plane z each
+// of the 27 taps is one tcgen05.mma per 128-row M-tile whose A descriptor is the staged plane
+// z + dz shifted by dy rows and dx points (rows of the M-tile are consecutive staged positions,
+// so the two halo columns of every row produce outputs that are discarded), B the tap's
+// 16 x 16 weights, D an FP32 accumulator of 16 TMEM columns.  The epilogue applies tanh and
+// writes BF16 half-planes.  All waits are bounded; a timeout sets *status.
+__global__ void __launch_bounds__(128) k_tc_mid(const uint4* __restrict__ in, const __nv_bfloat16* __restrict__ wp,
+                                                uint4* __restrict__ out, int n1, int n2, int n3, int tiles_x,
+                                                int tiles_y, int tiles_z, unsigned* status) {
+  extern __shared__ __align__(128) unsigned char tsm[];
+  constexpr int PLANE_BYTES = 2 * TC_PB * 16;
+  unsigned char* ring = tsm;                                   // [slot][half][TC_PB][16 B]
+  unsigned char* wsm = tsm + TC_SLOTS * PLANE_BYTES;           // [27][2][16][16 B]
+  uint64_t* done = reinterpret_cast<uint64_t*>(wsm + 27 * 512);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const size_t ng = (size_t)n1 * n2 * n3;
+  int t = blockIdx.x;
+  const int bx = t % tiles_x;
+  t /= tiles_x;
+  const int by = t % tiles_y;
+  t /= tiles_y;
+  const int bz = t % tiles_z;
+  const int band = blockIdx.y;
+  const int x0 = bx * TC_TX, y0 = by * TC_TY, z0 = bz * TC_TZ;
+  const int zend = min(z0 + TC_TZ, n3);
+  const uint4* ib = in + (size_t)band * 2 * ng;
+  uint4* ob = out + (size_t)band * 2 * ng;
+
+  for (int e = tid; e < 27 * 32; e += 128)
+    reinterpret_cast<uint4*>(wsm)[e] = __ldg(reinterpret_cast<const uint4*>(wp) + e);
+  if (tid == 0) {
+    mbar_init(done, 1);
+    fence_mbar_init();
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(64u));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  // stage input plane z (periodic) into ring slot: position 1 + r * TC_HX + c holds point
+  // (x0 - 1 + c, y0 - 1 + r) for r < TC_HY, c < TC_HX
+  auto load_plane = [&](int z) {
+    unsigned char* pb = ring + (size_t)(((z % TC_SLOTS) + TC_SLOTS) % TC_SLOTS) * PLANE_BYTES;
+    const int zg = wrapi(z, n3);
+    for (int e = tid; e < 2 * TC_HY * TC_HX; e += 128) {
+      const int c = e % TC_HX, r = (e / TC_HX) % TC_HY, hh = e / (TC_HX * TC_HY);
+      const int gx = wrapi(x0 - 1 + c, n1), gy = wrapi(y0 - 1 + r, n2);
+      const uint4 v = __ldg(ib + (size_t)hh * ng + ((size_t)zg * n2 + gy) * n1 + gx);
+      reinterpret_cast<uint4*>(pb)[(size_t)hh * TC_PB + 1 + r * TC_HX + c] = v;
+    }
+  };
+  load_plane(z0 - 1);
+  load_plane(z0);
+  load_plane(z0 + 1);
+  fence_proxy_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  // M = 128, N = 16, BF16 x BF16 -> FP32, both K-major
+  const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(16 >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+  bool ok = true;
+  for (int z = z0; z < zend && ok; ++z) {
+    // planes z-1, z, z+1 are staged (and visible to the tensor cores)
+    if (tid == 0) {
+#pragma unroll 1
+      for (int mt = 0; mt < TC_NM; ++mt) {
+#pragma unroll 1
+        for (int tap = 0; tap < 27; ++tap) {
+          const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+          const unsigned char* pb =
+              ring + (size_t)((((z + dz) % TC_SLOTS) + TC_SLOTS) % TC_SLOTS) * PLANE_BYTES;
+          const int row0 = 1 + TC_HX + mt * 128 + dy * TC_HX + dx;  // staged position of M row 0
+          const uint64_t da = umma_desc_nosw(smem_u32(pb + (size_t)row0 * 16), TC_PB * 16, 128);
+          const uint64_t db = umma_desc_nosw(smem_u32(wsm + tap * 512), 256, 128);
+          umma_bf16(tmem + (uint32_t)(mt * 16), da, db, idesc, tap > 0 ? 1u : 0u);
+        }
+      }
+      umma_commit(done);
+    }
+    // stage plane z+2 while the MMAs run: its ring slot held plane z-2, last read by the MMAs of
+    // plane z-1, which completed before the previous epilogue
+    if (z + 2 <= zend) load_plane(z + 2);
+    ok = mbar_wait_bounded(done, (uint32_t)((z - z0) & 1), TC_POLLS);
+    tc_fence_after();
+    if (ok) {
+#pragma unroll 1
+      for (int mt = 0; mt < TC_NM; ++mt) {
+        float v[16];
+        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(mt * 16), v);
+        const int e = mt * 128 + warp * 32 + lane;  // output position from row 1, column 0
+        const int r = e / TC_HX, cx = e % TC_HX;
+        const int gx = x0 - 1 + cx, gy = y0 + r;
+        if (r < TC_TY && cx >= 1 && cx <= TC_TX && gx < n1 && gy < n2) {
+          __align__(16) __nv_bfloat16 hb[16];
+#pragma unroll
+          for (int cc = 0; cc < 16; ++cc) hb[cc] = __float2bfloat16(tanhf(v[cc]));
+          const size_t pt = ((size_t)z * n2 + gy) * n1 + gx;
+          ob[pt] = *reinterpret_cast<const uint4*>(hb);
+          ob[ng + pt] = *reinterpret_cast<const uint4*>(hb + 8);
+        }
+      }
+    }
+    fence_proxy_async_smem();  // plane z+2 written through the generic proxy, read by the next MMAs
+    tc_fence_before();
+    if (__syncthreads_or(!ok)) ok = false;
+    tc_fence_after();
+  }
+  if (!ok && tid == 0) atomicOr(status, DEV_WAIT_TIMEOUT);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64u));
+}
+
 }  // namespace lpc
 
 // ---------------------------------------------------------------------------
@@ -418,6 +669,7 @@ __global__ void k_extract(const float* __restrict__ fx, const float* __restrict_
 // ---------------------------------------------------------------------------
 struct LpcState {
   DBuf w, wb, wt, dw, m, v;   // FP32 master, BF16 copy, BF16 transposed, grads, Adam moments
+  DBuf tcw, tca;              // tensor-core path: packed layer-2/3 weights, BF16 activations
   DBuf act, dact, batch_x, batch_t, dy, idx, loss, s2;
   DBuf set_x, set_t;          // training set: [capacity][pn^3] inputs and targets
   DBuf hv, hs;                // harvest work fields / per-band scalars
@@ -664,8 +916,61 @@ int lpc_train(Ctx& c, const float* x, const float* t, int npatch, int n, int mar
 
 // Preconditioner application on full periodic grids: pg_b = rms(g_b) f(g_b / rms(g_b)).
 // g, pg: nb bands of ng FP32 values (real build).
+// Preconditioner application with the two 16 -> 16 layers on the tensor cores (BF16
+// activations, FP32 accumulation in TMEM) and the thin first and last layers on CUDA cores.
+static int lpc_apply_tc(Ctx& c, const float* g, float* pg, int nb) {
+  const int n1 = c.p.n1, n2 = c.p.n2, n3 = c.p.n3;
+  const size_t ng = c.ng;
+  const int nbc = (int)std::max<size_t>(1, std::min<size_t>(nb, (size_t)(8ull << 30) / (64 * ng)));
+  RS_TRY(g_lpc.tcw.ensure(sizeof(__nv_bfloat16) * 2 * 27 * 256));
+  RS_TRY(g_lpc.tca.ensure((size_t)64 * ng * nbc));
+  RS_TRY(g_lpc.s2.ensure(sizeof(double) * nbc));
+  __nv_bfloat16* w2 = g_lpc.tcw.as<__nv_bfloat16>();
+  __nv_bfloat16* w3 = w2 + 27 * 256;
+  lpc::k_tc_pack_w<<<27, 256, 0, c.stream>>>(g_lpc.w.as<float>() + lpc::woff(1), w2);
+  lpc::k_tc_pack_w<<<27, 256, 0, c.stream>>>(g_lpc.w.as<float>() + lpc::woff(2), w3);
+  c.launches += 2;
+  constexpr size_t smem = (size_t)lpc::TC_SLOTS * 2 * lpc::TC_PB * 16 + 27 * 512 + 16;
+  static bool attr = false;
+  if (!attr) {
+    RS_CUDA(cudaFuncSetAttribute(lpc::k_tc_mid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr = true;
+  }
+  const int tx = (n1 + lpc::TC_TX - 1) / lpc::TC_TX, ty = (n2 + lpc::TC_TY - 1) / lpc::TC_TY;
+  const int tz = (n3 + lpc::TC_TZ - 1) / lpc::TC_TZ;
+  uint4* A = g_lpc.tca.as<uint4>();
+  uint4* B = A + 2 * ng * nbc;
+  const __nv_bfloat16* wb = g_lpc.wb.as<__nv_bfloat16>();
+  ProfScope ps(c, "lpc", 0.0, 2.0 * 27 * (16 + 256 + 256 + 16) * (double)ng * nb);
+  for (int b0 = 0; b0 < nb; b0 += nbc) {
+    const int nn = std::min(nbc, nb - b0);
+    RS_CUDA(cudaMemsetAsync(g_lpc.s2.p, 0, sizeof(double) * nn, c.stream));
+    lpc::k_rms<<<dim3(64, nn), 256, 0, c.stream>>>(g + (size_t)b0 * ng, g_lpc.s2.as<double>(), ng);
+    const unsigned pblk = (unsigned)std::min<size_t>((ng + 255) / 256, 4 * 148);
+    const double pts = (double)ng * nn;
+    {
+      ProfScope pl(c, "lpc_layer1", 36.0 * pts, 2.0 * 27 * 16 * pts);
+      lpc::k_tc_layer1<<<dim3(pblk, nn), 256, 0, c.stream>>>(g + (size_t)b0 * ng, g_lpc.s2.as<double>(),
+                                                              wb + lpc::woff(0), A, n1, n2, n3);
+    }
+    {
+      ProfScope pl(c, "lpc_mid", 2 * 64.0 * pts, 2 * 2.0 * 27 * 256 * pts);
+      lpc::k_tc_mid<<<dim3(tx * ty * tz, nn), 128, smem, c.stream>>>(A, w2, B, n1, n2, n3, tx, ty, tz, c.d_status);
+      lpc::k_tc_mid<<<dim3(tx * ty * tz, nn), 128, smem, c.stream>>>(B, w3, A, n1, n2, n3, tx, ty, tz, c.d_status);
+    }
+    {
+      ProfScope pl(c, "lpc_layer4", 36.0 * pts, 2.0 * 27 * 16 * pts);
+      lpc::k_tc_layer4<<<dim3(pblk, nn), 256, 0, c.stream>>>(A, g_lpc.s2.as<double>(), wb + lpc::woff(3),
+                                                              pg + (size_t)b0 * ng, n1, n2, n3);
+    }
+    c.launches += 5;
+  }
+  return check_launch("lpc_apply_tc");
+}
+
 int lpc_apply(Ctx& c, const float* g, float* pg, int nb) {
   RS_CHECK(g_lpc.ready, RSDFT_ERR_STATE, "learned preconditioner not initialised");
+  if (c.lpc_fp32 == 0) return lpc_apply_tc(c, g, pg, nb);
   const lpc::Dims d = make_dims(c.p.n1, c.p.n2, c.p.n3, 1);
   const size_t vol = c.ng;
   // band chunk so that activations stay within ~2 GiB
@@ -812,7 +1117,8 @@ bool lpc_ready() { return g_lpc.ready; }
 void lpc_release() {
   DBuf* bufs[] = {&g_lpc.w, &g_lpc.wb, &g_lpc.wt, &g_lpc.dw, &g_lpc.m, &g_lpc.v, &g_lpc.act, &g_lpc.dact,
                   &g_lpc.batch_x, &g_lpc.batch_t, &g_lpc.dy, &g_lpc.idx, &g_lpc.loss, &g_lpc.s2,
-                  &g_lpc.set_x, &g_lpc.set_t, &g_lpc.hv, &g_lpc.hs, &g_lpc.io_a, &g_lpc.io_b};
+                  &g_lpc.set_x, &g_lpc.set_t, &g_lpc.hv, &g_lpc.hs, &g_lpc.io_a, &g_lpc.io_b,
+                  &g_lpc.tcw, &g_lpc.tca};
   for (DBuf* b : bufs) b->release();
   g_lpc.ready = false;
   g_lpc.set_cap = g_lpc.set_n = g_lpc.set_pn = 0;
@@ -918,6 +1224,7 @@ int rsdft_gpu_lpc_dataset_get(int first, int count, float* x, float* t) {
 
 int rsdft_gpu_lpc_dataset_add(const float* x, const float* t, int count, int* added) {
   LPC_CTX();
+  (void)c;
   RS_CHECK(x && t && count >= 0, RSDFT_ERR_ARG, "bad lpc_dataset_add arguments");
   RS_CHECK(g_lpc.set_cap > 0, RSDFT_ERR_STATE, "no training set: call lpc_dataset first");
   const int n = std::min(count, g_lpc.set_cap - g_lpc.set_n);
@@ -952,6 +1259,13 @@ int rsdft_gpu_lpc_precond_f(const float* g, float* pg, int nb, int mem) {
   RS_TRY(lpc_apply(c, dg, dp, nb));
   if (mem == RSDFT_MEM_HOST) RS_CUDA(cudaMemcpyAsync(pg, dp, sizeof(float) * n, cudaMemcpyDeviceToHost, c.stream));
   RS_CUDA(cudaStreamSynchronize(c.stream));
+  return 0;
+}
+
+int rsdft_gpu_lpc_inference(int mode) {
+  LPC_CTX();
+  RS_CHECK(mode == 0 || mode == 1, RSDFT_ERR_ARG, "inference mode %d: 0 (tensor cores) or 1 (FP32)", mode);
+  c.lpc_fp32 = mode;
   return 0;
 }
 

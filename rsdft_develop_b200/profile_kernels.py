@@ -2,7 +2,7 @@
 
     python -m rsdft_develop_b200.profile_kernels gemm [m] [k]      # split-BF16 tcgen05 GEMMs
     python -m rsdft_develop_b200.profile_kernels pc [config] [bands]   # precond_hprsdft (FP64)
-    python -m rsdft_develop_b200.profile_kernels lpc [config] [bands]  # learned preconditioner
+    python -m rsdft_develop_b200.profile_kernels lpc [config] [bands] [tc|fp32]  # learned preconditioner
 
 gemm: the overlap S = A A^T (m x m, K = k) and the rotation X <- X V (m bands of k points),
 each checked against cuBLAS DGEMM (the relative error is printed).  pc / lpc: one application
@@ -44,15 +44,22 @@ def main(argv=None):
             ms, n, _, _ = g.profile_get("pc")
             print(f"precond_hprsdft {cfg} bands={nb}: {ms:.3f} ms ({n} scopes)")
     elif what == "lpc":
+        mode = argv[3] if len(argv) > 3 else "tc"
         with api.BandUpdate(prob, precision=api.PREC_MIXED, pc_mode=api.PC_LEARNED) as g:
             w = np.load(lpc_train.default_weights_path(prob.h))
             g.lpc_set_weights(w)
+            g.lpc_inference(fp32=(mode == "fp32"))
             x = g_in.astype(np.float32)
             g.lpc_precond(x)
             g.profile(True)
             g.lpc_precond(x)
             ms, n, _, fl = g.profile_get("lpc")
-            print(f"learned preconditioner {cfg} bands={nb}: {ms:.3f} ms, {fl / max(ms, 1e-9) / 1e9:.1f} TFLOP/s")
+            print(f"learned preconditioner ({mode}) {cfg} bands={nb}: {ms:.3f} ms, "
+                  f"{fl / max(ms, 1e-9) / 1e9:.1f} TFLOP/s")
+            for part in ("lpc_layer1", "lpc_mid", "lpc_layer4"):
+                pms, _, pby, pfl = g.profile_get(part)
+                if pms > 0:
+                    print(f"  {part}: {pms:.3f} ms, {pby / pms / 1e6:.0f} GB/s, {pfl / pms / 1e9:.1f} TFLOP/s")
     else:
         raise SystemExit(f"unknown kernel family {what!r}")
 

@@ -116,6 +116,31 @@ def test_harvested_pairs_satisfy_screened_relation():
     assert np.all(np.isfinite(x)) and np.max(np.abs(x)) > 0.1
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["c0", "t1"])
+def test_tensor_core_inference_matches_fp32(name):
+    """The tensor-core application (BF16 activations, FP32 accumulation in TMEM) against the
+    FP32 CUDA-core one and against the oracle, on full periodic bands.  BF16 activations carry
+    8 significant bits, so the outputs agree to ~1e-2 of their scale (tested at 3e-2)."""
+    prob = synth.make_problem(name)
+    w = L.init_weights(13)
+    rng = np.random.default_rng(8)
+    g = rng.normal(size=(3, prob.ng)).astype(np.float32)
+    with api.BandUpdate(prob, precision=api.PREC_MIXED) as gpu:
+        gpu.lpc_set_weights(w)
+        gpu.lpc_inference(fp32=False)
+        tc = gpu.lpc_precond(g)
+        gpu.lpc_inference(fp32=True)
+        f32 = gpu.lpc_precond(g)
+    n1, n2, n3 = prob.n
+    rms = np.sqrt(np.mean(g.astype(np.float64) ** 2, axis=1))
+    ref = L.forward(w, (g / rms[:, None]).reshape(3, n3, n2, n1).astype(np.float64), True).reshape(3, -1) * rms[:, None]
+    scale = np.max(np.abs(ref))
+    assert np.max(np.abs(f32 - ref)) < 2e-5 * scale
+    assert np.max(np.abs(tc - ref)) < 3e-2 * scale
+    assert np.max(np.abs(tc - f32)) > 1e-6 * scale  # BF16 activations: a distinct computation
+
+
 def _sweeps_to(prob, pc, tol, weights=None, seed=21, maxsw=300):
     with api.BandUpdate(prob, precision=api.PREC_MIXED, pc_mode=pc) as g:
         if weights is not None:
