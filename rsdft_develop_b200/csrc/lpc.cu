@@ -471,8 +471,16 @@ __device__ __forceinline__ int wrapi(int a, int n) {
   return r < 0 ? r + n : r;
 }
 
+__device__ __forceinline__ int wrap1(int a, int n) { return a < 0 ? a + n : (a >= n ? a - n : a); }
+// hardware tanh (sm_75+ instruction; relative error ~5e-4, below the BF16 rounding of the result)
+__device__ __forceinline__ float tanh_fast(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 // Layer 1 (1 -> 16, tanh) on CUDA cores: x = g / rms(g) read from the FP32 band, written as
-// BF16 half-planes.  One thread per grid point.
+// BF16 half-planes.  A thread owns 4 consecutive x points (n1 a multiple of 4).
 __global__ void __launch_bounds__(256) k_tc_layer1(const float* __restrict__ g, const double* __restrict__ s2,
                                                    const __nv_bfloat16* __restrict__ w1, uint4* __restrict__ out,
                                                    int n1, int n2, int n3) {
@@ -484,34 +492,52 @@ __global__ void __launch_bounds__(256) k_tc_layer1(const float* __restrict__ g, 
   const double rms = sqrt(s2[b] / (double)ng);
   const float sc = rms > 0.0 ? (float)(1.0 / rms) : 0.f;
   const float* gb = g + (size_t)b * ng;
-  for (size_t pt = blockIdx.x * (size_t)blockDim.x + threadIdx.x; pt < ng; pt += (size_t)gridDim.x * blockDim.x) {
-    const int x = (int)(pt % n1), y = (int)((pt / n1) % n2), z = (int)(pt / ((size_t)n1 * n2));
-    float acc[16];
+  uint4* ob = out + (size_t)b * 2 * ng;
+  const int q1 = n1 / 4;
+  const size_t nq = ng / 4;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < nq; t += (size_t)gridDim.x * blockDim.x) {
+    const int xq = (int)(t % q1), y = (int)((t / q1) % n2), z = (int)(t / ((size_t)q1 * n2));
+    const int x0 = xq * 4;
+    float acc[4][16];
 #pragma unroll
-    for (int c = 0; c < 16; ++c) acc[c] = 0.f;
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int c = 0; c < 16; ++c) acc[i][c] = 0.f;
 #pragma unroll
     for (int kz = 0; kz < 3; ++kz)
 #pragma unroll
-      for (int ky = 0; ky < 3; ++ky)
+      for (int ky = 0; ky < 3; ++ky) {
+        const float* row = gb + ((size_t)wrap1(z + kz - 1, n3) * n2 + wrap1(y + ky - 1, n2)) * n1;
+        float v[6];
+        const float4 m = *reinterpret_cast<const float4*>(row + x0);
+        v[0] = __ldg(row + wrap1(x0 - 1, n1));
+        v[1] = m.x; v[2] = m.y; v[3] = m.z; v[4] = m.w;
+        v[5] = __ldg(row + wrap1(x0 + 4, n1));
 #pragma unroll
         for (int kx = 0; kx < 3; ++kx) {
-          const size_t q = ((size_t)wrapi(z + kz - 1, n3) * n2 + wrapi(y + ky - 1, n2)) * n1 + wrapi(x + kx - 1, n1);
-          const float v = __ldg(gb + q) * sc;
           const float* wt = ws + ((kz * 3 + ky) * 3 + kx) * 16;
 #pragma unroll
-          for (int c = 0; c < 16; ++c) acc[c] = fmaf(wt[c], v, acc[c]);
-        }
-    __align__(16) __nv_bfloat16 h[16];
+          for (int i = 0; i < 4; ++i) {
+            const float xv = v[i + kx] * sc;
 #pragma unroll
-    for (int c = 0; c < 16; ++c) h[c] = __float2bfloat16(tanhf(acc[c]));
-    uint4* ob = out + (size_t)b * 2 * ng;
-    ob[pt] = *reinterpret_cast<const uint4*>(h);
-    ob[ng + pt] = *reinterpret_cast<const uint4*>(h + 8);
+            for (int c = 0; c < 16; ++c) acc[i][c] = fmaf(wt[c], xv, acc[i][c]);
+          }
+        }
+      }
+    const size_t pt0 = ((size_t)z * n2 + y) * n1 + x0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      __align__(16) __nv_bfloat16 h[16];
+#pragma unroll
+      for (int c = 0; c < 16; ++c) h[c] = __float2bfloat16(tanh_fast(acc[i][c]));
+      ob[pt0 + i] = *reinterpret_cast<const uint4*>(h);
+      ob[ng + pt0 + i] = *reinterpret_cast<const uint4*>(h + 8);
+    }
   }
 }
 
 // Layer 4 (16 -> 1, linear) on CUDA cores from BF16 half-planes, times rms(g): the
-// preconditioned band.  One thread per grid point.
+// preconditioned band.  A thread owns 4 consecutive x points.
 __global__ void __launch_bounds__(256) k_tc_layer4(const uint4* __restrict__ in, const double* __restrict__ s2,
                                                    const __nv_bfloat16* __restrict__ w4, float* __restrict__ pg,
                                                    int n1, int n2, int n3) {
@@ -522,46 +548,66 @@ __global__ void __launch_bounds__(256) k_tc_layer4(const uint4* __restrict__ in,
   const int b = blockIdx.y;
   const float rms = (float)sqrt(s2[b] / (double)ng);
   const uint4* ib = in + (size_t)b * 2 * ng;
-  for (size_t pt = blockIdx.x * (size_t)blockDim.x + threadIdx.x; pt < ng; pt += (size_t)gridDim.x * blockDim.x) {
-    const int x = (int)(pt % n1), y = (int)((pt / n1) % n2), z = (int)(pt / ((size_t)n1 * n2));
-    float acc = 0.f;
+  const int q1 = n1 / 4;
+  const size_t nq = ng / 4;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < nq; t += (size_t)gridDim.x * blockDim.x) {
+    const int xq = (int)(t % q1), y = (int)((t / q1) % n2), z = (int)(t / ((size_t)q1 * n2));
+    const int x0 = xq * 4;
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
     for (int kz = 0; kz < 3; ++kz)
 #pragma unroll
-      for (int ky = 0; ky < 3; ++ky)
+      for (int ky = 0; ky < 3; ++ky) {
+        const size_t rb = ((size_t)wrap1(z + kz - 1, n3) * n2 + wrap1(y + ky - 1, n2)) * n1;
 #pragma unroll
-        for (int kx = 0; kx < 3; ++kx) {
-          const size_t q = ((size_t)wrapi(z + kz - 1, n3) * n2 + wrapi(y + ky - 1, n2)) * n1 + wrapi(x + kx - 1, n1);
-          const float* wt = ws + ((kz * 3 + ky) * 3 + kx) * 16;
+        for (int hh = 0; hh < 2; ++hh) {
+          const uint4* row = ib + (size_t)hh * ng + rb;
 #pragma unroll
-          for (int hh = 0; hh < 2; ++hh) {
-            const uint4 u = __ldg(ib + (size_t)hh * ng + q);
+          for (int j = 0; j < 6; ++j) {
+            const int xx = j == 0 ? wrap1(x0 - 1, n1) : (j == 5 ? wrap1(x0 + 4, n1) : x0 + j - 1);
+            const uint4 u = __ldg(row + xx);
             const __nv_bfloat16* hv = reinterpret_cast<const __nv_bfloat16*>(&u);
+            float a8[8];
 #pragma unroll
-            for (int c = 0; c < 8; ++c) acc = fmaf(wt[hh * 8 + c], __bfloat162float(hv[c]), acc);
+            for (int c = 0; c < 8; ++c) a8[c] = __bfloat162float(hv[c]);
+#pragma unroll
+            for (int kx = 0; kx < 3; ++kx) {
+              const int i = j - kx;  // output point fed by input j through tap kx
+              if (i >= 0 && i < 4) {
+                const float* wt = ws + ((kz * 3 + ky) * 3 + kx) * 16 + hh * 8;
+#pragma unroll
+                for (int c = 0; c < 8; ++c) acc[i] = fmaf(wt[c], a8[c], acc[i]);
+              }
+            }
           }
         }
-    pg[(size_t)b * ng + pt] = acc * rms;
+      }
+    *reinterpret_cast<float4*>(pg + (size_t)b * ng + ((size_t)z * n2 + y) * n1 + x0) =
+        make_float4(acc[0] * rms, acc[1] * rms, acc[2] * rms, acc[3] * rms);
   }
 }
 
 // Layers 2 and 3 (16 -> 16, tanh) on the tensor cores.  A CTA (4 warps) owns a 32 x 11 output
 // tile of x-rows over TC_TZ planes of one band.  Input planes (with a one-point periodic halo)
-// are staged into a ring of TC_SLOTS planes in the half-plane layout; for output plane z each
-// of the 27 taps is one tcgen05.mma per 128-row M-tile whose A descriptor is the staged plane
-// z + dz shifted by dy rows and dx points (rows of the M-tile are consecutive staged positions,
-// so the two halo columns of every row produce outputs that are discarded), B the tap's
-// 16 x 16 weights, D an FP32 accumulator of 16 TMEM columns.  The epilogue applies tanh and
-// writes BF16 half-planes.  All waits are bounded; a timeout sets *status.
+// arrive by bulk copies (TMA engine; contiguous row pieces in the half-plane layout) in a ring
+// of TC_SLOTS planes; for output plane z each of the 27 taps is one tcgen05.mma per 128-row
+// M-tile whose A descriptor is the staged plane z + dz shifted by dy rows and dx points (rows of
+// an M-tile are consecutive staged positions, so the two halo columns of every row produce
+// outputs that are discarded), B the tap's 16 x 16 weights, D an FP32 accumulator of 16 TMEM
+// columns.  Two accumulator sets let the MMAs of plane z+1 run during the epilogue (tanh,
+// BF16 half-planes) of plane z.  All waits are bounded; a timeout sets *status and every copy
+// in flight is waited for before the CTA exits.
 __global__ void __launch_bounds__(128) k_tc_mid(const uint4* __restrict__ in, const __nv_bfloat16* __restrict__ wp,
                                                 uint4* __restrict__ out, int n1, int n2, int n3, int tiles_x,
                                                 int tiles_y, int tiles_z, unsigned* status) {
   extern __shared__ __align__(128) unsigned char tsm[];
   constexpr int PLANE_BYTES = 2 * TC_PB * 16;
+  constexpr uint32_t STAGED_BYTES = 2u * TC_HY * TC_HX * 16u;
   unsigned char* ring = tsm;                                   // [slot][half][TC_PB][16 B]
   unsigned char* wsm = tsm + TC_SLOTS * PLANE_BYTES;           // [27][2][16][16 B]
-  uint64_t* done = reinterpret_cast<uint64_t*>(wsm + 27 * 512);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+  uint64_t* full = reinterpret_cast<uint64_t*>(wsm + 27 * 512);  // [TC_SLOTS]
+  uint64_t* done = full + TC_SLOTS;                              // [2]
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 2);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const size_t ng = (size_t)n1 * n2 * n3;
   int t = blockIdx.x;
@@ -573,93 +619,149 @@ __global__ void __launch_bounds__(128) k_tc_mid(const uint4* __restrict__ in, co
   const int band = blockIdx.y;
   const int x0 = bx * TC_TX, y0 = by * TC_TY, z0 = bz * TC_TZ;
   const int zend = min(z0 + TC_TZ, n3);
+  const int nplanes = zend - z0 + 2;  // staged planes z0-1 .. zend
   const uint4* ib = in + (size_t)band * 2 * ng;
   uint4* ob = out + (size_t)band * 2 * ng;
 
   for (int e = tid; e < 27 * 32; e += 128)
     reinterpret_cast<uint4*>(wsm)[e] = __ldg(reinterpret_cast<const uint4*>(wp) + e);
   if (tid == 0) {
-    mbar_init(done, 1);
+    for (int i = 0; i < TC_SLOTS; ++i) mbar_init(&full[i], 1);
+    mbar_init(&done[0], 1);
+    mbar_init(&done[1], 1);
     fence_mbar_init();
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
-                 "r"(64u));
+                 "r"(128u));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  // stage input plane z (periodic) into ring slot: position 1 + r * TC_HX + c holds point
-  // (x0 - 1 + c, y0 - 1 + r) for r < TC_HY, c < TC_HX
-  auto load_plane = [&](int z) {
-    unsigned char* pb = ring + (size_t)(((z % TC_SLOTS) + TC_SLOTS) % TC_SLOTS) * PLANE_BYTES;
-    const int zg = wrapi(z, n3);
-    for (int e = tid; e < 2 * TC_HY * TC_HX; e += 128) {
-      const int c = e % TC_HX, r = (e / TC_HX) % TC_HY, hh = e / (TC_HX * TC_HY);
-      const int gx = wrapi(x0 - 1 + c, n1), gy = wrapi(y0 - 1 + r, n2);
-      const uint4 v = __ldg(ib + (size_t)hh * ng + ((size_t)zg * n2 + gy) * n1 + gx);
-      reinterpret_cast<uint4*>(pb)[(size_t)hh * TC_PB + 1 + r * TC_HX + c] = v;
-    }
-  };
-  load_plane(z0 - 1);
-  load_plane(z0);
-  load_plane(z0 + 1);
-  fence_proxy_async_smem();
+  fence_proxy_async_smem();  // the weights were written through the generic proxy
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
-  // M = 128, N = 16, BF16 x BF16 -> FP32, both K-major
-  const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(16 >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
-  bool ok = true;
-  for (int z = z0; z < zend && ok; ++z) {
-    // planes z-1, z, z+1 are staged (and visible to the tensor cores)
-    if (tid == 0) {
-#pragma unroll 1
-      for (int mt = 0; mt < TC_NM; ++mt) {
-#pragma unroll 1
-        for (int tap = 0; tap < 27; ++tap) {
-          const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
-          const unsigned char* pb =
-              ring + (size_t)((((z + dz) % TC_SLOTS) + TC_SLOTS) % TC_SLOTS) * PLANE_BYTES;
-          const int row0 = 1 + TC_HX + mt * 128 + dy * TC_HX + dx;  // staged position of M row 0
-          const uint64_t da = umma_desc_nosw(smem_u32(pb + (size_t)row0 * 16), TC_PB * 16, 128);
-          const uint64_t db = umma_desc_nosw(smem_u32(wsm + tap * 512), 256, 128);
-          umma_bf16(tmem + (uint32_t)(mt * 16), da, db, idesc, tap > 0 ? 1u : 0u);
+
+  // thread 0: bulk-copy staged plane i (= z0 - 1 + i) into ring slot i % TC_SLOTS; position
+  // 1 + r * TC_HX + c holds point (x0 - 1 + c, y0 - 1 + r), copied as contiguous x pieces
+  int issued = 0;
+  auto issue_plane = [&]() {
+    const int i = issued++;
+    const int slot = i % TC_SLOTS;
+    unsigned char* pb = ring + (size_t)slot * PLANE_BYTES;
+    const int zg = wrapi(z0 - 1 + i, n3);
+    mbar_arrive_expect_tx(&full[slot], STAGED_BYTES);
+    for (int hh = 0; hh < 2; ++hh)
+      for (int r = 0; r < TC_HY; ++r) {
+        const int gy = wrapi(y0 - 1 + r, n2);
+        const uint4* src = ib + (size_t)hh * ng + ((size_t)zg * n2 + gy) * n1;
+        unsigned char* dst = pb + ((size_t)hh * TC_PB + 1 + (size_t)r * TC_HX) * 16;
+        int c = 0;
+        while (c < TC_HX) {
+          const int gx = wrapi(x0 - 1 + c, n1);
+          const int len = min(TC_HX - c, n1 - gx);
+          bulk_g2s(dst + (size_t)c * 16, src + gx, (uint32_t)len * 16u, &full[slot]);
+          c += len;
         }
       }
-      umma_commit(done);
+  };
+  int landed = 0;  // thread 0: planes 0 .. landed-1 have been observed complete (waited in order)
+  auto plane_ready = [&](int i) {
+    const bool r = mbar_wait_bounded(&full[i % TC_SLOTS], (uint32_t)((i / TC_SLOTS) & 1), TC_POLLS);
+    if (r) landed = i + 1;
+    return r;
+  };
+  // M = 128, N = 16, BF16 x BF16 -> FP32, both K-major
+  const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(16 >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+  // Descriptors are built once: a tap only moves the start address (16-byte units, one point
+  // of a half-plane), which the descriptor holds in its low 14 bits; every shared address here
+  // is below 2^18 bytes, so the additions never carry out of that field.
+  const uint64_t dring = umma_desc_nosw(smem_u32(ring), TC_PB * 16, 128);
+  const uint64_t dwts = umma_desc_nosw(smem_u32(wsm), 256, 128);
+  auto issue_mma = [&](int z) {  // thread 0; planes z-1, z, z+1 ready
+    const int buf = (z - z0) & 1;
+    const int s0 = (z - z0) % TC_SLOTS;  // slot of plane z - 1
+    uint64_t dpl[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) dpl[d] = dring + (uint64_t)(((s0 + d) % TC_SLOTS) * (PLANE_BYTES >> 4));
+#pragma unroll
+    for (int mt = 0; mt < TC_NM; ++mt) {
+#pragma unroll
+      for (int tap = 0; tap < 27; ++tap) {
+        const int dz = tap / 9, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+        const int row0 = 1 + TC_HX + mt * 128 + dy * TC_HX + dx;  // staged position of M row 0
+        umma_bf16(tmem + (uint32_t)(buf * 64 + mt * 16), dpl[dz] + (uint64_t)row0, dwts + (uint64_t)(tap * 32),
+                  idesc, tap > 0 ? 1u : 0u);
+      }
     }
-    // stage plane z+2 while the MMAs run: its ring slot held plane z-2, last read by the MMAs of
-    // plane z-1, which completed before the previous epilogue
-    if (z + 2 <= zend) load_plane(z + 2);
-    ok = mbar_wait_bounded(done, (uint32_t)((z - z0) & 1), TC_POLLS);
+    umma_commit(&done[buf]);
+  };
+  int mma_issued = 0, mma_waited = 0;  // thread 0: MMA groups committed / observed complete
+
+  bool ok = true;
+  if (tid == 0) {
+    for (int i = 0; i < TC_SLOTS && i < nplanes; ++i) issue_plane();
+    ok = plane_ready(0) && plane_ready(1) && plane_ready(2);
     tc_fence_after();
     if (ok) {
+      issue_mma(z0);
+      ++mma_issued;
+    }
+  }
+  for (int z = z0; z < zend; ++z) {
+    const int rel = z - z0;
+    if (tid == 0 && ok && z + 1 < zend) {
+      ok = plane_ready(rel + 3);  // plane z + 2 (issued while earlier planes were computed)
+      if (ok) {
+        issue_mma(z + 1);
+        ++mma_issued;
+      }
+    }
+    const bool waited = mbar_wait_bounded(&done[rel & 1], (uint32_t)((rel >> 1) & 1), TC_POLLS);
+    if (waited && tid == 0) mma_waited = rel + 1;
+    tc_fence_after();
+    if (waited && ok) {
+      // the MMAs of plane z have read plane z - 1: its slot takes plane z + 3
+      if (tid == 0 && issued < nplanes) issue_plane();
 #pragma unroll 1
       for (int mt = 0; mt < TC_NM; ++mt) {
         float v[16];
-        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(mt * 16), v);
+        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((rel & 1) * 64 + mt * 16), v);
         const int e = mt * 128 + warp * 32 + lane;  // output position from row 1, column 0
         const int r = e / TC_HX, cx = e % TC_HX;
         const int gx = x0 - 1 + cx, gy = y0 + r;
         if (r < TC_TY && cx >= 1 && cx <= TC_TX && gx < n1 && gy < n2) {
           __align__(16) __nv_bfloat16 hb[16];
 #pragma unroll
-          for (int cc = 0; cc < 16; ++cc) hb[cc] = __float2bfloat16(tanhf(v[cc]));
+          for (int cc = 0; cc < 16; ++cc) hb[cc] = __float2bfloat16(tanh_fast(v[cc]));
           const size_t pt = ((size_t)z * n2 + gy) * n1 + gx;
           ob[pt] = *reinterpret_cast<const uint4*>(hb);
           ob[ng + pt] = *reinterpret_cast<const uint4*>(hb + 8);
         }
       }
     }
-    fence_proxy_async_smem();  // plane z+2 written through the generic proxy, read by the next MMAs
     tc_fence_before();
-    if (__syncthreads_or(!ok)) ok = false;
+    // all reads of this accumulator set are done before the MMAs of plane z + 2 reuse it
+    const int bad = __syncthreads_or(!(waited && ok));
     tc_fence_after();
+    if (bad) {
+      ok = false;
+      break;
+    }
   }
-  if (!ok && tid == 0) atomicOr(status, DEV_WAIT_TIMEOUT);
+  if (tid == 0) {
+    if (!ok) atomicOr(status, DEV_WAIT_TIMEOUT);
+    // copies in flight and committed MMAs complete before the shared memory is released
+    // (only those not yet observed: a slot's barrier has moved on past the earlier phases)
+    bool drained = true;
+    for (int i = landed; i < issued; ++i) drained = plane_ready(i) && drained;
+    for (int m = mma_waited; m < mma_issued; ++m)
+      drained = mbar_wait_bounded(&done[m & 1], (uint32_t)((m >> 1) & 1), TC_POLLS) && drained;
+    if (!drained) atomicOr(status, DEV_WAIT_TIMEOUT);
+  }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64u));
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128u));
 }
 
 }  // namespace lpc
@@ -930,7 +1032,7 @@ static int lpc_apply_tc(Ctx& c, const float* g, float* pg, int nb) {
   lpc::k_tc_pack_w<<<27, 256, 0, c.stream>>>(g_lpc.w.as<float>() + lpc::woff(1), w2);
   lpc::k_tc_pack_w<<<27, 256, 0, c.stream>>>(g_lpc.w.as<float>() + lpc::woff(2), w3);
   c.launches += 2;
-  constexpr size_t smem = (size_t)lpc::TC_SLOTS * 2 * lpc::TC_PB * 16 + 27 * 512 + 16;
+  constexpr size_t smem = (size_t)lpc::TC_SLOTS * 2 * lpc::TC_PB * 16 + 27 * 512 + 8 * (lpc::TC_SLOTS + 2) + 16;
   static bool attr = false;
   if (!attr) {
     RS_CUDA(cudaFuncSetAttribute(lpc::k_tc_mid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -946,7 +1048,7 @@ static int lpc_apply_tc(Ctx& c, const float* g, float* pg, int nb) {
     const int nn = std::min(nbc, nb - b0);
     RS_CUDA(cudaMemsetAsync(g_lpc.s2.p, 0, sizeof(double) * nn, c.stream));
     lpc::k_rms<<<dim3(64, nn), 256, 0, c.stream>>>(g + (size_t)b0 * ng, g_lpc.s2.as<double>(), ng);
-    const unsigned pblk = (unsigned)std::min<size_t>((ng + 255) / 256, 4 * 148);
+    const unsigned pblk = (unsigned)std::min<size_t>((ng / 4 + 255) / 256, 8 * 148);
     const double pts = (double)ng * nn;
     {
       ProfScope pl(c, "lpc_layer1", 36.0 * pts, 2.0 * 27 * 16 * pts);
@@ -970,7 +1072,7 @@ static int lpc_apply_tc(Ctx& c, const float* g, float* pg, int nb) {
 
 int lpc_apply(Ctx& c, const float* g, float* pg, int nb) {
   RS_CHECK(g_lpc.ready, RSDFT_ERR_STATE, "learned preconditioner not initialised");
-  if (c.lpc_fp32 == 0) return lpc_apply_tc(c, g, pg, nb);
+  if (c.lpc_fp32 == 0 && c.p.n1 % 4 == 0) return lpc_apply_tc(c, g, pg, nb);
   const lpc::Dims d = make_dims(c.p.n1, c.p.n2, c.p.n3, 1);
   const size_t vol = c.ng;
   // band chunk so that activations stay within ~2 GiB
