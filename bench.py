@@ -202,6 +202,8 @@ def main():
     ap.add_argument("--sweeps-to-tol", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer (C ABI) solves (large configs)")
+    ap.add_argument("--gemm-terms", default="3,3",
+                    help="BF16 terms of the mixed overlap/Hsub and rotation contractions (2 or 3 each)")
     args = ap.parse_args()
     dist, rank, ws = _dist()
     if args.impl == "reference":
@@ -223,6 +225,8 @@ def main():
         pc = "learned" if (prec == api.PREC_MIXED and os.path.exists(wpath)) else "hprsdft"
     pc_mode = {"learned": api.PC_LEARNED, "hprsdft": api.PC_HPRSDFT, "none": api.PC_NONE}[pc]
     g = api.BandUpdate(prob, precision=prec, pc_mode=pc_mode)
+    terms = tuple(int(t) for t in args.gemm_terms.split(","))
+    g.gemm_terms(*terms)
     if pc == "learned":
         g.lpc_set_weights(np.load(wpath))
     mb_ref = mb_ref_of(prob.nband)
@@ -337,12 +341,13 @@ def main():
             "metric": METRIC, "value": t_solve, "unit": "s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": per_step, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.precision == "fp64" else "f32+bf16x3+f64",
+            "dtype": "f64" if args.precision == "fp64" else "f32+bf16x%d/x%d+f64" % terms,
             "data": "synthetic (seeded Gaussian V_loc, Gaussian s/p projectors, seeded psi0)",
             "config": {"workload": args.config, "grid": list(prob.n), "bands": prob.nband,
                        "atoms": prob.cfg.natom, "projectors": prob.nzlma, "precision": args.precision,
                        "pc": pc, "lpc_fallbacks": lpc_state[2] if pc == "learned" else None,
                        "lpc_weights": os.path.relpath(wpath, ROOT) if pc == "learned" else None,
+                       "gemm_terms": list(terms) if prec == api.PREC_MIXED else None,
                        "mb_ref": mb_ref, "sweeps_to_tol": iters, "final_res_max": res_max,
                        "l2": "inputs larger than L2 (psi >= 0.5 GB)", "parallelism": f"replicas x{ws}"},
             "gpu_launches": int(launches),

@@ -146,10 +146,17 @@ int rsdft_gpu_subspace_diag(int k, int s, double* esp);
 int rsdft_gpu_residual(int k, int s, double* esp, double* res);
 /* Preconditioner alone (precond_hprsdft): pgk = P gk; test entry. */
 int rsdft_gpu_precond_d(int k, const double* gk, double* pgk, int ld, int nb, int mem);
+/* The same on FP32 bands, as mixed-precision CG runs it: the mloop CG steps evaluated in the
+ * s-step (Krylov-basis) form, 3 mloop + 3 passes over the bands (mloop <= 4). */
+int rsdft_gpu_precond_f(int k, const float* gk, float* pgk, int ld, int nb, int mem);
+/* FP32 precond_hprsdft form: 1 (default) s-step, 0 the recurrence form of the FP64 path. */
+int rsdft_gpu_set_pc_form(int sstep);
 
 /* calc_sweep: up to nsweep iterations of CG -> GS -> SD over all (k, s); stops early when the
- * FP64 residual max over bands <= tol (tol <= 0: never).  iters receives the sweeps done;
- * esp/res (host, nband*nk*nspin, k-major after band) receive the final FP64 values. */
+ * FP64 residual max over bands <= tol (tol <= 0: never).  The FP64 residual is evaluated in
+ * the sweeps where CG's own residual of the bands it returned is within 30 x tol (and in the
+ * last).  iters receives the sweeps done; esp/res (host, nband*nk*nspin, k-major after band)
+ * receive the final FP64 values. */
 int rsdft_gpu_sweep(int nsweep, double tol, int* iters, double* esp, double* res);
 /* Convergence band set of rsdft_gpu_sweep: bands 1..mb_ref are judged (0: all bands), as the
  * reference's init_sweep(iconv_check, mb_ref, tol) does for its band and DOS drivers
@@ -219,6 +226,13 @@ long long rsdft_gpu_kernel_launches(void);
  * op 0: C = A B^T (A: m x k, B: n x k); op 1: X <- X V (X: m bands x k points, V: m x m).
  * err receives max|x3 - dgemm| / max|dgemm|.  No counterpart in the reference. */
 int rsdft_gpu_selftest_gemm(int m, int n, long long k, int op, double* err);
+/* BF16 terms per FP32 value in the mixed-precision tensor-core contractions (2 or 3 each):
+ * overlap_terms for S = dV Psi^T Psi and Hsub = dV Psi^T H Psi, rotation_terms for
+ * Psi <- Psi V.  Three terms (the default for both) keep about FP32 accuracy per product; two
+ * keep about 2^-16.  Two-term overlaps converge on small grids but leave the largest band
+ * residual of the 128^3 / 2048-band problem wandering between 1e-7 and 1e-4; two-term rotations
+ * stall the residual near 5e-9.  No counterpart in the reference. */
+int rsdft_gpu_set_gemm_terms(int overlap_terms, int rotation_terms);
 
 #ifdef __cplusplus
 }

@@ -50,8 +50,8 @@ EXPORTS = [
     "rsdft_gpu_set_wf_z", "rsdft_gpu_get_wf_z", "rsdft_gpu_random_wf", "rsdft_gpu_hamiltonian_d",
     "rsdft_gpu_hamiltonian_z", "rsdft_gpu_hamiltonian_f", "rsdft_gpu_hamiltonian_c",
     "rsdft_gpu_conjugate_gradient", "rsdft_gpu_gram_schmidt", "rsdft_gpu_subspace_diag",
-    "rsdft_gpu_residual", "rsdft_gpu_precond_d", "rsdft_gpu_sweep", "rsdft_gpu_profile",
-    "rsdft_gpu_profile_get", "rsdft_gpu_kernel_launches", "rsdft_gpu_selftest_gemm", "rsdft_gpu_init_sweep",
+    "rsdft_gpu_residual", "rsdft_gpu_precond_d", "rsdft_gpu_precond_f", "rsdft_gpu_set_pc_form", "rsdft_gpu_sweep", "rsdft_gpu_profile",
+    "rsdft_gpu_profile_get", "rsdft_gpu_kernel_launches", "rsdft_gpu_selftest_gemm", "rsdft_gpu_set_gemm_terms", "rsdft_gpu_init_sweep",
     "rsdft_gpu_hamiltonian_noalloc_d",
     "rsdft_gpu_lpc_init", "rsdft_gpu_lpc_set_weights", "rsdft_gpu_lpc_get_weights", "rsdft_gpu_lpc_forward",
     "rsdft_gpu_lpc_loss_grad", "rsdft_gpu_lpc_dataset", "rsdft_gpu_lpc_harvest", "rsdft_gpu_lpc_dataset_get",
@@ -106,8 +106,11 @@ def load_library(path: str = LIB_PATH):
         "rsdft_gpu_conjugate_gradient": [i, i, vp, vp], "rsdft_gpu_gram_schmidt": [i, i],
         "rsdft_gpu_subspace_diag": [i, i, vp], "rsdft_gpu_residual": [i, i, vp, vp],
         "rsdft_gpu_precond_d": [i, vp, vp, i, i, i],
+        "rsdft_gpu_precond_f": [i, vp, vp, i, i, i],
+        "rsdft_gpu_set_pc_form": [i],
         "rsdft_gpu_sweep": [i, d, C.POINTER(C.c_int), vp, vp],
         "rsdft_gpu_selftest_gemm": [i, i, C.c_longlong, i, C.POINTER(C.c_double)],
+        "rsdft_gpu_set_gemm_terms": [i, i],
         "rsdft_gpu_init_sweep": [i],
         "rsdft_gpu_hamiltonian_noalloc_d": [i, i, vp, vp, i, i],
         "rsdft_gpu_lpc_init": [C.c_ulonglong], "rsdft_gpu_lpc_set_weights": [vp, i],
@@ -291,6 +294,13 @@ class BandUpdate:
         _call(self.lib.rsdft_gpu_precond_d, k, _ptr(g), _ptr(out), self.prob.ng, g.shape[0], MEM_HOST)
         return out
 
+    def precond_f32(self, gk: np.ndarray, k: int = 1) -> np.ndarray:
+        """precond_hprsdft on FP32 bands (the mixed-precision CG's evaluation)."""
+        g = np.ascontiguousarray(np.atleast_2d(gk), np.float32)
+        out = np.zeros_like(g)
+        _call(self.lib.rsdft_gpu_precond_f, k, _ptr(g), _ptr(out), self.prob.ng, g.shape[0], MEM_HOST)
+        return out
+
     def conjugate_gradient(self, k: int = 1, s: int = 1):
         nb = self.nband(k)
         esp = np.zeros(nb)
@@ -424,6 +434,14 @@ class BandUpdate:
         e = C.c_double(0.0)
         _call(self.lib.rsdft_gpu_selftest_gemm, m, n, k, op, C.byref(e))
         return e.value
+
+    def pc_form(self, sstep: bool) -> None:
+        """FP32 precond_hprsdft evaluation: s-step (default) or the recurrence form."""
+        _call(self.lib.rsdft_gpu_set_pc_form, 1 if sstep else 0)
+
+    def gemm_terms(self, overlap: int, rotation: int) -> None:
+        """BF16 terms (2 or 3) of the mixed-precision overlap/Hsub and rotation contractions."""
+        _call(self.lib.rsdft_gpu_set_gemm_terms, overlap, rotation)
 
     def kernel_launches(self) -> int:
         return int(self.lib.rsdft_gpu_kernel_launches())

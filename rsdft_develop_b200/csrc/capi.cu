@@ -259,7 +259,7 @@ static void destroy(Ctx* c) {
   }
   for (auto e : c->event_pool) cudaEventDestroy(e);
   DBuf* bufs[] = {&c->vloc64, &c->vloc32, &c->ws_coef, &c->ws_io_a, &c->ws_io_b, &c->ws_cg, &c->ws_red,
-                  &c->ws_scal, &c->ws_dense, &c->ws_hpsi, &c->ws_rot, &c->ws_solver, &c->ws_info, &c->ws_gemm, &c->ws_out, &c->ws_f64,
+                  &c->ws_scal, &c->ws_dense, &c->ws_hpsi, &c->ws_flag, &c->ws_rot, &c->ws_solver, &c->ws_info, &c->ws_gemm, &c->ws_out, &c->ws_f64,
                   &c->nl.gofs, &c->nl.gjj, &c->nl.gplist, &c->nl.gD, &c->nl.rec_rowptr, &c->nl.rec_pt, &c->nl.rec_g};
   for (DBuf* b : bufs) b->release();
   for (auto& pk : c->nl.perk) {
@@ -542,26 +542,38 @@ int rsdft_gpu_hamiltonian_c(int k, int s, const float* tpsi, float* htpsi, int l
   return hamiltonian_entry<float>(k, s, tpsi, htpsi, ld, nb, mem, true);
 }
 
-int rsdft_gpu_precond_d(int k, const double* gk, double* pgk, int ld, int nb, int mem) {
+}  // extern "C"
+
+template <typename T>
+static int precond_entry(int k, const T* gk, T* pgk, int ld, int nb, int mem) {
   REQUIRE_CTX();
   Ctx& c = *g_ctx;
   RS_CHECK(!c.cplx, RSDFT_ERR_STATE, "real entry on a complex16 context");
   RS_CHECK(k >= 1 && k <= c.p.nk, RSDFT_ERR_ARG, "k out of range");
   RS_CHECK(gk && pgk && (size_t)ld >= c.ng && nb >= 0, RSDFT_ERR_ARG, "bad precond arguments");
   if (nb == 0) return 0;
-  const double* din;
+  const T* din;
   RS_TRY(stage_in(c, c.ws_io_a, gk, (size_t)ld, nb, mem, &din));
-  double* dout = pgk;
+  T* dout = pgk;
   if (mem == RSDFT_MEM_HOST) {
-    RS_TRY(c.ws_io_b.ensure(sizeof(double) * (size_t)ld * nb));
-    dout = c.ws_io_b.as<double>();
+    RS_TRY(c.ws_io_b.ensure(sizeof(T) * (size_t)ld * nb));
+    dout = c.ws_io_b.as<T>();
   }
-  RS_TRY(precond_real<double>(c, din, dout, (size_t)ld, nb));
+  RS_TRY(precond_real<T>(c, din, dout, (size_t)ld, nb));
   if (mem == RSDFT_MEM_HOST) {
-    RS_CUDA(cudaMemcpyAsync(pgk, dout, sizeof(double) * (size_t)ld * nb, cudaMemcpyDeviceToHost, c.stream));
+    RS_CUDA(cudaMemcpyAsync(pgk, dout, sizeof(T) * (size_t)ld * nb, cudaMemcpyDeviceToHost, c.stream));
     RS_CUDA(cudaStreamSynchronize(c.stream));
   }
   return check_status(c);
+}
+
+extern "C" {
+
+int rsdft_gpu_precond_d(int k, const double* gk, double* pgk, int ld, int nb, int mem) {
+  return precond_entry<double>(k, gk, pgk, ld, nb, mem);
+}
+int rsdft_gpu_precond_f(int k, const float* gk, float* pgk, int ld, int nb, int mem) {
+  return precond_entry<float>(k, gk, pgk, ld, nb, mem);
 }
 
 int rsdft_gpu_conjugate_gradient(int k, int s, double* esp, double* res) {
@@ -628,16 +640,23 @@ int rsdft_gpu_sweep(int nsweep, double tol, int* iters, double* esp, double* res
   double best = 1e300;
   int stall = 0;
   int it = 0;
+  std::vector<double> cg_res((size_t)nbmax);
   for (it = 1; it <= nsweep; ++it) {
-    double rmax = 0.0;
+    double rmax = 0.0, cg_rmax = 0.0;
     for (int s = 0; s < c.p.nspin; ++s)
       for (int k = 0; k < c.p.nk; ++k) {
         RS_CHECK(c.wfn(k, s).valid, RSDFT_ERR_STATE, "no wavefunctions resident for (k,s)=(%d,%d)", k + 1, s + 1);
-        RS_TRY(cg_run(c, k, s, nullptr, nullptr));
-        RS_TRY(gs_run(c, k, s, 1));
-        RS_TRY(sd_run(c, k, s, nullptr));
+        RS_TRY(cg_run(c, k, s, nullptr, cg_res.data()));
+        const int nconv = c.mb_ref > 0 ? std::min(c.mb_ref, c.kp[k].nband) : c.kp[k].nband;
+        for (int n = 0; n < nconv; ++n) cg_rmax = std::max(cg_rmax, cg_res[n]);
+        RS_TRY(gssd_run(c, k, s, nullptr, true));
       }
-    if (tol > 0.0 || it == nsweep) {
+    // The FP64 check (an FP64 H x of every band) runs once CG's own residual of the bands it
+    // returned is within kResGate x tol: before that the check cannot pass.  The learned-PC
+    // guard judges every sweep.
+    constexpr double kResGate = 30.0;
+    const bool judge = tol > 0.0 && (cg_rmax <= kResGate * tol || pc_effective(c) == RSDFT_PC_LEARNED);
+    if (judge || it == nsweep) {
       for (int s = 0; s < c.p.nspin; ++s)
         for (int k = 0; k < c.p.nk; ++k) {
           const int nb = c.kp[k].nband;
@@ -701,8 +720,24 @@ long long rsdft_gpu_kernel_launches(void) { return g_ctx ? g_ctx->launches : 0; 
 int rsdft_gpu_selftest_gemm(int m, int n, long long k, int op, double* err) {
   REQUIRE_CTX();
   RS_CHECK(m > 0 && n > 0 && k > 0 && err && (op == 0 || op == 1), RSDFT_ERR_ARG, "bad selftest arguments");
-  RS_TRY(selftest_gemm(*g_ctx, m, n, k, op, err));
+  RS_TRY(selftest_gemm(*g_ctx, m, n, k, op, op == 0 ? g_ctx->gemm_terms_sm : g_ctx->gemm_terms_rot, err));
   return check_status(*g_ctx);
+}
+
+int rsdft_gpu_set_pc_form(int sstep) {
+  REQUIRE_CTX();
+  RS_CHECK(sstep == 0 || sstep == 1, RSDFT_ERR_ARG, "sstep must be 0 or 1");
+  g_ctx->pc_sstep = sstep;
+  return 0;
+}
+
+int rsdft_gpu_set_gemm_terms(int overlap_terms, int rotation_terms) {
+  REQUIRE_CTX();
+  RS_CHECK((overlap_terms == 2 || overlap_terms == 3) && (rotation_terms == 2 || rotation_terms == 3), RSDFT_ERR_ARG,
+           "split terms must be 2 or 3");
+  g_ctx->gemm_terms_sm = overlap_terms;
+  g_ctx->gemm_terms_rot = rotation_terms;
+  return 0;
 }
 
 }  // extern "C"

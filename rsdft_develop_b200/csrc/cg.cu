@@ -28,7 +28,10 @@ constexpr int kPS = 8;  // partial slots per (band, chunk)
 
 enum Scal {
   S_E = 0, S_E1, S_RB, S_GKGK, S_RES, S_W, S_U1, S_U1I, S_U2, S_U2I, S_ACT, S_BETA, S_ACC,
-  S_RR0, S_RR1, S_PCA, S_PCB, S_PCACT, S_COUNT
+  S_RR0, S_RR1, S_PCA, S_PCB, S_PCACT,
+  S_MU0, S_MU7 = S_MU0 + 7,  // s-step preconditioner: moments <v0 | B^i v0>, i < 2 mloop
+  S_XI0, S_XI3 = S_XI0 + 3,  // s-step preconditioner: PG = G + sum_i xi_i B^i v0
+  S_COUNT
 };
 
 struct Blk {
@@ -346,7 +349,7 @@ __global__ void k_sc_solve2(Blk k, double dV) {
 }
 
 // residual growth guard (cg_module.f90:360-363)
-__global__ void k_sc_reject(Blk k, double dV) {
+__global__ void k_sc_reject(Blk k, double dV, int* rejected) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= k.nbb || SC(k, S_ACT, b) == 0.0) return;
   const double rb = sum_part(k, b, 0) * dV;
@@ -354,6 +357,7 @@ __global__ void k_sc_reject(Blk k, double dV) {
   if (rb / SC(k, S_RES, b) > 1.0e8) {
     SC(k, S_E, b) = SC(k, S_E1, b);
     SC(k, S_ACC, b) = 0.0;
+    atomicAdd(rejected, 1);  // x keeps its value while H x has moved on
   } else {
     SC(k, S_ACC, b) = 1.0;
   }
@@ -537,6 +541,102 @@ __global__ void k_pc_sc_beta(Blk k) {
   SC(k, S_PCB, b) = rr1 / SC(k, S_RR0, b);
 }
 
+// ---- s-step form of the same mloop CG steps (FP32 bands) ----
+// Every vector of the preconditioner's CG lies in the Krylov space of r0 = G - A G, so it is
+// evaluated in the basis v_i = B^i r0 (i < mloop), B = (A - c0 I) / c0 the off-diagonal part
+// of the 7-point operator scaled to spectrum [-1, 1] (A = c0 (B + I)), with every inner
+// product taken from the moments mu_j = <r0 | B^j r0>, j < 2 mloop.  The recurrence
+// (alpha, beta, the update of PG) then runs on coefficient vectors per band in FP64 and the
+// bands are touched in 3 mloop + 3 passes (12 for mloop = 3) instead of 26.
+
+// Vn = B V and partials <V|Vn>, <Vn|Vn>; WRITE = false: only <V|B V>.  qb holds B's
+// coefficients (c0 = 0).
+template <typename T, bool WRITE>
+__global__ void __launch_bounds__(kThreads) k_pcs_shift(Blk k, PcCoef qb, const T* __restrict__ V, T* __restrict__ Vn) {
+  if (SC(k, S_PCACT, blockIdx.y) == 0.0) return;
+  T s0 = T(0), s1 = T(0);
+  {
+    PC_ROWS_BEGIN(k, qb)
+    const T* vv = V + off;
+    const T w = (T)qb.c1 * (vv[j + xp] + vv[j + xm]) + (T)qb.c2 * (vv[j + yp] + vv[j + ym]) +
+                (T)qb.c3 * (vv[j + zp] + vv[j + zm]);
+    if (WRITE) Vn[off + j] = w;
+    s0 += vv[j] * w;
+    s1 += w * w;
+    PC_ROWS_END
+  }
+  double v[2] = {(double)s0, (double)s1};
+  block_partials<2>(v, k, blockIdx.y);
+}
+
+// after the shift pass that made v_i (i >= 1): mu_{2i-1}, mu_{2i}; after the read-only pass
+// (i = m): mu_{2m-1}, then the CG recurrence on coefficients, leaving xi_0 .. xi_{m-1}
+__global__ void k_pcs_sc(Blk k, int i, int m, double c0) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= k.nbb || SC(k, S_PCACT, b) == 0.0) return;
+  if (i == 0) {  // after k_pc_first
+    SC(k, S_MU0, b) = SC(k, S_RR1, b);
+    return;
+  }
+  SC(k, S_MU0 + 2 * i - 1, b) = sum_part(k, b, 0);
+  if (i < m) {
+    SC(k, S_MU0 + 2 * i, b) = sum_part(k, b, 1);
+    return;
+  }
+  double mu[8];
+  for (int j = 0; j < 2 * m; ++j) mu[j] = SC(k, S_MU0 + j, b);
+  double p[5] = {1.0, 0.0, 0.0, 0.0, 0.0}, r[5] = {1.0, 0.0, 0.0, 0.0, 0.0};
+  double xi[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, f[5];
+  double rr1 = mu[0], rr0;
+  for (int it = 1; it <= m; ++it) {
+    // f = A p = c0 (B p + p); p has degree it - 1, f degree it
+    for (int j = 0; j <= it; ++j) f[j] = c0 * ((j > 0 ? p[j - 1] : 0.0) + (j < it ? p[j] : 0.0));
+    double pAp = 0.0;
+    for (int a = 0; a < it; ++a)
+      for (int c = 0; c <= it; ++c) pAp += p[a] * f[c] * mu[a + c];
+    rr0 = rr1;
+    const double al = rr0 / pAp;
+    for (int j = 0; j < it; ++j) xi[j] += al * p[j];
+    if (it == m) break;
+    for (int j = 0; j <= it; ++j) r[j] -= al * f[j];
+    rr1 = 0.0;
+    for (int a = 0; a <= it; ++a)
+      for (int c = 0; c <= it; ++c) rr1 += r[a] * r[c] * mu[a + c];
+    const double be = rr1 / rr0;
+    for (int j = 0; j <= it; ++j) p[j] = r[j] + be * p[j];
+  }
+  for (int j = 0; j < m; ++j) SC(k, S_XI0 + j, b) = xi[j];
+}
+
+// PG = G + sum_{i < M} xi_i v_i (PG = G where the preconditioner is inactive), and the
+// partial <PG|G> that CG takes next (bands CG still updates)
+template <typename T, int M>
+__global__ void __launch_bounds__(kThreads) k_pcs_combine(Blk k, const T* __restrict__ G, const T* __restrict__ V0,
+                                                          const T* __restrict__ V1, const T* __restrict__ V2,
+                                                          const T* __restrict__ V3, T* __restrict__ PG) {
+  BAND_LOOP(k, 1);
+  const bool on = SC(k, S_PCACT, b) != 0.0;
+  T x[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) x[j] = (on && j < M) ? (T)SC(k, S_XI0 + j, b) : T(0);
+  double vt = 0.0;  // accumulated as k_dot does
+  for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) {
+    const T g = G[off + i];
+    T v = g;
+    if (on) {
+      v += x[0] * V0[off + i];
+      if (M > 1) v += x[1] * V1[off + i];
+      if (M > 2) v += x[2] * V2[off + i];
+      if (M > 3) v += x[3] * V3[off + i];
+    }
+    PG[off + i] = v;
+    vt += (double)v * (double)g;
+  }
+  if (SC(k, S_ACT, b) == 0.0) return;
+  double d[1] = {vt};
+  block_partials<1>(d, k, b);
+}
+
 // ---------------------------------------------------------------------------
 // host drivers
 // ---------------------------------------------------------------------------
@@ -560,8 +660,11 @@ static int pick_nch(size_t ng, int nbb) {
 // precond_hprsdft (cgpc_hprsdft_module.f90:133-270) on a band block: PG = G + sum_it a_it Q_it
 // for mloop CG steps on A x = G from x = G.  Buffers: X0 holds R0 = Q1, then X0/X1/X2 rotate
 // between the residual and the current/next directions; F = A Q.
+// *pg_dot: set when the partials of <PG|G> (bands with S_ACT set) were left in the partial
+// buffer by the last pass
 template <typename T>
-static int pc_block(Ctx& c, Blk& k, const T* G, T* PG, T* X0, T* X1, T* X2, T* F) {
+static int pc_block(Ctx& c, Blk& k, const T* G, T* PG, T* X0, T* X1, T* X2, T* F, bool* pg_dot = nullptr) {
+  if (pg_dot) *pg_dot = false;
   PcCoef q;
   const double* H = c.p.hgrid;
   q.c0 = c.p.ggg[0] / (H[0] * H[0]) + c.p.ggg[1] / (H[1] * H[1]) + c.p.ggg[2] / (H[2] * H[2]);
@@ -573,6 +676,33 @@ static int pc_block(Ctx& c, Blk& k, const T* G, T* PG, T* X0, T* X1, T* X2, T* F
   ProfScope ps(c, "pc");
   if (c.p.mloop < 1) {
     LAUNCH_E(k_copy<T>, G, PG);
+    return check_launch("pc");
+  }
+  if (std::is_same<T, float>::value && c.pc_sstep && c.p.mloop <= 4) {
+    // s-step form (FP32 bands): v0 = R0 in X0, v1 = B v0 in X1, v2 in X2, v3 in F
+    const int m = c.p.mloop;
+    PcCoef qb = q;
+    qb.c1 = q.c1 / q.c0;
+    qb.c2 = q.c2 / q.c0;
+    qb.c3 = q.c3 / q.c0;
+    qb.c0 = 0.0;
+    T* v[4] = {X0, X1, X2, F};
+    LAUNCH_E(k_pc_first<T>, q, G, X0);
+    LAUNCH_S(k_pc_sc_first);
+    LAUNCH_S(k_pcs_sc, 0, m, q.c0);
+    for (int i = 1; i < m; ++i) {
+      LAUNCH_E((k_pcs_shift<T, true>), qb, v[i - 1], v[i]);
+      LAUNCH_S(k_pcs_sc, i, m, q.c0);
+    }
+    LAUNCH_E((k_pcs_shift<T, false>), qb, v[m - 1], v[m - 1]);
+    LAUNCH_S(k_pcs_sc, m, m, q.c0);
+    switch (m) {
+      case 1: LAUNCH_E((k_pcs_combine<T, 1>), G, v[0], v[1], v[2], v[3], PG); break;
+      case 2: LAUNCH_E((k_pcs_combine<T, 2>), G, v[0], v[1], v[2], v[3], PG); break;
+      case 3: LAUNCH_E((k_pcs_combine<T, 3>), G, v[0], v[1], v[2], v[3], PG); break;
+      default: LAUNCH_E((k_pcs_combine<T, 4>), G, v[0], v[1], v[2], v[3], PG); break;
+    }
+    if (pg_dot) *pg_dot = true;
     return check_launch("pc");
   }
   LAUNCH_E(k_pc_first<T>, q, G, X0);
@@ -639,9 +769,19 @@ static int cg_block_run(Ctx& c, int kk, int s, double* h_esp, double* h_res) {
   const int nb = c.kp[kk].nband;
   const size_t nreal = c.ng * NC;
   int nbb = c.p.cg_block > 0 ? std::min(c.p.cg_block, nb) : nb;
+  // real build: H x of all bands lives in ws_hpsi, where the fused GS/SD step that follows in
+  // the sweep finds it; the other eight vectors per band are block workspace
+  c.cg_hx_ready = false;
+  T* HXall = nullptr;
+  if (NC == 1) {
+    RS_TRY(c.ws_hpsi.ensure(sizeof(T) * nreal * (size_t)nb));
+    HXall = c.ws_hpsi.as<T>();
+  }
+  RS_TRY(c.ws_flag.ensure(sizeof(int) * 4));
+  RS_CUDA(cudaMemsetAsync(c.ws_flag.p, 0, sizeof(int), c.stream));
   size_t freeb = 0, totb = 0;
   cudaMemGetInfo(&freeb, &totb);
-  const size_t per_band = 9 * nreal * sizeof(T);
+  const size_t per_band = (HXall ? 8 : 9) * nreal * sizeof(T);
   const size_t budget = (size_t)(0.4 * (double)(freeb + c.ws_cg.bytes));
   if (c.p.cg_block <= 0)
     while (nbb > 1 && (size_t)nbb * per_band > budget) nbb = (nbb + 1) / 2;
@@ -654,8 +794,8 @@ static int cg_block_run(Ctx& c, int kk, int s, double* h_esp, double* h_res) {
   k.sc = c.ws_scal.as<double>();
   k.part = c.ws_red.as<double>();
   T* base = c.ws_cg.as<T>();
-  T* HX = base;
-  T* HP = HX + nreal * nbb;
+  T* HX = HXall ? nullptr : base;
+  T* HP = HXall ? base : HX + nreal * nbb;
   T* G = HP + nreal * nbb;
   T* PG = G + nreal * nbb;
   T* P = PG + nreal * nbb;
@@ -673,6 +813,7 @@ static int cg_block_run(Ctx& c, int kk, int s, double* h_esp, double* h_res) {
     k.nbb = nn;
     k.nch = pick_nch(nreal, nn);
     T* X = psi + (size_t)b0 * nreal;
+    if (HXall) HX = HXall + (size_t)b0 * nreal;
     RS_TRY(hpsi_any<T>(c, kk, s, X, HX, nreal, nn));
     {
       ProfScope ps(c, "cg");
@@ -688,17 +829,18 @@ static int cg_block_run(Ctx& c, int kk, int s, double* h_esp, double* h_res) {
       }
       if (icg == c.p.ncg + 1) break;
       const int pcm = pc_effective(c);
+      bool pg_dot = false;  // <PG|G> partials already formed by the preconditioner's last pass
       if (pcm == RSDFT_PC_NONE) {
         ProfScope ps(c, "cg");
         LAUNCH_E(k_copy<T>, G, PG);
       } else if (pcm == RSDFT_PC_LEARNED && std::is_same<T, float>::value && NC == 1) {
         RS_TRY(lpc_apply(c, reinterpret_cast<const float*>(G), reinterpret_cast<float*>(PG), nn));
       } else {
-        RS_TRY(pc_block<T>(c, k, G, PG, R, Q, Q2, F));
+        RS_TRY(pc_block<T>(c, k, G, PG, R, Q, Q2, F, &pg_dot));
       }
       {
         ProfScope ps(c, "cg");
-        LAUNCH_E(k_dot<T>, PG, G, (int)S_ACT);
+        if (!pg_dot) LAUNCH_E(k_dot<T>, PG, G, (int)S_ACT);
         LAUNCH_S(k_sc_beta, dV, icg == 1 ? 1 : 0);
         LAUNCH_E(k_make_p<T>, PG, P, icg == 1 ? 1 : 0);
       }
@@ -708,7 +850,7 @@ static int cg_block_run(Ctx& c, int kk, int s, double* h_esp, double* h_res) {
         LAUNCH_E((k_dots6<T, NC>), X, P, HX, HP);
         LAUNCH_S(k_sc_solve2<NC>, dV);
         LAUNCH_E((k_update_hg<T, NC>), X, P, HX, HP, G, gfac);
-        LAUNCH_S(k_sc_reject, dV);
+        LAUNCH_S(k_sc_reject, dV, c.ws_flag.as<int>());
         LAUNCH_E((k_update_x<T, NC>), X, P);
       }
     }
@@ -724,6 +866,11 @@ static int cg_block_run(Ctx& c, int kk, int s, double* h_esp, double* h_res) {
       if (h_esp) std::memcpy(h_esp + b0, hE.data(), sizeof(double) * nn);
       if (h_res) std::memcpy(h_res + b0, hR.data(), sizeof(double) * nn);
     }
+  }
+  if (HXall) {
+    c.cg_hx_ready = true;
+    c.cg_hx_k = kk;
+    c.cg_hx_s = s;
   }
   return 0;
 }

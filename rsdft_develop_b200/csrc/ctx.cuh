@@ -87,7 +87,10 @@ struct Ctx {
   DBuf ws_red;                     // reduction partials
   DBuf ws_scal;                    // per-band scalars (double)
   DBuf ws_dense;                   // M x M matrices
-  DBuf ws_hpsi;                    // H psi for subspace diag (nb x ng)
+  DBuf ws_hpsi;                    // H psi of all bands (nb x ng): CG's running H x, subspace diag
+  DBuf ws_flag;                    // device counters (CG line-search rejections)
+  bool cg_hx_ready = false;        // ws_hpsi holds H x of every band of (cg_hx_k, cg_hx_s) after CG
+  int cg_hx_k = -1, cg_hx_s = -1;
   DBuf ws_rot;                     // rotation / GS temporaries
   DBuf ws_solver;                  // cusolver workspace
   DBuf ws_info;                    // cusolver info
@@ -100,6 +103,9 @@ struct Ctx {
   int pc_cur = 0;                  // preconditioner in use by CG (pc_mode, or its fallback)
   int lpc_fallbacks = 0;           // sweeps-level switches from the learned to the plain PC
   int lpc_fp32 = 0;                // learned PC inference: 0 tensor cores (BF16 activations), 1 FP32 CUDA cores
+  int gemm_terms_sm = 3;           // BF16 terms of the overlap / Hsub contractions (mixed precision)
+  int gemm_terms_rot = 3;          // BF16 terms of the band rotations (mixed precision)
+  int pc_sstep = 1;                // FP32 precond_hprsdft in s-step form (0: the recurrence form)
 
   // profiling
   bool profiling = false;
@@ -157,13 +163,16 @@ int precond_real(Ctx& c, const T* g, T* pg, size_t ld, int nb);
 // ---- dense ----
 int gs_run(Ctx& c, int k, int s, int passes);
 int sd_run(Ctx& c, int k, int s, double* h_esp);
+int gssd_run(Ctx& c, int k, int s, double* h_esp, bool use_cg_hx);  // fused GS + SD of the sweep
 int residual_run(Ctx& c, int k, int s, double* d_esp, double* d_res);
 
 // ---- split-BF16 tensor-core GEMMs (gemm_x3.cu) ----
 int gemm_tn_x3(Ctx& c, const float* A, long long lda, int M, const float* B, long long ldb, int N, long long K,
-               double alpha, double* C, long long ldc, int swapB);
-int gemm_rotate_x3(Ctx& c, float* X, long long ldx, int nb, long long G, const double* V, int ldv);
-int selftest_gemm(Ctx& c, int m, int n, long long k, int op, double* err);
+               double alpha, double* C, long long ldc, int swapB, int terms);
+int gemm_tn2_x3(Ctx& c, const float* X, const float* Y, long long ld, int nb, long long K, double alpha, double* S,
+                double* M, int terms);
+int gemm_rotate_x3(Ctx& c, float* X, long long ldx, int nb, long long G, const double* V, int ldv, int terms);
+int selftest_gemm(Ctx& c, int m, int n, long long k, int op, int terms, double* err);
 
 // ---- util ----
 int random_wf(Ctx& c, int k, int s, uint64_t seed);

@@ -147,7 +147,8 @@ static int gs_mixed_real(Ctx& c, int k, int s, int passes) {
   for (int pass = 0; pass < std::max(1, passes); ++pass) {
     RS_CUDA(cudaMemsetAsync(S, 0, sizeof(double) * (size_t)nb * nb, c.stream));
     // S[m][n] = dV sum_g X[m][g] X[n][g] (symmetric, row/column major alike)
-    RS_TRY(gemm_tn_x3(c, X, (long long)c.ng, nb, X, (long long)c.ng, nb, (long long)c.ng, c.p.dv, S, nb, 0));
+    RS_TRY(gemm_tn_x3(c, X, (long long)c.ng, nb, X, (long long)c.ng, nb, (long long)c.ng, c.p.dv, S, nb, 0,
+                      c.gemm_terms_sm));
     {
       ProfScope ps(c, "gs");
       RS_CUSOLVER(cusolverDnDpotrf(c.cusolver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, c.ws_solver.as<double>(), lwork,
@@ -161,7 +162,7 @@ static int gs_mixed_real(Ctx& c, int k, int s, int passes) {
                             nb, &one, S, nb, Ri, nb));
     }
     // X <- X R^-1
-    RS_TRY(gemm_rotate_x3(c, X, (long long)c.ng, nb, (long long)c.ng, Ri, nb));
+    RS_TRY(gemm_rotate_x3(c, X, (long long)c.ng, nb, (long long)c.ng, Ri, nb, c.gemm_terms_rot));
   }
   return 0;
 }
@@ -178,11 +179,12 @@ static int sd_mixed_real(Ctx& c, int k, int s, double* h_esp) {
   double* W = H + (size_t)nb * nb;
   RS_CUDA(cudaMemsetAsync(H, 0, sizeof(double) * (size_t)nb * nb, c.stream));
   // H[m][n] = dV sum_g X[m][g] (HX)[n][g]; Hsub = (H + H^T)/2 = 1/2 dV (X^T HX + HX^T X)
-  RS_TRY(gemm_tn_x3(c, X, (long long)c.ng, nb, HX, (long long)c.ng, nb, (long long)c.ng, c.p.dv, H, nb, 0));
+  RS_TRY(gemm_tn_x3(c, X, (long long)c.ng, nb, HX, (long long)c.ng, nb, (long long)c.ng, c.p.dv, H, nb, 0,
+                      c.gemm_terms_sm));
   k_symmetrize<<<64, 256, 0, c.stream>>>(H, nb);
   c.launches++;
   RS_TRY(eig_solve(c, nb, H, W));
-  RS_TRY(gemm_rotate_x3(c, X, (long long)c.ng, nb, (long long)c.ng, H, nb));
+  RS_TRY(gemm_rotate_x3(c, X, (long long)c.ng, nb, (long long)c.ng, H, nb, c.gemm_terms_rot));
   if (h_esp) {
     RS_CUDA(cudaMemcpyAsync(h_esp, W, sizeof(double) * nb, cudaMemcpyDeviceToHost, c.stream));
     RS_CUDA(cudaStreamSynchronize(c.stream));
@@ -289,6 +291,104 @@ int sd_run(Ctx& c, int k, int s, double* h_esp) {
     RS_CUDA(cudaStreamSynchronize(c.stream));
   }
   return f64_commit(c, k, s, v);
+}
+
+// One Gram-Schmidt + subspace_diag step of the sweep (real build) as a Cholesky-Rayleigh-Ritz
+// with a single rotation: S = dV X^T X, M = dV X^T (H X), S = R^T R, Hsub = R^-T M R^-1 =
+// V diag(e) V^T, X <- X (R^-1 V).  In exact arithmetic this is gram_schmidt (the Q factor of
+// X = Q R, src/gram_schmidt/gram_schmidt_t_module.f90:85-308) followed by subspace_diag_la
+// (src/subspace_diag/subspace_diag_la_module.f90:18-223): H is linear, so H (X R^-1) =
+// (H X) R^-1 and Hsub of the orthonormalised block is R^-T M R^-1; the orthonormalised block is
+// never formed, which saves one of the four ng x nb x nb contractions per sweep.
+int gssd_run(Ctx& c, int k, int s, double* h_esp, bool use_cg_hx) {
+  if (c.cplx) {
+    RS_TRY(gs_run(c, k, s, 1));
+    return sd_run(c, k, s, h_esp);
+  }
+  const int nb = c.kp[k].nband;
+  const int ng = (int)c.ng;
+  RS_TRY(c.ws_dense.ensure(sizeof(double) * (3 * (size_t)nb * nb + nb)));
+  RS_TRY(c.ws_info.ensure(sizeof(int) * 4));
+  double* S = c.ws_dense.as<double>();
+  double* M = S + (size_t)nb * nb;
+  double* T = M + (size_t)nb * nb;
+  double* W = T + (size_t)nb * nb;
+  const double dV = c.p.dv, zero = 0.0, one = 1.0;
+  F64View v;
+  float* X32 = nullptr;
+  // H X of the bands as CG left them (kept up to date by its line-search updates), when the
+  // CG that just ran covered every band of (k, s) in one array and rejected no step
+  bool reuse = use_cg_hx && c.cg_hx_ready && c.cg_hx_k == k && c.cg_hx_s == s &&
+               c.ws_hpsi.bytes >= (c.mixed ? sizeof(float) : sizeof(double)) * c.ng * nb;
+  c.cg_hx_ready = false;
+  if (reuse) {
+    int rejected = 0;
+    RS_CUDA(cudaMemcpyAsync(&rejected, c.ws_flag.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    RS_CUDA(cudaStreamSynchronize(c.stream));
+    reuse = rejected == 0;
+  }
+  if (c.mixed) {
+    X32 = c.wfn(k, s).psi.as<float>();
+    RS_TRY(c.ws_hpsi.ensure(sizeof(float) * c.ng * nb));
+    float* HX = c.ws_hpsi.as<float>();
+    if (!reuse) RS_TRY(hpsi_real<float>(c, k, s, X32, HX, c.ng, nb));
+    RS_CUDA(cudaMemsetAsync(S, 0, sizeof(double) * 2 * (size_t)nb * nb, c.stream));
+    RS_TRY(gemm_tn2_x3(c, X32, HX, (long long)c.ng, nb, (long long)c.ng, dV, S, M, c.gemm_terms_sm));
+  } else {
+    RS_TRY(f64_view(c, k, s, v));
+    RS_TRY(c.ws_hpsi.ensure(sizeof(double) * c.ng * nb));
+    double* HX = c.ws_hpsi.as<double>();
+    if (!reuse) RS_TRY(hpsi_real<double>(c, k, s, v.x, HX, c.ng, nb));
+    ProfScope ps(c, "sd_gemm", 0.0, 2.0 * 2.0 * c.ng * (double)nb * nb);
+    RS_CUBLAS(cublasDsyrk(c.cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, nb, ng, &dV, v.x, ng, &zero, S, nb));
+    RS_CUBLAS(cublasDgemm(c.cublas, CUBLAS_OP_T, CUBLAS_OP_N, nb, nb, ng, &dV, v.x, ng, HX, ng, &zero, M, nb));
+  }
+  {
+    ProfScope ps(c, "gs");
+    k_symmetrize<<<64, 256, 0, c.stream>>>(M, nb);
+    c.launches++;
+    int lwork = 0;
+    RS_CUSOLVER(cusolverDnDpotrf_bufferSize(c.cusolver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, &lwork));
+    RS_TRY(c.ws_solver.ensure(sizeof(double) * (size_t)std::max(lwork, 1)));
+    RS_CUSOLVER(cusolverDnDpotrf(c.cusolver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, c.ws_solver.as<double>(), lwork,
+                                 c.ws_info.as<int>()));
+    int info = 0;
+    RS_TRY(read_info(c, c.ws_info.as<int>(), &info));
+    RS_CHECK(info == 0, RSDFT_ERR_NOT_SPD, "overlap matrix not positive definite (potrf info=%d)", info);
+    // T <- R^-1 (upper triangle of S holds R)
+    k_identity<<<64, 256, 0, c.stream>>>(T, nb);
+    c.launches++;
+    RS_CUBLAS(cublasDtrsm(c.cublas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, nb, nb,
+                          &one, S, nb, T, nb));
+    // S <- M R^-1 ; M <- R^-T (M R^-1) = Hsub
+    RS_CUBLAS(cublasDgemm(c.cublas, CUBLAS_OP_N, CUBLAS_OP_N, nb, nb, nb, &one, M, nb, T, nb, &zero, S, nb));
+    RS_CUBLAS(cublasDgemm(c.cublas, CUBLAS_OP_T, CUBLAS_OP_N, nb, nb, nb, &one, T, nb, S, nb, &zero, M, nb));
+    k_symmetrize<<<64, 256, 0, c.stream>>>(M, nb);
+    c.launches++;
+  }
+  RS_TRY(eig_solve(c, nb, M, W));
+  // S <- R^-1 V: the single rotation
+  RS_CUBLAS(cublasDgemm(c.cublas, CUBLAS_OP_N, CUBLAS_OP_N, nb, nb, nb, &one, T, nb, M, nb, &zero, S, nb));
+  if (c.mixed) {
+    RS_TRY(gemm_rotate_x3(c, X32, (long long)c.ng, nb, (long long)c.ng, S, nb, c.gemm_terms_rot));
+  } else {
+    ProfScope ps(c, "sd_rot", 0.0, 2.0 * c.ng * (double)nb * nb);
+    size_t ch = std::max<size_t>(1024, (size_t)(256u << 20) / (sizeof(double) * (size_t)nb));
+    ch = std::min<size_t>(ch, c.ng);
+    RS_TRY(c.ws_rot.ensure(sizeof(double) * ch * nb));
+    for (size_t g0 = 0; g0 < c.ng; g0 += ch) {
+      const int m = (int)std::min(ch, c.ng - g0);
+      RS_CUBLAS(cublasDgemm(c.cublas, CUBLAS_OP_N, CUBLAS_OP_N, m, nb, nb, &one, v.x + g0, ng, S, nb, &zero,
+                            c.ws_rot.as<double>(), m));
+      RS_CUDA(cudaMemcpy2DAsync(v.x + g0, sizeof(double) * c.ng, c.ws_rot.p, sizeof(double) * m,
+                                sizeof(double) * m, nb, cudaMemcpyDeviceToDevice, c.stream));
+    }
+  }
+  if (h_esp) {
+    RS_CUDA(cudaMemcpyAsync(h_esp, W, sizeof(double) * nb, cudaMemcpyDeviceToHost, c.stream));
+    RS_CUDA(cudaStreamSynchronize(c.stream));
+  }
+  return c.mixed ? 0 : f64_commit(c, k, s, v);
 }
 
 }  // namespace rsdft

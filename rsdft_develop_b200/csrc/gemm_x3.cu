@@ -1,11 +1,12 @@
-// Split-BF16 (3-term) GEMMs on the 5th-generation tensor cores (tcgen05, sm_100a).
+// Split-BF16 GEMMs on the 5th-generation tensor cores (tcgen05, sm_100a).
 //
 // Each FP32 (or FP64) operand value x is split into three BF16 terms
 //   x0 = bf16(x), x1 = bf16(x - x0), x2 = bf16(x - x0 - x1)
 // and a product a*b is formed from the six leading cross terms
 //   a0b0 + a0b1 + a1b0 + a0b2 + a1b1 + a2b0
 // accumulated in FP32 in tensor memory (about FP32 accuracy; the dropped terms are
-// O(2^-24) relative).  Split-K partial tiles are added into FP64 results.
+// O(2^-24) relative).  Split-K partial tiles are added into FP64 results.  With two terms
+// (x0, x1; products a0b0 + a0b1 + a1b0) each product is good to about 2^-16 relative.
 //
 // Dense band-space work of the band update that runs through here in mixed precision:
 //   overlap  S = dV Psi^T Psi (Gram-Schmidt, gram_schmidt_t_module.f90 / CholQR S),
@@ -13,10 +14,11 @@
 //   rotation Psi <- Psi V        (subspace_diag_la_module.f90:190; GS: Psi <- Psi R^-1).
 //
 // Kernel structure: one CTA computes a 128 x BN output tile over a K range.  Warp 0 (one
-// elected lane) streams the six operand planes of each 64-wide K block into shared memory
-// with 3-D TMA tile loads (128B swizzle, zero fill past the matrix edge) through an S-deep
-// mbarrier ring; warp 1 (one elected lane) issues 24 tcgen05.mma (6 term pairs x 4 K=16
-// steps) per block into a 128 x BN FP32 accumulator in tensor memory and releases each
+// elected lane) streams the 2T operand planes (T terms of A and of B) of each 64-wide K block
+// into shared memory with 3-D TMA tile loads (128B swizzle, zero fill past the matrix edge)
+// through an S-deep mbarrier ring; warp 1 (one elected lane) issues 4 x (6 or 3) tcgen05.mma
+// (term pairs x 4 K=16 steps) per block into a 128 x BN FP32 accumulator in tensor memory and
+// releases each
 // stage with tcgen05.commit; after the last block all four warps read their 32 TMEM lanes
 // with tcgen05.ld and write the tile.  Every wait is bounded: a timeout sets the device
 // status word, drains, frees the tensor memory and returns.
@@ -86,7 +88,9 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
 
 struct Out {
   int mode;        // 0: C[m][n] += alpha * D (FP64 atomics); 1: Y[n*ldy + m] = D (FP32 store)
-  double* C;
+  double* C;       // columns n < nsplit (mode 0)
+  double* C2;      // columns n >= nsplit go to C2[m][n - nsplit] (mode 0)
+  int nsplit;
   long long ldc;
   double alpha;
   float* Y;
@@ -94,14 +98,15 @@ struct Out {
   int M, N;        // valid extents
 };
 
-// A: 3 planes of [M][K], B: 3 planes of [N][K], bf16, K-major.  grid = (mtiles, ntiles, ksplit).
-template <int BN, int S>
+// A: T planes of [M][K], B: T planes of [N][K], bf16, K-major.  grid = (mtiles, ntiles, ksplit).
+template <int BN, int S, int T>
 __global__ void __launch_bounds__(kThreads, 1) k_gemm_x3(const __grid_constant__ CUtensorMap ta,
                                                         const __grid_constant__ CUtensorMap tb, int kblocks_total,
                                                         int kblocks_per_split, Out o, unsigned* status) {
   constexpr int A_BYTES = BM * BK * 2;       // one plane tile, 16 KB
   constexpr int B_BYTES = BN * BK * 2;
-  constexpr int STAGE = 3 * A_BYTES + 3 * B_BYTES;
+  constexpr int STAGE = T * A_BYTES + T * B_BYTES;
+  constexpr int NP = T == 3 ? 6 : 3;  // term pairs formed
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // 1024-byte alignment of every tile (swizzle atoms)
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -147,8 +152,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_x3(const __grid_constant__
         unsigned char* st = smem + s * STAGE;
         mbar_arrive_expect_tx(&full[s], (uint32_t)STAGE);
         const int kx = (kb0 + i) * BK;
-        for (int t = 0; t < 3; ++t) tma_load_3d(st + t * A_BYTES, &ta, kx, m0, t, &full[s]);
-        for (int t = 0; t < 3; ++t) tma_load_3d(st + 3 * A_BYTES + t * B_BYTES, &tb, kx, n0, t, &full[s]);
+        for (int t = 0; t < T; ++t) tma_load_3d(st + t * A_BYTES, &ta, kx, m0, t, &full[s]);
+        for (int t = 0; t < T; ++t) tma_load_3d(st + T * A_BYTES + t * B_BYTES, &tb, kx, n0, t, &full[s]);
       }
     } else if (warp == 1 && lane == 0) {
       // MMA issuer: M=128, N=BN, bf16 x bf16 -> f32, both K-major
@@ -166,9 +171,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_x3(const __grid_constant__
 #pragma unroll
         for (int kk = 0; kk < BK / 16; ++kk) {
 #pragma unroll
-          for (int p = 0; p < 6; ++p) {
+          for (int p = 0; p < NP; ++p) {
             const uint64_t da = sw128_desc(st + ta_[p] * A_BYTES) + (uint64_t)(kk * 2);
-            const uint64_t db = sw128_desc(st + 3 * A_BYTES + tb_[p] * B_BYTES) + (uint64_t)(kk * 2);
+            const uint64_t db = sw128_desc(st + T * A_BYTES + tb_[p] * B_BYTES) + (uint64_t)(kk * 2);
             mma_bf16(tmem, da, db, idesc, (i > 0 || kk > 0 || p > 0) ? 1u : 0u);
           }
         }
@@ -197,7 +202,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_x3(const __grid_constant__
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
             const int col = n0 + c0 + j;
-            if (col < o.N) atomicAdd(o.C + (long long)row * o.ldc + col, o.alpha * (double)v[j]);
+            if (col < o.N) {
+              double* dst = col < o.nsplit ? o.C + (long long)row * o.ldc + col
+                                           : o.C2 + (long long)row * o.ldc + (col - o.nsplit);
+              atomicAdd(dst, o.alpha * (double)v[j]);
+            }
           }
         } else {
 #pragma unroll
@@ -226,9 +235,8 @@ __device__ __forceinline__ void split3(double x, __nv_bfloat16& a, __nv_bfloat16
 // planes[t][row][kk] = split(X[row][k0 + kk]) for kk < kc (rows of length ldx); zero pad to kpad.
 // sign_swap: complex "B'" operand (x_re, x_im) -> (x_im, -x_re) on the interleaved view.
 __global__ void k_split_rows(const float* __restrict__ X, long long ldx, int rows, long long k0, int kc, int kpad,
-                             __nv_bfloat16* __restrict__ P, int swap) {
-  const long long plane = (long long)rows * kpad;
-  const long long n = plane;
+                             __nv_bfloat16* __restrict__ P, int swap, long long plane, int terms) {
+  const long long n = (long long)rows * kpad;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     const int r = (int)(t / kpad), kk = (int)(t % kpad);
     double x = 0.0;
@@ -244,13 +252,13 @@ __global__ void k_split_rows(const float* __restrict__ X, long long ldx, int row
     split3(x, a, b, c);
     P[t] = a;
     P[plane + t] = b;
-    P[2 * plane + t] = c;
+    if (terms == 3) P[2 * plane + t] = c;
   }
 }
 
 // planes[t][g][m] = split(X[m][g0 + g]) : transposed chunk (32x32 smem tiles)
 __global__ void k_split_transpose(const float* __restrict__ X, long long ldx, int nb, long long g0, int gc, int nbpad,
-                                  __nv_bfloat16* __restrict__ P) {
+                                  __nv_bfloat16* __restrict__ P, int terms) {
   __shared__ float tile[32][33];
   const int gx = blockIdx.x * 32, mx = blockIdx.y * 32;
   for (int j = threadIdx.y; j < 32; j += blockDim.y) {
@@ -267,13 +275,14 @@ __global__ void k_split_transpose(const float* __restrict__ X, long long ldx, in
       const long long o = (long long)g * nbpad + m;
       P[o] = a;
       P[plane + o] = b;
-      P[2 * plane + o] = c;
+      if (terms == 3) P[2 * plane + o] = c;
     }
   }
 }
 
 // planes[t][n][m] = split(V[m + n*ldv]) (V column-major FP64 = row-major V^T)
-__global__ void k_split_small(const double* __restrict__ V, int ldv, int nb, int nbpad, __nv_bfloat16* __restrict__ P) {
+__global__ void k_split_small(const double* __restrict__ V, int ldv, int nb, int nbpad, __nv_bfloat16* __restrict__ P,
+                              int terms) {
   const long long plane = (long long)nb * nbpad;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < plane; t += (long long)gridDim.x * blockDim.x) {
     const int n = (int)(t / nbpad), m = (int)(t % nbpad);
@@ -282,7 +291,7 @@ __global__ void k_split_small(const double* __restrict__ V, int ldv, int nb, int
     split3(x, a, b, c);
     P[t] = a;
     P[plane + t] = b;
-    P[2 * plane + t] = c;
+    if (terms == 3) P[2 * plane + t] = c;
   }
 }
 
@@ -303,11 +312,13 @@ static int get_encode() {
   return 0;
 }
 
-// 3-D map over [3 planes][rows][kpad] bf16, box {64, box_rows, 1}, 128B swizzle
-static int make_map(CUtensorMap* m, const void* base, long long rows, long long kpad, int box_rows) {
+// 3-D map over [planes][rows][kpad] bf16 (plane stride plane_rows x kpad), box {64, box_rows, 1},
+// 128B swizzle
+static int make_map(CUtensorMap* m, const void* base, long long rows, long long kpad, int box_rows, int planes,
+                    long long plane_rows) {
   RS_TRY(get_encode());
-  cuuint64_t dims[3] = {(cuuint64_t)kpad, (cuuint64_t)rows, 3};
-  cuuint64_t strides[2] = {(cuuint64_t)kpad * 2, (cuuint64_t)rows * kpad * 2};
+  cuuint64_t dims[3] = {(cuuint64_t)kpad, (cuuint64_t)rows, (cuuint64_t)planes};
+  cuuint64_t strides[2] = {(cuuint64_t)kpad * 2, (cuuint64_t)plane_rows * kpad * 2};
   cuuint32_t box[3] = {64, (cuuint32_t)box_rows, 1};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims, strides, box, estr,
@@ -317,15 +328,15 @@ static int make_map(CUtensorMap* m, const void* base, long long rows, long long 
   return 0;
 }
 
-template <int BN, int S>
+template <int BN, int S, int T>
 static int launch_x3(Ctx& c, const CUtensorMap& ta, const CUtensorMap& tb, int M, int N, long long kpad,
                      const x3::Out& o, int ksplit) {
   const int kbt = (int)(kpad / x3::BK);
   const int kps = (kbt + ksplit - 1) / ksplit;
   ksplit = (kbt + kps - 1) / kps;
-  constexpr int STAGE = 3 * x3::BM * x3::BK * 2 + 3 * BN * x3::BK * 2;
+  constexpr int STAGE = T * x3::BM * x3::BK * 2 + T * BN * x3::BK * 2;
   const size_t smem = (size_t)S * STAGE + 1024 + 256;
-  auto kern = x3::k_gemm_x3<BN, S>;
+  auto kern = x3::k_gemm_x3<BN, S, T>;
   static bool attr = false;
   if (!attr) {
     RS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -337,66 +348,116 @@ static int launch_x3(Ctx& c, const CUtensorMap& ta, const CUtensorMap& tb, int M
   return check_launch("gemm_x3");
 }
 
-constexpr int kBN = 128;
-constexpr int kStages = 2;
+// Tile width by term count: three terms, 128 x 128 tiles in 2 stages of 96 KB; two terms,
+// 128 x 256 tiles in 2 stages of 96 KB (the wider tile reads each operand byte for twice the
+// products, which the two-term form needs: its loads per product are 1.5x the three-term's).
+static int bn_for(int terms) { return terms == 3 ? 128 : 256; }
+
+static int launch_terms(Ctx& c, int terms, const CUtensorMap& ta, const CUtensorMap& tb, int M, int N, long long kpad,
+                        const x3::Out& o, int ksplit) {
+  if (terms == 3) return launch_x3<128, 2, 3>(c, ta, tb, M, N, kpad, o, ksplit);
+  return launch_x3<256, 2, 2>(c, ta, tb, M, N, kpad, o, ksplit);
+}
+
+// Split-K chunk of a contraction with rows_total operand rows: the BF16 planes of one chunk stay
+// within 512 MB.
+static long long chunk_k(long long rows_total, int terms, long long K) {
+  const long long kc_max = std::max<long long>(64, ((long long)(512u << 20) / (2LL * terms * rows_total)) / 64 * 64);
+  return std::min<long long>(kc_max, (K + 63) / 64 * 64);
+}
+
+static int split_ksplit(int M, int N, int kpad, int bn) {
+  const int tiles = ((M + 127) / 128) * ((N + bn - 1) / bn);
+  const int kbt = kpad / 64;
+  return std::max(1, std::min(kbt, (2 * 148 + tiles - 1) / tiles));
+}
 
 // C[m][n] += alpha * sum_k A[m][k] B[n][k]; A: [M][lda] FP32, B: [N][ldb] FP32 (real view).
 // swapB: B is read as the complex "i-rotated" view (b_re, b_im) -> (b_im, -b_re).
+// terms: 3 (about FP32 accuracy) or 2 (see the head of this file).
 int gemm_tn_x3(Ctx& c, const float* A, long long lda, int M, const float* B, long long ldb, int N, long long K,
-               double alpha, double* C, long long ldc, int swapB) {
-  const long long kc_max = std::max<long long>(64, ((long long)(512u << 20) / (6LL * (M + N))) / 64 * 64);
-  const long long kc = std::min<long long>(kc_max, (K + 63) / 64 * 64);
-  RS_TRY(c.ws_gemm.ensure(sizeof(__nv_bfloat16) * 3 * (size_t)(M + N) * kc));
+               double alpha, double* C, long long ldc, int swapB, int terms) {
+  RS_CHECK(terms == 2 || terms == 3, RSDFT_ERR_ARG, "split terms must be 2 or 3");
+  const long long kc = chunk_k(M + N, terms, K);
+  RS_TRY(c.ws_gemm.ensure(sizeof(__nv_bfloat16) * terms * (size_t)(M + N) * kc));
   __nv_bfloat16* PA = c.ws_gemm.as<__nv_bfloat16>();
-  __nv_bfloat16* PB = PA + 3 * (size_t)M * kc;
-  const double flops = 2.0 * 6.0 * (double)M * N * K;
+  __nv_bfloat16* PB = PA + terms * (size_t)M * kc;
+  const double flops = 2.0 * (terms == 3 ? 6.0 : 3.0) * (double)M * N * K;
   ProfScope ps(c, "gemm", 0.0, flops);
   for (long long k0 = 0; k0 < K; k0 += kc) {
     const int kcur = (int)std::min<long long>(kc, K - k0);
     const int kpad = (kcur + 63) / 64 * 64;
-    x3::k_split_rows<<<4 * 148, 256, 0, c.stream>>>(A, lda, M, k0, kcur, kpad, PA, 0);
-    x3::k_split_rows<<<4 * 148, 256, 0, c.stream>>>(B, ldb, N, k0, kcur, kpad, PB, swapB);
+    x3::k_split_rows<<<4 * 148, 256, 0, c.stream>>>(A, lda, M, k0, kcur, kpad, PA, 0, (long long)M * kpad, terms);
+    x3::k_split_rows<<<4 * 148, 256, 0, c.stream>>>(B, ldb, N, k0, kcur, kpad, PB, swapB, (long long)N * kpad, terms);
     c.launches += 2;
     RS_TRY(check_launch("split_rows"));
     CUtensorMap ta, tb;
-    RS_TRY(make_map(&ta, PA, M, kpad, x3::BM));
-    RS_TRY(make_map(&tb, PB, N, kpad, kBN));
+    RS_TRY(make_map(&ta, PA, M, kpad, x3::BM, terms, M));
+    RS_TRY(make_map(&tb, PB, N, kpad, bn_for(terms), terms, N));
     x3::Out o{};
-    o.mode = 0; o.C = C; o.ldc = ldc; o.alpha = alpha; o.M = M; o.N = N;
-    const int tiles = ((M + 127) / 128) * ((N + kBN - 1) / kBN);
-    const int kbt = kpad / 64;
-    int ksplit = std::max(1, std::min(kbt, (2 * 148 + tiles - 1) / tiles));
-    RS_TRY((launch_x3<kBN, kStages>(c, ta, tb, M, N, kpad, o, ksplit)));
+    o.mode = 0; o.C = C; o.C2 = C; o.nsplit = N; o.ldc = ldc; o.alpha = alpha; o.M = M; o.N = N;
+    RS_TRY(launch_terms(c, terms, ta, tb, M, N, kpad, o, split_ksplit(M, N, kpad, bn_for(terms))));
+  }
+  return 0;
+}
+
+// S[m][n] += alpha * sum_k X[m][k] X[n][k] and M[m][n] += alpha * sum_k X[m][k] Y[n][k] in one
+// contraction of X against [X; Y] (N = 2 nb): X is split once per chunk and serves as A and as
+// the first nb rows of B.  X, Y: [nb][ld] FP32; S, M: nb x nb, leading dimension nb.
+int gemm_tn2_x3(Ctx& c, const float* X, const float* Y, long long ld, int nb, long long K, double alpha, double* S,
+                double* M, int terms) {
+  RS_CHECK(terms == 2 || terms == 3, RSDFT_ERR_ARG, "split terms must be 2 or 3");
+  const long long kc = chunk_k(2LL * nb, terms, K);
+  RS_TRY(c.ws_gemm.ensure(sizeof(__nv_bfloat16) * terms * (size_t)(2 * nb) * kc));
+  __nv_bfloat16* P = c.ws_gemm.as<__nv_bfloat16>();
+  const double flops = 2.0 * (terms == 3 ? 6.0 : 3.0) * (double)nb * (2.0 * nb) * K;
+  ProfScope ps(c, "gemm", 0.0, flops);
+  for (long long k0 = 0; k0 < K; k0 += kc) {
+    const int kcur = (int)std::min<long long>(kc, K - k0);
+    const int kpad = (kcur + 63) / 64 * 64;
+    const long long plane = 2LL * nb * kpad;  // [terms][2 nb][kpad]: rows of X, then rows of Y
+    x3::k_split_rows<<<4 * 148, 256, 0, c.stream>>>(X, ld, nb, k0, kcur, kpad, P, 0, plane, terms);
+    x3::k_split_rows<<<4 * 148, 256, 0, c.stream>>>(Y, ld, nb, k0, kcur, kpad, P + (size_t)nb * kpad, 0, plane,
+                                                   terms);
+    c.launches += 2;
+    RS_TRY(check_launch("split_rows"));
+    CUtensorMap ta, tb;
+    RS_TRY(make_map(&ta, P, nb, kpad, x3::BM, terms, 2LL * nb));
+    RS_TRY(make_map(&tb, P, 2LL * nb, kpad, bn_for(terms), terms, 2LL * nb));
+    x3::Out o{};
+    o.mode = 0; o.C = S; o.C2 = M; o.nsplit = nb; o.ldc = nb; o.alpha = alpha; o.M = nb; o.N = 2 * nb;
+    RS_TRY(launch_terms(c, terms, ta, tb, nb, 2 * nb, kpad, o, split_ksplit(nb, 2 * nb, kpad, bn_for(terms))));
   }
   return 0;
 }
 
 // X[n][g] <- sum_m X[m][g] V[m][n] for all g (in place, grid chunks); X: [nb][ldx] FP32,
 // V: nb x nb FP64 column-major (ldv).
-int gemm_rotate_x3(Ctx& c, float* X, long long ldx, int nb, long long G, const double* V, int ldv) {
+int gemm_rotate_x3(Ctx& c, float* X, long long ldx, int nb, long long G, const double* V, int ldv, int terms) {
+  RS_CHECK(terms == 2 || terms == 3, RSDFT_ERR_ARG, "split terms must be 2 or 3");
   const int nbpad = (nb + 63) / 64 * 64;
-  const long long gc_max = std::max<long long>(128, ((long long)(512u << 20) / (6LL * nbpad)) / 128 * 128);
+  const long long gc_max = std::max<long long>(128, ((long long)(512u << 20) / (2LL * terms * nbpad)) / 128 * 128);
   const long long gc = std::min<long long>(gc_max, (G + 127) / 128 * 128);
-  RS_TRY(c.ws_gemm.ensure(sizeof(__nv_bfloat16) * 3 * ((size_t)gc * nbpad + (size_t)nb * nbpad)));
+  RS_TRY(c.ws_gemm.ensure(sizeof(__nv_bfloat16) * terms * ((size_t)gc * nbpad + (size_t)nb * nbpad)));
   __nv_bfloat16* PV = c.ws_gemm.as<__nv_bfloat16>();
-  __nv_bfloat16* PX = PV + 3 * (size_t)nb * nbpad;
-  const double flops = 2.0 * 6.0 * (double)nb * nb * G;
+  __nv_bfloat16* PX = PV + terms * (size_t)nb * nbpad;
+  const double flops = 2.0 * (terms == 3 ? 6.0 : 3.0) * (double)nb * nb * G;
   ProfScope ps(c, "gemm", 0.0, flops);
-  x3::k_split_small<<<4 * 148, 256, 0, c.stream>>>(V, ldv, nb, nbpad, PV);
+  x3::k_split_small<<<4 * 148, 256, 0, c.stream>>>(V, ldv, nb, nbpad, PV, terms);
   c.launches++;
   CUtensorMap tb;
-  RS_TRY(make_map(&tb, PV, nb, nbpad, kBN));
+  RS_TRY(make_map(&tb, PV, nb, nbpad, bn_for(terms), terms, nb));
   for (long long g0 = 0; g0 < G; g0 += gc) {
     const int gcur = (int)std::min<long long>(gc, G - g0);
     dim3 tg((gcur + 31) / 32, (nbpad + 31) / 32);
-    x3::k_split_transpose<<<tg, dim3(32, 8), 0, c.stream>>>(X, ldx, nb, g0, gcur, nbpad, PX);
+    x3::k_split_transpose<<<tg, dim3(32, 8), 0, c.stream>>>(X, ldx, nb, g0, gcur, nbpad, PX, terms);
     c.launches++;
     RS_TRY(check_launch("split_transpose"));
     CUtensorMap ta;
-    RS_TRY(make_map(&ta, PX, gcur, nbpad, x3::BM));
+    RS_TRY(make_map(&ta, PX, gcur, nbpad, x3::BM, terms, gcur));
     x3::Out o{};
     o.mode = 1; o.Y = X + g0; o.ldy = ldx; o.M = gcur; o.N = nb;
-    RS_TRY((launch_x3<kBN, kStages>(c, ta, tb, gcur, nb, nbpad, o, 1)));
+    RS_TRY(launch_terms(c, terms, ta, tb, gcur, nb, nbpad, o, 1));
   }
   return 0;
 }
@@ -423,7 +484,7 @@ __global__ void k_f2d_x3(const float* s, double* d, long long n) {
 }
 }  // namespace x3
 
-int selftest_gemm(Ctx& c, int m, int n, long long k, int op, double* err) {
+int selftest_gemm(Ctx& c, int m, int n, long long k, int op, int terms, double* err) {
   DBuf a, b, ad, bd, cc, cref, v;
   const long long na = op == 0 ? (long long)m * k : (long long)m * k;  // op1: X [m=nb][k=G]
   const long long nbv = op == 0 ? (long long)n * k : (long long)m * m;
@@ -441,7 +502,7 @@ int selftest_gemm(Ctx& c, int m, int n, long long k, int op, double* err) {
     RS_TRY(cc.ensure(sizeof(double) * (size_t)m * n));
     RS_TRY(cref.ensure(sizeof(double) * (size_t)m * n));
     RS_CUDA(cudaMemsetAsync(cc.p, 0, sizeof(double) * (size_t)m * n, c.stream));
-    RS_TRY(gemm_tn_x3(c, a.as<float>(), k, m, b.as<float>(), k, n, k, 1.0, cc.as<double>(), n, 0));
+    RS_TRY(gemm_tn_x3(c, a.as<float>(), k, m, b.as<float>(), k, n, k, 1.0, cc.as<double>(), n, 0, terms));
     // reference, column-major m x n: C_cm = A_cm^T B_cm with A_cm (k x m), B_cm (k x n)
     if (cublasDgemm(c.cublas, CUBLAS_OP_T, CUBLAS_OP_N, m, n, (int)k, &one, ad.as<double>(), (int)k, bd.as<double>(),
                     (int)k, &zero, cref.as<double>(), m) != CUBLAS_STATUS_SUCCESS)
@@ -467,7 +528,7 @@ int selftest_gemm(Ctx& c, int m, int n, long long k, int op, double* err) {
     if (cublasDgemm(c.cublas, CUBLAS_OP_N, CUBLAS_OP_N, (int)k, m, m, &one, ad.as<double>(), (int)k, v.as<double>(), m,
                     &zero, cref.as<double>(), (int)k) != CUBLAS_STATUS_SUCCESS)
       RS_CHECK(false, RSDFT_ERR_CUDA, "reference dgemm failed");
-    RS_TRY(gemm_rotate_x3(c, a.as<float>(), k, m, k, v.as<double>(), m));
+    RS_TRY(gemm_rotate_x3(c, a.as<float>(), k, m, k, v.as<double>(), m, terms));
     std::vector<float> hy((size_t)na);
     h2.resize((size_t)na);
     RS_CUDA(cudaMemcpyAsync(hy.data(), a.p, sizeof(float) * hy.size(), cudaMemcpyDeviceToHost, c.stream));

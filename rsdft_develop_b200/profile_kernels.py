@@ -1,11 +1,12 @@
 """Drive one kernel family on the GPU for timing and ncu captures.
 
-    python -m rsdft_develop_b200.profile_kernels gemm [m] [k]      # split-BF16 tcgen05 GEMMs
-    python -m rsdft_develop_b200.profile_kernels pc [config] [bands]   # precond_hprsdft (FP64)
+    python -m rsdft_develop_b200.profile_kernels gemm [m] [k] [terms]   # split-BF16 tcgen05 GEMMs
+    python -m rsdft_develop_b200.profile_kernels pc|pc32 [config] [bands]   # precond_hprsdft (FP64 / FP32)
     python -m rsdft_develop_b200.profile_kernels lpc [config] [bands] [tc|fp32]  # learned preconditioner
 
 gemm: the overlap S = A A^T (m x m, K = k) and the rotation X <- X V (m bands of k points),
-each checked against cuBLAS DGEMM (the relative error is printed).  pc / lpc: one application
+each checked against cuBLAS DGEMM (the relative error is printed), with 3 (default) or 2 BF16
+terms per value.  pc / lpc: one application
 to `bands` seeded random bands of the configuration's grid, timed by the library's profiling
 (CUDA events on its stream) after one untimed call.
 """
@@ -24,25 +25,32 @@ def main(argv=None):
     if what == "gemm":
         m = int(argv[1]) if len(argv) > 1 else 256
         k = int(argv[2]) if len(argv) > 2 else 262144
+        terms = int(argv[3]) if len(argv) > 3 else 3
         with api.BandUpdate(synth.make_problem("t0")) as g:
+            g.gemm_terms(terms, terms)
+            g.selftest_gemm(m, m, k, 0)  # untimed: module load, tensor-map encoder
             g.profile(True)
             e0 = g.selftest_gemm(m, m, k, 0)
+            ms0, _, _, fl0 = g.profile_get("gemm")
             e1 = g.selftest_gemm(m, m, k, 1)
-            ms, n, _, _ = g.profile_get("gemm")
-            print(f"gemm m={m} k={k}: overlap rel.err {e0:.2e}, rotation rel.err {e1:.2e}; "
-                  f"{n} x3 launches {ms:.3f} ms total")
+            ms, n, _, fl = g.profile_get("gemm")
+            print(f"gemm m={m} k={k} terms={terms}: overlap rel.err {e0:.2e} {ms0:.3f} ms "
+                  f"({fl0 / max(ms0, 1e-9) / 1e9:.0f} TFLOP/s bf16), rotation rel.err {e1:.2e} {ms - ms0:.3f} ms "
+                  f"({(fl - fl0) / max(ms - ms0, 1e-9) / 1e9:.0f} TFLOP/s bf16); {n} calls")
         return
     cfg = argv[1] if len(argv) > 1 else "c1"
     prob = synth.make_problem(cfg)
     nb = int(argv[2]) if len(argv) > 2 else min(64, prob.nband)
     g_in = synth.random_wavefunctions(3, nb, prob.ng)
-    if what == "pc":
-        with api.BandUpdate(prob) as g:
-            g.precond(g_in)
+    if what in ("pc", "pc32"):
+        f32 = what == "pc32"
+        with api.BandUpdate(prob, precision=api.PREC_MIXED if f32 else api.PREC_FP64) as g:
+            run = (lambda: g.precond_f32(g_in)) if f32 else (lambda: g.precond(g_in))
+            run()
             g.profile(True)
-            g.precond(g_in)
+            run()
             ms, n, _, _ = g.profile_get("pc")
-            print(f"precond_hprsdft {cfg} bands={nb}: {ms:.3f} ms ({n} scopes)")
+            print(f"precond_hprsdft ({'FP32 s-step' if f32 else 'FP64'}) {cfg} bands={nb}: {ms:.3f} ms ({n} scopes)")
     elif what == "lpc":
         mode = argv[3] if len(argv) > 3 else "tc"
         with api.BandUpdate(prob, precision=api.PREC_MIXED, pc_mode=api.PC_LEARNED) as g:

@@ -19,7 +19,7 @@ def _rel(a, b):
     return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
 
 
-@pytest.mark.parametrize("name", ["t0", "t1", "c0", "c1"])
+@pytest.mark.parametrize("name", ["t0", "t1", "c0", "c1", "c2"])
 def test_hpsi_fp64_matches_oracle(oracle_mod, name):
     prob = synth.make_problem(name)
     o = oracle_mod.Oracle(prob)
@@ -31,7 +31,7 @@ def test_hpsi_fp64_matches_oracle(oracle_mod, name):
     assert _rel(out, ref) < TOL64
 
 
-@pytest.mark.parametrize("name", ["t1", "c0", "c1"])
+@pytest.mark.parametrize("name", ["t1", "c0", "c1", "c2"])
 def test_hpsi_fp32_matches_oracle(oracle_mod, name):
     prob = synth.make_problem(name)
     o = oracle_mod.Oracle(prob)

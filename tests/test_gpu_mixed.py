@@ -1,5 +1,5 @@
-"""Mixed precision: split-BF16 (3-term) tensor-core GEMMs, FP32 stencils/CG, FP64 dense solves
-and FP64 residuals.
+"""Mixed precision: split-BF16 tensor-core GEMMs (two terms in the overlap/Hsub sums, three in
+the rotations), FP32 stencils/CG/preconditioner, FP64 dense solves and FP64 residuals.
 
 Acceptance: the GEMMs stay within 5e-5 (overlaps, K up to 2.6e5) / 2e-5 (rotations) of
 max|C| against cuBLAS DGEMM on the same FP32 inputs -- the tensor cores' FP32 accumulation
@@ -18,6 +18,7 @@ pytestmark = pytest.mark.gpu
 @pytest.mark.parametrize("m,n,k,tol", [(256, 256, 262144, 5e-5), (100, 37, 1000, 5e-6), (384, 200, 70000, 5e-5)])
 def test_gemm_x3_overlap_vs_dgemm(m, n, k, tol):
     with api.BandUpdate(synth.make_problem("t0")) as g:
+        g.gemm_terms(3, 3)
         err = g.selftest_gemm(m, n, k, 0)
     assert err < tol
 
@@ -25,8 +26,61 @@ def test_gemm_x3_overlap_vs_dgemm(m, n, k, tol):
 @pytest.mark.parametrize("m,k", [(256, 262144), (37, 1000), (1024, 50000)])
 def test_gemm_x3_rotation_vs_dgemm(m, k):
     with api.BandUpdate(synth.make_problem("t0")) as g:
+        g.gemm_terms(3, 3)
         err = g.selftest_gemm(m, m, k, 1)
     assert err < 2e-5
+
+
+@pytest.mark.parametrize("m,n,k", [(256, 256, 262144), (100, 37, 1000), (384, 200, 70000)])
+def test_gemm_two_terms_overlap_vs_dgemm(m, n, k):
+    """Two BF16 terms per value: each product is good to about 2^-16, but the rounding is
+    unbiased, so over K terms the sum keeps the three-term error level set by the FP32
+    accumulation (long sums) or stays within 2^-16 of max|C| (short ones)."""
+    with api.BandUpdate(synth.make_problem("t0")) as g:
+        g.gemm_terms(3, 3)
+        e3 = g.selftest_gemm(m, n, k, 0)
+        g.gemm_terms(2, 3)
+        e2 = g.selftest_gemm(m, n, k, 0)
+    assert e2 < max(2.0 * e3, 3e-5), (e2, e3)
+
+
+def test_gemm_two_terms_rotation_vs_dgemm():
+    with api.BandUpdate(synth.make_problem("t0")) as g:
+        g.gemm_terms(3, 2)
+        err = g.selftest_gemm(256, 256, 262144, 1)
+    assert err < 5e-5
+
+
+def test_gemm_terms_argument_checked():
+    with api.BandUpdate(synth.make_problem("t0")) as g:
+        with pytest.raises(api.RsdftError):
+            g.gemm_terms(1, 3)
+
+
+@pytest.mark.parametrize("name,mloop", [("t0", 3), ("c0", 3), ("c0", 1), ("c0", 2), ("c0", 4)])
+def test_mixed_precond_matches_oracle(oracle_mod, name, mloop):
+    """precond_hprsdft on FP32 bands (the s-step evaluation of the mloop CG steps) against the
+    FP64 oracle's recurrence on the same FP32-representable input: FP32-level agreement."""
+    prob = synth.make_problem(name)
+    o = oracle_mod.Oracle(prob, mloop=mloop)
+    g = synth.random_wavefunctions(33, 5, prob.ng).astype(np.float32)
+    ref = o.precond(g.astype(np.float64))
+    with api.BandUpdate(prob, precision=api.PREC_MIXED, mloop=mloop) as gpu:
+        out = gpu.precond_f32(g)
+    assert np.max(np.abs(out - ref)) < 2e-5 * np.max(np.abs(ref))
+
+
+def test_mixed_precond_zero_band(oracle_mod):
+    """A zero band stays zero (the reference's rr < 1e-24 exit) next to a normal band."""
+    prob = synth.make_problem("t0")
+    o = oracle_mod.Oracle(prob)
+    g = synth.random_wavefunctions(34, 2, prob.ng).astype(np.float32)
+    g[0] = 0.0
+    ref = o.precond(g.astype(np.float64))
+    with api.BandUpdate(prob, precision=api.PREC_MIXED) as gpu:
+        out = gpu.precond_f32(g)
+    assert np.all(out[0] == 0.0)
+    assert np.max(np.abs(out[1] - ref[1])) < 2e-5 * np.max(np.abs(ref[1]))
 
 
 def test_mixed_gram_schmidt(oracle_mod):
@@ -66,9 +120,13 @@ def test_mixed_cg_tracks_fp64(oracle_mod):
     assert np.max(np.abs(esp - e_ref)) < 1e-5
 
 
-def test_mixed_solver_reaches_fp64_accuracy(oracle_mod):
+@pytest.mark.parametrize("terms", [(3, 3), (2, 3)])
+def test_mixed_solver_reaches_fp64_accuracy(oracle_mod, terms):
     """At equal FP64 residual the mixed and FP64 solves are equally accurate; at res <= 1e-10
-    the mixed eigenvalues are within 1e-8 Ha of the converged FP64 oracle."""
+    the mixed eigenvalues are within 1e-8 Ha of the converged FP64 oracle, with three BF16
+    terms in the rotations and two or three in the overlap/Hsub contractions.  (Two-term
+    rotations write 2^-16-relative noise into every band each sweep; the residual then stalls
+    near 5e-9, so they are not used.)"""
     prob = synth.make_problem("t0")
     o = oracle_mod.Oracle(prob)
     psi = o.gram_schmidt(synth.random_wavefunctions(64, prob.nband, prob.ng))
@@ -78,12 +136,14 @@ def test_mixed_solver_reaches_fp64_accuracy(oracle_mod):
     errs = {}
     for prec in (api.PREC_FP64, api.PREC_MIXED):
         with api.BandUpdate(prob, precision=prec) as g:
+            g.gemm_terms(*terms)
             g.set_wf(psi)
             it, esp, res = g.calc_sweep(400, tol=1e-8)
             assert res.max() <= 1e-8, (prec, it, res.max())
             errs[prec] = np.max(np.abs(np.sort(esp[0, 0]) - np.sort(e_ref)))
     assert errs[api.PREC_MIXED] <= 3.0 * errs[api.PREC_FP64] + 1e-9, errs
     with api.BandUpdate(prob, precision=api.PREC_MIXED) as g:
+        g.gemm_terms(*terms)
         g.set_wf(psi)
         it, esp, res = g.calc_sweep(600, tol=1e-10)
         u = g.get_wf()
