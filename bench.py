@@ -254,7 +254,8 @@ def main():
     dt_ms = ev0.elapsed_time(ev1)
     launches = g.kernel_launches() - launches0
     st_ms, st_n, st_bytes, _ = g.profile_get("hpsi_stencil")
-    names = ["hpsi_stencil", "nl_gather", "cg", "pc", "lpc", "gs", "gemm", "sd_gemm", "sd_eig", "sd_rot", "residual"]
+    names = ["hpsi_stencil", "nl_gather", "nl_scatter", "cg", "pc", "lpc", "gs", "gemm", "sd_gemm", "sd_eig",
+             "sd_rot", "residual"]
     shares = {n: g.profile_get(n)[0] for n in names}
     g.profile(False)
     lpc_state = g.lpc_status()
@@ -320,7 +321,7 @@ def main():
     achieved = (st_bytes / st_n) / ((st_ms / st_n) * 1e-3) / 1e9 if st_n else 0.0
     ratio = NCU_TRAFFIC_RATIO.get((args.config, args.precision))
     kname = "k_stencil_stream<float>" if prec == api.PREC_MIXED else "k_stencil_stream<double>"
-    roof = {"bound": "hbm", "kernel": f"{kname} (hpsi: stencil+Vloc+nonlocal scatter)",
+    roof = {"bound": "hbm", "kernel": f"{kname} (hpsi: 37-point stencil + V_loc; the nonlocal scatter is a separate kernel)",
             "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
             "frac": round(achieved / hbm, 4), "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
             "traffic": (ratio * st_bytes / st_n) if ratio else None,

@@ -51,7 +51,7 @@ EXPORTS = [
     "rsdft_gpu_hamiltonian_z", "rsdft_gpu_hamiltonian_f", "rsdft_gpu_hamiltonian_c",
     "rsdft_gpu_conjugate_gradient", "rsdft_gpu_gram_schmidt", "rsdft_gpu_subspace_diag",
     "rsdft_gpu_residual", "rsdft_gpu_precond_d", "rsdft_gpu_precond_f", "rsdft_gpu_set_pc_form", "rsdft_gpu_sweep", "rsdft_gpu_profile",
-    "rsdft_gpu_profile_get", "rsdft_gpu_kernel_launches", "rsdft_gpu_selftest_gemm", "rsdft_gpu_set_gemm_terms", "rsdft_gpu_init_sweep",
+    "rsdft_gpu_profile_get", "rsdft_gpu_kernel_launches", "rsdft_gpu_selftest_gemm", "rsdft_gpu_set_gemm_terms", "rsdft_gpu_set_gemm_tile", "rsdft_gpu_set_nl_form", "rsdft_gpu_init_sweep",
     "rsdft_gpu_hamiltonian_noalloc_d",
     "rsdft_gpu_lpc_init", "rsdft_gpu_lpc_set_weights", "rsdft_gpu_lpc_get_weights", "rsdft_gpu_lpc_forward",
     "rsdft_gpu_lpc_loss_grad", "rsdft_gpu_lpc_dataset", "rsdft_gpu_lpc_harvest", "rsdft_gpu_lpc_dataset_get",
@@ -110,7 +110,7 @@ def load_library(path: str = LIB_PATH):
         "rsdft_gpu_set_pc_form": [i],
         "rsdft_gpu_sweep": [i, d, C.POINTER(C.c_int), vp, vp],
         "rsdft_gpu_selftest_gemm": [i, i, C.c_longlong, i, C.POINTER(C.c_double)],
-        "rsdft_gpu_set_gemm_terms": [i, i],
+        "rsdft_gpu_set_gemm_terms": [i, i], "rsdft_gpu_set_gemm_tile": [i], "rsdft_gpu_set_nl_form": [i],
         "rsdft_gpu_init_sweep": [i],
         "rsdft_gpu_hamiltonian_noalloc_d": [i, i, vp, vp, i, i],
         "rsdft_gpu_lpc_init": [C.c_ulonglong], "rsdft_gpu_lpc_set_weights": [vp, i],
@@ -438,6 +438,16 @@ class BandUpdate:
     def pc_form(self, sstep: bool) -> None:
         """FP32 precond_hprsdft evaluation: s-step (default) or the recurrence form."""
         _call(self.lib.rsdft_gpu_set_pc_form, 1 if sstep else 0)
+
+    def nl_form(self, fused: bool) -> None:
+        """Nonlocal term of the real hpsi: inside the stencil (fused) or by a scatter after it."""
+        _call(self.lib.rsdft_gpu_set_nl_form, 1 if fused else 0)
+
+    def gemm_tile(self, wide: bool = True, tri: bool = False, update: bool = False) -> None:
+        """Three-term GEMM tiles: 128 x 256 over K blocks of 32 (default) or 128 x 128 over 64;
+        tri: the overlap/Hsub contraction forms only its upper triangle; update: the band
+        rotation in update form.  The defaults are the library's."""
+        _call(self.lib.rsdft_gpu_set_gemm_tile, (1 if wide else 0) | (2 if tri else 0) | (0 if update else 4))
 
     def gemm_terms(self, overlap: int, rotation: int) -> None:
         """BF16 terms (2 or 3) of the mixed-precision overlap/Hsub and rotation contractions."""

@@ -196,6 +196,15 @@ static int build_nonlocal(Ctx& c, int nzlma, int maxmjj, const int* mjj, const i
   RS_CUDA(cudaMemcpy(nl.rec_rowptr.p, rowptr.data(), rowptr.size() * sizeof(int), cudaMemcpyHostToDevice));
   RS_CUDA(cudaMemcpy(nl.rec_pt.p, rpt.data(), nrec * sizeof(int), cudaMemcpyHostToDevice));
   RS_CUDA(cudaMemcpy(nl.rec_g.p, rg.data(), nrec * sizeof(int), cudaMemcpyHostToDevice));
+  {  // covered grid points (the nonlocal scatter's work list)
+    std::vector<int> cov;
+    for (size_t i = 0; i < c.ng; ++i)
+      if (rowptr[i + 1] > rowptr[i]) cov.push_back((int)i);
+    nl.ncov = (int)cov.size();
+    RS_TRY(nl.cov.ensure(std::max<size_t>(1, cov.size()) * sizeof(int)));
+    if (!cov.empty())
+      RS_CUDA(cudaMemcpy(nl.cov.p, cov.data(), cov.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
   nl.perk.assign(c.p.nk, NonlocalTables::PerK());
   nl.h_rowptr.swap(rowptr);
   nl.seg_max.clear();
@@ -260,7 +269,7 @@ static void destroy(Ctx* c) {
   for (auto e : c->event_pool) cudaEventDestroy(e);
   DBuf* bufs[] = {&c->vloc64, &c->vloc32, &c->ws_coef, &c->ws_io_a, &c->ws_io_b, &c->ws_cg, &c->ws_red,
                   &c->ws_scal, &c->ws_dense, &c->ws_hpsi, &c->ws_flag, &c->ws_rot, &c->ws_solver, &c->ws_info, &c->ws_gemm, &c->ws_out, &c->ws_f64,
-                  &c->nl.gofs, &c->nl.gjj, &c->nl.gplist, &c->nl.gD, &c->nl.rec_rowptr, &c->nl.rec_pt, &c->nl.rec_g};
+                  &c->nl.gofs, &c->nl.gjj, &c->nl.gplist, &c->nl.gD, &c->nl.rec_rowptr, &c->nl.rec_pt, &c->nl.rec_g, &c->nl.cov};
   for (DBuf* b : bufs) b->release();
   for (auto& pk : c->nl.perk) {
     pk.gw64.release(); pk.gw32.release(); pk.ru64.release(); pk.ru32.release();
@@ -728,6 +737,23 @@ int rsdft_gpu_set_pc_form(int sstep) {
   REQUIRE_CTX();
   RS_CHECK(sstep == 0 || sstep == 1, RSDFT_ERR_ARG, "sstep must be 0 or 1");
   g_ctx->pc_sstep = sstep;
+  return 0;
+}
+
+int rsdft_gpu_set_nl_form(int fused) {
+  REQUIRE_CTX();
+  RS_CHECK(fused == 0 || fused == 1, RSDFT_ERR_ARG, "fused must be 0 or 1");
+  g_ctx->nl_fused = fused;
+  g_ctx->stencil_tune.clear();  // the stencil's best configuration depends on it
+  return 0;
+}
+
+int rsdft_gpu_set_gemm_tile(int flags) {
+  REQUIRE_CTX();
+  RS_CHECK(flags >= 0 && flags <= 7, RSDFT_ERR_ARG, "tile flags must be in 0..7");
+  g_ctx->gemm_wide = flags & 1;
+  g_ctx->gemm_tri = (flags >> 1) & 1;
+  g_ctx->rot_update = ((flags >> 2) & 1) ? 0 : 1;
   return 0;
 }
 

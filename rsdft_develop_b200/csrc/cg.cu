@@ -372,57 +372,103 @@ struct PcCoef {
   int n1, n2, n3, nc;
 };
 
-// Row-structured loop for the 7-point operator: the CTA's chunk of x-rows (rows of n1 * nc
-// reals), 8 rows at a time, 32 consecutive reals per row step; neighbour offsets are formed
-// once per row (y, z) and per element (x) with periodic wrap, in 32/64-bit integer adds.
-#define PC_ROWS_BEGIN(k, q)                                                                      \
+// 16 bytes of T (4 FP32 or 2 FP64 reals): the unit every preconditioner thread loads and
+// stores, so that each memory instruction moves 16 bytes.
+template <typename T>
+struct Vec {
+  static constexpr int W = 16 / (int)sizeof(T);
+  T v[W];
+};
+template <typename T>
+__device__ __forceinline__ Vec<T> ldv(const T* p) {
+  Vec<T> r;
+  if constexpr (sizeof(T) == 4) {
+    const float4 a = *reinterpret_cast<const float4*>(p);
+    r.v[0] = a.x; r.v[1] = a.y; r.v[2] = a.z; r.v[3] = a.w;
+  } else {
+    const double2 a = *reinterpret_cast<const double2*>(p);
+    r.v[0] = a.x; r.v[1] = a.y;
+  }
+  return r;
+}
+template <typename T>
+__device__ __forceinline__ void stv(T* p, const Vec<T>& r) {
+  if constexpr (sizeof(T) == 4)
+    *reinterpret_cast<float4*>(p) = make_float4(r.v[0], r.v[1], r.v[2], r.v[3]);
+  else
+    *reinterpret_cast<double2*>(p) = make_double2(r.v[0], r.v[1]);
+}
+
+// Walk of the CTA's chunk of x-rows (rows of n1 * NCP reals) in groups of W consecutive reals,
+// consecutive threads on consecutive groups; per group the periodic neighbour offsets of its
+// row (y, z) and the offsets xl / xr, from the group start, of the reals just left and right
+// of the group (x, wrapping within the row).  Needs n1 * NCP to be a multiple of W.
+#define PC_GROUPS_BEGIN(k, q, T)                                                                 \
+  constexpr int VW = Vec<T>::W;                                                                  \
   const int b = blockIdx.y;                                                                      \
   const size_t off = (size_t)b * (k).ng;                                                         \
-  const int L = (q).n1 * (q).nc;                                                                 \
+  const int L = (q).n1 * NCP;                                                                    \
+  const int NGR = L / VW;                                                                          \
   const int nrow = (q).n2 * (q).n3;                                                              \
   const int per = (nrow + (k).nch - 1) / (k).nch;                                                \
   const int r0 = per * blockIdx.x, r1 = min(nrow, r0 + per);                                     \
-  const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;                                        \
   const long long pln = (long long)(q).n2 * L;                                                   \
-  for (int row = r0 + ly; row < r1; row += kThreads / 32) {                                      \
+  for (int t = r0 * NGR + (int)threadIdx.x; t < r1 * NGR; t += kThreads) {                         \
+    const int row = t / NGR, gq = t - row * NGR;                                                     \
     const int i2 = row % (q).n2, i3 = row / (q).n2;                                              \
-    const long long rb = (long long)row * L;                                                     \
     const long long ym = i2 == 0 ? (long long)((q).n2 - 1) * L : -(long long)L;                  \
     const long long yp = i2 == (q).n2 - 1 ? -(long long)((q).n2 - 1) * L : (long long)L;         \
     const long long zm = i3 == 0 ? (long long)((q).n3 - 1) * pln : -pln;                         \
     const long long zp = i3 == (q).n3 - 1 ? -(long long)((q).n3 - 1) * pln : pln;                \
-    for (int x = lx; x < L; x += 32) {                                                           \
-      const int i1 = (q).nc == 1 ? x : (x >> 1);                                                 \
-      const int xm = i1 == 0 ? ((q).n1 - 1) * (q).nc : -(q).nc;                                  \
-      const int xp = i1 == (q).n1 - 1 ? -((q).n1 - 1) * (q).nc : (q).nc;                         \
-      const long long j = rb + x;
-#define PC_ROWS_END \
-  }                 \
-  }
+    const long long j = (long long)row * L + (long long)gq * VW;                                  \
+    const int xl = gq == 0 ? L - NCP : -NCP;                                                     \
+    const int xr = gq == NGR - 1 ? VW - L : VW;
+#define PC_GROUPS_END }
 
-// 7-point operator at element j in the storage type's arithmetic (FP32 bands: FP32 math, no
-// per-element conversions)
-template <typename T>
-__device__ __forceinline__ T apply7r(const T* __restrict__ g, long long j, int xm, int xp, long long ym, long long yp,
-                                     long long zm, long long zp, const PcCoef& q) {
-  return (T)q.c0 * g[j] + (T)q.c1 * (g[j + xp] + g[j + xm]) + (T)q.c2 * (g[j + yp] + g[j + ym]) +
-         (T)q.c3 * (g[j + zp] + g[j + zm]);
+// 7-point operator on the group at j, in the storage type's arithmetic (FP32 bands: FP32 math,
+// no per-element conversions); c receives the group's own values.  Same expression per real as
+// the scalar form c0 g + c1 (g[x+1] + g[x-1]) + c2 (g[y+1] + g[y-1]) + c3 (g[z+1] + g[z-1]).
+template <typename T, int NCP>
+__device__ __forceinline__ Vec<T> apply7v(const T* __restrict__ g, long long j, int xl, int xr, long long ym,
+                                          long long yp, long long zm, long long zp, const PcCoef& q, Vec<T>& c) {
+  constexpr int W = Vec<T>::W;
+  c = ldv(g + j);
+  const Vec<T> a = ldv(g + j + ym), bq = ldv(g + j + yp), d = ldv(g + j + zm), e = ldv(g + j + zp);
+  T lft[NCP], rgt[NCP];
+#pragma unroll
+  for (int i = 0; i < NCP; ++i) {
+    lft[i] = g[j + xl + i];
+    rgt[i] = g[j + xr + i];
+  }
+  Vec<T> o;
+#pragma unroll
+  for (int i = 0; i < W; ++i) {
+    const T xm = i >= NCP ? c.v[i >= NCP ? i - NCP : 0] : lft[i < NCP ? i : 0];
+    const T xp = i + NCP < W ? c.v[i + NCP < W ? i + NCP : 0] : rgt[i + NCP >= W ? i + NCP - W : 0];
+    o.v[i] = (T)q.c0 * c.v[i] + (T)q.c1 * (xp + xm) + (T)q.c2 * (bq.v[i] + a.v[i]) + (T)q.c3 * (e.v[i] + d.v[i]);
+  }
+  return o;
 }
 
 // R = G - A G (the initial residual for the starting guess PG = G, also the first direction);
 // partial |R|^2
-template <typename T>
+template <typename T, int NCP>
 __global__ void __launch_bounds__(kThreads) k_pc_first(Blk k, PcCoef q, const T* __restrict__ G,
                                                        T* __restrict__ R) {
   if (SC(k, S_ACT, blockIdx.y) == 0.0) return;
   T vt = T(0);  // per-thread partial in the storage type, added in FP64 across threads
   {
-    PC_ROWS_BEGIN(k, q)
-    const T* g = G + off;
-    const T r = g[j] - apply7r(g, j, xm, xp, ym, yp, zm, zp, q);
-    R[off + j] = r;
-    vt += r * r;
-    PC_ROWS_END
+    PC_GROUPS_BEGIN(k, q, T)
+    Vec<T> c;
+    const Vec<T> ag = apply7v<T, NCP>(G + off, j, xl, xr, ym, yp, zm, zp, q, c);
+    Vec<T> r;
+#pragma unroll
+    for (int i = 0; i < VW; ++i) {
+      r.v[i] = c.v[i] - ag.v[i];
+      vt += r.v[i] * r.v[i];
+    }
+    stv(R + off + j, r);
+    PC_GROUPS_END
   }
   double v[1] = {(double)vt};
   block_partials<1>(v, k, blockIdx.y);
@@ -430,7 +476,7 @@ __global__ void __launch_bounds__(kThreads) k_pc_first(Blk k, PcCoef q, const T*
 
 // Qn = R + b Q and F = A Qn = A R + b A Q in one pass (Qn written to a third buffer, since
 // the stencil reads Q's neighbours); partial <Qn|F>
-template <typename T>
+template <typename T, int NCP>
 __global__ void __launch_bounds__(kThreads) k_pc_dirapply(Blk k, PcCoef q, const T* __restrict__ R,
                                                           const T* __restrict__ Q, T* __restrict__ Qn,
                                                           T* __restrict__ F) {
@@ -438,56 +484,80 @@ __global__ void __launch_bounds__(kThreads) k_pc_dirapply(Blk k, PcCoef q, const
   const T bb = (T)SC(k, S_PCB, blockIdx.y);
   T vt = T(0);
   {
-    PC_ROWS_BEGIN(k, q)
-    const T* rr = R + off;
-    const T* qq = Q + off;
-    const T qn = rr[j] + bb * qq[j];
-    const T f = apply7r(rr, j, xm, xp, ym, yp, zm, zp, q) + bb * apply7r(qq, j, xm, xp, ym, yp, zm, zp, q);
-    Qn[off + j] = qn;
-    F[off + j] = f;
-    vt += qn * f;
-    PC_ROWS_END
+    PC_GROUPS_BEGIN(k, q, T)
+    Vec<T> cr, cq;
+    const Vec<T> ar = apply7v<T, NCP>(R + off, j, xl, xr, ym, yp, zm, zp, q, cr);
+    const Vec<T> aq = apply7v<T, NCP>(Q + off, j, xl, xr, ym, yp, zm, zp, q, cq);
+    Vec<T> qn, f;
+#pragma unroll
+    for (int i = 0; i < VW; ++i) {
+      qn.v[i] = cr.v[i] + bb * cq.v[i];
+      f.v[i] = ar.v[i] + bb * aq.v[i];
+      vt += qn.v[i] * f.v[i];
+    }
+    stv(Qn + off + j, qn);
+    stv(F + off + j, f);
+    PC_GROUPS_END
   }
   double v[1] = {(double)vt};
   block_partials<1>(v, k, blockIdx.y);
 }
 
 // F = A Q ; partial <Q|F>
-template <typename T>
+template <typename T, int NCP>
 __global__ void __launch_bounds__(kThreads) k_pc_apply(Blk k, PcCoef q, const T* __restrict__ Q, T* __restrict__ F) {
   if (SC(k, S_PCACT, blockIdx.y) == 0.0) return;
   T vt = T(0);
   {
-    PC_ROWS_BEGIN(k, q)
-    const T* qq = Q + off;
-    const T f = apply7r(qq, j, xm, xp, ym, yp, zm, zp, q);
-    F[off + j] = f;
-    vt += qq[j] * f;
-    PC_ROWS_END
+    PC_GROUPS_BEGIN(k, q, T)
+    Vec<T> cq;
+    const Vec<T> f = apply7v<T, NCP>(Q + off, j, xl, xr, ym, yp, zm, zp, q, cq);
+#pragma unroll
+    for (int i = 0; i < VW; ++i) vt += cq.v[i] * f.v[i];
+    stv(F + off + j, f);
+    PC_GROUPS_END
   }
   double v[1] = {(double)vt};
   block_partials<1>(v, k, blockIdx.y);
 }
+
+// Elementwise walk of a band in 16-byte groups (the chunking of BAND_LOOP, in groups)
+#define GROUP_LOOP(k, T)                                                    \
+  constexpr int VW = Vec<T>::W;                                             \
+  const int b = blockIdx.y;                                                 \
+  const size_t off = (size_t)b * (k).ng;                                    \
+  const size_t ngr = (k).ng / VW;                                           \
+  const size_t per = (ngr + (k).nch - 1) / (k).nch;                         \
+  const size_t g0 = per * blockIdx.x, g1 = min(ngr, g0 + per);
 
 // first step: PG = G + a Q (starting guess G); (if !last) Rn = Q - a F (Q = R0); partial |Rn|^2
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_pc_update1(Blk k, const T* __restrict__ G, const T* __restrict__ Q,
                                                          const T* __restrict__ F, T* __restrict__ Rn,
                                                          T* __restrict__ PG, int last) {
-  BAND_LOOP(k, 1);
+  GROUP_LOOP(k, T);
   if (SC(k, S_PCACT, b) == 0.0) {
-    for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) PG[off + i] = G[off + i];
+    for (size_t gi = g0 + threadIdx.x; gi < g1; gi += kThreads) stv(PG + off + gi * VW, ldv(G + off + gi * VW));
     return;
   }
   const T a = (T)SC(k, S_PCA, b);
   T vt = T(0);
-  for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) {
-    const T qi = Q[off + i];
-    PG[off + i] = G[off + i] + a * qi;
+  for (size_t gi = g0 + threadIdx.x; gi < g1; gi += kThreads) {
+    const size_t e = off + gi * VW;
+    const Vec<T> qv = ldv(Q + e), gv = ldv(G + e);
+    Vec<T> pg;
+#pragma unroll
+    for (int i = 0; i < VW; ++i) pg.v[i] = gv.v[i] + a * qv.v[i];
+    stv(PG + e, pg);
     if (!last) {
-      const T r = qi - a * F[off + i];
-      Rn[off + i] = r;
-      vt += r * r;
+      const Vec<T> fv = ldv(F + e);
+      Vec<T> r;
+#pragma unroll
+      for (int i = 0; i < VW; ++i) {
+        r.v[i] = qv.v[i] - a * fv.v[i];
+        vt += r.v[i] * r.v[i];
+      }
+      stv(Rn + e, r);
     }
   }
   double v[1] = {(double)vt};
@@ -498,17 +568,26 @@ __global__ void __launch_bounds__(kThreads) k_pc_update1(Blk k, const T* __restr
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_pc_update(Blk k, const T* __restrict__ Q, const T* __restrict__ F,
                                                         T* __restrict__ R, T* __restrict__ PG, int last) {
-  BAND_LOOP(k, 1);
+  GROUP_LOOP(k, T);
   if (SC(k, S_PCACT, b) == 0.0) return;
   const T a = (T)SC(k, S_PCA, b);
   T vt = T(0);
-  for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) {
-    const T qi = Q[off + i];
-    PG[off + i] = PG[off + i] + a * qi;
+  for (size_t gi = g0 + threadIdx.x; gi < g1; gi += kThreads) {
+    const size_t e = off + gi * VW;
+    const Vec<T> qv = ldv(Q + e);
+    Vec<T> pg = ldv(PG + e);
+#pragma unroll
+    for (int i = 0; i < VW; ++i) pg.v[i] = pg.v[i] + a * qv.v[i];
+    stv(PG + e, pg);
     if (!last) {
-      const T r = R[off + i] - a * F[off + i];
-      R[off + i] = r;
-      vt += r * r;
+      const Vec<T> fv = ldv(F + e);
+      Vec<T> r = ldv(R + e);
+#pragma unroll
+      for (int i = 0; i < VW; ++i) {
+        r.v[i] = r.v[i] - a * fv.v[i];
+        vt += r.v[i] * r.v[i];
+      }
+      stv(R + e, r);
     }
   }
   double v[1] = {(double)vt};
@@ -551,19 +630,21 @@ __global__ void k_pc_sc_beta(Blk k) {
 
 // Vn = B V and partials <V|Vn>, <Vn|Vn>; WRITE = false: only <V|B V>.  qb holds B's
 // coefficients (c0 = 0).
-template <typename T, bool WRITE>
+template <typename T, int NCP, bool WRITE>
 __global__ void __launch_bounds__(kThreads) k_pcs_shift(Blk k, PcCoef qb, const T* __restrict__ V, T* __restrict__ Vn) {
   if (SC(k, S_PCACT, blockIdx.y) == 0.0) return;
   T s0 = T(0), s1 = T(0);
   {
-    PC_ROWS_BEGIN(k, qb)
-    const T* vv = V + off;
-    const T w = (T)qb.c1 * (vv[j + xp] + vv[j + xm]) + (T)qb.c2 * (vv[j + yp] + vv[j + ym]) +
-                (T)qb.c3 * (vv[j + zp] + vv[j + zm]);
-    if (WRITE) Vn[off + j] = w;
-    s0 += vv[j] * w;
-    s1 += w * w;
-    PC_ROWS_END
+    PC_GROUPS_BEGIN(k, qb, T)
+    Vec<T> cv;
+    const Vec<T> w = apply7v<T, NCP>(V + off, j, xl, xr, ym, yp, zm, zp, qb, cv);  // qb.c0 = 0
+    if (WRITE) stv(Vn + off + j, w);
+#pragma unroll
+    for (int i = 0; i < VW; ++i) {
+      s0 += cv.v[i] * w.v[i];
+      s1 += w.v[i] * w.v[i];
+    }
+    PC_GROUPS_END
   }
   double v[2] = {(double)s0, (double)s1};
   block_partials<2>(v, k, blockIdx.y);
@@ -614,23 +695,39 @@ template <typename T, int M>
 __global__ void __launch_bounds__(kThreads) k_pcs_combine(Blk k, const T* __restrict__ G, const T* __restrict__ V0,
                                                           const T* __restrict__ V1, const T* __restrict__ V2,
                                                           const T* __restrict__ V3, T* __restrict__ PG) {
-  BAND_LOOP(k, 1);
+  GROUP_LOOP(k, T);
   const bool on = SC(k, S_PCACT, b) != 0.0;
   T x[4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) x[j] = (on && j < M) ? (T)SC(k, S_XI0 + j, b) : T(0);
   double vt = 0.0;  // accumulated as k_dot does
-  for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) {
-    const T g = G[off + i];
-    T v = g;
+  for (size_t gi = g0 + threadIdx.x; gi < g1; gi += kThreads) {
+    const size_t e = off + gi * VW;
+    const Vec<T> gv = ldv(G + e);
+    Vec<T> pv = gv;
     if (on) {
-      v += x[0] * V0[off + i];
-      if (M > 1) v += x[1] * V1[off + i];
-      if (M > 2) v += x[2] * V2[off + i];
-      if (M > 3) v += x[3] * V3[off + i];
+      const Vec<T> a0 = ldv(V0 + e);
+#pragma unroll
+      for (int i = 0; i < VW; ++i) pv.v[i] += x[0] * a0.v[i];
+      if (M > 1) {
+        const Vec<T> a1 = ldv(V1 + e);
+#pragma unroll
+        for (int i = 0; i < VW; ++i) pv.v[i] += x[1] * a1.v[i];
+      }
+      if (M > 2) {
+        const Vec<T> a2 = ldv(V2 + e);
+#pragma unroll
+        for (int i = 0; i < VW; ++i) pv.v[i] += x[2] * a2.v[i];
+      }
+      if (M > 3) {
+        const Vec<T> a3 = ldv(V3 + e);
+#pragma unroll
+        for (int i = 0; i < VW; ++i) pv.v[i] += x[3] * a3.v[i];
+      }
     }
-    PG[off + i] = v;
-    vt += (double)v * (double)g;
+    stv(PG + e, pv);
+#pragma unroll
+    for (int i = 0; i < VW; ++i) vt += (double)pv.v[i] * (double)gv.v[i];
   }
   if (SC(k, S_ACT, b) == 0.0) return;
   double d[1] = {vt};
@@ -673,7 +770,15 @@ static int pc_block(Ctx& c, Blk& k, const T* G, T* PG, T* X0, T* X1, T* X2, T* F
   q.c3 = -0.5 * c.p.ggg[2] / (H[2] * H[2]);
   q.n1 = c.p.n1; q.n2 = c.p.n2; q.n3 = c.p.n3;
   q.nc = c.cplx ? 2 : 1;
+  RS_CHECK((q.n1 * q.nc) % Vec<T>::W == 0, RSDFT_ERR_UNSUPPORTED,
+           "preconditioner needs x-rows of a multiple of %d reals", Vec<T>::W);
   ProfScope ps(c, "pc");
+  // kernels on rows of n1 * nc reals: real (1) or complex (2) interleaved view
+#define LAUNCH_PC(kern, ...)                                   \
+  do {                                                         \
+    if (q.nc == 1) LAUNCH_E((kern<T, 1>), __VA_ARGS__);        \
+    else LAUNCH_E((kern<T, 2>), __VA_ARGS__);                  \
+  } while (0)
   if (c.p.mloop < 1) {
     LAUNCH_E(k_copy<T>, G, PG);
     return check_launch("pc");
@@ -687,14 +792,16 @@ static int pc_block(Ctx& c, Blk& k, const T* G, T* PG, T* X0, T* X1, T* X2, T* F
     qb.c3 = q.c3 / q.c0;
     qb.c0 = 0.0;
     T* v[4] = {X0, X1, X2, F};
-    LAUNCH_E(k_pc_first<T>, q, G, X0);
+    LAUNCH_PC(k_pc_first, q, G, X0);
     LAUNCH_S(k_pc_sc_first);
     LAUNCH_S(k_pcs_sc, 0, m, q.c0);
     for (int i = 1; i < m; ++i) {
-      LAUNCH_E((k_pcs_shift<T, true>), qb, v[i - 1], v[i]);
+      if (q.nc == 1) LAUNCH_E((k_pcs_shift<T, 1, true>), qb, v[i - 1], v[i]);
+      else LAUNCH_E((k_pcs_shift<T, 2, true>), qb, v[i - 1], v[i]);
       LAUNCH_S(k_pcs_sc, i, m, q.c0);
     }
-    LAUNCH_E((k_pcs_shift<T, false>), qb, v[m - 1], v[m - 1]);
+    if (q.nc == 1) LAUNCH_E((k_pcs_shift<T, 1, false>), qb, v[m - 1], v[m - 1]);
+    else LAUNCH_E((k_pcs_shift<T, 2, false>), qb, v[m - 1], v[m - 1]);
     LAUNCH_S(k_pcs_sc, m, m, q.c0);
     switch (m) {
       case 1: LAUNCH_E((k_pcs_combine<T, 1>), G, v[0], v[1], v[2], v[3], PG); break;
@@ -705,9 +812,9 @@ static int pc_block(Ctx& c, Blk& k, const T* G, T* PG, T* X0, T* X1, T* X2, T* F
     if (pg_dot) *pg_dot = true;
     return check_launch("pc");
   }
-  LAUNCH_E(k_pc_first<T>, q, G, X0);
+  LAUNCH_PC(k_pc_first, q, G, X0);
   LAUNCH_S(k_pc_sc_first);
-  LAUNCH_E(k_pc_apply<T>, q, X0, F);
+  LAUNCH_PC(k_pc_apply, q, X0, F);
   LAUNCH_S(k_pc_sc_alpha);
   LAUNCH_E(k_pc_update1<T>, G, X0, F, X1, PG, c.p.mloop == 1 ? 1 : 0);
   T* r = X1;   // residual
@@ -715,12 +822,13 @@ static int pc_block(Ctx& c, Blk& k, const T* G, T* PG, T* X0, T* X1, T* X2, T* F
   T* qn = X2;  // next direction
   for (int it = 2; it <= c.p.mloop; ++it) {
     LAUNCH_S(k_pc_sc_beta);
-    LAUNCH_E(k_pc_dirapply<T>, q, r, qo, qn, F);
+    LAUNCH_PC(k_pc_dirapply, q, r, qo, qn, F);
     LAUNCH_S(k_pc_sc_alpha);
     const int last = it == c.p.mloop;
     LAUNCH_E(k_pc_update<T>, qn, F, r, PG, last);
     std::swap(qo, qn);
   }
+#undef LAUNCH_PC
   return check_launch("pc");
 }
 

@@ -38,6 +38,8 @@ struct NonlocalTables {
   std::vector<int> h_slot;        // for each (lma, j): footprint slot in its group
   std::vector<int> h_rec_src;     // for each record: its footprint slot
   std::vector<int> h_rowptr;      // host copy of rec_rowptr
+  DBuf cov;                       // grid points with at least one record, ascending
+  int ncov = 0;
   std::map<int, int> seg_max;     // tile_y -> largest record segment of one (plane, y-tile)
 };
 
@@ -106,6 +108,10 @@ struct Ctx {
   int gemm_terms_sm = 3;           // BF16 terms of the overlap / Hsub contractions (mixed precision)
   int gemm_terms_rot = 3;          // BF16 terms of the band rotations (mixed precision)
   int pc_sstep = 1;                // FP32 precond_hprsdft in s-step form (0: the recurrence form)
+  int gemm_wide = 1;               // three-term GEMM tiles 128 x 256 (K blocks of 32), else 128 x 128
+  int gemm_tri = 0;                // overlap / Hsub: form only the tiles reaching the upper triangle
+  int rot_update = 0;              // mixed rotation in update form X + X (C - I)
+  int nl_fused = 0;                // nonlocal term inside the stencil (1) or by the scatter kernel after it (0)
 
   // profiling
   bool profiling = false;
@@ -171,7 +177,8 @@ int gemm_tn_x3(Ctx& c, const float* A, long long lda, int M, const float* B, lon
                double alpha, double* C, long long ldc, int swapB, int terms);
 int gemm_tn2_x3(Ctx& c, const float* X, const float* Y, long long ld, int nb, long long K, double alpha, double* S,
                 double* M, int terms);
-int gemm_rotate_x3(Ctx& c, float* X, long long ldx, int nb, long long G, const double* V, int ldv, int terms);
+int gemm_rotate_x3(Ctx& c, float* X, long long ldx, int nb, long long G, const double* V, int ldv, int terms,
+                   bool add = false);
 int selftest_gemm(Ctx& c, int m, int n, long long k, int op, int terms, double* err);
 
 // ---- util ----

@@ -82,6 +82,25 @@ __global__ void k_symmetrize(double* H, int n) {
     }
   }
 }
+__global__ void k_fill_lower(double* H, int n) {
+  // H(i, j) <- H(j, i) for i > j (column-major): the lower triangle from the upper
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)n * n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % n), j = (int)(t / n);
+    if (i > j) H[i + (long long)j * n] = H[j + (long long)i * n];
+  }
+}
+// Rotation in update form: each column j of C = R^-1 V (an eigenvector, defined up to sign)
+// is signed so that C(j, j) >= 0, then C <- C - I.  Near convergence C is close to I, so the
+// rotation X (I + D) = X + X D forms a small correction.
+__global__ void k_rotation_update_form(double* C, int n) {
+  const int j = blockIdx.x;
+  if (j >= n) return;
+  double* col = C + (long long)j * n;
+  const double sg = col[j] < 0.0 ? -1.0 : 1.0;
+  __syncthreads();  // every thread has read C(j, j) before any thread writes the column
+  for (int i = threadIdx.x; i < n; i += blockDim.x) col[i] = sg * col[i] - (i == j ? 1.0 : 0.0);
+}
 __global__ void k_identity(double* I, int n) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)n * n;
        t += (long long)gridDim.x * blockDim.x)
@@ -340,12 +359,17 @@ int gssd_run(Ctx& c, int k, int s, double* h_esp, bool use_cg_hx) {
     double* HX = c.ws_hpsi.as<double>();
     if (!reuse) RS_TRY(hpsi_real<double>(c, k, s, v.x, HX, c.ng, nb));
     ProfScope ps(c, "sd_gemm", 0.0, 2.0 * 2.0 * c.ng * (double)nb * nb);
+    // S and M = dV X^T (H X) are symmetric (H is): their upper triangles only
     RS_CUBLAS(cublasDsyrk(c.cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, nb, ng, &dV, v.x, ng, &zero, S, nb));
-    RS_CUBLAS(cublasDgemm(c.cublas, CUBLAS_OP_T, CUBLAS_OP_N, nb, nb, ng, &dV, v.x, ng, HX, ng, &zero, M, nb));
+    RS_CUBLAS(cublasDsyrkx(c.cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, nb, ng, &dV, v.x, ng, HX, ng, &zero, M,
+                           nb));
   }
   {
     ProfScope ps(c, "gs");
-    k_symmetrize<<<64, 256, 0, c.stream>>>(M, nb);
+    if (!c.mixed || c.gemm_tri)
+      k_fill_lower<<<64, 256, 0, c.stream>>>(M, nb);  // the upper triangle of M was formed
+    else
+      k_symmetrize<<<64, 256, 0, c.stream>>>(M, nb);  // both triangles were formed: average
     c.launches++;
     int lwork = 0;
     RS_CUSOLVER(cusolverDnDpotrf_bufferSize(c.cusolver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, &lwork));
@@ -370,7 +394,11 @@ int gssd_run(Ctx& c, int k, int s, double* h_esp, bool use_cg_hx) {
   // S <- R^-1 V: the single rotation
   RS_CUBLAS(cublasDgemm(c.cublas, CUBLAS_OP_N, CUBLAS_OP_N, nb, nb, nb, &one, T, nb, M, nb, &zero, S, nb));
   if (c.mixed) {
-    RS_TRY(gemm_rotate_x3(c, X32, (long long)c.ng, nb, (long long)c.ng, S, nb, c.gemm_terms_rot));
+    if (c.rot_update) {
+      k_rotation_update_form<<<nb, 256, 0, c.stream>>>(S, nb);
+      c.launches++;
+    }
+    RS_TRY(gemm_rotate_x3(c, X32, (long long)c.ng, nb, (long long)c.ng, S, nb, c.gemm_terms_rot, c.rot_update != 0));
   } else {
     ProfScope ps(c, "sd_rot", 0.0, 2.0 * c.ng * (double)nb * nb);
     size_t ch = std::max<size_t>(1024, (size_t)(256u << 20) / (sizeof(double) * (size_t)nb));

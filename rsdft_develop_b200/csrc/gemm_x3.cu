@@ -6,7 +6,9 @@
 //   a0b0 + a0b1 + a1b0 + a0b2 + a1b1 + a2b0
 // accumulated in FP32 in tensor memory (about FP32 accuracy; the dropped terms are
 // O(2^-24) relative).  Split-K partial tiles are added into FP64 results.  With two terms
-// (x0, x1; products a0b0 + a0b1 + a1b0) each product is good to about 2^-16 relative.
+// (x0, x1) all four pairs are formed, (a0 + a1)(b0 + b1) exactly: each product keeps the
+// values' 16-bit representation error (about 2^-17 relative, unbiased), which a contraction
+// over K points averages down.
 //
 // Dense band-space work of the band update that runs through here in mixed precision:
 //   overlap  S = dV Psi^T Psi (Gram-Schmidt, gram_schmidt_t_module.f90 / CholQR S),
@@ -14,11 +16,11 @@
 //   rotation Psi <- Psi V        (subspace_diag_la_module.f90:190; GS: Psi <- Psi R^-1).
 //
 // Kernel structure: one CTA computes a 128 x BN output tile over a K range.  Warp 0 (one
-// elected lane) streams the 2T operand planes (T terms of A and of B) of each 64-wide K block
-// into shared memory with 3-D TMA tile loads (128B swizzle, zero fill past the matrix edge)
-// through an S-deep mbarrier ring; warp 1 (one elected lane) issues 4 x (6 or 3) tcgen05.mma
-// (term pairs x 4 K=16 steps) per block into a 128 x BN FP32 accumulator in tensor memory and
-// releases each
+// elected lane) streams the 2T operand planes (T terms of A and of B) of each KB-wide K block
+// into shared memory with 3-D TMA tile loads (128B or 64B swizzle, zero fill past the matrix
+// edge) through an S-deep mbarrier ring; warp 1 (one elected lane) issues KB/16 x (6 or 4)
+// tcgen05.mma (K=16 steps x term pairs) per block into a 128 x BN FP32 accumulator in tensor
+// memory and releases each
 // stage with tcgen05.commit; after the last block all four warps read their 32 TMEM lanes
 // with tcgen05.ld and write the tile.  Every wait is bounded: a timeout sets the device
 // status word, drains, frees the tensor memory and returns.
@@ -34,7 +36,6 @@ namespace rsdft {
 namespace x3 {
 
 constexpr int BM = 128;       // tile rows (TMEM lanes)
-constexpr int BK = 64;        // K block (128 bytes of bf16 = one swizzle row)
 constexpr int kThreads = 128;
 constexpr uint32_t kPolls = 1u << 24;
 
@@ -46,13 +47,16 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
-__device__ __forceinline__ uint64_t sw128_desc(const void* tile) {
+// K-major operand tile with rows of KB bf16 (KB = 64: 128-byte rows, 128B swizzle; KB = 32:
+// 64-byte rows, 64B swizzle), 8-row groups stored contiguously
+template <int KB>
+__device__ __forceinline__ uint64_t swz_desc(const void* tile) {
   const uint64_t addr = smem_u32(tile);
-  uint64_t d = (addr >> 4) & 0x3FFFull;  // start address
-  d |= 1ull << 16;                       // LBO = 16 B (ignored for swizzled K-major)
-  d |= 64ull << 32;                      // SBO = 1024 B between 8-row groups
-  d |= 1ull << 46;                       // descriptor version (sm_100)
-  d |= 2ull << 61;                       // SWIZZLE_128B
+  uint64_t d = (addr >> 4) & 0x3FFFull;                  // start address
+  d |= 1ull << 16;                                       // LBO = 16 B (ignored for swizzled K-major)
+  d |= (uint64_t)((8 * KB * 2) >> 4) << 32;              // SBO: bytes between 8-row groups
+  d |= 1ull << 46;                                       // descriptor version (sm_100)
+  d |= (uint64_t)(KB == 64 ? 2 : 4) << 61;               // SWIZZLE_128B / SWIZZLE_64B
   return d;
 }
 
@@ -87,10 +91,12 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
 }
 
 struct Out {
-  int mode;        // 0: C[m][n] += alpha * D (FP64 atomics); 1: Y[n*ldy + m] = D (FP32 store)
+  int mode;        // 0: C[m][n] += alpha * D (FP64 atomics); 1: Y[n*ldy + m] = D (FP32 store);
+                   // 2: Y[n*ldy + m] += D (FP32)
   double* C;       // columns n < nsplit (mode 0)
   double* C2;      // columns n >= nsplit go to C2[m][n - nsplit] (mode 0)
   int nsplit;
+  int tri;         // mode 0: only tiles reaching the triangle n <= m of each part are formed
   long long ldc;
   double alpha;
   float* Y;
@@ -98,15 +104,16 @@ struct Out {
   int M, N;        // valid extents
 };
 
-// A: T planes of [M][K], B: T planes of [N][K], bf16, K-major.  grid = (mtiles, ntiles, ksplit).
-template <int BN, int S, int T>
+// A: T planes of [M][K], B: T planes of [N][K], bf16, K-major, in K blocks of KB.
+// grid = (mtiles, ntiles, ksplit).
+template <int BN, int S, int T, int KB>
 __global__ void __launch_bounds__(kThreads, 1) k_gemm_x3(const __grid_constant__ CUtensorMap ta,
                                                         const __grid_constant__ CUtensorMap tb, int kblocks_total,
                                                         int kblocks_per_split, Out o, unsigned* status) {
-  constexpr int A_BYTES = BM * BK * 2;       // one plane tile, 16 KB
-  constexpr int B_BYTES = BN * BK * 2;
+  constexpr int A_BYTES = BM * KB * 2;       // one plane tile
+  constexpr int B_BYTES = BN * KB * 2;
   constexpr int STAGE = T * A_BYTES + T * B_BYTES;
-  constexpr int NP = T == 3 ? 6 : 3;  // term pairs formed
+  constexpr int NP = T == 3 ? 6 : 4;  // term pairs formed
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // 1024-byte alignment of every tile (swizzle atoms)
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -117,6 +124,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_x3(const __grid_constant__
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  // symmetric results: a tile wholly above the diagonal (n > m everywhere) is left out
+  if (o.tri && (n0 >= o.nsplit ? n0 - o.nsplit : n0) >= m0 + BM) return;
   const int kb0 = blockIdx.z * kblocks_per_split;
   const int kb1 = min(kblocks_total, kb0 + kblocks_per_split);
   const int nkb = kb1 - kb0;
@@ -151,15 +160,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_x3(const __grid_constant__
         }
         unsigned char* st = smem + s * STAGE;
         mbar_arrive_expect_tx(&full[s], (uint32_t)STAGE);
-        const int kx = (kb0 + i) * BK;
+        const int kx = (kb0 + i) * KB;
         for (int t = 0; t < T; ++t) tma_load_3d(st + t * A_BYTES, &ta, kx, m0, t, &full[s]);
         for (int t = 0; t < T; ++t) tma_load_3d(st + T * A_BYTES + t * B_BYTES, &tb, kx, n0, t, &full[s]);
       }
     } else if (warp == 1 && lane == 0) {
       // MMA issuer: M=128, N=BN, bf16 x bf16 -> f32, both K-major
       const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
-      const int ta_[6] = {0, 0, 1, 0, 1, 2};
-      const int tb_[6] = {0, 1, 0, 2, 1, 0};
+      // three terms: the six leading pairs; two terms: all four pairs (the exact product of
+      // the two-term values, so no pair is dropped and the rounding left is unbiased)
+      const int ta_[6] = {0, 0, 1, T == 3 ? 0 : 1, 1, 2};
+      const int tb_[6] = {0, 1, 0, T == 3 ? 2 : 1, 1, 0};
       for (int i = 0; i < nkb; ++i) {
         const int s = i % S;
         if (!mbar_wait_bounded(&full[s], (uint32_t)((i / S) & 1), kPolls)) {
@@ -169,11 +180,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_x3(const __grid_constant__
         fence_after();
         unsigned char* st = smem + s * STAGE;
 #pragma unroll
-        for (int kk = 0; kk < BK / 16; ++kk) {
+        for (int kk = 0; kk < KB / 16; ++kk) {
 #pragma unroll
           for (int p = 0; p < NP; ++p) {
-            const uint64_t da = sw128_desc(st + ta_[p] * A_BYTES) + (uint64_t)(kk * 2);
-            const uint64_t db = sw128_desc(st + T * A_BYTES + tb_[p] * B_BYTES) + (uint64_t)(kk * 2);
+            const uint64_t da = swz_desc<KB>(st + ta_[p] * A_BYTES) + (uint64_t)(kk * 2);
+            const uint64_t db = swz_desc<KB>(st + T * A_BYTES + tb_[p] * B_BYTES) + (uint64_t)(kk * 2);
             mma_bf16(tmem, da, db, idesc, (i > 0 || kk > 0 || p > 0) ? 1u : 0u);
           }
         }
@@ -208,11 +219,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_x3(const __grid_constant__
               atomicAdd(dst, o.alpha * (double)v[j]);
             }
           }
-        } else {
+        } else if (o.mode == 1) {
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
             const int col = n0 + c0 + j;
             if (col < o.N) o.Y[(long long)col * o.ldy + row] = v[j];
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const int col = n0 + c0 + j;
+            if (col < o.N) o.Y[(long long)col * o.ldy + row] += v[j];
           }
         }
       }
@@ -312,31 +329,43 @@ static int get_encode() {
   return 0;
 }
 
-// 3-D map over [planes][rows][kpad] bf16 (plane stride plane_rows x kpad), box {64, box_rows, 1},
-// 128B swizzle
+// Tile shape of a contraction: three terms, 128 x 128 tiles in K blocks of 64 (2 stages of
+// 96 KB) or, wide (the default), 128 x 256 tiles in K blocks of 32 (3 stages of 72 KB: each
+// operand byte feeds twice the products); two terms, 128 x 256 tiles in K blocks of 64.
+struct TileCfg {
+  int bn, kb;
+};
+static TileCfg tile_for(const Ctx& c, int terms) {
+  if (terms == 2) return {256, 64};
+  return c.gemm_wide ? TileCfg{256, 32} : TileCfg{128, 64};
+}
+
+// 3-D map over [planes][rows][kpad] bf16 (plane stride plane_rows x kpad), box {kb, box_rows, 1},
+// 128B swizzle (kb = 64) or 64B swizzle (kb = 32)
 static int make_map(CUtensorMap* m, const void* base, long long rows, long long kpad, int box_rows, int planes,
-                    long long plane_rows) {
+                    long long plane_rows, int kb) {
   RS_TRY(get_encode());
   cuuint64_t dims[3] = {(cuuint64_t)kpad, (cuuint64_t)rows, (cuuint64_t)planes};
   cuuint64_t strides[2] = {(cuuint64_t)kpad * 2, (cuuint64_t)plane_rows * kpad * 2};
-  cuuint32_t box[3] = {64, (cuuint32_t)box_rows, 1};
+  cuuint32_t box[3] = {(cuuint32_t)kb, (cuuint32_t)box_rows, 1};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims, strides, box, estr,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                        CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        kb == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   RS_CHECK(r == CUDA_SUCCESS, RSDFT_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
   return 0;
 }
 
-template <int BN, int S, int T>
+template <int BN, int S, int T, int KB>
 static int launch_x3(Ctx& c, const CUtensorMap& ta, const CUtensorMap& tb, int M, int N, long long kpad,
                      const x3::Out& o, int ksplit) {
-  const int kbt = (int)(kpad / x3::BK);
+  const int kbt = (int)(kpad / KB);
   const int kps = (kbt + ksplit - 1) / ksplit;
   ksplit = (kbt + kps - 1) / kps;
-  constexpr int STAGE = T * x3::BM * x3::BK * 2 + T * BN * x3::BK * 2;
+  constexpr int STAGE = T * x3::BM * KB * 2 + T * BN * KB * 2;
   const size_t smem = (size_t)S * STAGE + 1024 + 256;
-  auto kern = x3::k_gemm_x3<BN, S, T>;
+  auto kern = x3::k_gemm_x3<BN, S, T, KB>;
   static bool attr = false;
   if (!attr) {
     RS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -348,15 +377,12 @@ static int launch_x3(Ctx& c, const CUtensorMap& ta, const CUtensorMap& tb, int M
   return check_launch("gemm_x3");
 }
 
-// Tile width by term count: three terms, 128 x 128 tiles in 2 stages of 96 KB; two terms,
-// 128 x 256 tiles in 2 stages of 96 KB (the wider tile reads each operand byte for twice the
-// products, which the two-term form needs: its loads per product are 1.5x the three-term's).
-static int bn_for(int terms) { return terms == 3 ? 128 : 256; }
-
 static int launch_terms(Ctx& c, int terms, const CUtensorMap& ta, const CUtensorMap& tb, int M, int N, long long kpad,
                         const x3::Out& o, int ksplit) {
-  if (terms == 3) return launch_x3<128, 2, 3>(c, ta, tb, M, N, kpad, o, ksplit);
-  return launch_x3<256, 2, 2>(c, ta, tb, M, N, kpad, o, ksplit);
+  const TileCfg t = tile_for(c, terms);
+  if (terms == 2) return launch_x3<256, 2, 2, 64>(c, ta, tb, M, N, kpad, o, ksplit);
+  if (t.bn == 256) return launch_x3<256, 3, 3, 32>(c, ta, tb, M, N, kpad, o, ksplit);
+  return launch_x3<128, 2, 3, 64>(c, ta, tb, M, N, kpad, o, ksplit);
 }
 
 // Split-K chunk of a contraction with rows_total operand rows: the BF16 planes of one chunk stay
@@ -366,8 +392,9 @@ static long long chunk_k(long long rows_total, int terms, long long K) {
   return std::min<long long>(kc_max, (K + 63) / 64 * 64);
 }
 
-static int split_ksplit(int M, int N, int kpad, int bn) {
-  const int tiles = ((M + 127) / 128) * ((N + bn - 1) / bn);
+static int split_ksplit(int M, int N, int kpad, int bn, bool tri = false) {
+  int tiles = ((M + 127) / 128) * ((N + bn - 1) / bn);
+  if (tri) tiles = (tiles + ((M + 127) / 128)) / 2;  // about half the tiles are formed
   const int kbt = kpad / 64;
   return std::max(1, std::min(kbt, (2 * 148 + tiles - 1) / tiles));
 }
@@ -382,7 +409,7 @@ int gemm_tn_x3(Ctx& c, const float* A, long long lda, int M, const float* B, lon
   RS_TRY(c.ws_gemm.ensure(sizeof(__nv_bfloat16) * terms * (size_t)(M + N) * kc));
   __nv_bfloat16* PA = c.ws_gemm.as<__nv_bfloat16>();
   __nv_bfloat16* PB = PA + terms * (size_t)M * kc;
-  const double flops = 2.0 * (terms == 3 ? 6.0 : 3.0) * (double)M * N * K;
+  const double flops = 2.0 * (terms == 3 ? 6.0 : 4.0) * (double)M * N * K;
   ProfScope ps(c, "gemm", 0.0, flops);
   for (long long k0 = 0; k0 < K; k0 += kc) {
     const int kcur = (int)std::min<long long>(kc, K - k0);
@@ -392,25 +419,28 @@ int gemm_tn_x3(Ctx& c, const float* A, long long lda, int M, const float* B, lon
     c.launches += 2;
     RS_TRY(check_launch("split_rows"));
     CUtensorMap ta, tb;
-    RS_TRY(make_map(&ta, PA, M, kpad, x3::BM, terms, M));
-    RS_TRY(make_map(&tb, PB, N, kpad, bn_for(terms), terms, N));
+    const TileCfg tc = tile_for(c, terms);
+    RS_TRY(make_map(&ta, PA, M, kpad, x3::BM, terms, M, tc.kb));
+    RS_TRY(make_map(&tb, PB, N, kpad, tc.bn, terms, N, tc.kb));
     x3::Out o{};
     o.mode = 0; o.C = C; o.C2 = C; o.nsplit = N; o.ldc = ldc; o.alpha = alpha; o.M = M; o.N = N;
-    RS_TRY(launch_terms(c, terms, ta, tb, M, N, kpad, o, split_ksplit(M, N, kpad, bn_for(terms))));
+    RS_TRY(launch_terms(c, terms, ta, tb, M, N, kpad, o, split_ksplit(M, N, kpad, tc.bn)));
   }
   return 0;
 }
 
 // S[m][n] += alpha * sum_k X[m][k] X[n][k] and M[m][n] += alpha * sum_k X[m][k] Y[n][k] in one
 // contraction of X against [X; Y] (N = 2 nb): X is split once per chunk and serves as A and as
-// the first nb rows of B.  X, Y: [nb][ld] FP32; S, M: nb x nb, leading dimension nb.
+// the first nb rows of B.  X, Y: [nb][ld] FP32; S, M: nb x nb, leading dimension nb.  Both are
+// symmetric (Y = H X with H symmetric), so only the tiles reaching n <= m are formed: complete
+// for n <= m (the upper triangle of the column-major matrices), partial above.
 int gemm_tn2_x3(Ctx& c, const float* X, const float* Y, long long ld, int nb, long long K, double alpha, double* S,
                 double* M, int terms) {
   RS_CHECK(terms == 2 || terms == 3, RSDFT_ERR_ARG, "split terms must be 2 or 3");
   const long long kc = chunk_k(2LL * nb, terms, K);
   RS_TRY(c.ws_gemm.ensure(sizeof(__nv_bfloat16) * terms * (size_t)(2 * nb) * kc));
   __nv_bfloat16* P = c.ws_gemm.as<__nv_bfloat16>();
-  const double flops = 2.0 * (terms == 3 ? 6.0 : 3.0) * (double)nb * (2.0 * nb) * K;
+  const double flops = 2.0 * (terms == 3 ? 6.0 : 4.0) * (double)nb * (2.0 * nb) * K;
   ProfScope ps(c, "gemm", 0.0, flops);
   for (long long k0 = 0; k0 < K; k0 += kc) {
     const int kcur = (int)std::min<long long>(kc, K - k0);
@@ -422,18 +452,22 @@ int gemm_tn2_x3(Ctx& c, const float* X, const float* Y, long long ld, int nb, lo
     c.launches += 2;
     RS_TRY(check_launch("split_rows"));
     CUtensorMap ta, tb;
-    RS_TRY(make_map(&ta, P, nb, kpad, x3::BM, terms, 2LL * nb));
-    RS_TRY(make_map(&tb, P, 2LL * nb, kpad, bn_for(terms), terms, 2LL * nb));
+    const TileCfg tc = tile_for(c, terms);
+    RS_TRY(make_map(&ta, P, nb, kpad, x3::BM, terms, 2LL * nb, tc.kb));
+    RS_TRY(make_map(&tb, P, 2LL * nb, kpad, tc.bn, terms, 2LL * nb, tc.kb));
     x3::Out o{};
     o.mode = 0; o.C = S; o.C2 = M; o.nsplit = nb; o.ldc = nb; o.alpha = alpha; o.M = nb; o.N = 2 * nb;
-    RS_TRY(launch_terms(c, terms, ta, tb, nb, 2 * nb, kpad, o, split_ksplit(nb, 2 * nb, kpad, bn_for(terms))));
+    o.tri = c.gemm_tri;
+    RS_TRY(launch_terms(c, terms, ta, tb, nb, 2 * nb, kpad, o, split_ksplit(nb, 2 * nb, kpad, tc.bn, c.gemm_tri != 0)));
   }
   return 0;
 }
 
 // X[n][g] <- sum_m X[m][g] V[m][n] for all g (in place, grid chunks); X: [nb][ldx] FP32,
-// V: nb x nb FP64 column-major (ldv).
-int gemm_rotate_x3(Ctx& c, float* X, long long ldx, int nb, long long G, const double* V, int ldv, int terms) {
+// V: nb x nb FP64 column-major (ldv).  add: X[n][g] <- X[n][g] + sum_m X[m][g] V[m][n] (the
+// update form X (I + V): with V small the FP32 accumulation error scales with |X V|, not |X|).
+int gemm_rotate_x3(Ctx& c, float* X, long long ldx, int nb, long long G, const double* V, int ldv, int terms,
+                   bool add) {
   RS_CHECK(terms == 2 || terms == 3, RSDFT_ERR_ARG, "split terms must be 2 or 3");
   const int nbpad = (nb + 63) / 64 * 64;
   const long long gc_max = std::max<long long>(128, ((long long)(512u << 20) / (2LL * terms * nbpad)) / 128 * 128);
@@ -441,12 +475,13 @@ int gemm_rotate_x3(Ctx& c, float* X, long long ldx, int nb, long long G, const d
   RS_TRY(c.ws_gemm.ensure(sizeof(__nv_bfloat16) * terms * ((size_t)gc * nbpad + (size_t)nb * nbpad)));
   __nv_bfloat16* PV = c.ws_gemm.as<__nv_bfloat16>();
   __nv_bfloat16* PX = PV + terms * (size_t)nb * nbpad;
-  const double flops = 2.0 * (terms == 3 ? 6.0 : 3.0) * (double)nb * nb * G;
+  const double flops = 2.0 * (terms == 3 ? 6.0 : 4.0) * (double)nb * nb * G;
   ProfScope ps(c, "gemm", 0.0, flops);
   x3::k_split_small<<<4 * 148, 256, 0, c.stream>>>(V, ldv, nb, nbpad, PV, terms);
   c.launches++;
   CUtensorMap tb;
-  RS_TRY(make_map(&tb, PV, nb, nbpad, bn_for(terms), terms, nb));
+  const TileCfg tc = tile_for(c, terms);
+  RS_TRY(make_map(&tb, PV, nb, nbpad, tc.bn, terms, nb, tc.kb));
   for (long long g0 = 0; g0 < G; g0 += gc) {
     const int gcur = (int)std::min<long long>(gc, G - g0);
     dim3 tg((gcur + 31) / 32, (nbpad + 31) / 32);
@@ -454,9 +489,9 @@ int gemm_rotate_x3(Ctx& c, float* X, long long ldx, int nb, long long G, const d
     c.launches++;
     RS_TRY(check_launch("split_transpose"));
     CUtensorMap ta;
-    RS_TRY(make_map(&ta, PX, gcur, nbpad, x3::BM, terms, gcur));
+    RS_TRY(make_map(&ta, PX, gcur, nbpad, x3::BM, terms, gcur, tc.kb));
     x3::Out o{};
-    o.mode = 1; o.Y = X + g0; o.ldy = ldx; o.M = gcur; o.N = nb;
+    o.mode = add ? 2 : 1; o.Y = X + g0; o.ldy = ldx; o.M = gcur; o.N = nb;
     RS_TRY(launch_terms(c, terms, ta, tb, gcur, nb, nbpad, o, 1));
   }
   return 0;
@@ -528,7 +563,7 @@ int selftest_gemm(Ctx& c, int m, int n, long long k, int op, int terms, double* 
     if (cublasDgemm(c.cublas, CUBLAS_OP_N, CUBLAS_OP_N, (int)k, m, m, &one, ad.as<double>(), (int)k, v.as<double>(), m,
                     &zero, cref.as<double>(), (int)k) != CUBLAS_STATUS_SUCCESS)
       RS_CHECK(false, RSDFT_ERR_CUDA, "reference dgemm failed");
-    RS_TRY(gemm_rotate_x3(c, a.as<float>(), k, m, k, v.as<double>(), m, terms));
+    RS_TRY(gemm_rotate_x3(c, a.as<float>(), k, m, k, v.as<double>(), m, terms, false));
     std::vector<float> hy((size_t)na);
     h2.resize((size_t)na);
     RS_CUDA(cudaMemcpyAsync(hy.data(), a.p, sizeof(float) * hy.size(), cudaMemcpyDeviceToHost, c.stream));

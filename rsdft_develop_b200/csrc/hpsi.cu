@@ -119,11 +119,83 @@ int record_segment_max(Ctx& c, int tile_y) {
   return mx;
 }
 
-// vloc_override / c0_shift: the kinetic-only operator (T + shift) used for training targets
+// ---------------------------------------------------------------------------
+// nonlocal scatter after the stencil: out_b[pt] += sum over the point's records r
+// uV_r . c_b[atom_r] (src/ps_nloc_mr_module.f90:1159-1258, the psi(JJP) += uVk ... update).
+// One thread per grid point that some projector reaches (the covered list, ascending), bands
+// looped inside the CTA so the point's few records stay in L1; one read-modify-write of H psi
+// per covered point and band.
+// ---------------------------------------------------------------------------
+template <typename T, int PG>
+__global__ void __launch_bounds__(256) k_nl_scatter(const int* __restrict__ cov, int ncov,
+                                                    const int* __restrict__ rowptr, const int* __restrict__ rg,
+                                                    const T* __restrict__ ru, int pgr, const T* __restrict__ coef,
+                                                    int ldc, T* __restrict__ out, long long ld, int nb, int bchunk) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ncov) return;
+  const int pt = __ldg(cov + i);
+  const int r0 = __ldg(rowptr + pt), r1 = __ldg(rowptr + pt + 1);
+  const int b0 = blockIdx.y * bchunk, b1 = min(nb, b0 + bchunk);
+  const int np = PG > 0 ? PG : pgr;
+  constexpr int BU = 4;  // bands in flight per thread
+  for (int b = b0; b < b1; b += BU) {
+    T acc[BU], cur[BU];
+#pragma unroll
+    for (int u = 0; u < BU; ++u) {
+      acc[u] = T(0);
+      cur[u] = b + u < b1 ? out[(size_t)(b + u) * ld + pt] : T(0);
+    }
+    for (int r = r0; r < r1; ++r) {
+      const T* uv = ru + (size_t)r * np;
+      const size_t go = (size_t)__ldg(rg + r) * np;
+#pragma unroll
+      for (int u = 0; u < BU; ++u) {
+        if (b + u >= b1) break;
+        const T* cc = coef + (size_t)(b + u) * ldc + go;
+#pragma unroll
+        for (int q = 0; q < (PG > 0 ? PG : 1); ++q) acc[u] = ::fma(__ldg(uv + q), __ldg(cc + q), acc[u]);
+        if (PG == 0)
+          for (int q = 1; q < np; ++q) acc[u] = ::fma(__ldg(uv + q), __ldg(cc + q), acc[u]);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < BU; ++u)
+      if (b + u < b1) out[(size_t)(b + u) * ld + pt] = cur[u] + acc[u];
+  }
+}
+
+template <typename T>
+static int nl_scatter(Ctx& c, int k, const T* coef, T* out, size_t ld, int nb) {
+  const NonlocalTables& nl = c.nl;
+  if (nl.ncov == 0 || nb <= 0) return 0;
+  const T* ru = std::is_same<T, double>::value ? (const T*)nl.perk[k].ru64.as<double>()
+                                               : (const T*)nl.perk[k].ru32.as<float>();
+  const int ldc = nl.ngroups * nl.pg;
+  const int bchunk = 16;
+  const dim3 grid((nl.ncov + 255) / 256, (nb + bchunk - 1) / bchunk);
+  ProfScope ps(c, "nl_scatter", (double)nb * nl.ncov * 2.0 * sizeof(T) + (double)nl.nrec * (4 + nl.pg * sizeof(T)));
+  if (nl.pg == 4)
+    k_nl_scatter<T, 4><<<grid, 256, 0, c.stream>>>(nl.cov.as<int>(), nl.ncov, nl.rec_rowptr.as<int>(),
+                                                    nl.rec_g.as<int>(), ru, nl.pg, coef, ldc, out, (long long)ld, nb,
+                                                    bchunk);
+  else
+    k_nl_scatter<T, 0><<<grid, 256, 0, c.stream>>>(nl.cov.as<int>(), nl.ncov, nl.rec_rowptr.as<int>(),
+                                                    nl.rec_g.as<int>(), ru, nl.pg, coef, ldc, out, (long long)ld, nb,
+                                                    bchunk);
+  c.launches++;
+  return check_launch("nl_scatter");
+}
+
+// vloc_override / c0_shift: the kinetic-only operator (T + shift) used for training targets.
+// With coef the nonlocal term is added: by the separate scatter kernel after the stencil
+// (default), or inside the stencil (c.nl_fused).
 template <typename T, int MD>
 static int launch_stencil(Ctx& c, int k, int s, const T* psi, T* out, size_t ld, int nb, const T* coef,
                           const T* vloc_override = nullptr, double c0_shift = 0.0) {
-  return launch_stencil_stream<T, MD>(c, k, s, psi, out, ld, nb, coef, vloc_override, c0_shift);
+  if (coef == nullptr || c.nl_fused)
+    return launch_stencil_stream<T, MD>(c, k, s, psi, out, ld, nb, coef, vloc_override, c0_shift);
+  RS_TRY((launch_stencil_stream<T, MD>(c, k, s, psi, out, ld, nb, nullptr, vloc_override, c0_shift)));
+  return nl_scatter<T>(c, k, coef, out, ld, nb);
 }
 
 template <typename T>

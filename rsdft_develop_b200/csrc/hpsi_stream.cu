@@ -22,8 +22,9 @@
 //    row and clears them (two buffers by plane parity; the per-step barrier orders both).
 //  * R (rows per thread: register blocking against occupancy) is picked per shape by timing
 //    both variants on the first call (autotuning).
-// All waits are bounded; a timeout sets the device status word (RSDFT_ERR_TIMEOUT) and every
-// CTA drains its own copies in flight before it exits.
+// Thread 0 issues the plane stages and thread 32 the record segments.  All waits are bounded;
+// a timeout sets the device status word (RSDFT_ERR_TIMEOUT) and every CTA drains its own
+// copies in flight before it exits.
 #include "stencil.cuh"
 
 namespace rsdft {
@@ -208,7 +209,10 @@ __global__ void __launch_bounds__(256, 3 - R) k_stencil_stream(const StArgs<T, M
   if (rw < nwork) rit = item_of<T, MD>(a, rw);
   int pf_rs = 0, pf_re = 0;  // row pointers of the record cursor's plane (loaded a step ahead)
   auto rec_base = [&]() { return ((rit.z0 + rpi) * n2 + rit.y0) * n1; };
-  if (tid == 0 && nl_on && RS > 0 && rw < nwork) {
+  // thread 0 issues the plane stages, thread kRecTid (another warp) the record segments, so
+  // that neither warp carries both producers' work into the per-step barrier
+  const int rec_tid = blockDim.x > 32 ? 32 : 0;
+  if (tid == rec_tid && nl_on && RS > 0 && rw < nwork) {
     pf_rs = __ldg(a.rec_rowptr + rec_base());
     pf_re = __ldg(a.rec_rowptr + rec_base() + rit.ty_valid * n1);
   }
@@ -319,8 +323,10 @@ __global__ void __launch_bounds__(256, 3 - R) k_stencil_stream(const StArgs<T, M
       if (tid == 0) {
         fence_proxy_async_smem();  // slots refilled below were read through the generic proxy
         while (gis < gq + S && pw < nwork) issue_stage();
-        if (nl_on && RS > 0)
-          while (gri < grc + RS && rw < nwork) issue_rec();
+      }
+      if (tid == rec_tid && nl_on && RS > 0) {
+        fence_proxy_async_smem();
+        while (gri < grc + RS && rw < nwork) issue_rec();
       }
       const int slot = (int)(gq % S);
       bool ok = mbar_wait_bounded(&bar[slot], (uint32_t)((gq / S) & 1), kWaitPolls);
@@ -487,12 +493,15 @@ __global__ void __launch_bounds__(256, 3 - R) k_stencil_stream(const StArgs<T, M
       }
     }
   }
+  // drain copies still in flight before the CTA's shared memory is released (each producer its
+  // own ring, only the phases not consumed: a slot's barrier has moved on past earlier ones)
   if (aborted && tid == 0) {
     atomicOr(a.status, DEV_WAIT_TIMEOUT);
-    // drain copies still in flight before the CTA's shared memory is released
     for (long long q = gq; q < gis; ++q) mbar_wait_bounded(&bar[q % S], (uint32_t)((q / S) & 1), kWaitPolls);
-    for (long long q = grc; q < gri; ++q) mbar_wait_bounded(&recfull[q % RS], (uint32_t)((q / RS) & 1), kWaitPolls);
   }
+  if (aborted && tid == rec_tid)
+    for (long long q = grc; q < gri; ++q) mbar_wait_bounded(&recfull[q % RS], (uint32_t)((q / RS) & 1), kWaitPolls);
+  if (aborted) __syncthreads();
 }
 
 // One variant (rows per thread R) configured for this grid and launched on the library stream.

@@ -1,6 +1,6 @@
 """Drive one kernel family on the GPU for timing and ncu captures.
 
-    python -m rsdft_develop_b200.profile_kernels gemm [m] [k] [terms]   # split-BF16 tcgen05 GEMMs
+    python -m rsdft_develop_b200.profile_kernels gemm [m] [k] [terms] [wide|narrow]   # split-BF16 tcgen05 GEMMs
     python -m rsdft_develop_b200.profile_kernels pc|pc32 [config] [bands]   # precond_hprsdft (FP64 / FP32)
     python -m rsdft_develop_b200.profile_kernels lpc [config] [bands] [tc|fp32]  # learned preconditioner
 
@@ -26,15 +26,17 @@ def main(argv=None):
         m = int(argv[1]) if len(argv) > 1 else 256
         k = int(argv[2]) if len(argv) > 2 else 262144
         terms = int(argv[3]) if len(argv) > 3 else 3
+        wide = (argv[4] if len(argv) > 4 else "wide") == "wide"
         with api.BandUpdate(synth.make_problem("t0")) as g:
             g.gemm_terms(terms, terms)
+            g.gemm_tile(wide)
             g.selftest_gemm(m, m, k, 0)  # untimed: module load, tensor-map encoder
             g.profile(True)
             e0 = g.selftest_gemm(m, m, k, 0)
             ms0, _, _, fl0 = g.profile_get("gemm")
             e1 = g.selftest_gemm(m, m, k, 1)
             ms, n, _, fl = g.profile_get("gemm")
-            print(f"gemm m={m} k={k} terms={terms}: overlap rel.err {e0:.2e} {ms0:.3f} ms "
+            print(f"gemm m={m} k={k} terms={terms} {'wide' if wide else 'narrow'}: overlap rel.err {e0:.2e} {ms0:.3f} ms "
                   f"({fl0 / max(ms0, 1e-9) / 1e9:.0f} TFLOP/s bf16), rotation rel.err {e1:.2e} {ms - ms0:.3f} ms "
                   f"({(fl - fl0) / max(ms - ms0, 1e-9) / 1e9:.0f} TFLOP/s bf16); {n} calls")
         return

@@ -43,6 +43,27 @@ def test_hpsi_fp32_matches_oracle(oracle_mod, name):
     assert _rel(out.astype(np.float64), ref) < TOL32
 
 
+@pytest.mark.parametrize("fp32", [False, True])
+@pytest.mark.parametrize("name", ["t1", "c0", "c2"])
+def test_hpsi_nonlocal_forms_agree(oracle_mod, name, fp32):
+    """The nonlocal term added inside the streaming stencil and by the scatter kernel after it
+    (the default) both match the oracle."""
+    prob = synth.make_problem(name)
+    o = oracle_mod.Oracle(prob)
+    psi = synth.random_wavefunctions(24, 6, prob.ng)
+    if fp32:
+        psi = psi.astype(np.float32).astype(np.float64)
+    ref = o.hpsi(psi)
+    outs = []
+    with api.BandUpdate(prob) as g:
+        for fused in (True, False):
+            g.nl_form(fused)
+            out = g.hamiltonian(psi, fp32=fp32)
+            outs.append(out.astype(np.float64))
+            assert _rel(outs[-1], ref) < (TOL32 if fp32 else TOL64), fused
+    assert _rel(outs[0], outs[1]) < (TOL32 if fp32 else TOL64)
+
+
 def test_hpsi_without_nonlocal(oracle_mod):
     prob = synth.make_problem("c0")
     o = oracle_mod.Oracle(prob, nonlocal_on=False)

@@ -15,18 +15,23 @@ from tests import npref
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("m,n,k,tol", [(256, 256, 262144, 5e-5), (100, 37, 1000, 5e-6), (384, 200, 70000, 5e-5)])
-def test_gemm_x3_overlap_vs_dgemm(m, n, k, tol):
+@pytest.mark.parametrize("wide", [True, False])
+@pytest.mark.parametrize("m,n,k,tol", [(256, 256, 262144, 5e-5), (100, 37, 1000, 5e-6), (384, 200, 70000, 5e-5),
+                                      (300, 520, 4160, 5e-6)])
+def test_gemm_x3_overlap_vs_dgemm(m, n, k, tol, wide):
     with api.BandUpdate(synth.make_problem("t0")) as g:
         g.gemm_terms(3, 3)
+        g.gemm_tile(wide)
         err = g.selftest_gemm(m, n, k, 0)
     assert err < tol
 
 
-@pytest.mark.parametrize("m,k", [(256, 262144), (37, 1000), (1024, 50000)])
-def test_gemm_x3_rotation_vs_dgemm(m, k):
+@pytest.mark.parametrize("wide", [True, False])
+@pytest.mark.parametrize("m,k", [(256, 262144), (37, 1000), (1024, 50000), (300, 4160)])
+def test_gemm_x3_rotation_vs_dgemm(m, k, wide):
     with api.BandUpdate(synth.make_problem("t0")) as g:
         g.gemm_terms(3, 3)
+        g.gemm_tile(wide)
         err = g.selftest_gemm(m, m, k, 1)
     assert err < 2e-5
 
