@@ -223,7 +223,8 @@ int rsdft_gpu_profile_get(const char* name, double* total_ms, long long* launche
 /* Launch count of all library kernels since init (for launch accounting). */
 long long rsdft_gpu_kernel_launches(void);
 /* Diagnostic: the split-BF16 tensor-core GEMM against cuBLAS DGEMM on the same FP32 inputs.
- * op 0: C = A B^T (A: m x k, B: n x k); op 1: X <- X V (X: m bands x k points, V: m x m).
+ * op 0: C = A B^T (A: m x k, B: n x k); op 1: X <- X V (X: m bands x k points, V: m x m);
+ * op 2 (n == m): the fused overlap/Hsub form [A A^T | A B^T] as the sweep computes it.
  * err receives max|x3 - dgemm| / max|dgemm|.  No counterpart in the reference. */
 int rsdft_gpu_selftest_gemm(int m, int n, long long k, int op, double* err);
 /* BF16 terms per FP32 value in the mixed-precision tensor-core contractions (2 or 3 each):

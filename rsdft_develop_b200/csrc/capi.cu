@@ -728,8 +728,8 @@ long long rsdft_gpu_kernel_launches(void) { return g_ctx ? g_ctx->launches : 0; 
 
 int rsdft_gpu_selftest_gemm(int m, int n, long long k, int op, double* err) {
   REQUIRE_CTX();
-  RS_CHECK(m > 0 && n > 0 && k > 0 && err && (op == 0 || op == 1), RSDFT_ERR_ARG, "bad selftest arguments");
-  RS_TRY(selftest_gemm(*g_ctx, m, n, k, op, op == 0 ? g_ctx->gemm_terms_sm : g_ctx->gemm_terms_rot, err));
+  RS_CHECK(m > 0 && n > 0 && k > 0 && err && op >= 0 && op <= 2, RSDFT_ERR_ARG, "bad selftest arguments");
+  RS_TRY(selftest_gemm(*g_ctx, m, n, k, op, op == 1 ? g_ctx->gemm_terms_rot : g_ctx->gemm_terms_sm, err));
   return check_status(*g_ctx);
 }
 

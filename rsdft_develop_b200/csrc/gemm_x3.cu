@@ -124,8 +124,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_x3(const __grid_constant__
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-  // symmetric results: a tile wholly above the diagonal (n > m everywhere) is left out
-  if (o.tri && (n0 >= o.nsplit ? n0 - o.nsplit : n0) >= m0 + BM) return;
+  // symmetric results: a tile wholly above the diagonal (n > m everywhere) is left out; a tile
+  // that straddles the two parts is judged by the smallest column of each part it holds
+  if (o.tri) {
+    const bool s_part = n0 < o.nsplit, m_part = n0 + BN > o.nsplit;
+    const bool s_above = !s_part || n0 >= m0 + BM;
+    const bool m_above = !m_part || max(n0 - o.nsplit, 0) >= m0 + BM;
+    if (s_above && m_above) return;
+  }
   const int kb0 = blockIdx.z * kblocks_per_split;
   const int kb1 = min(kblocks_total, kb0 + kblocks_per_split);
   const int nkb = kb1 - kb0;
@@ -273,6 +279,42 @@ __global__ void k_split_rows(const float* __restrict__ X, long long ldx, int row
   }
 }
 
+// FP32 value into three BF16 terms in FP32 arithmetic: x - bf16(x) and the next remainder are
+// exact in FP32, so the terms equal those of the FP64 split of the same value
+__device__ __forceinline__ void split3f(float x, __nv_bfloat16& a, __nv_bfloat16& b, __nv_bfloat16& c) {
+  a = __float2bfloat16(x);
+  const float r = x - __bfloat162float(a);
+  b = __float2bfloat16(r);
+  c = __float2bfloat16(r - __bfloat162float(b));
+}
+
+// k_split_rows for 16-byte aligned rows: four consecutive K values per thread (one 16-byte load,
+// one 8-byte store per term plane).  rows * kpad / 4 < 2^31.
+__global__ void k_split_rows4(const float* __restrict__ X, long long ldx, int rows, long long k0, int kc, int kpad,
+                              __nv_bfloat16* __restrict__ P, long long plane, int terms) {
+  const int g4 = kpad >> 2;
+  const int n = rows * g4;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int r = t / g4, kk = (t - r * g4) << 2;
+    const float* src = X + (long long)r * ldx + k0 + kk;
+    float v[4] = {0.f, 0.f, 0.f, 0.f};
+    if (kk + 3 < kc) {
+      const float4 x = *reinterpret_cast<const float4*>(src);
+      v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+    } else {
+      for (int i = 0; i < 4; ++i)
+        if (kk + i < kc) v[i] = src[i];
+    }
+    __align__(8) __nv_bfloat16 a[4], b[4], c[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) split3f(v[i], a[i], b[i], c[i]);
+    const long long o = (long long)r * kpad + kk;
+    *reinterpret_cast<uint2*>(P + o) = *reinterpret_cast<const uint2*>(a);
+    *reinterpret_cast<uint2*>(P + plane + o) = *reinterpret_cast<const uint2*>(b);
+    if (terms == 3) *reinterpret_cast<uint2*>(P + 2 * plane + o) = *reinterpret_cast<const uint2*>(c);
+  }
+}
+
 // planes[t][g][m] = split(X[m][g0 + g]) : transposed chunk (32x32 smem tiles)
 __global__ void k_split_transpose(const float* __restrict__ X, long long ldx, int nb, long long g0, int gc, int nbpad,
                                   __nv_bfloat16* __restrict__ P, int terms) {
@@ -385,6 +427,18 @@ static int launch_terms(Ctx& c, int terms, const CUtensorMap& ta, const CUtensor
   return launch_x3<128, 2, 3, 64>(c, ta, tb, M, N, kpad, o, ksplit);
 }
 
+// X rows [0, rows) from column k0 into the term planes (pstride elements apart) of one chunk
+static void split_rows(Ctx& c, const float* X, long long ldx, int rows, long long k0, int kc, int kpad,
+                       __nv_bfloat16* P, int swap, long long pstride, int terms) {
+  const bool vec = !swap && (reinterpret_cast<uintptr_t>(X) & 15) == 0 && ldx % 4 == 0 && k0 % 4 == 0 &&
+                   (long long)rows * (kpad / 4) < (1LL << 31);
+  if (vec)
+    x3::k_split_rows4<<<8 * 148, 256, 0, c.stream>>>(X, ldx, rows, k0, kc, kpad, P, pstride, terms);
+  else
+    x3::k_split_rows<<<4 * 148, 256, 0, c.stream>>>(X, ldx, rows, k0, kc, kpad, P, swap, pstride, terms);
+  c.launches++;
+}
+
 // Split-K chunk of a contraction with rows_total operand rows: the BF16 planes of one chunk stay
 // within 512 MB.
 static long long chunk_k(long long rows_total, int terms, long long K) {
@@ -414,9 +468,8 @@ int gemm_tn_x3(Ctx& c, const float* A, long long lda, int M, const float* B, lon
   for (long long k0 = 0; k0 < K; k0 += kc) {
     const int kcur = (int)std::min<long long>(kc, K - k0);
     const int kpad = (kcur + 63) / 64 * 64;
-    x3::k_split_rows<<<4 * 148, 256, 0, c.stream>>>(A, lda, M, k0, kcur, kpad, PA, 0, (long long)M * kpad, terms);
-    x3::k_split_rows<<<4 * 148, 256, 0, c.stream>>>(B, ldb, N, k0, kcur, kpad, PB, swapB, (long long)N * kpad, terms);
-    c.launches += 2;
+    split_rows(c, A, lda, M, k0, kcur, kpad, PA, 0, (long long)M * kpad, terms);
+    split_rows(c, B, ldb, N, k0, kcur, kpad, PB, swapB, (long long)N * kpad, terms);
     RS_TRY(check_launch("split_rows"));
     CUtensorMap ta, tb;
     const TileCfg tc = tile_for(c, terms);
@@ -446,10 +499,8 @@ int gemm_tn2_x3(Ctx& c, const float* X, const float* Y, long long ld, int nb, lo
     const int kcur = (int)std::min<long long>(kc, K - k0);
     const int kpad = (kcur + 63) / 64 * 64;
     const long long plane = 2LL * nb * kpad;  // [terms][2 nb][kpad]: rows of X, then rows of Y
-    x3::k_split_rows<<<4 * 148, 256, 0, c.stream>>>(X, ld, nb, k0, kcur, kpad, P, 0, plane, terms);
-    x3::k_split_rows<<<4 * 148, 256, 0, c.stream>>>(Y, ld, nb, k0, kcur, kpad, P + (size_t)nb * kpad, 0, plane,
-                                                   terms);
-    c.launches += 2;
+    split_rows(c, X, ld, nb, k0, kcur, kpad, P, 0, plane, terms);
+    split_rows(c, Y, ld, nb, k0, kcur, kpad, P + (size_t)nb * kpad, 0, plane, terms);
     RS_TRY(check_launch("split_rows"));
     CUtensorMap ta, tb;
     const TileCfg tc = tile_for(c, terms);
@@ -522,7 +573,7 @@ __global__ void k_f2d_x3(const float* s, double* d, long long n) {
 int selftest_gemm(Ctx& c, int m, int n, long long k, int op, int terms, double* err) {
   DBuf a, b, ad, bd, cc, cref, v;
   const long long na = op == 0 ? (long long)m * k : (long long)m * k;  // op1: X [m=nb][k=G]
-  const long long nbv = op == 0 ? (long long)n * k : (long long)m * m;
+  const long long nbv = op == 0 ? (long long)n * k : op == 2 ? (long long)m * k : (long long)m * m;
   RS_TRY(a.ensure(sizeof(float) * na));
   RS_TRY(ad.ensure(sizeof(double) * na));
   RS_TRY(b.ensure(sizeof(float) * nbv));
@@ -533,7 +584,38 @@ int selftest_gemm(Ctx& c, int m, int n, long long k, int op, int terms, double* 
   x3::k_f2d_x3<<<256, 256, 0, c.stream>>>(b.as<float>(), bd.as<double>(), nbv);
   const double one = 1.0, zero = 0.0;
   std::vector<double> h1, h2;
-  if (op == 0) {
+  if (op == 2) {
+    // fused [S | M] = [A A^T | A B^T] (B: m x k) through gemm_tn2_x3, against DGEMM on the
+    // elements the contraction guarantees (n <= m when only triangle tiles are formed)
+    RS_CHECK(n == m, RSDFT_ERR_ARG, "op 2 needs n == m");
+    RS_TRY(cc.ensure(sizeof(double) * 2 * (size_t)m * m));
+    RS_TRY(cref.ensure(sizeof(double) * 2 * (size_t)m * m));
+    RS_CUDA(cudaMemsetAsync(cc.p, 0, sizeof(double) * 2 * (size_t)m * m, c.stream));
+    RS_TRY(gemm_tn2_x3(c, a.as<float>(), b.as<float>(), k, m, k, 1.0, cc.as<double>(),
+                       cc.as<double>() + (size_t)m * m, terms));
+    double* rS = cref.as<double>();
+    double* rM = rS + (size_t)m * m;
+    if (cublasDgemm(c.cublas, CUBLAS_OP_T, CUBLAS_OP_N, m, m, (int)k, &one, ad.as<double>(), (int)k, ad.as<double>(),
+                    (int)k, &zero, rS, m) != CUBLAS_STATUS_SUCCESS ||
+        cublasDgemm(c.cublas, CUBLAS_OP_T, CUBLAS_OP_N, m, m, (int)k, &one, ad.as<double>(), (int)k, bd.as<double>(),
+                    (int)k, &zero, rM, m) != CUBLAS_STATUS_SUCCESS)
+      RS_CHECK(false, RSDFT_ERR_CUDA, "reference dgemm failed");
+    h1.resize(2 * (size_t)m * m);
+    h2.resize(2 * (size_t)m * m);
+    RS_CUDA(cudaMemcpyAsync(h1.data(), cc.p, sizeof(double) * h1.size(), cudaMemcpyDeviceToHost, c.stream));
+    RS_CUDA(cudaMemcpyAsync(h2.data(), cref.p, sizeof(double) * h2.size(), cudaMemcpyDeviceToHost, c.stream));
+    RS_CUDA(cudaStreamSynchronize(c.stream));
+    double mx = 0.0, me = 0.0;
+    for (int part = 0; part < 2; ++part)
+      for (int i = 0; i < m; ++i)
+        for (int j = 0; j < m; ++j) {
+          if (c.gemm_tri && j > i) continue;
+          const double r = h2[(size_t)part * m * m + i + (size_t)j * m];
+          mx = std::max(mx, std::fabs(r));
+          me = std::max(me, std::fabs(h1[(size_t)part * m * m + (size_t)i * m + j] - r));
+        }
+    *err = me / std::max(mx, 1e-300);
+  } else if (op == 0) {
     RS_TRY(cc.ensure(sizeof(double) * (size_t)m * n));
     RS_TRY(cref.ensure(sizeof(double) * (size_t)m * n));
     RS_CUDA(cudaMemsetAsync(cc.p, 0, sizeof(double) * (size_t)m * n, c.stream));

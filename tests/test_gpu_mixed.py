@@ -56,6 +56,19 @@ def test_gemm_two_terms_rotation_vs_dgemm():
     assert err < 5e-5
 
 
+@pytest.mark.parametrize("tri", [False, True])
+@pytest.mark.parametrize("wide", [True, False])
+@pytest.mark.parametrize("m,k", [(512, 65536), (1024, 21824), (200, 4160)])
+def test_fused_overlap_hsub_vs_dgemm(m, k, wide, tri):
+    """[S | Hsub] in one contraction, full or triangle tiles (tiles wholly above the diagonal
+    are left out from nb = 256 / 512 bands on), against DGEMM on the guaranteed elements."""
+    with api.BandUpdate(synth.make_problem("t0")) as g:
+        g.gemm_terms(3, 3)
+        g.gemm_tile(wide, tri)
+        err = g.selftest_gemm(m, m, k, 2)
+    assert err < 5e-5, err
+
+
 def test_gemm_terms_argument_checked():
     with api.BandUpdate(synth.make_problem("t0")) as g:
         with pytest.raises(api.RsdftError):
