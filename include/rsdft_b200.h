@@ -234,11 +234,12 @@ int rsdft_gpu_selftest_gemm(int m, int n, long long k, int op, double* err);
  * residual of the 128^3 / 2048-band problem wandering between 1e-7 and 1e-4; two-term rotations
  * stall the residual near 5e-9.  No counterpart in the reference. */
 int rsdft_gpu_set_gemm_terms(int overlap_terms, int rotation_terms);
-/* Tiling of the three-term tensor-core contractions, flags (default 5): bit 0 set, 128 x 256
- * output tiles over K blocks of 32 (else 128 x 128 over 64); bit 1 set, the overlap and Hsub
- * contraction forms only the tiles reaching the upper triangle (the rest of Hsub mirrored),
- * else both triangles (Hsub averaged); bit 2 set, the band rotation in plain form X C, else in
- * the update form X + X (C - I).  Measurement knob; no counterpart in the reference. */
+/* Tiling of the three-term tensor-core contractions, flags (default 7): bit 0 set, 128 x 256
+ * output tiles over K blocks of 32 (else 128 x 128 over 64); bit 1 set, the overlap S of the
+ * fused overlap/Hsub contraction is formed by the tiles reaching its upper triangle only (its
+ * two triangles hold the same products), and with bit 3 also set Hsub the same way (the rest
+ * mirrored; else both triangles, averaged); bit 2 set, the band rotation in plain form X C, else
+ * in the update form X + X (C - I).  Measurement knob; no counterpart in the reference. */
 int rsdft_gpu_set_gemm_tile(int flags);
 /* Where the real build's hpsi adds the nonlocal term: 0 (default) a scatter kernel after the
  * stencil (one read-modify-write per covered point and band), 1 inside the streaming stencil

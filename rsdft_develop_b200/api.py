@@ -443,11 +443,14 @@ class BandUpdate:
         """Nonlocal term of the real hpsi: inside the stencil (fused) or by a scatter after it."""
         _call(self.lib.rsdft_gpu_set_nl_form, 1 if fused else 0)
 
-    def gemm_tile(self, wide: bool = True, tri: bool = False, update: bool = False) -> None:
+    def gemm_tile(self, wide: bool = True, tri: int = 1, update: bool = False) -> None:
         """Three-term GEMM tiles: 128 x 256 over K blocks of 32 (default) or 128 x 128 over 64;
-        tri: the overlap/Hsub contraction forms only its upper triangle; update: the band
-        rotation in update form.  The defaults are the library's."""
-        _call(self.lib.rsdft_gpu_set_gemm_tile, (1 if wide else 0) | (2 if tri else 0) | (0 if update else 4))
+        tri: 1 the overlap S by upper-triangle tiles (default), 2 S and Hsub, 0 neither;
+        update: the band rotation in update form.  The defaults are the library's."""
+        flags = (1 if wide else 0) | (0 if update else 4)
+        if tri:
+            flags |= 2 | (8 if tri == 2 else 0)
+        _call(self.lib.rsdft_gpu_set_gemm_tile, flags)
 
     def gemm_terms(self, overlap: int, rotation: int) -> None:
         """BF16 terms (2 or 3) of the mixed-precision overlap/Hsub and rotation contractions."""

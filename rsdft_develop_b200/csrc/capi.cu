@@ -750,9 +750,9 @@ int rsdft_gpu_set_nl_form(int fused) {
 
 int rsdft_gpu_set_gemm_tile(int flags) {
   REQUIRE_CTX();
-  RS_CHECK(flags >= 0 && flags <= 7, RSDFT_ERR_ARG, "tile flags must be in 0..7");
+  RS_CHECK(flags >= 0 && flags <= 15, RSDFT_ERR_ARG, "tile flags must be in 0..15");
   g_ctx->gemm_wide = flags & 1;
-  g_ctx->gemm_tri = (flags >> 1) & 1;
+  g_ctx->gemm_tri = ((flags >> 1) & 1) ? (((flags >> 3) & 1) ? 2 : 1) : 0;
   g_ctx->rot_update = ((flags >> 2) & 1) ? 0 : 1;
   return 0;
 }

@@ -109,7 +109,7 @@ struct Ctx {
   int gemm_terms_rot = 3;          // BF16 terms of the band rotations (mixed precision)
   int pc_sstep = 1;                // FP32 precond_hprsdft in s-step form (0: the recurrence form)
   int gemm_wide = 1;               // three-term GEMM tiles 128 x 256 (K blocks of 32), else 128 x 128
-  int gemm_tri = 0;                // overlap / Hsub: form only the tiles reaching the upper triangle
+  int gemm_tri = 1;                // S by upper-triangle tiles (1), S and Hsub (2), neither (0)
   int rot_update = 0;              // mixed rotation in update form X + X (C - I)
   int nl_fused = 0;                // nonlocal term inside the stencil (1) or by the scatter kernel after it (0)
 

@@ -366,7 +366,7 @@ int gssd_run(Ctx& c, int k, int s, double* h_esp, bool use_cg_hx) {
   }
   {
     ProfScope ps(c, "gs");
-    if (!c.mixed || c.gemm_tri)
+    if (!c.mixed || c.gemm_tri == 2)
       k_fill_lower<<<64, 256, 0, c.stream>>>(M, nb);  // the upper triangle of M was formed
     else
       k_symmetrize<<<64, 256, 0, c.stream>>>(M, nb);  // both triangles were formed: average

@@ -96,7 +96,7 @@ struct Out {
   double* C;       // columns n < nsplit (mode 0)
   double* C2;      // columns n >= nsplit go to C2[m][n - nsplit] (mode 0)
   int nsplit;
-  int tri;         // mode 0: only tiles reaching the triangle n <= m of each part are formed
+  int tri;         // mode 0: 1, the first part only by tiles reaching n <= m; 2, both parts
   long long ldc;
   double alpha;
   float* Y;
@@ -124,12 +124,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_x3(const __grid_constant__
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-  // symmetric results: a tile wholly above the diagonal (n > m everywhere) is left out; a tile
-  // that straddles the two parts is judged by the smallest column of each part it holds
+  // tri = 1: the first part (columns n < nsplit, the overlap S, whose two triangles hold the
+  // same products) is formed only where it reaches n <= m: a tile wholly above the diagonal is
+  // left out unless it also holds columns of the second part (formed in full).
+  // tri = 2: both parts by triangle tiles.
   if (o.tri) {
     const bool s_part = n0 < o.nsplit, m_part = n0 + BN > o.nsplit;
     const bool s_above = !s_part || n0 >= m0 + BM;
-    const bool m_above = !m_part || max(n0 - o.nsplit, 0) >= m0 + BM;
+    const bool m_above = !m_part || (o.tri == 2 && max(n0 - o.nsplit, 0) >= m0 + BM);
     if (s_above && m_above) return;
   }
   const int kb0 = blockIdx.z * kblocks_per_split;
@@ -448,7 +450,7 @@ static long long chunk_k(long long rows_total, int terms, long long K) {
 
 static int split_ksplit(int M, int N, int kpad, int bn, bool tri = false) {
   int tiles = ((M + 127) / 128) * ((N + bn - 1) / bn);
-  if (tri) tiles = (tiles + ((M + 127) / 128)) / 2;  // about half the tiles are formed
+  if (tri) tiles = std::max(1, tiles * 3 / 4);  // about a quarter of the tiles (half of S) are left out
   const int kbt = kpad / 64;
   return std::max(1, std::min(kbt, (2 * 148 + tiles - 1) / tiles));
 }
@@ -508,7 +510,7 @@ int gemm_tn2_x3(Ctx& c, const float* X, const float* Y, long long ld, int nb, lo
     RS_TRY(make_map(&tb, P, 2LL * nb, kpad, tc.bn, terms, 2LL * nb, tc.kb));
     x3::Out o{};
     o.mode = 0; o.C = S; o.C2 = M; o.nsplit = nb; o.ldc = nb; o.alpha = alpha; o.M = nb; o.N = 2 * nb;
-    o.tri = c.gemm_tri;
+    o.tri = c.gemm_tri;  // 0, 1 (S by triangle tiles) or 2 (S and Hsub)
     RS_TRY(launch_terms(c, terms, ta, tb, nb, 2 * nb, kpad, o, split_ksplit(nb, 2 * nb, kpad, tc.bn, c.gemm_tri != 0)));
   }
   return 0;
@@ -609,7 +611,7 @@ int selftest_gemm(Ctx& c, int m, int n, long long k, int op, int terms, double* 
     for (int part = 0; part < 2; ++part)
       for (int i = 0; i < m; ++i)
         for (int j = 0; j < m; ++j) {
-          if (c.gemm_tri && j > i) continue;
+          if (j > i && (c.gemm_tri == 2 || (c.gemm_tri == 1 && part == 0))) continue;
           const double r = h2[(size_t)part * m * m + i + (size_t)j * m];
           mx = std::max(mx, std::fabs(r));
           me = std::max(me, std::fabs(h1[(size_t)part * m * m + (size_t)i * m + j] - r));

@@ -56,12 +56,13 @@ def test_gemm_two_terms_rotation_vs_dgemm():
     assert err < 5e-5
 
 
-@pytest.mark.parametrize("tri", [False, True])
+@pytest.mark.parametrize("tri", [0, 1, 2])
 @pytest.mark.parametrize("wide", [True, False])
 @pytest.mark.parametrize("m,k", [(512, 65536), (1024, 21824), (200, 4160)])
 def test_fused_overlap_hsub_vs_dgemm(m, k, wide, tri):
-    """[S | Hsub] in one contraction, full or triangle tiles (tiles wholly above the diagonal
-    are left out from nb = 256 / 512 bands on), against DGEMM on the guaranteed elements."""
+    """[S | Hsub] in one contraction: full, S by triangle tiles (the default), or both by
+    triangle tiles (tiles wholly above the diagonal are left out from nb = 256 / 512 bands on;
+    nb = 200 has tiles straddling S and Hsub), against DGEMM on the guaranteed elements."""
     with api.BandUpdate(synth.make_problem("t0")) as g:
         g.gemm_terms(3, 3)
         g.gemm_tile(wide, tri)
