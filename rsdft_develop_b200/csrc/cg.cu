@@ -800,8 +800,8 @@ static int pc_block(Ctx& c, Blk& k, const T* G, T* PG, T* X0, T* X1, T* X2, T* F
       else LAUNCH_E((k_pcs_shift<T, 2, true>), qb, v[i - 1], v[i]);
       LAUNCH_S(k_pcs_sc, i, m, q.c0);
     }
-    if (q.nc == 1) LAUNCH_E((k_pcs_shift<T, 1, false>), qb, v[m - 1], v[m - 1]);
-    else LAUNCH_E((k_pcs_shift<T, 2, false>), qb, v[m - 1], v[m - 1]);
+    if (q.nc == 1) LAUNCH_E((k_pcs_shift<T, 1, false>), qb, v[m - 1], (T*)nullptr);
+    else LAUNCH_E((k_pcs_shift<T, 2, false>), qb, v[m - 1], (T*)nullptr);
     LAUNCH_S(k_pcs_sc, m, m, q.c0);
     switch (m) {
       case 1: LAUNCH_E((k_pcs_combine<T, 1>), G, v[0], v[1], v[2], v[3], PG); break;

@@ -334,8 +334,8 @@ __global__ void k_rms(const float* __restrict__ g, double* __restrict__ s2, size
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
   if ((threadIdx.x & 31) == 0) atomicAdd(s2 + blockIdx.y, acc);
 }
-__global__ void k_scale(const float* __restrict__ g, float* __restrict__ x, const double* __restrict__ s2, size_t vol,
-                        int inverse) {
+// x = g * f per band (x may be g: in place)
+__global__ void k_scale(const float* g, float* x, const double* __restrict__ s2, size_t vol, int inverse) {
   const double r = sqrt(s2[blockIdx.y] / (double)vol);
   const float f = r > 0.0 ? (float)(inverse ? r : 1.0 / r) : 0.f;
   const float* gb = g + (size_t)blockIdx.y * vol;
