@@ -6,7 +6,9 @@
 // the device.  A band that leaves the reference's icg loop early (|E-E1| < 1e-15, which
 // follows a rejected step, :233) is masked out for the rest of the call, which reproduces the
 // per-band exits of MB_d = 1 exactly.  precond_hprsdft
-// (src/conjugate_gradient/cgpc_hprsdft_module.f90:133-270) is batched the same way.
+// (src/conjugate_gradient/cgpc_hprsdft_module.f90:133-270) is batched the same way: FP64 bands
+// run its CG recurrence (26 passes at mloop = 3), FP32 bands the same mloop steps in s-step
+// form (k_pcs_*: Krylov basis, moments, FP64 recurrence on coefficients; 12 passes).
 //
 // complex16 arrays are handled through their interleaved real view (2*ML0 reals per band,
 // the same view the reference's dot_product takes with mm = 2*ML0, cg_module.f90:478):
@@ -15,7 +17,9 @@
 // complex coefficients have NC = 2 variants.
 //
 // Reductions are deterministic: each CTA writes a per-band partial sum and the scalar
-// kernels add the partials of a band in a fixed order.
+// kernels add the partials of a band in a fixed order.  In the real build H x of every band is
+// kept in one array (ctx ws_hpsi) so that the fused Gram-Schmidt / subspace step of the sweep
+// can take it instead of recomputing it.
 #include <cstring>
 
 #include "ctx.cuh"

@@ -9,7 +9,8 @@
 //   subspace_diag_la (src/subspace_diag/subspace_diag_la_module.f90:18-223):
 //   Hsub = 1/2 dV (Psi^H H Psi + (H Psi)^H Psi) (dsyr2k / zher2k), dsyev / zheevd, Psi <- Psi V.
 // FP64 path: cuBLAS syrk/herk, syr2k/her2k, trsm, gemm and cuSOLVER potrf, syevd/heevd.
-// Mixed mode keeps psi in FP32; the split-BF16 tensor-core path lives in gemm_bf16x3.cu.
+// Mixed mode keeps psi in FP32; the split-BF16 tensor-core contractions live in gemm_x3.cu.
+// Inside the sweep the two steps run fused as one Cholesky-Rayleigh-Ritz step (gssd_run).
 #include <cstring>
 
 #include "ctx.cuh"

@@ -7,9 +7,11 @@
 //                   Dij pairs, scatter psi(JJP) += uVk * sum Dij uVunk); the KB form
 //                   src/d_ps_nloc2_op_module.f90:146-288 is the diagonal-Dij case.
 //
-// This file holds the host side of hpsi and the atom-centred gather: the projector gather +
-// Dij runs first and writes the coefficient rows c_b (atom-major, PG-padded); the stencil with
-// V_loc and the nonlocal scatter is the persistent streaming kernel of hpsi_stream.cu.
+// This file holds the host side of hpsi, the atom-centred gather and the nonlocal scatter: the
+// projector gather + Dij runs first and writes the coefficient rows c_b (atom-major,
+// PG-padded); the stencil with V_loc is the persistent streaming kernel of hpsi_stream.cu;
+// the scatter then adds uV . c_b at every covered grid point (or, selectable, the stencil adds
+// it from records staged per plane).
 #include "stencil.cuh"
 
 namespace rsdft {

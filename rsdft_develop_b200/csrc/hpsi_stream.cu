@@ -16,7 +16,8 @@
 //    wrap inside the staged full row, y taps read neighbouring staged rows, z taps are pushed
 //    into 2*Md+1 rotating register accumulators (each plane is read once from HBM).  FP32 runs
 //    on float2 pairs with sm_100's packed FMA/ADD/MUL; FP64 on scalars with the same pairing.
-//  * Nonlocal term: one step ahead, all threads of the CTA share out the next plane's staged
+//  * Nonlocal term (the fused form; by default hpsi adds it with a scatter kernel after this
+//    kernel instead): one step ahead, all threads of the CTA share out the next plane's staged
 //    records evenly, each adding uV . c_b[atom] into that plane's buffer with a shared-memory
 //    atomic; on the next step each thread takes its own points' sums with one vector load per
 //    row and clears them (two buffers by plane parity; the per-step barrier orders both).
