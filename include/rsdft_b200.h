@@ -158,7 +158,7 @@ int rsdft_gpu_set_pc_form(int sstep);
  * last).  iters receives the sweeps done; esp/res (host, nband*nk*nspin, k-major after band)
  * receive the final FP64 values. */
 int rsdft_gpu_sweep(int nsweep, double tol, int* iters, double* esp, double* res);
-/* Convergence band set of rsdft_gpu_sweep: bands 1..mb_ref are judged (0: all bands), as the
+/* Convergence band set of rsdft_gpu_sweep: bands 1..mb_ref are checked (0: all bands), as the
  * reference's init_sweep(iconv_check, mb_ref, tol) does for its band and DOS drivers
  * (src/sweep_module.f90:46-60,267-278; src/band_module.f90:207; src/dos_module.f90:64-75). */
 int rsdft_gpu_init_sweep(int mb_ref);

@@ -326,7 +326,7 @@ class BandUpdate:
         return esp, res
 
     def init_sweep(self, mb_ref: int = 0):
-        """Judge convergence on bands 1..mb_ref (0: all), as init_sweep(..., mb_ref, ...)."""
+        """Check convergence on bands 1..mb_ref (0: all), as init_sweep(..., mb_ref, ...)."""
         _call(self.lib.rsdft_gpu_init_sweep, int(mb_ref))
 
     def calc_sweep(self, nsweep: int, tol: float = 0.0):

@@ -643,7 +643,7 @@ int rsdft_gpu_sweep(int nsweep, double tol, int* iters, double* esp, double* res
   Ctx& c = *g_ctx;
   const int nbmax = c.p.mb;
   std::vector<double> e((size_t)nbmax), r((size_t)nbmax);
-  // learned-PC guard: every sweep is judged by the FP64 residual without preconditioning; when
+  // learned-PC guard: every sweep is checked by the FP64 residual without preconditioning; when
   // it has not dropped below 0.9x its best value for 3 sweeps running, CG falls back to
   // precond_hprsdft for the rest of the run
   double best = 1e300;
@@ -662,10 +662,10 @@ int rsdft_gpu_sweep(int nsweep, double tol, int* iters, double* esp, double* res
       }
     // The FP64 check (an FP64 H x of every band) runs once CG's own residual of the bands it
     // returned is within kResGate x tol: before that the check cannot pass.  The learned-PC
-    // guard judges every sweep.
+    // guard checks every sweep.
     constexpr double kResGate = 30.0;
-    const bool judge = tol > 0.0 && (cg_rmax <= kResGate * tol || pc_effective(c) == RSDFT_PC_LEARNED);
-    if (judge || it == nsweep) {
+    const bool check_fp64 = tol > 0.0 && (cg_rmax <= kResGate * tol || pc_effective(c) == RSDFT_PC_LEARNED);
+    if (check_fp64 || it == nsweep) {
       for (int s = 0; s < c.p.nspin; ++s)
         for (int k = 0; k < c.p.nk; ++k) {
           const int nb = c.kp[k].nband;

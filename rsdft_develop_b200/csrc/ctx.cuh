@@ -72,7 +72,7 @@ struct Ctx {
   cusolverDnHandle_t cusolver = nullptr;
   unsigned* d_status = nullptr;
   long long launches = 0;
-  int mb_ref = 0;  // bands 1..mb_ref judged for convergence (0: all)
+  int mb_ref = 0;  // bands 1..mb_ref checked for convergence (0: all)
   bool eig_jacobi = false;          // subspace eigensolver: Jacobi (syevj) instead of syevd
   syevjInfo_t syevj = nullptr;
 
