@@ -194,10 +194,10 @@ static int nl_scatter(Ctx& c, int k, const T* coef, T* out, size_t ld, int nb) {
 template <typename T, int MD>
 static int launch_stencil(Ctx& c, int k, int s, const T* psi, T* out, size_t ld, int nb, const T* coef,
                           const T* vloc_override = nullptr, double c0_shift = 0.0) {
-  if (coef == nullptr || c.nl_fused)
+  if (coef != nullptr && c.nl_fused)
     return launch_stencil_stream<T, MD>(c, k, s, psi, out, ld, nb, coef, vloc_override, c0_shift);
-  RS_TRY((launch_stencil_stream<T, MD>(c, k, s, psi, out, ld, nb, nullptr, vloc_override, c0_shift)));
-  return nl_scatter<T>(c, k, coef, out, ld, nb);
+  RS_TRY((launch_stencil_ws<T, MD>(c, k, s, psi, out, ld, nb, vloc_override, c0_shift)));
+  return coef ? nl_scatter<T>(c, k, coef, out, ld, nb) : 0;
 }
 
 template <typename T>

@@ -32,64 +32,6 @@ namespace rsdft {
 
 namespace {
 
-template <typename T> struct Lanes;
-// FP32: 4 x points per thread as two float2 pairs, packed arithmetic
-template <> struct Lanes<float> {
-  using P2 = float2;
-  using U = float4;
-  static constexpr int W = 4;
-  static constexpr bool packed = true;
-  static __device__ __forceinline__ P2 fma(P2 c, P2 a, P2 b) { return __ffma2_rn(c, a, b); }
-  static __device__ __forceinline__ P2 add(P2 a, P2 b) { return __fadd2_rn(a, b); }
-  static __device__ __forceinline__ P2 mul(P2 a, P2 b) { return __fmul2_rn(a, b); }
-  static __device__ __forceinline__ P2 dup(float c) { return make_float2(c, c); }
-  static __device__ __forceinline__ P2 mk(float x, float y) { return make_float2(x, y); }
-  static __device__ __forceinline__ P2 pair(const U& u, int j) {
-    return j == 0 ? make_float2(u.x, u.y) : make_float2(u.z, u.w);
-  }
-  static __device__ __forceinline__ U join(const P2 (&p)[2]) { return make_float4(p[0].x, p[0].y, p[1].x, p[1].y); }
-  static __device__ __forceinline__ void split(const U& u, float* w) {
-    w[0] = u.x;
-    w[1] = u.y;
-    w[2] = u.z;
-    w[3] = u.w;
-  }
-  static __device__ __forceinline__ float dot4(const float* u, const float* c) {
-    const float4 a = *reinterpret_cast<const float4*>(u), b = *reinterpret_cast<const float4*>(c);
-    return fmaf(a.x, b.x, fmaf(a.y, b.y, fmaf(a.z, b.z, a.w * b.w)));
-  }
-};
-// FP64: 2 x points per thread as one double2 pair, scalar arithmetic
-template <> struct Lanes<double> {
-  using P2 = double2;
-  using U = double2;
-  static constexpr int W = 2;
-  static constexpr bool packed = false;
-  static __device__ __forceinline__ P2 fma(P2 c, P2 a, P2 b) {
-    return make_double2(::fma(c.x, a.x, b.x), ::fma(c.y, a.y, b.y));
-  }
-  static __device__ __forceinline__ P2 add(P2 a, P2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-  static __device__ __forceinline__ P2 mul(P2 a, P2 b) { return make_double2(a.x * b.x, a.y * b.y); }
-  static __device__ __forceinline__ P2 dup(double c) { return make_double2(c, c); }
-  static __device__ __forceinline__ P2 mk(double x, double y) { return make_double2(x, y); }
-  static __device__ __forceinline__ P2 pair(const U& u, int) { return u; }
-  static __device__ __forceinline__ U join(const P2 (&p)[1]) { return p[0]; }
-  static __device__ __forceinline__ void split(const U& u, double* w) {
-    w[0] = u.x;
-    w[1] = u.y;
-  }
-  static __device__ __forceinline__ double dot4(const double* u, const double* c) {
-    const double2 a0 = *reinterpret_cast<const double2*>(u), a1 = *reinterpret_cast<const double2*>(u + 2);
-    const double2 b0 = *reinterpret_cast<const double2*>(c), b1 = *reinterpret_cast<const double2*>(c + 2);
-    return ::fma(a0.x, b0.x, ::fma(a0.y, b0.y, ::fma(a1.x, b1.x, a1.y * b1.y)));
-  }
-};
-
-template <typename T>
-__device__ __forceinline__ typename Lanes<T>::U ldu(const T* p) {
-  return *reinterpret_cast<const typename Lanes<T>::U*>(p);
-}
-
 // z push for rotation slot S: acc[S] += t, acc[S -+ m] += cz_m v, then emit slot S - Md
 template <typename T, int MD, int R, int S>
 __device__ __forceinline__ void zpush(typename Lanes<T>::P2 (&acc)[2 * MD + 1][R][Lanes<T>::W / 2],
