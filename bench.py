@@ -1,19 +1,33 @@
 """Benchmark: seconds to band residual 1e-8 on one B200 (plus hpsi HBM GB/s).
 
-A step is one complete band-update solve of the seeded synthetic problem: device-side
-seeded wavefunctions -> Gram-Schmidt -> calc_sweep (CG -> GS -> SD per sweep, FP64
-residual check after each sweep) until max_n res(n) <= 1e-8, res = dV |H psi - e psi|^2
-(the reference's definition, src/conjugate_gradient/cg_module.f90:231).
+Default workload: the 128^3 grid / 2048-band real8 problem (512 s+p atoms), mixed precision
+with precond_hprsdft.  A step is one complete band-update solve through the C ABI, as a Fortran
+host would drive it: set_wf from pinned host FP64 wavefunctions (host -> device), gram_schmidt,
+calc_sweep (CG -> fused GS/SD per sweep, FP64 residual check) until max_n res(n) <= 1e-8 over
+bands 1..mb_ref, res = dV |H psi - e psi|^2 (src/conjugate_gradient/cg_module.f90:231), then
+get_wf back into pinned host memory (device -> host).  Every step starts from the same seeded
+wavefunctions.
 
-JSON line keys beyond the driver contract: ``roofline`` (hpsi stencil kernel, CUDA events
-inside the library on its own stream over the timed region), ``cpu_baseline`` (the CPU
-oracle that restates the reference's CPU path, timed on a bounded sample), ``e2e`` (same
-solve through the C ABI from pinned host buffers, host<->device copies inside the timed
-region), ``clocks`` (nvidia-smi samples during the timed region).
+JSON line keys beyond the driver contract:
+  value / ms_per_step  device time of the solve with the inputs resident (CUDA events on the
+                       library stream between the end of the host->device copy and the end of
+                       the last sweep), mean over the timed steps
+  e2e                  wall time of the whole step, copies included (same loop)
+  roofline             the hpsi stencil kernel: algorithmic bytes (read psi + write H psi per
+                       band, V_loc once) over its CUDA-event time, both taken inside the library
+                       on its own stream during the timed steps
+  compare              one solve of the plain FP64 method (the drop-in's FP64 path with
+                       precond_hprsdft) from the same input; optional mixed + learned solve
+  errors               eigenvalues and subspace of the timed solve against that FP64 solve
+  cpu_baseline         the CPU oracle (restatement of the reference CPU path) on the host
+                       cores: a measured sweep where the problem is small, else sampled CG and
+                       dense costs extrapolated to a sweep, times the FP64 method's sweeps
+  clocks               nvidia-smi samples during the timed steps
 
---impl reference runs the CPU restatement of the reference path (oracle/) on the host
-cores for the same config and metric.  Multi-GPU runs are independent replicas (the path
-is one GPU per problem): every rank solves its own copy, the time is the max over ranks.
+--impl reference times the same CPU oracle alone (bounded sample per step) for the same config.
+--kernel hpsi|gemm|pc|lpc runs one kernel family on its own (timing and ncu captures).
+Multi-GPU runs are independent replicas (one problem per GPU): every rank solves its own copy
+and the time is the max over ranks.
 """
 from __future__ import annotations
 
@@ -34,15 +48,16 @@ sys.path.insert(0, ROOT)
 METRIC = "s to band residual 1e-8: mixed+learned vs plain FP64 on 1 GPU; hpsi HBM GB/s"
 TOL = 1e-8
 MAX_SWEEPS = 600
+SEED = 1
 
-# DRAM traffic per stencil launch from ncu (dram__bytes_read.sum + dram__bytes_write.sum over
-# the algorithmic bytes), by (config, precision); source: profiles/hpsi_stencil_c1.md
-# (316.3 + 226.2 MB against 537.9 MB for all 256 bands).
-NCU_TRAFFIC_RATIO: dict = {("c1", "mixed"): 1.009}
+# Sweeps the plain FP64 method needs from the seeded start to max res <= 1e-8 over bands
+# 1..mb_ref (the same algorithm on CPU and GPU), measured with the library's FP64 path on a
+# B200; the reference arm multiplies its per-sweep CPU time by these.
+SWEEPS_FP64 = {"c0": 75, "c1": 43, "c2": 47, "c3": 50}
 
-# Sweeps the plain FP64 method needs to reach max res <= 1e-8 from the seeded start
-# (same algorithm on CPU and GPU; measured by the FP64 GPU path).
-SWEEPS_TO_TOL = {"c0": 75, "c1": None}
+# DRAM traffic of one hpsi stencil launch over its algorithmic bytes, from an ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum) of the same kernel, per (config, precision).
+NCU_TRAFFIC_RATIO: dict = {}
 
 
 def _peaks():
@@ -54,6 +69,8 @@ def _peaks():
 
 
 class ClockSampler:
+    """nvidia-smi clock / throttle samples every 200 ms while the block runs."""
+
     def __init__(self, index: int):
         self.index = index
         self.proc = None
@@ -98,12 +115,21 @@ class ClockSampler:
                 pass
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        pw = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
-        loaded = [s for s, p in zip(sm, pw) if p > 200.0] or sm
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in rows]
+        smax = [num(r[2]) for r in rows]
+        pw = [num(r[3]) for r in rows]
+        loaded = [s for s, p in zip(sm, pw) if s is not None and p is not None and p > 200.0]
+        loaded = loaded or [s for s in sm if s is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        smax = [s for s in smax if s is not None]
+        pw = [p for p in pw if p is not None]
         return {"sm_mhz": statistics.median(loaded) if loaded else None,
                 "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
                 "samples": len(rows), "power_w_max": max(pw) if pw else None}
@@ -113,15 +139,15 @@ def _dist():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     if ws <= 1:
         return None, 0, 1
+    import datetime
     import torch.distributed as dist
     os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-    import datetime
-    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=3600))
     return dist, dist.get_rank(), ws
 
 
-def _max_over_ranks(dist, x: float) -> float:
-    if dist is None:
+def _max_over_ranks(dist, x):
+    if dist is None or x is None:
         return x
     import torch
     t = torch.tensor([x], dtype=torch.float64)
@@ -134,30 +160,73 @@ def _barrier(dist):
         dist.barrier()
 
 
-def cpu_sweep_time(cfg_name: str, nthreads: int, nsweep: int = 1):
-    """Seconds per oracle sweep (CG+GS+SD) on the host cores, after an untimed GS."""
+def mb_ref_of(nband: int) -> int:
+    """Convergence band set: bands 1..mb_ref, mb_ref = (nband + nocc)/2 with nocc = 3/4 nband
+    (the reference's DOS driver rule max_ref_band = (nb + nocc)/2, src/dos_module.f90:64-65)."""
+    return nband - nband // 8
+
+
+# ----------------------------------------------------------------------------------------
+# CPU oracle timing (the reference arm and cpu_baseline)
+# ----------------------------------------------------------------------------------------
+FULL_SWEEP_MAX = 64 ** 3 * 256  # grid points x bands up to which one whole oracle sweep is timed
+
+
+def cpu_sweep_estimate(prob, nthreads: int, seed: int = 7):
+    """Seconds per CG + GS + SD sweep of the oracle on `nthreads` host threads.
+
+    Small problems: one whole sweep, timed.  Larger ones: the oracle's CG on a few bands (its
+    work is independent per band, MB_d = 1) and its Gram-Schmidt + subspace diagonalisation on
+    m bands (work ~ Ng m^2) are timed on the configuration's own grid and operator and scaled
+    to all bands.  Returns (seconds, description, kind)."""
     from oracle import oracle as orc
-    from rsdft_develop_b200 import synth
     orc.build()
     orc.set_threads(nthreads)
-    prob = synth.make_problem(cfg_name)
     o = orc.Oracle(prob)
-    psi = o.gram_schmidt(synth.random_wavefunctions(1, prob.nband, prob.ng))
+    nb, ng = prob.nband, prob.ng
+    rng = np.random.default_rng(seed)
+    if ng * nb <= FULL_SWEEP_MAX:
+        from rsdft_develop_b200 import synth
+        psi = o.gram_schmidt(synth.random_wavefunctions(seed, nb, ng))
+        t0 = time.perf_counter()
+        o.sweep(psi, 1)
+        t = time.perf_counter() - t0
+        return t, f"one whole oracle sweep (CG+GS+SD, {nb} bands)", "measured"
+    ncg_b = 8
+    m = 128
+    psi = rng.standard_normal((m, ng))
     t0 = time.perf_counter()
-    o.sweep(psi, nsweep)
-    return (time.perf_counter() - t0) / nsweep
+    q = o.gram_schmidt(psi)
+    o.subspace_diag(q)
+    t_dense = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    o.cg(q[:ncg_b])
+    t_cg = (time.perf_counter() - t0) / ncg_b
+    # subspace_diag applies H to each band (work ~ Ng m): that part scales with the bands, the
+    # rest of GS + SD (the Ng m^2 products) with their square
+    t0 = time.perf_counter()
+    o.hpsi(q[:ncg_b])
+    t_h = (time.perf_counter() - t0) / ncg_b
+    t_quad = max(0.0, t_dense - m * t_h)
+    est = nb * (t_cg + t_h) + (nb / m) ** 2 * t_quad
+    desc = (f"extrapolated: oracle CG on {ncg_b} bands ({t_cg:.3f} s per band) and H psi ({t_h:.4f} s per band) "
+            f"x {nb} bands + oracle GS+SD products on {m} bands ({t_quad:.2f} s) x ({nb}/{m})^2")
+    return est, desc, "extrapolated"
 
 
 def run_reference(args, dist, rank, ws):
+    """The CPU restatement of the reference path (oracle/) on the host cores, same config."""
     if rank != 0:
         return
+    from rsdft_develop_b200 import synth
+    prob = synth.make_problem(args.config)
     nthreads = os.cpu_count() or 1
-    n_conv = SWEEPS_TO_TOL.get(args.config) or args.sweeps_to_tol
-    samples = []
+    n_conv = SWEEPS_FP64[args.config]
+    samples, desc, kind = [], "", ""
     for i in range(args.warmup + args.steps):
-        t = cpu_sweep_time(args.config, nthreads)
+        per, desc, kind = cpu_sweep_estimate(prob, nthreads, seed=7 + i)
         if i >= args.warmup:
-            samples.append(t)
+            samples.append(per)
     per = statistics.median(samples)
     val = per * n_conv
     line = {
@@ -165,27 +234,305 @@ def run_reference(args, dist, rank, ws):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1000.0,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded)",
-        "config": {"workload": args.config, "precision": "fp64", "sweeps_to_tol": n_conv},
+        "config": {"workload": args.config, "grid": list(prob.n), "bands": prob.nband, "atoms": prob.cfg.natom,
+                   "precision": "fp64", "pc": "hprsdft", "sweeps_to_tol": n_conv, "mb_ref": mb_ref_of(prob.nband)},
         "cpu_baseline": {"value": val, "unit": "s", "cores": nthreads, "kind": "port",
-                         "sample": f"1 CG+GS+SD sweep of {args.config} per step on {nthreads} host threads "
-                                   f"(oracle/ restatement of the reference CPU path), x {n_conv} sweeps"},
+                         "sample": f"per step: {desc}; median {per:.2f} s per sweep on {nthreads} host threads "
+                                   f"(oracle/ restatement of the reference CPU path) x {n_conv} sweeps, the "
+                                   f"FP64 method's count to max res <= 1e-8 (measured on the GPU)",
+                         "estimate": kind},
         "e2e": {"value": val, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
-def mb_ref_of(nband: int) -> int:
-    """Convergence band set: bands 1..mb_ref, mb_ref = (nband + nocc)/2 with nocc = 3/4 nband
-    (the reference's DOS driver rule max_ref_band = (nb + nocc)/2, src/dos_module.f90:64-65)."""
-    return nband - nband // 8
+# ----------------------------------------------------------------------------------------
+# error of a solve against the FP64 solve of the same input
+# ----------------------------------------------------------------------------------------
+def gap_index(esp: np.ndarray, lo: int, hi: int) -> int:
+    """Band count m in [lo, hi] whose gap e_{m+1} - e_m is largest (a subspace boundary)."""
+    gaps = esp[lo:hi + 1] - esp[lo - 1:hi]
+    return lo + int(np.argmax(gaps))
 
 
-def solve(g, seed: int, tol: float):
-    """One complete solve on the resident (device-generated) wavefunctions; returns sweeps."""
-    g.random_wf(seed)
-    g.gram_schmidt()
-    it, esp, res = g.calc_sweep(MAX_SWEEPS, tol=tol)
-    return it, esp, res
+def principal_angle_max(a_host, b_host, m: int, dv: float) -> float:
+    """Largest principal angle (rad) between span(a[:m]) and span(b[:m]) in the dV inner
+    product; a, b are host tensors (nb, ng) of FP64 bands.  Evaluated on the GPU in FP64."""
+    import torch
+    A = a_host[:m].cuda()
+    B = b_host[:m].cuda()
+    ga = (A @ A.T) * dv
+    gb = (B @ B.T) * dv
+    M = (A @ B.T) * dv
+    del A, B
+    la = torch.linalg.cholesky(ga)
+    lb = torch.linalg.cholesky(gb)
+    X = torch.linalg.solve_triangular(la, M, upper=False)
+    X = torch.linalg.solve_triangular(lb, X.T, upper=False).T
+    s = torch.linalg.svdvals(X)
+    smin = float(s.min().clamp(max=1.0))
+    # sin(theta) = sqrt(1 - s^2), accurate for small angles
+    return float(np.arcsin(min(1.0, np.sqrt(max(0.0, (1.0 - smin) * (1.0 + smin))))))
+
+
+# ----------------------------------------------------------------------------------------
+# our arm
+# ----------------------------------------------------------------------------------------
+def run_ours(args, dist, rank, ws):
+    import torch
+    from rsdft_develop_b200 import api, lpc_train, synth
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    prob = synth.make_problem(args.config)
+    nb, ng = prob.nband, prob.ng
+    mb_ref = mb_ref_of(nb)
+    prec = api.PREC_MIXED if args.precision == "mixed" else api.PREC_FP64
+    pc = args.pc
+    wpath = lpc_train.default_weights_path(prob.h)
+    pc_mode = {"learned": api.PC_LEARNED, "hprsdft": api.PC_HPRSDFT, "none": api.PC_NONE}[pc]
+    terms = tuple(int(t) for t in args.gemm_terms.split(","))
+    compare_arms = [a for a in args.compare.split(",") if a and a != "none"]
+
+    # the common input: seeded FP64 wavefunctions in pinned host memory, made by the library's
+    # device generator (bit-identical to synth.random_wavefunctions)
+    pin_in = torch.empty((nb, ng), dtype=torch.float64, pin_memory=True)
+    pin_out = torch.empty((nb, ng), dtype=torch.float64, pin_memory=True)
+    with api.BandUpdate(prob, precision=api.PREC_FP64) as g0:
+        g0.random_wf(SEED)
+        g0.get_wf_host(pin_in.data_ptr(), nb)
+
+    g = api.BandUpdate(prob, precision=prec, pc_mode=pc_mode)
+    g.gemm_terms(*terms)
+    if pc == "learned":
+        g.lpc_set_weights(np.load(wpath))
+    g.init_sweep(mb_ref)
+    stream = torch.cuda.ExternalStream(g.stream())
+
+    def step():
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ev[0].record(stream)
+        g.set_wf_host(pin_in.data_ptr(), nb)
+        ev[1].record(stream)
+        g.gram_schmidt()
+        it, esp, res = g.calc_sweep(MAX_SWEEPS, tol=TOL)
+        ev[2].record(stream)
+        g.get_wf_host(pin_out.data_ptr(), nb)
+        ev[3].record(stream)
+        ev[3].synchronize()
+        wall = time.perf_counter() - t0
+        return it, esp, res, ev[1].elapsed_time(ev[2]) / 1000.0, wall
+
+    for _ in range(args.warmup):
+        step()
+    g.synchronize()
+    _barrier(dist)
+    torch.cuda.synchronize()
+    launches0 = g.kernel_launches()
+    g.profile(2)  # the hpsi stencil's own CUDA events only: no host synchronisation
+    iters, solve_s, wall_s = [], [], []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            it, esp, res, ts, tw = step()
+            iters.append(it)
+            solve_s.append(ts)
+            wall_s.append(tw)
+    torch.cuda.synchronize()
+    _barrier(dist)
+    launches = g.kernel_launches() - launches0
+    st_ms, st_n, st_bytes, _ = g.profile_get("hpsi_stencil")
+    g.profile(0)
+    tune = {k: g.profile_get(k)[0] for k in ("stencil_tile_y", "stencil_warps", "stencil_stages", "stencil_zchunks")}
+    lpc_state = g.lpc_status()
+    shares = {}
+    if args.shares:  # one extra, untimed solve with every kernel family timed
+        g.profile(1)
+        step()
+        names = ["hpsi_stencil", "nl_gather", "nl_scatter", "cg", "pc", "lpc", "gs", "gemm", "sd_gemm", "sd_eig",
+                 "sd_rot", "residual"]
+        shares = {n: round(g.profile_get(n)[0], 3) for n in names}
+        g.profile(0)
+    clocks = clk.summary()
+    esp_main = esp[0, 0].copy()
+    res_max = float(np.max(res[..., :mb_ref]))
+    g.close()
+    t_solve = _max_over_ranks(dist, statistics.mean(solve_s))
+    e2e_val = _max_over_ranks(dist, statistics.mean(wall_s))
+
+    # comparison solves on the same GPU and input (after the timed steps; the FP64 result
+    # overwrites the input buffer, which is no longer needed)
+    compare, errors = {}, None
+    arms = []
+    if "mixed_learned" in compare_arms and os.path.exists(wpath) and not (prec == api.PREC_MIXED and pc == "learned"):
+        arms.append(("mixed_learned", api.PREC_MIXED, api.PC_LEARNED))
+    if "mixed_hprsdft" in compare_arms and not (prec == api.PREC_MIXED and pc == "hprsdft"):
+        arms.append(("mixed_hprsdft", api.PREC_MIXED, api.PC_HPRSDFT))
+    if "fp64" in compare_arms and prec != api.PREC_FP64:
+        arms.append(("fp64_hprsdft", api.PREC_FP64, api.PC_HPRSDFT))
+    for name, pr, pm in arms:
+        with api.BandUpdate(prob, precision=pr, pc_mode=pm) as h:
+            if pm == api.PC_LEARNED:
+                h.lpc_set_weights(np.load(wpath))
+            h.init_sweep(mb_ref)
+            hs = torch.cuda.ExternalStream(h.stream())
+            h.set_wf_host(pin_in.data_ptr(), nb)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(hs)
+            h.gram_schmidt()
+            itc, espc, resc = h.calc_sweep(MAX_SWEEPS, tol=TOL)
+            e1.record(hs)
+            e1.synchronize()
+            tc = _max_over_ranks(dist, e0.elapsed_time(e1) / 1000.0)
+            entry = {"s": round(tc, 4), "sweeps": itc, "final_res_max": float(np.max(resc[..., :mb_ref]))}
+            if pm == api.PC_LEARNED:
+                entry["lpc_fallbacks"] = h.lpc_status()[2]
+            if name == "fp64_hprsdft":
+                h.get_wf_host(pin_in.data_ptr(), nb)
+                esp64 = espc[0, 0].copy()
+        compare[name] = entry
+        if name == "fp64_hprsdft":
+            compare["speedup_vs_fp64_hprsdft"] = round(tc / t_solve, 3)
+            m = gap_index(esp64, max(1, mb_ref - 32), mb_ref)
+            ang = principal_angle_max(pin_out, pin_in, m, prob.dV)
+            errors = {"vs": "fp64_hprsdft solve of the same input",
+                      "eig_err_max_Ha": float(np.max(np.abs(esp_main[:mb_ref] - esp64[:mb_ref]))),
+                      "principal_angle_max_rad": ang, "subspace_bands": m,
+                      "gap_Ha": float(esp64[m] - esp64[m - 1])}
+
+    hbm, bf16, peak_kind = _peaks()
+    avg_ms = (st_ms / st_n) if st_n else None
+    bytes_launch = (st_bytes / st_n) if st_n else None
+    achieved = bytes_launch / (avg_ms * 1e-3) / 1e9 if st_n else 0.0
+    ratio = NCU_TRAFFIC_RATIO.get((args.config, args.precision))
+    kname = "k_stencil_ws<float>" if prec == api.PREC_MIXED else "k_stencil_ws<double>"
+    roof = {"bound": "hbm", "kernel": f"{kname}: hpsi 37-point stencil + V_loc (nonlocal scatter separate)",
+            "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+            "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+            "traffic": (ratio * bytes_launch) if (ratio and bytes_launch) else None,
+            "launches": st_n, "avg_launch_ms": avg_ms, "algorithmic_bytes_per_launch": bytes_launch,
+            "config": tune}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        nthreads = os.cpu_count() or 1
+        per, desc, kind = cpu_sweep_estimate(prob, nthreads)
+        n_conv = compare.get("fp64_hprsdft", {}).get("sweeps") or SWEEPS_FP64.get(args.config)
+        cpu = {"value": per * n_conv, "unit": "s", "cores": nthreads, "kind": "port", "estimate": kind,
+               "sample": f"{desc}: {per:.2f} s per sweep on {nthreads} host threads (oracle/ restatement of the "
+                         f"reference CPU path) x {n_conv} sweeps of the FP64 method to max res <= 1e-8"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": t_solve, "unit": "s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_solve * 1000.0, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32+bf16x%d/x%d+f64" % terms,
+            "data": "synthetic (seeded Gaussian V_loc, Gaussian s/p projectors, seeded psi0)",
+            "config": {"workload": args.config, "grid": list(prob.n), "bands": nb, "atoms": prob.cfg.natom,
+                       "projectors": prob.nzlma, "precision": args.precision, "pc": pc,
+                       "lpc_fallbacks": lpc_state[2] if pc == "learned" else None,
+                       "gemm_terms": list(terms) if prec == api.PREC_MIXED else None,
+                       "mb_ref": mb_ref, "tol": TOL, "sweeps_to_tol": iters, "final_res_max": res_max,
+                       "l2": "inputs larger than L2 (psi >= 0.5 GB)", "parallelism": f"replicas x{ws}"},
+            "gpu_launches": int(launches),
+            "roofline": roof,
+            "errors": errors,
+            "compare": compare,
+            "time_shares_ms": shares or None,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_val, "unit": "s", "h2d_bytes_per_step": int(nb * ng * 8),
+                    "d2h_bytes_per_step": int(nb * ng * 8 + 2 * esp.nbytes)},
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------------------
+# single kernel families (timing and ncu captures)
+# ----------------------------------------------------------------------------------------
+def run_kernel(args):
+    import torch
+    from rsdft_develop_b200 import api, lpc_train, synth
+    what = args.kernel
+    reps = args.reps
+    if what == "gemm":
+        m, k = args.bands or 256, args.points or 262144
+        terms = int(args.gemm_terms.split(",")[0])
+        with api.BandUpdate(synth.make_problem("t0")) as g:
+            g.gemm_terms(terms, terms)
+            g.selftest_gemm(m, m, k, 0)  # untimed: module load, tensor-map encoder
+            g.profile(1)
+            e0 = g.selftest_gemm(m, m, k, 0)
+            ms0, _, _, fl0 = g.profile_get("gemm")
+            e1 = g.selftest_gemm(m, m, k, 1)
+            ms, n, _, fl = g.profile_get("gemm")
+            print(f"gemm m={m} k={k} terms={terms}: overlap rel.err {e0:.2e} {ms0:.3f} ms "
+                  f"({fl0 / max(ms0, 1e-9) / 1e9:.0f} TFLOP/s bf16), rotation rel.err {e1:.2e} {ms - ms0:.3f} ms "
+                  f"({(fl - fl0) / max(ms - ms0, 1e-9) / 1e9:.0f} TFLOP/s bf16)", flush=True)
+        return
+    prob = synth.make_problem(args.config)
+    nb = min(args.bands or prob.nband, prob.nband)
+    if what == "hpsi":
+        precs = {"both": ("fp64", "fp32"), "fp64": ("fp64",), "fp32": ("fp32",)}[args.hpsi_prec]
+        with api.BandUpdate(prob, nonlocal_on=not args.no_nonlocal) as g:
+            x = torch.empty((nb, prob.ng), dtype=torch.float64, device="cuda")
+            x.uniform_(-1.0, 1.0)
+            for name in precs:
+                f32 = name == "fp32"
+                a = x.float() if f32 else x
+                b = torch.empty_like(a)
+                g.hamiltonian_device(a.data_ptr(), b.data_ptr(), nb, fp32=f32)  # untimed first call
+                g.synchronize()
+                g.profile(1)
+                for _ in range(reps):
+                    g.hamiltonian_device(a.data_ptr(), b.data_ptr(), nb, fp32=f32)
+                g.synchronize()
+                ms, n, by, _ = g.profile_get("hpsi_stencil")
+                gms, gn, _, _ = g.profile_get("nl_gather")
+                sms, sn, _, _ = g.profile_get("nl_scatter")
+                pre = "stencil" if f32 else "stencil64"
+                cfg = {k: g.profile_get(f"{pre}_{k}")[0] for k in ("tile_y", "warps", "stages", "zchunks")}
+                print(f"hpsi {args.config} {name} bands={nb}: stencil {ms / max(n, 1):.3f} ms "
+                      f"({by / max(ms, 1e-9) / 1e6:.1f} GB/s algorithmic), gather {gms / max(gn, 1):.3f} ms, "
+                      f"scatter {sms / max(sn, 1):.3f} ms; {cfg}", flush=True)
+                g.profile(0)
+                del a, b
+        return
+    rng = np.random.default_rng(3)
+    g_in = rng.standard_normal((nb, prob.ng))
+    if what == "pc":
+        for f32 in (False, True):
+            with api.BandUpdate(prob, precision=api.PREC_MIXED if f32 else api.PREC_FP64) as g:
+                run = (lambda: g.precond_f32(g_in)) if f32 else (lambda: g.precond(g_in))
+                run()
+                g.profile(1)
+                for _ in range(reps):
+                    run()
+                ms, n, _, _ = g.profile_get("pc")
+                print(f"precond_hprsdft ({'FP32 s-step' if f32 else 'FP64'}) {args.config} bands={nb}: "
+                      f"{ms / reps:.3f} ms per application", flush=True)
+    elif what == "lpc":
+        with api.BandUpdate(prob, precision=api.PREC_MIXED, pc_mode=api.PC_LEARNED) as g:
+            g.lpc_set_weights(np.load(lpc_train.default_weights_path(prob.h)))
+            x = g_in.astype(np.float32)
+            for mode in ("tc", "fp32"):
+                g.lpc_inference(fp32=(mode == "fp32"))
+                g.lpc_precond(x)
+                g.profile(1)
+                for _ in range(reps):
+                    g.lpc_precond(x)
+                ms, n, _, fl = g.profile_get("lpc")
+                print(f"learned preconditioner ({mode}) {args.config} bands={nb}: {ms / reps:.3f} ms per "
+                      f"application, {fl / max(ms, 1e-9) / 1e9:.1f} TFLOP/s", flush=True)
+                for part in ("lpc_layer1", "lpc_mid", "lpc_layer4"):
+                    pms, _, pby, pfl = g.profile_get(part)
+                    if pms > 0:
+                        print(f"  {part}: {pms / reps:.3f} ms, {pfl / pms / 1e9:.1f} TFLOP/s", flush=True)
+                g.profile(0)
+    else:
+        raise SystemExit(f"unknown kernel family {what!r}")
 
 
 def main():
@@ -194,175 +541,35 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c1")
+    ap.add_argument("--config", default="c3", help="workload: c0, c1, c2, c3 (real8) (default c3)")
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
-    ap.add_argument("--pc", default="hprsdft", choices=["auto", "learned", "hprsdft", "none"],
-                    help="CG preconditioner; auto = learned when trained weights for the grid spacing exist")
-    ap.add_argument("--no-compare", action="store_true",
-                    help="skip the comparison solves (plain FP64, and mixed with precond_hprsdft)")
-    ap.add_argument("--sweeps-to-tol", type=int, default=100)
+    ap.add_argument("--pc", default="hprsdft", choices=["learned", "hprsdft", "none"], help="CG preconditioner")
+    ap.add_argument("--compare", default="fp64",
+                    help="comma list of comparison solves: fp64, mixed_hprsdft, mixed_learned, none")
+    ap.add_argument("--shares", action="store_true", help="one extra untimed solve with per-kernel times")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer (C ABI) solves (large configs)")
     ap.add_argument("--gemm-terms", default="3,3",
                     help="BF16 terms of the mixed overlap/Hsub and rotation contractions (2 or 3 each)")
+    ap.add_argument("--kernel", default="solve", choices=["solve", "hpsi", "gemm", "pc", "lpc"],
+                    help="solve (the benchmark) or one kernel family on its own")
+    ap.add_argument("--bands", type=int, default=0, help="--kernel: bands (default all / 256 for gemm)")
+    ap.add_argument("--points", type=int, default=0, help="--kernel gemm: K points")
+    ap.add_argument("--reps", type=int, default=3, help="--kernel: timed repetitions")
+    ap.add_argument("--hpsi-prec", default="both", choices=["both", "fp64", "fp32"])
+    ap.add_argument("--no-nonlocal", action="store_true", help="--kernel hpsi: operator without projectors")
     args = ap.parse_args()
+    if args.kernel != "solve":
+        run_kernel(args)
+        return
     dist, rank, ws = _dist()
-    if args.impl == "reference":
-        run_reference(args, dist, rank, ws)
+    try:
+        if args.impl == "reference":
+            run_reference(args, dist, rank, ws)
+        else:
+            run_ours(args, dist, rank, ws)
+    finally:
         if dist is not None:
             dist.destroy_process_group()
-        return
-
-    import torch
-    from rsdft_develop_b200 import api, synth
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    from rsdft_develop_b200 import lpc_train
-    prob = synth.make_problem(args.config)
-    prec = api.PREC_MIXED if args.precision == "mixed" else api.PREC_FP64
-    wpath = lpc_train.default_weights_path(prob.h)
-    pc = args.pc
-    if pc == "auto":
-        pc = "learned" if (prec == api.PREC_MIXED and os.path.exists(wpath)) else "hprsdft"
-    pc_mode = {"learned": api.PC_LEARNED, "hprsdft": api.PC_HPRSDFT, "none": api.PC_NONE}[pc]
-    g = api.BandUpdate(prob, precision=prec, pc_mode=pc_mode)
-    terms = tuple(int(t) for t in args.gemm_terms.split(","))
-    g.gemm_terms(*terms)
-    if pc == "learned":
-        g.lpc_set_weights(np.load(wpath))
-    mb_ref = mb_ref_of(prob.nband)
-    g.init_sweep(mb_ref)
-    stream = torch.cuda.ExternalStream(g.stream())
-
-    for _ in range(args.warmup):
-        solve(g, 1, TOL)
-    g.synchronize()
-    _barrier(dist)
-    torch.cuda.synchronize()
-    launches0 = g.kernel_launches()
-    g.profile(True)
-    iters = []
-    with ClockSampler(local) as clk:
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
-        for _ in range(args.steps):
-            it, esp, res = solve(g, 1, TOL)
-            iters.append(it)
-        ev1.record(stream)
-        ev1.synchronize()
-    torch.cuda.synchronize()
-    dt_ms = ev0.elapsed_time(ev1)
-    launches = g.kernel_launches() - launches0
-    st_ms, st_n, st_bytes, _ = g.profile_get("hpsi_stencil")
-    names = ["hpsi_stencil", "nl_gather", "nl_scatter", "cg", "pc", "lpc", "gs", "gemm", "sd_gemm", "sd_eig",
-             "sd_rot", "residual"]
-    shares = {n: g.profile_get(n)[0] for n in names}
-    g.profile(False)
-    lpc_state = g.lpc_status()
-    clocks = clk.summary()
-    res_max = float(np.max(res[..., :mb_ref]))
-    per_step = dt_ms / args.steps
-    t_solve = _max_over_ranks(dist, per_step / 1000.0)
-
-    e2e_t, h2d, d2h = [], 0, 0
-    if not args.no_e2e:
-        # e2e: the same solve through the C ABI from pinned host buffers
-        psi0 = synth.random_wavefunctions(1, prob.nband, prob.ng)
-        pin = torch.from_numpy(psi0).pin_memory()
-        pin_np = pin.numpy()
-        out = torch.empty_like(pin).pin_memory().numpy()
-        e2e_t = []
-        for i in range(1 + args.steps):
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            g.set_wf(pin_np)
-            g.gram_schmidt()
-            it, esp, res = g.calc_sweep(MAX_SWEEPS, tol=TOL)
-            g.lib.rsdft_gpu_get_wf_d(1, 1, out.ctypes.data, prob.ng, prob.nband)
-            torch.cuda.synchronize()
-            if i > 0:
-                e2e_t.append(time.perf_counter() - t0)
-        h2d = int(psi0.nbytes)
-        d2h = int(out.nbytes + esp.nbytes + res.nbytes)
-    e2e_val = _max_over_ranks(dist, statistics.median(e2e_t)) if e2e_t else None
-
-    g.close()
-    # comparison solves on the same GPU: the plain FP64 method (the drop-in's FP64 path with
-    # precond_hprsdft) and, when the main arm is learned, mixed precision with precond_hprsdft
-    compare = {}
-    if not args.no_compare:
-        arms = [("fp64_hprsdft", api.PREC_FP64, api.PC_HPRSDFT)]
-        if pc != "hprsdft" and prec == api.PREC_MIXED:
-            arms.append(("mixed_hprsdft", api.PREC_MIXED, api.PC_HPRSDFT))
-        if pc != "learned" and os.path.exists(wpath):
-            arms.append(("mixed_learned", api.PREC_MIXED, api.PC_LEARNED))
-        for name, pr, pm in arms:
-            if pr == prec and pm == pc_mode:
-                continue
-            with api.BandUpdate(prob, precision=pr, pc_mode=pm) as h:
-                if pm == api.PC_LEARNED:
-                    h.lpc_set_weights(np.load(wpath))
-                h.init_sweep(mb_ref)
-                hs = torch.cuda.ExternalStream(h.stream())
-                solve(h, 1, TOL)
-                h.synchronize()
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                e0.record(hs)
-                itc, _, _ = solve(h, 1, TOL)
-                e1.record(hs)
-                e1.synchronize()
-                tc = _max_over_ranks(dist, e0.elapsed_time(e1) / 1000.0)
-            compare[name] = {"s": round(tc, 4), "sweeps": itc}
-        if "fp64_hprsdft" in compare:
-            compare["speedup_vs_fp64_hprsdft"] = round(compare["fp64_hprsdft"]["s"] / t_solve, 3)
-
-    hbm, bf16, peak_kind = _peaks()
-    achieved = (st_bytes / st_n) / ((st_ms / st_n) * 1e-3) / 1e9 if st_n else 0.0
-    ratio = NCU_TRAFFIC_RATIO.get((args.config, args.precision))
-    kname = "k_stencil_stream<float>" if prec == api.PREC_MIXED else "k_stencil_stream<double>"
-    roof = {"bound": "hbm", "kernel": f"{kname} (hpsi: 37-point stencil + V_loc; the nonlocal scatter is a separate kernel)",
-            "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
-            "frac": round(achieved / hbm, 4), "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-            "traffic": (ratio * st_bytes / st_n) if ratio else None,
-            "launches": st_n, "avg_launch_ms": (st_ms / st_n) if st_n else None,
-            "algorithmic_bytes_per_launch": (st_bytes / st_n) if st_n else None}
-
-    cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
-        nthreads = os.cpu_count() or 1
-        per = cpu_sweep_time(args.config, nthreads)
-        n_conv = int(statistics.median(iters))
-        cpu = {"value": per * n_conv, "unit": "s", "cores": nthreads, "kind": "port",
-               "sample": f"1 oracle CG+GS+SD sweep of {args.config} on {nthreads} host threads "
-                         f"({per:.2f} s), x {n_conv} sweeps the plain method needs to reach 1e-8"}
-
-    if rank == 0:
-        line = {
-            "metric": METRIC, "value": t_solve, "unit": "s", "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": per_step, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.precision == "fp64" else "f32+bf16x%d/x%d+f64" % terms,
-            "data": "synthetic (seeded Gaussian V_loc, Gaussian s/p projectors, seeded psi0)",
-            "config": {"workload": args.config, "grid": list(prob.n), "bands": prob.nband,
-                       "atoms": prob.cfg.natom, "projectors": prob.nzlma, "precision": args.precision,
-                       "pc": pc, "lpc_fallbacks": lpc_state[2] if pc == "learned" else None,
-                       "lpc_weights": os.path.relpath(wpath, ROOT) if pc == "learned" else None,
-                       "gemm_terms": list(terms) if prec == api.PREC_MIXED else None,
-                       "mb_ref": mb_ref, "sweeps_to_tol": iters, "final_res_max": res_max,
-                       "l2": "inputs larger than L2 (psi >= 0.5 GB)", "parallelism": f"replicas x{ws}"},
-            "gpu_launches": int(launches),
-            "roofline": roof,
-            "time_shares_ms": {k: round(v, 3) for k, v in shares.items()},
-            "compare": compare,
-            "cpu_baseline": cpu,
-            "e2e": {"value": e2e_val, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "clocks": clocks,
-        }
-        print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.destroy_process_group()
 
 
 if __name__ == "__main__":

@@ -212,7 +212,9 @@ int rsdft_gpu_lpc_inference(int mode);
 int rsdft_gpu_lpc_status(int* ready, int* pc_in_use, int* fallbacks, int* dataset);
 
 /* ---- measurement ---- */
-/* Per-kernel CUDA-event timing of the library's own launches (off by default). */
+/* Per-kernel CUDA-event timing of the library's own launches: 0 off (the default), 1 every
+ * kernel family, 2 the hpsi stencil only (two events per stencil launch and no host
+ * synchronisation, so a timed solve is not slowed by it). */
 int rsdft_gpu_profile(int on);
 /* total device time (ms), launch count, algorithmic bytes and flops recorded for kernel
  * family `name` ("hpsi_stencil", "nl_gather", "gemm", "cg", "pc", ...); any output may be NULL.

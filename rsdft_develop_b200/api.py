@@ -252,6 +252,16 @@ class BandUpdate:
             _call(self.lib.rsdft_gpu_get_wf_d, k, s, _ptr(a), self.prob.ng, nb)
         return a
 
+    def set_wf_host(self, ptr: int, nb: int, k: int = 1, s: int = 1):
+        """set_wf from a raw host pointer (e.g. pinned memory) holding nb bands of ML0 points."""
+        fn = self.lib.rsdft_gpu_set_wf_z if self.cplx else self.lib.rsdft_gpu_set_wf_d
+        _call(fn, k, s, C.c_void_p(ptr), self.prob.ng, nb)
+
+    def get_wf_host(self, ptr: int, nb: int, k: int = 1, s: int = 1):
+        """get_wf into a raw host pointer (e.g. pinned memory) with room for nb bands."""
+        fn = self.lib.rsdft_gpu_get_wf_z if self.cplx else self.lib.rsdft_gpu_get_wf_d
+        _call(fn, k, s, C.c_void_p(ptr), self.prob.ng, nb)
+
     def random_wf(self, seed: int, k: int = 1, s: int = 1):
         _call(self.lib.rsdft_gpu_random_wf, k, s, C.c_uint64(seed))
 
@@ -417,8 +427,10 @@ class BandUpdate:
         return tuple(x.value for x in v)
 
     # ---- measurement ----
-    def profile(self, on: bool):
-        _call(self.lib.rsdft_gpu_profile, 1 if on else 0)
+    def profile(self, on):
+        """Per-kernel CUDA-event timing: False/0 off, True/1 every kernel family, 2 the hpsi
+        stencil only."""
+        _call(self.lib.rsdft_gpu_profile, int(on))
 
     def profile_get(self, name: str):
         """(total ms, launches, algorithmic bytes, algorithmic flops) of a kernel family."""

@@ -44,7 +44,7 @@ static cudaEvent_t take_event(Ctx& c) {
 }
 ProfScope::ProfScope(Ctx& c_, const char* n, double bytes_, double flops_)
     : c(c_), name(n), bytes(bytes_), flops(flops_) {
-  if (!c.profiling) return;
+  if (!c.profiling || (c.profiling == 2 && std::strcmp(n, "hpsi_stencil") != 0)) return;
   e0 = take_event(c);
   e1 = take_event(c);
   cudaEventRecord(e0, c.stream);
@@ -472,6 +472,10 @@ static int wf_slot(Ctx& c, int k, int s, WaveFns** w) {
   return 0;
 }
 
+// Bands per chunk of the FP64 host <-> FP32 device transfers of the mixed-precision build
+// (staging buffer of at most 1 GiB).
+static int stage_bands(size_t n) { return (int)std::max<size_t>(1, ((size_t)1 << 30) / (sizeof(double) * n)); }
+
 static int set_wf(int k, int s, const double* unk, int ld, int nb, bool cplx) {
   REQUIRE_CTX();
   Ctx& c = *g_ctx;
@@ -487,10 +491,16 @@ static int set_wf(int k, int s, const double* unk, int ld, int nb, bool cplx) {
     RS_CUDA(cudaMemcpy2DAsync(w->psi.p, n * sizeof(double), unk, (size_t)ld * nc * sizeof(double),
                               n * sizeof(double), nb, cudaMemcpyHostToDevice, c.stream));
   } else {
-    RS_TRY(c.ws_io_a.ensure(sizeof(double) * n * nb));
-    RS_CUDA(cudaMemcpy2DAsync(c.ws_io_a.p, n * sizeof(double), unk, (size_t)ld * nc * sizeof(double),
-                              n * sizeof(double), nb, cudaMemcpyHostToDevice, c.stream));
-    RS_TRY(convert_d2f(c, c.ws_io_a.as<double>(), w->psi.as<float>(), n * nb));
+    // FP64 host bands pass through a bounded device staging buffer in band chunks
+    const int chunk = stage_bands(n);
+    RS_TRY(c.ws_io_a.ensure(sizeof(double) * n * (size_t)std::min(chunk, nb)));
+    for (int b0 = 0; b0 < nb; b0 += chunk) {
+      const int cb = std::min(chunk, nb - b0);
+      RS_CUDA(cudaMemcpy2DAsync(c.ws_io_a.p, n * sizeof(double), unk + (size_t)b0 * ld * nc,
+                                (size_t)ld * nc * sizeof(double), n * sizeof(double), cb, cudaMemcpyHostToDevice,
+                                c.stream));
+      RS_TRY(convert_d2f(c, c.ws_io_a.as<double>(), w->psi.as<float>() + (size_t)b0 * n, n * cb));
+    }
   }
   RS_CUDA(cudaStreamSynchronize(c.stream));
   w->valid = true;
@@ -512,10 +522,14 @@ static int get_wf(int k, int s, double* unk, int ld, int nb, bool cplx) {
     RS_CUDA(cudaMemcpy2DAsync(unk, (size_t)ld * nc * sizeof(double), w->psi.p, n * sizeof(double),
                               n * sizeof(double), nb, cudaMemcpyDeviceToHost, c.stream));
   } else {
-    RS_TRY(c.ws_io_a.ensure(sizeof(double) * n * nb));
-    RS_TRY(convert_f2d(c, w->psi.as<float>(), c.ws_io_a.as<double>(), n * nb));
-    RS_CUDA(cudaMemcpy2DAsync(unk, (size_t)ld * nc * sizeof(double), c.ws_io_a.p, n * sizeof(double),
-                              n * sizeof(double), nb, cudaMemcpyDeviceToHost, c.stream));
+    const int chunk = stage_bands(n);
+    RS_TRY(c.ws_io_a.ensure(sizeof(double) * n * (size_t)std::min(chunk, nb)));
+    for (int b0 = 0; b0 < nb; b0 += chunk) {
+      const int cb = std::min(chunk, nb - b0);
+      RS_TRY(convert_f2d(c, w->psi.as<float>() + (size_t)b0 * n, c.ws_io_a.as<double>(), n * cb));
+      RS_CUDA(cudaMemcpy2DAsync(unk + (size_t)b0 * ld * nc, (size_t)ld * nc * sizeof(double), c.ws_io_a.p,
+                                n * sizeof(double), n * sizeof(double), cb, cudaMemcpyDeviceToHost, c.stream));
+    }
   }
   RS_CUDA(cudaStreamSynchronize(c.stream));
   return check_status(c);
@@ -696,7 +710,8 @@ int rsdft_gpu_profile(int on) {
   REQUIRE_CTX();
   Ctx& c = *g_ctx;
   prof_flush(c);
-  c.profiling = on != 0;
+  RS_CHECK(on >= 0 && on <= 2, RSDFT_ERR_ARG, "profile mode must be 0, 1 or 2");
+  c.profiling = on;
   if (on) c.prof.clear();
   return 0;
 }

@@ -113,8 +113,8 @@ struct Ctx {
   int rot_update = 0;              // mixed rotation in update form X + X (C - I)
   int nl_fused = 0;                // nonlocal term inside the stencil (1) or by the scatter kernel after it (0)
 
-  // profiling
-  bool profiling = false;
+  // profiling: 0 off, 1 every kernel family, 2 the hpsi stencil only (light enough for a timed run)
+  int profiling = 0;
   std::map<std::string, ProfEntry> prof;
   struct Pending {
     std::string name;
