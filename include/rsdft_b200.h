@@ -126,14 +126,17 @@ int rsdft_gpu_hamiltonian_c(int k, int s, const float* tpsi, float* htpsi, int l
 /* hamiltonian on caller-owned DEVICE blocks (FP64, real8 build) that performs no device
  * allocation.  No counterpart in the reference.  For callers that cannot let a library call
  * cudaMalloc -- a host code that reserves the whole device memory pool up front, a caller
- * running inside another framework's pool or stream capture, or a loop where cudaMalloc's
- * implicit device synchronisation would stall -- the nonlocal coefficient scratch comes from a
- * fixed 4 MiB array compiled into the library (held on every GPU that loads it until the
- * process exits): nb x (atoms x padded projectors per atom) must not exceed 524288, larger
- * requests return RSDFT_ERR_ARG (split the bands into blocks).  The first call on a device
- * looks the array's device address up (cudaGetSymbolAddress); make that first call before any
- * stream capture.  All calls share the array: calls that overlap on the GPU race; nothing in
- * it has to start at zero (every call rewrites what it reads).  Runs on the library stream. */
+ * running inside another framework's memory pool, or a loop where cudaMalloc's implicit device
+ * synchronisation would stall -- the nonlocal coefficient scratch comes from a fixed 4 MiB array
+ * compiled into the library (held on every GPU that loads it until the process exits):
+ * nb x (atoms x padded projectors per atom) must not exceed 524288, larger requests return
+ * RSDFT_ERR_ARG (split the bands into blocks).  The first call of a context looks the array's
+ * device address up (cudaGetSymbolAddress, on the device that was current at rsdft_gpu_init;
+ * another current device returns RSDFT_ERR_STATE); make that first call before any stream
+ * capture.  The stencil runs in its stencil + scatter form whatever rsdft_gpu_set_nl_form
+ * selects (no tuning runs, no host synchronisation).  All calls share the array: calls that
+ * overlap on the GPU race; nothing in it has to start at zero (every call rewrites what it
+ * reads).  Runs on the library stream. */
 int rsdft_gpu_hamiltonian_noalloc_d(int k, int s, const double* tpsi, double* htpsi, int ld, int nb);
 /* conjugate_gradient on the resident unk(:,:,k,s); esp/res (host, length nband) as the
  * reference's esp(:,k,s)/res(:,k,s), res = dV |H psi - e psi|^2 (cg_module.f90:231,556). */
@@ -158,6 +161,12 @@ int rsdft_gpu_set_pc_form(int sstep);
  * last).  iters receives the sweeps done; esp/res (host, nband*nk*nspin, k-major after band)
  * receive the final FP64 values. */
 int rsdft_gpu_sweep(int nsweep, double tol, int* iters, double* esp, double* res);
+/* Switch the context between RSDFT_PREC_MIXED and RSDFT_PREC_FP64, converting the resident
+ * wavefunctions of every (k, s) (to FP32 by rounding, to FP64 exactly).  The FP64 final polish of
+ * a mixed-precision solve: rsdft_gpu_sweep to the FP32 floor (res ~ 1e-9 .. 1e-10) in mixed
+ * precision, then rsdft_gpu_set_precision(RSDFT_PREC_FP64) and rsdft_gpu_sweep to the tighter
+ * tolerance.  No counterpart in the reference (which has one precision per build). */
+int rsdft_gpu_set_precision(int precision);
 /* Convergence band set of rsdft_gpu_sweep: bands 1..mb_ref are checked (0: all bands), as the
  * reference's init_sweep(iconv_check, mb_ref, tol) does for its band and DOS drivers
  * (src/sweep_module.f90:46-60,267-278; src/band_module.f90:207; src/dos_module.f90:64-75). */
@@ -243,6 +252,12 @@ int rsdft_gpu_set_gemm_terms(int overlap_terms, int rotation_terms);
  * mirrored; else both triangles, averaged); bit 2 set, the band rotation in plain form X C, else
  * in the update form X + X (C - I).  Measurement knob; no counterpart in the reference. */
 int rsdft_gpu_set_gemm_tile(int flags);
+/* Diagnostic: polls a bounded wait of the real build's hpsi stencil makes before it gives up
+ * (0: it gives up at once; < 0: the default).  A wait that gives up ends the launch with
+ * RSDFT_ERR_TIMEOUT from the entry that reads the device status word; the kernel first lets its
+ * own bulk copies land, so the context stays usable.  Lets a test take the timeout path without
+ * any GPU fault.  No counterpart in the reference. */
+int rsdft_gpu_set_wait_polls(int polls);
 /* Where the real build's hpsi adds the nonlocal term: 0 (default) a scatter kernel after the
  * stencil (one read-modify-write per covered point and band), 1 inside the streaming stencil
  * (records staged per plane).  Measurement knob; no counterpart in the reference. */

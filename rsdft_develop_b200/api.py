@@ -51,7 +51,7 @@ EXPORTS = [
     "rsdft_gpu_hamiltonian_z", "rsdft_gpu_hamiltonian_f", "rsdft_gpu_hamiltonian_c",
     "rsdft_gpu_conjugate_gradient", "rsdft_gpu_gram_schmidt", "rsdft_gpu_subspace_diag",
     "rsdft_gpu_residual", "rsdft_gpu_precond_d", "rsdft_gpu_precond_f", "rsdft_gpu_set_pc_form", "rsdft_gpu_sweep", "rsdft_gpu_profile",
-    "rsdft_gpu_profile_get", "rsdft_gpu_kernel_launches", "rsdft_gpu_selftest_gemm", "rsdft_gpu_set_gemm_terms", "rsdft_gpu_set_gemm_tile", "rsdft_gpu_set_nl_form", "rsdft_gpu_init_sweep",
+    "rsdft_gpu_profile_get", "rsdft_gpu_kernel_launches", "rsdft_gpu_selftest_gemm", "rsdft_gpu_set_gemm_terms", "rsdft_gpu_set_gemm_tile", "rsdft_gpu_set_nl_form", "rsdft_gpu_init_sweep", "rsdft_gpu_set_wait_polls", "rsdft_gpu_set_precision",
     "rsdft_gpu_hamiltonian_noalloc_d",
     "rsdft_gpu_lpc_init", "rsdft_gpu_lpc_set_weights", "rsdft_gpu_lpc_get_weights", "rsdft_gpu_lpc_forward",
     "rsdft_gpu_lpc_loss_grad", "rsdft_gpu_lpc_dataset", "rsdft_gpu_lpc_harvest", "rsdft_gpu_lpc_dataset_get",
@@ -111,6 +111,7 @@ def load_library(path: str = LIB_PATH):
         "rsdft_gpu_sweep": [i, d, C.POINTER(C.c_int), vp, vp],
         "rsdft_gpu_selftest_gemm": [i, i, C.c_longlong, i, C.POINTER(C.c_double)],
         "rsdft_gpu_set_gemm_terms": [i, i], "rsdft_gpu_set_gemm_tile": [i], "rsdft_gpu_set_nl_form": [i],
+        "rsdft_gpu_set_wait_polls": [i], "rsdft_gpu_set_precision": [i],
         "rsdft_gpu_init_sweep": [i],
         "rsdft_gpu_hamiltonian_noalloc_d": [i, i, vp, vp, i, i],
         "rsdft_gpu_lpc_init": [C.c_ulonglong], "rsdft_gpu_lpc_set_weights": [vp, i],
@@ -335,6 +336,12 @@ class BandUpdate:
         _call(self.lib.rsdft_gpu_residual, k, s, _ptr(esp), _ptr(res))
         return esp, res
 
+    def set_precision(self, precision: int):
+        """Switch between PREC_MIXED and PREC_FP64, converting the resident wavefunctions (the
+        FP64 final polish of a mixed-precision solve is set_precision(PREC_FP64) + calc_sweep)."""
+        _call(self.lib.rsdft_gpu_set_precision, int(precision))
+        self.precision = precision
+
     def init_sweep(self, mb_ref: int = 0):
         """Check convergence on bands 1..mb_ref (0: all), as init_sweep(..., mb_ref, ...)."""
         _call(self.lib.rsdft_gpu_init_sweep, int(mb_ref))
@@ -454,6 +461,10 @@ class BandUpdate:
     def nl_form(self, fused: bool) -> None:
         """Nonlocal term of the real hpsi: inside the stencil (fused) or by a scatter after it."""
         _call(self.lib.rsdft_gpu_set_nl_form, 1 if fused else 0)
+
+    def wait_polls(self, polls: int) -> None:
+        """Polls of the hpsi stencil's bounded waits (0: give up at once; < 0: the default)."""
+        _call(self.lib.rsdft_gpu_set_wait_polls, int(polls))
 
     def gemm_tile(self, wide: bool = True, tri: int = 1, update: bool = False) -> None:
         """Three-term GEMM tiles: 128 x 256 over K blocks of 32 (default) or 128 x 128 over 64;

@@ -308,7 +308,7 @@ static int hamiltonian_entry(int k, int s, const T* tpsi, T* htpsi, int ld, int 
   Ctx& c = *g_ctx;
   RS_CHECK(cplx == c.cplx, RSDFT_ERR_STATE, "real/complex entry does not match the context");
   RS_CHECK(k >= 1 && k <= c.p.nk && s >= 1 && s <= c.p.nspin, RSDFT_ERR_ARG, "(k,s) out of range");
-  RS_CHECK(tpsi && htpsi && (size_t)ld >= c.ng && nb >= 0, RSDFT_ERR_ARG, "bad hamiltonian arguments");
+  RS_CHECK(tpsi && htpsi && ld > 0 && (size_t)ld >= c.ng && nb >= 0, RSDFT_ERR_ARG, "bad hamiltonian arguments");
   RS_CHECK(mem == RSDFT_MEM_HOST || mem == RSDFT_MEM_DEVICE, RSDFT_ERR_ARG, "bad memory space %d", mem);
   if (nb == 0) return 0;
   const int nc = cplx ? 2 : 1;
@@ -363,6 +363,7 @@ int rsdft_gpu_init(const rsdft_gpu_params* p) {
   c->mixed = p->precision == RSDFT_PREC_MIXED;
   if (c->p.ncg <= 0) c->p.ncg = 3;
   if (c->p.mloop <= 0) c->p.mloop = 3;
+  cudaGetDevice(&c->device);
   cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     set_error(RSDFT_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
@@ -645,6 +646,35 @@ int rsdft_gpu_residual(int k, int s, double* esp, double* res) {
   return check_status(c);
 }
 
+int rsdft_gpu_set_precision(int precision) {
+  REQUIRE_CTX();
+  Ctx& c = *g_ctx;
+  RS_CHECK(precision == RSDFT_PREC_FP64 || precision == RSDFT_PREC_MIXED, RSDFT_ERR_ARG,
+           "unknown precision mode %d", precision);
+  const bool to_mixed = precision == RSDFT_PREC_MIXED;
+  if (to_mixed == c.mixed) return 0;
+  const size_t nc = c.cplx ? 2 : 1;
+  for (int kk = 0; kk < c.p.nk; ++kk)
+    for (int s = 0; s < c.p.nspin; ++s) {
+      WaveFns& w = c.wfn(kk, s);
+      if (!w.valid || !w.psi.p) continue;
+      const size_t n = c.ng * nc * (size_t)c.kp[kk].nband;
+      DBuf nb;
+      RS_TRY(nb.ensure(n * (to_mixed ? sizeof(float) : sizeof(double))));
+      if (to_mixed)
+        RS_TRY(convert_d2f(c, w.psi.as<double>(), nb.as<float>(), n));
+      else
+        RS_TRY(convert_f2d(c, w.psi.as<float>(), nb.as<double>(), n));
+      RS_CUDA(cudaStreamSynchronize(c.stream));
+      w.psi.release();
+      w.psi = nb;
+    }
+  c.mixed = to_mixed;
+  c.p.precision = precision;
+  c.cg_hx_ready = false;  // CG's H x array holds the other precision
+  return check_status(c);
+}
+
 int rsdft_gpu_init_sweep(int mb_ref) {
   REQUIRE_CTX();
   RS_CHECK(mb_ref >= 0, RSDFT_ERR_ARG, "mb_ref must be >= 0");
@@ -720,6 +750,13 @@ int rsdft_gpu_profile_get(const char* name, double* total_ms, long long* launche
   REQUIRE_CTX();
   Ctx& c = *g_ctx;
   prof_flush(c);
+  if (name && std::strcmp(name, "workspace_bytes") == 0) {
+    if (total_ms) *total_ms = 0.0;
+    if (launches) *launches = 0;
+    if (bytes) *bytes = (double)c.workspace_bytes();
+    if (flops) *flops = 0.0;
+    return 0;
+  }
   auto it = c.prof.find(name ? name : "");
   const bool f = it != c.prof.end();
   if (!f && name) {
@@ -760,6 +797,12 @@ int rsdft_gpu_set_nl_form(int fused) {
   RS_CHECK(fused == 0 || fused == 1, RSDFT_ERR_ARG, "fused must be 0 or 1");
   g_ctx->nl_fused = fused;
   g_ctx->stencil_tune.clear();  // the stencil's best configuration depends on it
+  return 0;
+}
+
+int rsdft_gpu_set_wait_polls(int polls) {
+  REQUIRE_CTX();
+  g_ctx->wait_polls = polls < 0 ? -1 : polls;
   return 0;
 }
 

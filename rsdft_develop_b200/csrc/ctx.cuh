@@ -68,6 +68,8 @@ struct Ctx {
   bool cplx = false;
   bool mixed = false;
   cudaStream_t stream = nullptr;
+  int device = 0;                  // the CUDA device current at rsdft_gpu_init
+  double* noalloc_scratch = nullptr;  // device address of the allocation-free entry's fixed array
   cublasHandle_t cublas = nullptr;
   cusolverDnHandle_t cusolver = nullptr;
   unsigned* d_status = nullptr;
@@ -112,6 +114,7 @@ struct Ctx {
   int gemm_tri = 1;                // S by upper-triangle tiles (1), S and Hsub (2), neither (0)
   int rot_update = 0;              // mixed rotation in update form X + X (C - I)
   int nl_fused = 0;                // nonlocal term inside the stencil (1) or by the scatter kernel after it (0)
+  int wait_polls = -1;             // hpsi stencil's bounded waits: polls before giving up (-1: the default)
 
   // profiling: 0 off, 1 every kernel family, 2 the hpsi stencil only (light enough for a timed run)
   int profiling = 0;
@@ -125,6 +128,11 @@ struct Ctx {
   std::vector<cudaEvent_t> event_pool;
 
   WaveFns& wfn(int k, int s) { return wf[(size_t)k * p.nspin + s]; }
+  size_t workspace_bytes() const {  // device bytes of the context's growable workspaces
+    return ws_coef.bytes + ws_io_a.bytes + ws_io_b.bytes + ws_cg.bytes + ws_red.bytes + ws_scal.bytes + ws_dense.bytes +
+           ws_hpsi.bytes + ws_flag.bytes + ws_rot.bytes + ws_solver.bytes + ws_info.bytes + ws_gemm.bytes + ws_out.bytes +
+           ws_f64.bytes + vzero.bytes;
+  }
   size_t elem_bytes() const { return (mixed ? 4 : 8) * (cplx ? 2 : 1); }
 };
 

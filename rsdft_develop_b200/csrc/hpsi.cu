@@ -193,8 +193,8 @@ static int nl_scatter(Ctx& c, int k, const T* coef, T* out, size_t ld, int nb) {
 // (default), or inside the stencil (c.nl_fused).
 template <typename T, int MD>
 static int launch_stencil(Ctx& c, int k, int s, const T* psi, T* out, size_t ld, int nb, const T* coef,
-                          const T* vloc_override = nullptr, double c0_shift = 0.0) {
-  if (coef != nullptr && c.nl_fused)
+                          const T* vloc_override = nullptr, double c0_shift = 0.0, bool allow_fused = true) {
+  if (coef != nullptr && c.nl_fused && allow_fused)
     return launch_stencil_stream<T, MD>(c, k, s, psi, out, ld, nb, coef, vloc_override, c0_shift);
   RS_TRY((launch_stencil_ws<T, MD>(c, k, s, psi, out, ld, nb, vloc_override, c0_shift)));
   return coef ? nl_scatter<T>(c, k, coef, out, ld, nb) : 0;
@@ -222,7 +222,8 @@ template int hpsi_real<float>(Ctx&, int, int, const float*, float*, size_t, int)
 template int hpsi_real<double>(Ctx&, int, int, const double*, double*, size_t, int);
 
 // hpsi with caller-provided scratch for the nonlocal coefficient rows (coef_cap elements of
-// T); performs no device allocation.
+// T); performs no device allocation.  Always the stencil + scatter form: it needs no tuning
+// runs and no host synchronisation.
 template <typename T>
 int hpsi_real_scratch(Ctx& c, int k, int s, const T* psi, T* out, size_t ld, int nb, T* coef, size_t coef_cap) {
   RS_CHECK(!c.cplx, RSDFT_ERR_STATE, "real hpsi called on a complex16 context");
@@ -238,8 +239,8 @@ int hpsi_real_scratch(Ctx& c, int k, int s, const T* psi, T* out, size_t ld, int
     cf = coef;
     RS_TRY(nl_gather<T>(c, k, psi, ld, nb, cf));
   }
-  if (c.p.md == 6) return launch_stencil<T, 6>(c, k, s, psi, out, ld, nb, cf);
-  if (c.p.md == 4) return launch_stencil<T, 4>(c, k, s, psi, out, ld, nb, cf);
+  if (c.p.md == 6) return launch_stencil<T, 6>(c, k, s, psi, out, ld, nb, cf, nullptr, 0.0, false);
+  if (c.p.md == 4) return launch_stencil<T, 4>(c, k, s, psi, out, ld, nb, cf, nullptr, 0.0, false);
   RS_CHECK(false, RSDFT_ERR_UNSUPPORTED, "Md=%d not built in (4 and 6 are)", c.p.md);
 }
 template int hpsi_real_scratch<double>(Ctx&, int, int, const double*, double*, size_t, int, double*, size_t);

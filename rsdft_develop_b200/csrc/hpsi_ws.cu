@@ -46,6 +46,7 @@ struct WsArgs {
   T c0;
   T cx[MD], cy[MD], cz[MD];
   unsigned* status;
+  uint32_t polls;       // polls of a bounded wait before it gives up
 };
 
 struct WsItem {
@@ -68,8 +69,9 @@ __device__ __forceinline__ WsItem ws_item(const WsArgs<T, MD>& a, int w) {
 }
 
 // Bounded wait that also leaves when another thread of the CTA has given up.
-__device__ __forceinline__ bool ws_wait(uint64_t* bar, uint32_t parity, const volatile int* abort_flag) {
-  for (uint32_t it = 0; it < kWaitPolls; ++it) {
+__device__ __forceinline__ bool ws_wait(uint64_t* bar, uint32_t parity, const volatile int* abort_flag,
+                                        uint32_t polls) {
+  for (uint32_t it = 0; it < polls; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
     if ((it & 63u) == 63u) {
       if (*abort_flag) return false;
@@ -214,7 +216,7 @@ __global__ void __launch_bounds__(384, 1) k_stencil_ws(const WsArgs<T, MD> a) {
       const WsItem it = ws_item(a, w);
       const T* src = a.psi + (long long)it.band * a.ld;
       for (int q = 0; q < it.nplanes; ++q) {
-        if (round > 0 && !ws_wait(&empty[slot], (uint32_t)((round - 1) & 1), abort_flag)) {
+        if (round > 0 && !ws_wait(&empty[slot], (uint32_t)((round - 1) & 1), abort_flag, a.polls)) {
           ab = true;
           break;
         }
@@ -247,12 +249,14 @@ __global__ void __launch_bounds__(384, 1) k_stencil_ws(const WsArgs<T, MD> a) {
     if (ab) {
       *abort_flag = 1;
       atomicOr(a.status, DEV_WAIT_TIMEOUT);
-      // wait for the last copy issued into every slot before the CTA's shared memory goes away
-      for (int s = 0; s < S && s < issued; ++s) {
-        const int last = ((issued - 1 - s) / S) * S + s;
-        for (uint32_t it = 0; it < kWaitPolls; ++it)
-          if (mbar_try_wait(&full[s], (uint32_t)((last / S) & 1))) break;
-      }
+    }
+    // Before this thread exits, wait (with the full limit, whatever a.polls says) for the last
+    // copy issued into every slot: if consumers gave up, copies may still be in flight, and the
+    // CTA's shared memory must outlive them.  On the normal path they have all landed already.
+    for (int s = 0; s < S && s < issued; ++s) {
+      const int last = ((issued - 1 - s) / S) * S + s;
+      for (uint32_t it = 0; it < kWaitPolls; ++it)
+        if (mbar_try_wait(&full[s], (uint32_t)((last / S) & 1))) break;
     }
     return;
   }
@@ -309,7 +313,7 @@ __global__ void __launch_bounds__(384, 1) k_stencil_ws(const WsArgs<T, MD> a) {
         for (int j = 0; j < P; ++j) acc[q][r][j] = L::dup(T(0));
 
     for (int q = 0; q < it.nplanes; ++q) {
-      if (!ws_wait(&full[slot], (uint32_t)(round & 1), abort_flag)) {
+      if (!ws_wait(&full[slot], (uint32_t)(round & 1), abort_flag, a.polls)) {
         if (!*abort_flag) {
           *abort_flag = 1;
           atomicOr(a.status, DEV_WAIT_TIMEOUT);
@@ -512,6 +516,7 @@ int launch_stencil_ws(Ctx& c, int k, int s, const T* psi, T* out, size_t ld, int
     a.cz[m] = (T)c.p.coef_lap[2][m];
   }
   a.status = c.d_status;
+  a.polls = c.wait_polls >= 0 ? (uint32_t)c.wait_polls : kWaitPolls;
   {  // configuration, readable through rsdft_gpu_profile_get
     const std::string pre = f32 ? "stencil" : "stencil64";
     c.tune_ms[pre + "_stages"] = S;

@@ -19,11 +19,11 @@ def _rel(a, b):
     return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
 
 
-@pytest.mark.parametrize("name", ["t0", "t1", "c0", "c1", "c2"])
+@pytest.mark.parametrize("name", ["t0", "t1", "c0", "c1", "c2", "c3"])
 def test_hpsi_fp64_matches_oracle(oracle_mod, name):
     prob = synth.make_problem(name)
     o = oracle_mod.Oracle(prob)
-    nb = 5 if name != "c1" else 3
+    nb = {"c1": 3, "c3": 4}.get(name, 5)
     psi = synth.random_wavefunctions(21, nb, prob.ng)
     ref = o.hpsi(psi)
     with api.BandUpdate(prob) as g:
@@ -31,7 +31,7 @@ def test_hpsi_fp64_matches_oracle(oracle_mod, name):
     assert _rel(out, ref) < TOL64
 
 
-@pytest.mark.parametrize("name", ["t1", "c0", "c1", "c2"])
+@pytest.mark.parametrize("name", ["t1", "c0", "c1", "c2", "c3"])
 def test_hpsi_fp32_matches_oracle(oracle_mod, name):
     prob = synth.make_problem(name)
     o = oracle_mod.Oracle(prob)
