@@ -188,6 +188,9 @@ int gemm_tn2_x3(Ctx& c, const float* X, const float* Y, long long ld, int nb, lo
 int gemm_rotate_x3(Ctx& c, float* X, long long ldx, int nb, long long G, const double* V, int ldv, int terms,
                    bool add = false);
 int selftest_gemm(Ctx& c, int m, int n, long long k, int op, int terms, double* err);
+int gemm_tn_cat_x3(Ctx& c, const float* A, long long lda, int M, const float* const* B, const int* swap, int nparts,
+                   long long ldb, int np, long long K, double alpha, double* const* Cp, long long ldc, int terms);
+int gemm_rotate_cx3(Ctx& c, float* X, long long ldx, int nb, long long G, const double* Cz, int terms);
 
 // ---- util ----
 int random_wf(Ctx& c, int k, int s, uint64_t seed);

@@ -212,8 +212,144 @@ static int sd_mixed_real(Ctx& c, int k, int s, double* h_esp) {
   return 0;
 }
 
+// ---------------------------------------------------------------------------
+// mixed precision (complex16): psi stays FP32 (interleaved); the complex overlaps are real
+// split-BF16 contractions over the interleaved view, Re(conj(a) b) = x_a . x_b and
+// Im(conj(a) b) = x_a . J x_b with J (re, im) = (im, -re); the rotation by a complex matrix is
+// the real rotation of the (re, im) pairs by its 2 nb x 2 nb real form (gemm_x3.cu).  Cholesky,
+// R^-1 and the eigensolve stay FP64 (zpotrf, ztrsm, zheevd).
+// ---------------------------------------------------------------------------
+// Z(i, j) (column-major complex) = Re[i][j] + i Im[i][j] (row-major real parts)
+__global__ void k_assemble_z(const double* __restrict__ Re, const double* __restrict__ Im, int nb,
+                             cuDoubleComplex* __restrict__ Z) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)nb * nb;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % nb), j = (int)(t / nb);
+    Z[t] = make_cuDoubleComplex(Re[(long long)i * nb + j], Im[(long long)i * nb + j]);
+  }
+}
+// Z <- (Z + Z^H) / 2
+__global__ void k_hermitian_part(cuDoubleComplex* Z, int n) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)n * n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % n), j = (int)(t / n);
+    if (i < j) {
+      const cuDoubleComplex a = Z[i + (long long)j * n], b = Z[j + (long long)i * n];
+      const cuDoubleComplex m = make_cuDoubleComplex(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+      Z[i + (long long)j * n] = m;
+      Z[j + (long long)i * n] = make_cuDoubleComplex(m.x, -m.y);
+    } else if (i == j) {
+      Z[t].y = 0.0;
+    }
+  }
+}
+__global__ void k_identity_z(cuDoubleComplex* I, int n) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)n * n;
+       t += (long long)gridDim.x * blockDim.x)
+    I[t] = make_cuDoubleComplex((t % n) == (t / n) ? 1.0 : 0.0, 0.0);
+}
+
+// Complex S = dV X^H X (and, with HX, M = dV X^H (H X)) of FP32 interleaved bands, as FP64
+// column-major complex matrices.  R4 holds four nb x nb real scratch matrices.
+static int overlaps_cplx_mixed(Ctx& c, const float* X, const float* HX, int nb, double* R4, cuDoubleComplex* S,
+                               cuDoubleComplex* M) {
+  const size_t nn = (size_t)nb * nb;
+  const int nparts = HX ? 4 : 2;
+  RS_CUDA(cudaMemsetAsync(R4, 0, sizeof(double) * nn * nparts, c.stream));
+  const float* parts[4] = {X, X, HX, HX};
+  const int swap[4] = {0, 1, 0, 1};
+  double* outs[4] = {R4, R4 + nn, R4 + 2 * nn, R4 + 3 * nn};
+  const long long K = 2LL * (long long)c.ng;
+  RS_TRY(gemm_tn_cat_x3(c, X, K, nb, parts, swap, nparts, K, nb, K, c.p.dv, outs, nb, c.gemm_terms_sm));
+  k_assemble_z<<<64, 256, 0, c.stream>>>(outs[0], outs[1], nb, S);
+  c.launches++;
+  if (HX) {
+    k_assemble_z<<<64, 256, 0, c.stream>>>(outs[2], outs[3], nb, M);
+    c.launches++;
+  }
+  return check_launch("overlaps_cplx");
+}
+
+// zpotrf of S (upper) and T = R^-1 (upper triangle of S holds R afterwards)
+static int cholesky_inverse_z(Ctx& c, int nb, cuDoubleComplex* S, cuDoubleComplex* T) {
+  int lwork = 0, info = 0;
+  RS_CUSOLVER(cusolverDnZpotrf_bufferSize(c.cusolver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, &lwork));
+  RS_TRY(c.ws_solver.ensure(sizeof(cuDoubleComplex) * (size_t)std::max(lwork, 1)));
+  RS_CUSOLVER(cusolverDnZpotrf(c.cusolver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, c.ws_solver.as<cuDoubleComplex>(), lwork,
+                               c.ws_info.as<int>()));
+  RS_TRY(read_info(c, c.ws_info.as<int>(), &info));
+  RS_CHECK(info == 0, RSDFT_ERR_NOT_SPD, "overlap matrix not positive definite (zpotrf info=%d)", info);
+  k_identity_z<<<64, 256, 0, c.stream>>>(T, nb);
+  c.launches++;
+  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
+  RS_CUBLAS(cublasZtrsm(c.cublas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, nb, nb,
+                        &one, S, nb, T, nb));
+  return 0;
+}
+
+// gram_schmidt (Cholesky QR) and subspace_diag of complex FP32 bands; with both, the fused
+// Cholesky-Rayleigh-Ritz step of the sweep (one rotation X <- X R^-1 V).
+static int gssd_cplx_mixed(Ctx& c, int k, int s, bool gs, bool sd, double* h_esp) {
+  const int nb = c.kp[k].nband;
+  const size_t nn = (size_t)nb * nb;
+  float* X = c.wfn(k, s).psi.as<float>();
+  const long long ldx = 2LL * (long long)c.ng;
+  RS_TRY(c.ws_dense.ensure(sizeof(cuDoubleComplex) * 4 * nn + sizeof(double) * (4 * nn + nb)));
+  RS_TRY(c.ws_info.ensure(sizeof(int) * 4));
+  cuDoubleComplex* S = c.ws_dense.as<cuDoubleComplex>();
+  cuDoubleComplex* M = S + nn;
+  cuDoubleComplex* T = M + nn;
+  cuDoubleComplex* U = T + nn;
+  double* R4 = reinterpret_cast<double*>(U + nn);
+  double* W = R4 + 4 * nn;
+  float* HX = nullptr;
+  if (sd) {
+    RS_TRY(c.ws_hpsi.ensure(sizeof(float) * (size_t)ldx * nb));
+    HX = c.ws_hpsi.as<float>();
+    RS_TRY(hpsi_cplx<float>(c, k, s, X, HX, (size_t)ldx, nb));
+  }
+  RS_TRY(overlaps_cplx_mixed(c, X, HX, nb, R4, S, M));
+  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+  const cuDoubleComplex* C = nullptr;
+  {
+    ProfScope ps(c, "gs");
+    if (gs) RS_TRY(cholesky_inverse_z(c, nb, S, T));
+    if (sd) {
+      k_hermitian_part<<<64, 256, 0, c.stream>>>(M, nb);
+      c.launches++;
+      if (gs) {  // Hsub = T^H M T of the orthonormalised block
+        RS_CUBLAS(cublasZgemm(c.cublas, CUBLAS_OP_N, CUBLAS_OP_N, nb, nb, nb, &one, M, nb, T, nb, &zero, U, nb));
+        RS_CUBLAS(cublasZgemm(c.cublas, CUBLAS_OP_C, CUBLAS_OP_N, nb, nb, nb, &one, T, nb, U, nb, &zero, M, nb));
+        k_hermitian_part<<<64, 256, 0, c.stream>>>(M, nb);
+        c.launches++;
+      }
+    }
+  }
+  if (sd) {
+    RS_TRY(eig_solve(c, nb, M, W));
+    if (gs) {  // the single rotation R^-1 V
+      RS_CUBLAS(cublasZgemm(c.cublas, CUBLAS_OP_N, CUBLAS_OP_N, nb, nb, nb, &one, T, nb, M, nb, &zero, U, nb));
+      C = U;
+    } else {
+      C = M;
+    }
+  } else {
+    C = T;
+  }
+  RS_TRY(gemm_rotate_cx3(c, X, ldx, nb, (long long)c.ng, reinterpret_cast<const double*>(C), c.gemm_terms_rot));
+  if (h_esp && sd) {
+    RS_CUDA(cudaMemcpyAsync(h_esp, W, sizeof(double) * nb, cudaMemcpyDeviceToHost, c.stream));
+    RS_CUDA(cudaStreamSynchronize(c.stream));
+  }
+  return 0;
+}
+
 int gs_run(Ctx& c, int k, int s, int passes) {
   if (c.mixed && !c.cplx) return gs_mixed_real(c, k, s, passes);
+  if (c.mixed && c.cplx) {
+    for (int pass = 0; pass < std::max(1, passes); ++pass) RS_TRY(gssd_cplx_mixed(c, k, s, true, false, nullptr));
+    return 0;
+  }
   const int nb = c.kp[k].nband;
   const int ng = (int)c.ng;
   const size_t es = c.cplx ? sizeof(cuDoubleComplex) : sizeof(double);
@@ -260,6 +396,7 @@ int gs_run(Ctx& c, int k, int s, int passes) {
 
 int sd_run(Ctx& c, int k, int s, double* h_esp) {
   if (c.mixed && !c.cplx) return sd_mixed_real(c, k, s, h_esp);
+  if (c.mixed && c.cplx) return gssd_cplx_mixed(c, k, s, false, true, h_esp);
   const int nb = c.kp[k].nband;
   const int ng = (int)c.ng;
   const size_t es = c.cplx ? sizeof(cuDoubleComplex) : sizeof(double);
@@ -321,6 +458,7 @@ int sd_run(Ctx& c, int k, int s, double* h_esp) {
 // (H X) R^-1 and Hsub of the orthonormalised block is R^-T M R^-1; the orthonormalised block is
 // never formed, which saves one of the four ng x nb x nb contractions per sweep.
 int gssd_run(Ctx& c, int k, int s, double* h_esp, bool use_cg_hx) {
+  if (c.cplx && c.mixed) return gssd_cplx_mixed(c, k, s, true, true, h_esp);
   if (c.cplx) {
     RS_TRY(gs_run(c, k, s, 1));
     return sd_run(c, k, s, h_esp);

@@ -92,9 +92,9 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
 
 struct Out {
   int mode;        // 0: C[m][n] += alpha * D (FP64 atomics); 1: Y[n*ldy + m] = D (FP32 store);
-                   // 2: Y[n*ldy + m] += D (FP32)
-  double* C;       // columns n < nsplit (mode 0)
-  double* C2;      // columns n >= nsplit go to C2[m][n - nsplit] (mode 0)
+                   // 2: Y[n*ldy + m] += D (FP32); 3: complex interleaved store, column n = 2 j + c
+                   // of row m to Y[j*ldy + 2 m + c]
+  double* Cp[4];   // mode 0: columns [p nsplit, (p + 1) nsplit) go to Cp[p][m][n - p nsplit]
   int nsplit;
   int tri;         // mode 0: 1, the first part only by tiles reaching n <= m; 2, both parts
   long long ldc;
@@ -222,8 +222,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_x3(const __grid_constant__
           for (int j = 0; j < 32; ++j) {
             const int col = n0 + c0 + j;
             if (col < o.N) {
-              double* dst = col < o.nsplit ? o.C + (long long)row * o.ldc + col
-                                           : o.C2 + (long long)row * o.ldc + (col - o.nsplit);
+              const int part = col / o.nsplit;
+              double* dst = o.Cp[part] + (long long)row * o.ldc + (col - part * o.nsplit);
               atomicAdd(dst, o.alpha * (double)v[j]);
             }
           }
@@ -233,11 +233,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_x3(const __grid_constant__
             const int col = n0 + c0 + j;
             if (col < o.N) o.Y[(long long)col * o.ldy + row] = v[j];
           }
-        } else {
+        } else if (o.mode == 2) {
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
             const int col = n0 + c0 + j;
             if (col < o.N) o.Y[(long long)col * o.ldy + row] += v[j];
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 32; j += 2) {
+            const int col = n0 + c0 + j;  // even: (re, im) of band col / 2
+            if (col < o.N)
+              *reinterpret_cast<float2*>(o.Y + (long long)(col >> 1) * o.ldy + 2LL * row) = make_float2(v[j], v[j + 1]);
           }
         }
       }
@@ -338,6 +345,52 @@ __global__ void k_split_transpose(const float* __restrict__ X, long long ldx, in
       P[plane + o] = b;
       if (terms == 3) P[2 * plane + o] = c;
     }
+  }
+}
+
+// Complex bands (interleaved (re, im) FP32, [nb][ldx] reals): planes[t][g][2 m + c] =
+// split(X[m][2 (g0 + g) + c]) for the gc complex points of the chunk, K = 2 nb padded to kpad
+// (a 32-band x 16-point tile through shared memory per block).
+__global__ void k_split_transpose_c(const float* __restrict__ X, long long ldx, int nb, long long g0, int gc, int kpad,
+                                    __nv_bfloat16* __restrict__ P, int terms) {
+  __shared__ float tile[32][33];  // [band][real of the 16 points]
+  const int gx = blockIdx.x * 16, mx = blockIdx.y * 32;
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int m = mx + j, r = 2 * gx + threadIdx.x;  // real index within the chunk
+    tile[j][threadIdx.x] = (m < nb && r < 2 * gc) ? X[(long long)m * ldx + 2 * g0 + r] : 0.f;
+  }
+  __syncthreads();
+  const long long plane = (long long)gc * kpad;
+  // output k = 2 (mx + mm) + c for the block's 64 k values, 16 points
+  for (int j = threadIdx.y; j < 16; j += blockDim.y) {
+    const int g = gx + j;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int kk = threadIdx.x + 32 * h;  // 0..63 within the block
+      const int mm = kk >> 1, c = kk & 1;
+      const int k = 2 * mx + kk;
+      if (g < gc && k < kpad) {
+        __nv_bfloat16 a, b, cc;
+        split3((double)tile[mm][2 * j + c], a, b, cc);
+        const long long o = (long long)g * kpad + k;
+        P[o] = a;
+        P[plane + o] = b;
+        if (terms == 3) P[2 * plane + o] = cc;
+      }
+    }
+  }
+}
+
+// W (2 nb x 2 nb, column-major, FP64): the real form of the complex rotation C (nb x nb,
+// column-major interleaved) acting on (re, im) pairs: new_re_j = sum_m re_m Cr_mj - im_m Ci_mj,
+// new_im_j = sum_m re_m Ci_mj + im_m Cr_mj, with input k = 2 m + c and output n = 2 j + c'.
+__global__ void k_complex_rotation_real(const double* __restrict__ Cz, int nb, double* __restrict__ W) {
+  const long long n2 = 2LL * nb;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n2 * n2; t += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(t % n2), n = (int)(t / n2);
+    const int m = k >> 1, c = k & 1, j = n >> 1, cp = n & 1;
+    const double cr = Cz[2 * ((long long)m + (long long)j * nb)], ci = Cz[2 * ((long long)m + (long long)j * nb) + 1];
+    W[t] = cp == 0 ? (c == 0 ? cr : -ci) : (c == 0 ? ci : cr);
   }
 }
 
@@ -478,7 +531,7 @@ int gemm_tn_x3(Ctx& c, const float* A, long long lda, int M, const float* B, lon
     RS_TRY(make_map(&ta, PA, M, kpad, x3::BM, terms, M, tc.kb));
     RS_TRY(make_map(&tb, PB, N, kpad, tc.bn, terms, N, tc.kb));
     x3::Out o{};
-    o.mode = 0; o.C = C; o.C2 = C; o.nsplit = N; o.ldc = ldc; o.alpha = alpha; o.M = M; o.N = N;
+    o.mode = 0; o.Cp[0] = C; o.nsplit = N; o.ldc = ldc; o.alpha = alpha; o.M = M; o.N = N;
     RS_TRY(launch_terms(c, terms, ta, tb, M, N, kpad, o, split_ksplit(M, N, kpad, tc.bn)));
   }
   return 0;
@@ -509,7 +562,7 @@ int gemm_tn2_x3(Ctx& c, const float* X, const float* Y, long long ld, int nb, lo
     RS_TRY(make_map(&ta, P, nb, kpad, x3::BM, terms, 2LL * nb, tc.kb));
     RS_TRY(make_map(&tb, P, 2LL * nb, kpad, tc.bn, terms, 2LL * nb, tc.kb));
     x3::Out o{};
-    o.mode = 0; o.C = S; o.C2 = M; o.nsplit = nb; o.ldc = nb; o.alpha = alpha; o.M = nb; o.N = 2 * nb;
+    o.mode = 0; o.Cp[0] = S; o.Cp[1] = M; o.nsplit = nb; o.ldc = nb; o.alpha = alpha; o.M = nb; o.N = 2 * nb;
     o.tri = c.gemm_tri;  // 0, 1 (S by triangle tiles) or 2 (S and Hsub)
     RS_TRY(launch_terms(c, terms, ta, tb, nb, 2 * nb, kpad, o, split_ksplit(nb, 2 * nb, kpad, tc.bn, c.gemm_tri != 0)));
   }
@@ -546,6 +599,79 @@ int gemm_rotate_x3(Ctx& c, float* X, long long ldx, int nb, long long G, const d
     x3::Out o{};
     o.mode = add ? 2 : 1; o.Y = X + g0; o.ldy = ldx; o.M = gcur; o.N = nb;
     RS_TRY(launch_terms(c, terms, ta, tb, gcur, nb, nbpad, o, 1));
+  }
+  return 0;
+}
+
+// Cp[p][m][n] += alpha * sum_k A[m][k] B_p[n][k] for the parts p < nparts of B (np rows each,
+// read as is or, swap[p], as the complex i-rotated view), in one contraction of A against the
+// stacked parts: A is split once per K chunk.  A: [M][lda], B_p: [np][ldb] FP32 real views;
+// Cp[p]: M x np row-major (ldc).
+int gemm_tn_cat_x3(Ctx& c, const float* A, long long lda, int M, const float* const* B, const int* swap, int nparts,
+                   long long ldb, int np, long long K, double alpha, double* const* Cp, long long ldc, int terms) {
+  RS_CHECK(terms == 2 || terms == 3, RSDFT_ERR_ARG, "split terms must be 2 or 3");
+  RS_CHECK(nparts >= 1 && nparts <= 4, RSDFT_ERR_ARG, "1 to 4 operand parts");
+  const int N = nparts * np;
+  const long long kc = chunk_k(M + N, terms, K);
+  RS_TRY(c.ws_gemm.ensure(sizeof(__nv_bfloat16) * terms * (size_t)(M + N) * kc));
+  __nv_bfloat16* PA = c.ws_gemm.as<__nv_bfloat16>();
+  __nv_bfloat16* PB = PA + terms * (size_t)M * kc;
+  const double flops = 2.0 * (terms == 3 ? 6.0 : 4.0) * (double)M * N * K;
+  ProfScope ps(c, "gemm", 0.0, flops);
+  for (long long k0 = 0; k0 < K; k0 += kc) {
+    const int kcur = (int)std::min<long long>(kc, K - k0);
+    const int kpad = (kcur + 63) / 64 * 64;
+    split_rows(c, A, lda, M, k0, kcur, kpad, PA, 0, (long long)M * kpad, terms);
+    for (int p = 0; p < nparts; ++p)
+      split_rows(c, B[p], ldb, np, k0, kcur, kpad, PB + (size_t)p * np * kpad, swap[p], (long long)N * kpad, terms);
+    RS_TRY(check_launch("split_rows"));
+    CUtensorMap ta, tb;
+    const TileCfg tc = tile_for(c, terms);
+    RS_TRY(make_map(&ta, PA, M, kpad, x3::BM, terms, M, tc.kb));
+    RS_TRY(make_map(&tb, PB, N, kpad, tc.bn, terms, N, tc.kb));
+    x3::Out o{};
+    o.mode = 0;
+    for (int p = 0; p < nparts; ++p) o.Cp[p] = Cp[p];
+    o.nsplit = np; o.ldc = ldc; o.alpha = alpha; o.M = M; o.N = N;
+    RS_TRY(launch_terms(c, terms, ta, tb, M, N, kpad, o, split_ksplit(M, N, kpad, tc.bn)));
+  }
+  return 0;
+}
+
+// Complex bands X (nb bands of G complex points, interleaved FP32, leading dimension ldx reals)
+// rotated in place: X[j](g) <- sum_m X[m](g) C[m][j], C nb x nb complex column-major (ldc = nb),
+// as a real contraction over K = 2 nb: the (re, im) pairs of the nb input bands against the real
+// 2 nb x 2 nb form of C.
+int gemm_rotate_cx3(Ctx& c, float* X, long long ldx, int nb, long long G, const double* Cz, int terms) {
+  RS_CHECK(terms == 2 || terms == 3, RSDFT_ERR_ARG, "split terms must be 2 or 3");
+  const int n2 = 2 * nb;
+  const int kpad = (n2 + 63) / 64 * 64;
+  const long long gc_max = std::max<long long>(128, ((long long)(512u << 20) / (2LL * terms * kpad)) / 128 * 128);
+  const long long gc = std::min<long long>(gc_max, (G + 127) / 128 * 128);
+  RS_TRY(c.ws_gemm.ensure(sizeof(__nv_bfloat16) * terms * ((size_t)gc * kpad + (size_t)n2 * kpad)));
+  RS_TRY(c.ws_rot.ensure(sizeof(double) * (size_t)n2 * n2));
+  __nv_bfloat16* PV = c.ws_gemm.as<__nv_bfloat16>();
+  __nv_bfloat16* PX = PV + terms * (size_t)n2 * kpad;
+  const double flops = 2.0 * (terms == 3 ? 6.0 : 4.0) * (double)n2 * n2 * G;
+  ProfScope ps(c, "gemm", 0.0, flops);
+  double* Wr = c.ws_rot.as<double>();
+  x3::k_complex_rotation_real<<<4 * 148, 256, 0, c.stream>>>(Cz, nb, Wr);
+  x3::k_split_small<<<4 * 148, 256, 0, c.stream>>>(Wr, n2, n2, kpad, PV, terms);
+  c.launches += 2;
+  CUtensorMap tb;
+  const TileCfg tc = tile_for(c, terms);
+  RS_TRY(make_map(&tb, PV, n2, kpad, tc.bn, terms, n2, tc.kb));
+  for (long long g0 = 0; g0 < G; g0 += gc) {
+    const int gcur = (int)std::min<long long>(gc, G - g0);
+    dim3 tg((gcur + 15) / 16, (kpad / 2 + 31) / 32);
+    x3::k_split_transpose_c<<<tg, dim3(32, 8), 0, c.stream>>>(X, ldx, nb, g0, gcur, kpad, PX, terms);
+    c.launches++;
+    RS_TRY(check_launch("split_transpose_c"));
+    CUtensorMap ta;
+    RS_TRY(make_map(&ta, PX, gcur, kpad, x3::BM, terms, gcur, tc.kb));
+    x3::Out o{};
+    o.mode = 3; o.Y = X + 2 * g0; o.ldy = ldx; o.M = gcur; o.N = n2;
+    RS_TRY(launch_terms(c, terms, ta, tb, gcur, n2, kpad, o, 1));
   }
   return 0;
 }
