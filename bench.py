@@ -53,7 +53,7 @@ SEED = 1
 # Sweeps the plain FP64 method needs from the seeded start to max res <= 1e-8 over bands
 # 1..mb_ref (the same algorithm on CPU and GPU), measured with the library's FP64 path on a
 # B200; the reference arm multiplies its per-sweep CPU time by these.
-SWEEPS_FP64 = {"c0": 75, "c1": 43, "c2": 47, "c3": 50}
+SWEEPS_FP64 = {"c0": 75, "c1": 43, "c2": 46, "c3": 50, "c4": 45}
 
 # DRAM traffic of one hpsi stencil launch over its algorithmic bytes, from an ncu capture
 # (dram__bytes_read.sum + dram__bytes_write.sum) of the same kernel, per (config, precision).
@@ -185,8 +185,9 @@ def cpu_sweep_estimate(prob, nthreads: int, seed: int = 7):
     orc.set_threads(nthreads)
     o = orc.Oracle(prob)
     nb, ng = prob.nband, prob.ng
+    nbk = [int(x) for x in prob.nband_k]
     rng = np.random.default_rng(seed)
-    if ng * nb <= FULL_SWEEP_MAX:
+    if prob.nk == 1 and ng * nb <= FULL_SWEEP_MAX:
         from rsdft_develop_b200 import synth
         psi = o.gram_schmidt(synth.random_wavefunctions(seed, nb, ng))
         t0 = time.perf_counter()
@@ -194,8 +195,10 @@ def cpu_sweep_estimate(prob, nthreads: int, seed: int = 7):
         t = time.perf_counter() - t0
         return t, f"one whole oracle sweep (CG+GS+SD, {nb} bands)", "measured"
     ncg_b = 8
-    m = 128
+    m = min(128, nbk[0])
     psi = rng.standard_normal((m, ng))
+    if prob.is_complex:
+        psi = psi + 1j * rng.standard_normal((m, ng))
     t0 = time.perf_counter()
     q = o.gram_schmidt(psi)
     o.subspace_diag(q)
@@ -209,9 +212,10 @@ def cpu_sweep_estimate(prob, nthreads: int, seed: int = 7):
     o.hpsi(q[:ncg_b])
     t_h = (time.perf_counter() - t0) / ncg_b
     t_quad = max(0.0, t_dense - m * t_h)
-    est = nb * (t_cg + t_h) + (nb / m) ** 2 * t_quad
+    est = sum(n * (t_cg + t_h) + (n / m) ** 2 * t_quad for n in nbk)
+    kdesc = f" per k-point, summed over {prob.nk} k-points with {nbk} bands" if prob.nk > 1 else ""
     desc = (f"extrapolated: oracle CG on {ncg_b} bands ({t_cg:.3f} s per band) and H psi ({t_h:.4f} s per band) "
-            f"x {nb} bands + oracle GS+SD products on {m} bands ({t_quad:.2f} s) x ({nb}/{m})^2")
+            f"x the bands + oracle GS+SD products on {m} bands ({t_quad:.2f} s) x (bands/{m})^2{kdesc}")
     return est, desc, "extrapolated"
 
 
@@ -258,18 +262,20 @@ def gap_index(esp: np.ndarray, lo: int, hi: int) -> int:
 
 def principal_angle_max(a_host, b_host, m: int, dv: float) -> float:
     """Largest principal angle (rad) between span(a[:m]) and span(b[:m]) in the dV inner
-    product; a, b are host tensors (nb, ng) of FP64 bands.  Evaluated on the GPU in FP64."""
+    product; a, b are host tensors (nb, ng) of FP64 (or complex128) bands.  Evaluated on the GPU
+    in FP64."""
     import torch
     A = a_host[:m].cuda()
     B = b_host[:m].cuda()
-    ga = (A @ A.T) * dv
-    gb = (B @ B.T) * dv
-    M = (A @ B.T) * dv
+    ga = (A.conj() @ A.T) * dv
+    gb = (B.conj() @ B.T) * dv
+    M = (A.conj() @ B.T) * dv
     del A, B
     la = torch.linalg.cholesky(ga)
     lb = torch.linalg.cholesky(gb)
+    # singular values of La^-1 M Lb^-H: the cosines of the principal angles
     X = torch.linalg.solve_triangular(la, M, upper=False)
-    X = torch.linalg.solve_triangular(lb, X.T, upper=False).T
+    X = torch.linalg.solve_triangular(lb.conj(), X.T, upper=False).T
     s = torch.linalg.svdvals(X)
     smin = float(s.min().clamp(max=1.0))
     # sin(theta) = sqrt(1 - s^2), accurate for small angles
@@ -294,19 +300,26 @@ def run_ours(args, dist, rank, ws):
     terms = tuple(int(t) for t in args.gemm_terms.split(","))
     compare_arms = [a for a in args.compare.split(",") if a and a != "none"]
 
-    # the common input: seeded FP64 wavefunctions in pinned host memory, made by the library's
-    # device generator (bit-identical to synth.random_wavefunctions)
-    pin_in = torch.empty((nb, ng), dtype=torch.float64, pin_memory=True)
-    pin_out = torch.empty((nb, ng), dtype=torch.float64, pin_memory=True)
+    # the common input: seeded FP64 (complex128 for k-points) wavefunctions in pinned host memory,
+    # made by the library's device generator (bit-identical to synth.random_wavefunctions)
+    nk = prob.nk
+    nbk = [int(x) for x in prob.nband_k]
+    dt = torch.complex128 if prob.is_complex else torch.float64
+    pin_in = [torch.empty((nbk[k], ng), dtype=dt, pin_memory=True) for k in range(nk)]
+    pin_out = [torch.empty((nbk[k], ng), dtype=dt, pin_memory=True) for k in range(nk)]
     with api.BandUpdate(prob, precision=api.PREC_FP64) as g0:
-        g0.random_wf(SEED)
-        g0.get_wf_host(pin_in.data_ptr(), nb)
+        for k in range(nk):
+            g0.random_wf(SEED, k=k + 1)
+            g0.get_wf_host(pin_in[k].data_ptr(), nbk[k], k=k + 1)
+    # convergence band set: bands 1..mb_ref (one k-point), or per k-point the same 7/8 rule
+    sweep_ref = mb_ref if nk == 1 else -1
+    conv = [min(mb_ref, nb_) if nk == 1 else nb_ - nb_ // 8 for nb_ in nbk]
 
     g = api.BandUpdate(prob, precision=prec, pc_mode=pc_mode)
     g.gemm_terms(*terms)
     if pc == "learned":
         g.lpc_set_weights(np.load(wpath))
-    g.init_sweep(mb_ref)
+    g.init_sweep(sweep_ref)
     stream = torch.cuda.ExternalStream(g.stream())
 
     def step():
@@ -314,12 +327,15 @@ def run_ours(args, dist, rank, ws):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         ev[0].record(stream)
-        g.set_wf_host(pin_in.data_ptr(), nb)
+        for k in range(nk):
+            g.set_wf_host(pin_in[k].data_ptr(), nbk[k], k=k + 1)
         ev[1].record(stream)
-        g.gram_schmidt()
+        for k in range(nk):
+            g.gram_schmidt(k=k + 1)
         it, esp, res = g.calc_sweep(MAX_SWEEPS, tol=TOL)
         ev[2].record(stream)
-        g.get_wf_host(pin_out.data_ptr(), nb)
+        for k in range(nk):
+            g.get_wf_host(pin_out[k].data_ptr(), nbk[k], k=k + 1)
         ev[3].record(stream)
         ev[3].synchronize()
         wall = time.perf_counter() - t0
@@ -344,25 +360,25 @@ def run_ours(args, dist, rank, ws):
     launches = g.kernel_launches() - launches0
     st_ms, st_n, st_bytes, _ = g.profile_get("hpsi_stencil")
     g.profile(0)
-    tune = {k: g.profile_get(k)[0] for k in ("stencil_tile_y", "stencil_warps", "stencil_stages", "stencil_zchunks")}
+    tune = {k_: g.profile_get(k_)[0] for k_ in ("stencil_tile_y", "stencil_warps", "stencil_stages", "stencil_zchunks")}
     lpc_state = g.lpc_status()
     shares = {}
     if args.shares:  # one extra, untimed solve with every kernel family timed
         g.profile(1)
         step()
-        names = ["hpsi_stencil", "nl_gather", "nl_scatter", "cg", "pc", "lpc", "gs", "gemm", "sd_gemm", "sd_eig",
-                 "sd_rot", "residual"]
+        names = ["hpsi_stencil", "nl_gather", "nl_scatter", "cg", "pc", "lpc", "gs", "gemm", "sd_gemm",
+                 "sd_eig", "sd_rot", "residual"]
         shares = {n: round(g.profile_get(n)[0], 3) for n in names}
         g.profile(0)
     clocks = clk.summary()
-    esp_main = esp[0, 0].copy()
-    res_max = float(np.max(res[..., :mb_ref]))
+    esp_main = [esp[0, k, :nbk[k]].copy() for k in range(nk)]
+    res_max = float(max(np.max(res[0, k, :conv[k]]) for k in range(nk)))
     g.close()
     t_solve = _max_over_ranks(dist, statistics.mean(solve_s))
     e2e_val = _max_over_ranks(dist, statistics.mean(wall_s))
 
     # comparison solves on the same GPU and input (after the timed steps; the FP64 result
-    # overwrites the input buffer, which is no longer needed)
+    # overwrites the input buffers, which are no longer needed)
     compare, errors = {}, None
     arms = []
     if "mixed_learned" in compare_arms and os.path.exists(wpath) and not (prec == api.PREC_MIXED and pc == "learned"):
@@ -375,40 +391,51 @@ def run_ours(args, dist, rank, ws):
         with api.BandUpdate(prob, precision=pr, pc_mode=pm) as h:
             if pm == api.PC_LEARNED:
                 h.lpc_set_weights(np.load(wpath))
-            h.init_sweep(mb_ref)
+            h.init_sweep(sweep_ref)
             hs = torch.cuda.ExternalStream(h.stream())
-            h.set_wf_host(pin_in.data_ptr(), nb)
+            for k in range(nk):
+                h.set_wf_host(pin_in[k].data_ptr(), nbk[k], k=k + 1)
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(hs)
-            h.gram_schmidt()
+            for k in range(nk):
+                h.gram_schmidt(k=k + 1)
             itc, espc, resc = h.calc_sweep(MAX_SWEEPS, tol=TOL)
             e1.record(hs)
             e1.synchronize()
             tc = _max_over_ranks(dist, e0.elapsed_time(e1) / 1000.0)
-            entry = {"s": round(tc, 4), "sweeps": itc, "final_res_max": float(np.max(resc[..., :mb_ref]))}
+            entry = {"s": round(tc, 4), "sweeps": itc,
+                     "final_res_max": float(max(np.max(resc[0, k, :conv[k]]) for k in range(nk)))}
             if pm == api.PC_LEARNED:
                 entry["lpc_fallbacks"] = h.lpc_status()[2]
             if name == "fp64_hprsdft":
-                h.get_wf_host(pin_in.data_ptr(), nb)
-                esp64 = espc[0, 0].copy()
+                for k in range(nk):
+                    h.get_wf_host(pin_in[k].data_ptr(), nbk[k], k=k + 1)
+                esp64 = [espc[0, k, :nbk[k]].copy() for k in range(nk)]
         compare[name] = entry
         if name == "fp64_hprsdft":
             compare["speedup_vs_fp64_hprsdft"] = round(tc / t_solve, 3)
-            m = gap_index(esp64, max(1, mb_ref - 32), mb_ref)
-            ang = principal_angle_max(pin_out, pin_in, m, prob.dV)
-            errors = {"vs": "fp64_hprsdft solve of the same input",
-                      "eig_err_max_Ha": float(np.max(np.abs(esp_main[:mb_ref] - esp64[:mb_ref]))),
-                      "principal_angle_max_rad": ang, "subspace_bands": m,
-                      "gap_Ha": float(esp64[m] - esp64[m - 1])}
+            eig_err, ang, ms, gaps = 0.0, 0.0, [], []
+            for k in range(nk):
+                ck = conv[k]
+                eig_err = max(eig_err, float(np.max(np.abs(esp_main[k][:ck] - esp64[k][:ck]))))
+                m = gap_index(esp64[k], max(1, ck - 32), min(ck, nbk[k] - 1))
+                ang = max(ang, principal_angle_max(pin_out[k], pin_in[k], m, prob.dV))
+                ms.append(m)
+                gaps.append(float(esp64[k][m] - esp64[k][m - 1]))
+            errors = {"vs": "fp64_hprsdft solve of the same input", "eig_err_max_Ha": eig_err,
+                      "principal_angle_max_rad": ang, "subspace_bands": ms if nk > 1 else ms[0],
+                      "gap_Ha": gaps if nk > 1 else gaps[0]}
 
     hbm, bf16, peak_kind = _peaks()
     avg_ms = (st_ms / st_n) if st_n else None
     bytes_launch = (st_bytes / st_n) if st_n else None
     achieved = bytes_launch / (avg_ms * 1e-3) / 1e9 if st_n else 0.0
     ratio = NCU_TRAFFIC_RATIO.get((args.config, args.precision))
-    kname = "k_stencil_ws<float>" if prec == api.PREC_MIXED else "k_stencil_ws<double>"
-    roof = {"bound": "hbm", "kernel": f"{kname}: hpsi 37-point stencil + V_loc (nonlocal scatter separate)",
+    kname = ("k_stencil_ws_c" if prob.is_complex else "k_stencil_ws") + ("<float>" if prec == api.PREC_MIXED else "<double>")
+    kdesc = ("hpsi 37-point Bloch-phase stencil + V_loc (nonlocal scatter separate)" if prob.is_complex
+             else "hpsi 37-point stencil + V_loc (nonlocal scatter separate)")
+    roof = {"bound": "hbm", "kernel": f"{kname}: {kdesc}",
             "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
             "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
             "traffic": (ratio * bytes_launch) if (ratio and bytes_launch) else None,
@@ -431,11 +458,13 @@ def run_ours(args, dist, rank, ws):
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f32+bf16x%d/x%d+f64" % terms,
             "data": "synthetic (seeded Gaussian V_loc, Gaussian s/p projectors, seeded psi0)",
-            "config": {"workload": args.config, "grid": list(prob.n), "bands": nb, "atoms": prob.cfg.natom,
+            "config": {"workload": args.config, "grid": list(prob.n), "bands": nbk if nk > 1 else nb,
+                       "kpoints": nk, "storage": "complex128" if prob.is_complex else "real8", "atoms": prob.cfg.natom,
                        "projectors": prob.nzlma, "precision": args.precision, "pc": pc,
                        "lpc_fallbacks": lpc_state[2] if pc == "learned" else None,
                        "gemm_terms": list(terms) if prec == api.PREC_MIXED else None,
-                       "mb_ref": mb_ref, "tol": TOL, "sweeps_to_tol": iters, "final_res_max": res_max,
+                       "mb_ref": conv if nk > 1 else mb_ref, "tol": TOL, "sweeps_to_tol": iters,
+                       "final_res_max": res_max,
                        "l2": "inputs larger than L2 (psi >= 0.5 GB)", "parallelism": f"replicas x{ws}"},
             "gpu_launches": int(launches),
             "roofline": roof,
@@ -443,8 +472,8 @@ def run_ours(args, dist, rank, ws):
             "compare": compare,
             "time_shares_ms": shares or None,
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_val, "unit": "s", "h2d_bytes_per_step": int(nb * ng * 8),
-                    "d2h_bytes_per_step": int(nb * ng * 8 + 2 * esp.nbytes)},
+            "e2e": {"value": e2e_val, "unit": "s", "h2d_bytes_per_step": int(sum(p.nbytes for p in pin_in)),
+                    "d2h_bytes_per_step": int(sum(p.nbytes for p in pin_out) + 2 * esp.nbytes)},
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
@@ -478,7 +507,9 @@ def run_kernel(args):
     if what == "hpsi":
         precs = {"both": ("fp64", "fp32"), "fp64": ("fp64",), "fp32": ("fp32",)}[args.hpsi_prec]
         with api.BandUpdate(prob, nonlocal_on=not args.no_nonlocal) as g:
-            x = torch.empty((nb, prob.ng), dtype=torch.float64, device="cuda")
+            # complex bands are interleaved (re, im): 2 ng reals each
+            ncomp = 2 if prob.is_complex else 1
+            x = torch.empty((nb, ncomp * prob.ng), dtype=torch.float64, device="cuda")
             x.uniform_(-1.0, 1.0)
             for name in precs:
                 f32 = name == "fp32"

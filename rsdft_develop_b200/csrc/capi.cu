@@ -677,10 +677,22 @@ int rsdft_gpu_set_precision(int precision) {
 
 int rsdft_gpu_init_sweep(int mb_ref) {
   REQUIRE_CTX();
-  RS_CHECK(mb_ref >= 0, RSDFT_ERR_ARG, "mb_ref must be >= 0");
+  RS_CHECK(mb_ref >= -1, RSDFT_ERR_ARG, "mb_ref must be >= -1");
   g_ctx->mb_ref = mb_ref;
   return 0;
 }
+
+}  // extern "C"
+
+// Bands 1..n of k-point k checked for convergence by rsdft_gpu_sweep
+static int conv_bands(const Ctx& c, int k) {
+  const int nb = c.kp[k].nband;
+  if (c.mb_ref > 0) return std::min(c.mb_ref, nb);
+  if (c.mb_ref < 0) return nb - nb / 8;
+  return nb;
+}
+
+extern "C" {
 
 int rsdft_gpu_sweep(int nsweep, double tol, int* iters, double* esp, double* res) {
   REQUIRE_CTX();
@@ -700,7 +712,7 @@ int rsdft_gpu_sweep(int nsweep, double tol, int* iters, double* esp, double* res
       for (int k = 0; k < c.p.nk; ++k) {
         RS_CHECK(c.wfn(k, s).valid, RSDFT_ERR_STATE, "no wavefunctions resident for (k,s)=(%d,%d)", k + 1, s + 1);
         RS_TRY(cg_run(c, k, s, nullptr, cg_res.data()));
-        const int nconv = c.mb_ref > 0 ? std::min(c.mb_ref, c.kp[k].nband) : c.kp[k].nband;
+        const int nconv = conv_bands(c, k);
         for (int n = 0; n < nconv; ++n) cg_rmax = std::max(cg_rmax, cg_res[n]);
         RS_TRY(gssd_run(c, k, s, nullptr, true));
       }
@@ -714,7 +726,7 @@ int rsdft_gpu_sweep(int nsweep, double tol, int* iters, double* esp, double* res
         for (int k = 0; k < c.p.nk; ++k) {
           const int nb = c.kp[k].nband;
           RS_TRY(rsdft_gpu_residual(k + 1, s + 1, e.data(), r.data()));
-          const int nconv = c.mb_ref > 0 ? std::min(c.mb_ref, nb) : nb;
+          const int nconv = conv_bands(c, k);
           for (int n = 0; n < nconv; ++n) rmax = std::max(rmax, r[n]);
           const size_t off = ((size_t)s * c.p.nk + k) * nbmax;
           if (esp) std::memcpy(esp + off, e.data(), sizeof(double) * nb);

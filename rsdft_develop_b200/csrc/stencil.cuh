@@ -168,6 +168,9 @@ int launch_stencil_stream(Ctx& c, int k, int s, const T* psi, T* out, size_t ld,
 template <typename T, int MD>
 int launch_stencil_ws(Ctx& c, int k, int s, const T* psi, T* out, size_t ld, int nb, const T* vloc_override,
                       double c0_shift);
+// complex-build form (interleaved (re, im) bands, Bloch-phase zcoef taps); nonlocal afterwards
+template <typename T, int MD>
+int launch_stencil_ws_c(Ctx& c, int k, int s, const T* psi, T* out, size_t ld, int nb);
 // largest record segment of one (plane, y-tile) for y-tiles of tile_y rows (cached per tile_y)
 int record_segment_max(Ctx& c, int tile_y);
 
