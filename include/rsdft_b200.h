@@ -154,6 +154,13 @@ int rsdft_gpu_precond_d(int k, const double* gk, double* pgk, int ld, int nb, in
 int rsdft_gpu_precond_f(int k, const float* gk, float* pgk, int ld, int nb, int mem);
 /* FP32 precond_hprsdft form: 1 (default) s-step, 0 the recurrence form of the FP64 path. */
 int rsdft_gpu_set_pc_form(int sstep);
+/* Orthogonalisation of the preconditioned gradient inside conjugate_gradient, the reference's
+ * SWGS keyword (src/conjugate_gradient/cg_module.f90:47, cggs at :249-251 and :576-578):
+ * 0 off (the default), 1 cggs_1 (against the bands below, src/conjugate_gradient/
+ * cggs_module.f90:36-76), 2 cggs_2 (against all other bands, :79-121).  Bands of earlier CG
+ * blocks (cg_block) count with their updated values, bands of the same block with their values
+ * at the same CG step, as with the reference's MB_d blocks. */
+int rsdft_gpu_set_cggs(int iswitch);
 
 /* calc_sweep: up to nsweep iterations of CG -> GS -> SD over all (k, s); stops early when the
  * FP64 residual max over bands <= tol (tol <= 0: never).  The FP64 residual is evaluated in
@@ -169,7 +176,8 @@ int rsdft_gpu_sweep(int nsweep, double tol, int* iters, double* esp, double* res
 int rsdft_gpu_set_precision(int precision);
 /* Convergence band set of rsdft_gpu_sweep: bands 1..mb_ref are checked (0: all bands), as the
  * reference's init_sweep(iconv_check, mb_ref, tol) does for its band and DOS drivers
- * (src/sweep_module.f90:46-60,267-278; src/band_module.f90:207; src/dos_module.f90:64-75). */
+ * (src/sweep_module.f90:46-60,267-278; src/band_module.f90:207; src/dos_module.f90:64-75).
+ * mb_ref = -1: per k-point, bands 1..nband_k - nband_k/8 (k-points with uneven band counts). */
 int rsdft_gpu_init_sweep(int mb_ref);
 
 /* ---- learned preconditioner (no counterpart in the reference) ----

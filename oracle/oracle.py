@@ -36,6 +36,7 @@ class OrcProb(C.Structure):
         ("pairs", C.POINTER(C.c_int)), ("dij", C.POINTER(C.c_double)),
         ("ncg", C.c_int), ("mloop", C.c_int),
         ("is_complex", C.c_int),
+        ("cggs", C.c_int),
     ]
 
 
@@ -78,7 +79,7 @@ def set_threads(n: int) -> None:
 class Oracle:
     """Oracle bound to one k-point of a :class:`rsdft_develop_b200.synth.Problem`."""
 
-    def __init__(self, prob, k: int = 0, ncg: int = 3, mloop: int = 3, nonlocal_on: bool = True):
+    def __init__(self, prob, k: int = 0, ncg: int = 3, mloop: int = 3, nonlocal_on: bool = True, cggs: int = 0):
         self.prob = prob
         self.k = k
         p = OrcProb()
@@ -119,6 +120,7 @@ class Oracle:
         p.ncg = ncg
         p.mloop = mloop
         p.is_complex = 1 if prob.is_complex else 0
+        p.cggs = int(cggs)
         self.p = p
         self.dtype = np.complex128 if prob.is_complex else np.float64
         self.sfx = "z" if prob.is_complex else "d"

@@ -80,6 +80,7 @@ struct OrcProb {
   const double* dij;               // [npair]
   int ncg, mloop;
   int is_complex;
+  int cggs;                        // SWGS: 0 off, 1 cggs_1, 2 cggs_2 (bands then run in order)
 };
 
 static inline double conj_(double x) { return x; }
@@ -241,10 +242,33 @@ static int sygv2(cplx A[4], cplx B[4], double W[2]) {
   return info;
 }
 
-// One band of d/z_conjugate_gradient_1 with MB_d = 1.
+// cggs_1 / cggs_2 (src/conjugate_gradient/cggs_module.f90:36-121) on the preconditioned
+// gradient g of band b: xg(m) = dV sum_i conj(x(i,m)) g(i) for m < b (cggs_1) or m != b
+// (cggs_2), then g(i) -= sum_m x(i,m) xg(m).
 template <typename T>
-static void cg_band(const OrcProb* P, T* unk, double* esp, double* res) {
+static void cggs_band(const OrcProb* P, const T* unk_all, int b, int nb, T* g) {
   const size_t ng = (size_t)P->n1 * P->n2 * P->n3;
+  const int range = P->cggs == 1 ? b : nb;
+  std::vector<T> xg(std::max(range, 1), T(0));
+  for (int m = 0; m < range; ++m) {
+    if (m == b) continue;
+    const T* x = unk_all + (size_t)m * ng;
+    T s = T(0);
+    for (size_t i = 0; i < ng; ++i) s += conj_(x[i]) * g[i];
+    xg[m] = s * P->dV;
+  }
+  for (int m = 0; m < range; ++m) {
+    if (m == b) continue;
+    const T* x = unk_all + (size_t)m * ng;
+    for (size_t i = 0; i < ng; ++i) g[i] -= x[i] * xg[m];
+  }
+}
+
+// One band of d/z_conjugate_gradient_1 with MB_d = 1 (unk_all: every band, this one is b).
+template <typename T>
+static void cg_band(const OrcProb* P, T* unk_all, int b, int nb, double* esp, double* res) {
+  const size_t ng = (size_t)P->n1 * P->n2 * P->n3;
+  T* unk = unk_all + (size_t)b * ng;
   const double dV = P->dV;
   const bool cpx = P->is_complex;
   const double gfac = cpx ? -1.0 : -2.0;   // g = -2(Hx - Ex) real, -(Hx - Ex) complex
@@ -267,6 +291,7 @@ static void cg_band(const OrcProb* P, T* unk, double* esp, double* res) {
     if (std::fabs(E - E1) < 1.0e-15) break;
     if (icg == P->ncg + 1) break;
     precond_band(P, gk.data(), Pgk.data());
+    if (P->cggs) cggs_band(P, unk_all, b, nb, Pgk.data());
     s = 0;
     for (size_t i = 0; i < ng; ++i) s += re_(conj_(Pgk[i]) * gk[i]);
     rb = s * dV;
@@ -321,9 +346,12 @@ static void cg_band(const OrcProb* P, T* unk, double* esp, double* res) {
 
 template <typename T>
 static void cg_all(const OrcProb* P, T* unk, int nb, double* esp, double* res) {
-  const size_t ng = (size_t)P->n1 * P->n2 * P->n3;
+  if (P->cggs) {  // band n sees the updated bands below it: in order, as the reference's band loop
+    for (int b = 0; b < nb; ++b) cg_band(P, unk, b, nb, esp + b, res + b);
+    return;
+  }
 #pragma omp parallel for schedule(dynamic)
-  for (int b = 0; b < nb; ++b) cg_band(P, unk + b * ng, esp + b, res + b);
+  for (int b = 0; b < nb; ++b) cg_band(P, unk, b, nb, esp + b, res + b);
 }
 
 // ---------------------------------------------------------------------------

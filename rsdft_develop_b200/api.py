@@ -51,7 +51,7 @@ EXPORTS = [
     "rsdft_gpu_hamiltonian_z", "rsdft_gpu_hamiltonian_f", "rsdft_gpu_hamiltonian_c",
     "rsdft_gpu_conjugate_gradient", "rsdft_gpu_gram_schmidt", "rsdft_gpu_subspace_diag",
     "rsdft_gpu_residual", "rsdft_gpu_precond_d", "rsdft_gpu_precond_f", "rsdft_gpu_set_pc_form", "rsdft_gpu_sweep", "rsdft_gpu_profile",
-    "rsdft_gpu_profile_get", "rsdft_gpu_kernel_launches", "rsdft_gpu_selftest_gemm", "rsdft_gpu_set_gemm_terms", "rsdft_gpu_set_gemm_tile", "rsdft_gpu_set_nl_form", "rsdft_gpu_init_sweep", "rsdft_gpu_set_wait_polls", "rsdft_gpu_set_precision",
+    "rsdft_gpu_profile_get", "rsdft_gpu_kernel_launches", "rsdft_gpu_selftest_gemm", "rsdft_gpu_set_gemm_terms", "rsdft_gpu_set_gemm_tile", "rsdft_gpu_set_nl_form", "rsdft_gpu_init_sweep", "rsdft_gpu_set_wait_polls", "rsdft_gpu_set_precision", "rsdft_gpu_set_cggs",
     "rsdft_gpu_hamiltonian_noalloc_d",
     "rsdft_gpu_lpc_init", "rsdft_gpu_lpc_set_weights", "rsdft_gpu_lpc_get_weights", "rsdft_gpu_lpc_forward",
     "rsdft_gpu_lpc_loss_grad", "rsdft_gpu_lpc_dataset", "rsdft_gpu_lpc_harvest", "rsdft_gpu_lpc_dataset_get",
@@ -111,7 +111,7 @@ def load_library(path: str = LIB_PATH):
         "rsdft_gpu_sweep": [i, d, C.POINTER(C.c_int), vp, vp],
         "rsdft_gpu_selftest_gemm": [i, i, C.c_longlong, i, C.POINTER(C.c_double)],
         "rsdft_gpu_set_gemm_terms": [i, i], "rsdft_gpu_set_gemm_tile": [i], "rsdft_gpu_set_nl_form": [i],
-        "rsdft_gpu_set_wait_polls": [i], "rsdft_gpu_set_precision": [i],
+        "rsdft_gpu_set_wait_polls": [i], "rsdft_gpu_set_precision": [i], "rsdft_gpu_set_cggs": [i],
         "rsdft_gpu_init_sweep": [i],
         "rsdft_gpu_hamiltonian_noalloc_d": [i, i, vp, vp, i, i],
         "rsdft_gpu_lpc_init": [C.c_ulonglong], "rsdft_gpu_lpc_set_weights": [vp, i],
@@ -461,6 +461,11 @@ class BandUpdate:
     def nl_form(self, fused: bool) -> None:
         """Nonlocal term of the real hpsi: inside the stencil (fused) or by a scatter after it."""
         _call(self.lib.rsdft_gpu_set_nl_form, 1 if fused else 0)
+
+    def cggs(self, iswitch: int) -> None:
+        """SWGS: orthogonalise CG's preconditioned gradients against the lower bands (1) or all
+        other bands (2), or not at all (0, the default)."""
+        _call(self.lib.rsdft_gpu_set_cggs, int(iswitch))
 
     def wait_polls(self, polls: int) -> None:
         """Polls of the hpsi stencil's bounded waits (0: give up at once; < 0: the default)."""

@@ -812,6 +812,13 @@ int rsdft_gpu_set_nl_form(int fused) {
   return 0;
 }
 
+int rsdft_gpu_set_cggs(int iswitch) {
+  REQUIRE_CTX();
+  RS_CHECK(iswitch >= 0 && iswitch <= 2, RSDFT_ERR_ARG, "cggs switch must be 0, 1 or 2");
+  g_ctx->cggs = iswitch;
+  return 0;
+}
+
 int rsdft_gpu_set_wait_polls(int polls) {
   REQUIRE_CTX();
   g_ctx->wait_polls = polls < 0 ? -1 : polls;

@@ -863,6 +863,83 @@ int precond_real(Ctx& c, const T* g, T* pg, size_t ld, int nb) {
 template int precond_real<double>(Ctx&, const double*, double*, size_t, int);
 template int precond_real<float>(Ctx&, const float*, float*, size_t, int);
 
+// ---------------------------------------------------------------------------
+// cggs (src/conjugate_gradient/cggs_module.f90:14-124, called after the preconditioner at
+// src/conjugate_gradient/cg_module.f90:249-251 and :576-578): the preconditioned gradient of band
+// n loses its components along the current bands m (m < n: iswitch 1, cggs_1; m != n:
+// iswitch 2, cggs_2), classical Gram-Schmidt: all projections dV <x_m|Pg_n> first, then
+// Pg_n -= sum_m x_m <x_m|Pg_n> dV.  Bands of earlier CG blocks hold their final values, bands of
+// the current block their values at this CG step (the reference's MB_d block semantics).
+// The two products are plain library GEMMs (cuBLAS, in the storage precision).
+// ---------------------------------------------------------------------------
+// C (range x nn, column-major, NC reals per element): keep entry (m, j) where band m may be
+// projected out of band b0 + j, negated; zero elsewhere
+template <typename T, int NC>
+__global__ void k_cggs_mask(T* C, int range, int nn, int b0, int iswitch) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)range * nn;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int m = (int)(t % range), j = (int)(t / range), n = b0 + j;
+    const bool keep = iswitch == 1 ? m < n : m != n;
+#pragma unroll
+    for (int q = 0; q < NC; ++q) C[t * NC + q] = keep ? -C[t * NC + q] : T(0);
+  }
+}
+
+#define RS_CUBLAS_CG(call)                                                        \
+  do {                                                                            \
+    cublasStatus_t st_ = (call);                                                  \
+    RS_CHECK(st_ == CUBLAS_STATUS_SUCCESS, RSDFT_ERR_CUDA, "%s -> cuBLAS status %d", #call, (int)st_); \
+  } while (0)
+
+template <typename T, int NC>
+static int cggs_block(Ctx& c, const T* psi, int nb, int b0, int nn, T* PG) {
+  const int range = c.cggs == 1 ? b0 + nn : nb;
+  if (range <= 0 || nn <= 0) return 0;
+  const int ng = (int)c.ng;
+  RS_TRY(c.ws_dense.ensure(sizeof(T) * NC * (size_t)range * nn));
+  T* C = c.ws_dense.as<T>();
+  ProfScope ps(c, "cg");
+  if (NC == 1 && std::is_same<T, double>::value) {
+    const double dV = c.p.dv, zero = 0.0, one = 1.0;
+    const double* X = reinterpret_cast<const double*>(psi);
+    double* Pd = reinterpret_cast<double*>(PG);
+    double* Cd = reinterpret_cast<double*>(C);
+    RS_CUBLAS_CG(cublasDgemm(c.cublas, CUBLAS_OP_T, CUBLAS_OP_N, range, nn, ng, &dV, X, ng, Pd, ng, &zero, Cd, range));
+    k_cggs_mask<double, 1><<<64, 256, 0, c.stream>>>(Cd, range, nn, b0, c.cggs);
+    c.launches++;
+    RS_CUBLAS_CG(cublasDgemm(c.cublas, CUBLAS_OP_N, CUBLAS_OP_N, ng, nn, range, &one, X, ng, Cd, range, &one, Pd, ng));
+  } else if (NC == 1) {
+    const float dV = (float)c.p.dv, zero = 0.f, one = 1.f;
+    const float* X = reinterpret_cast<const float*>(psi);
+    float* Pf = reinterpret_cast<float*>(PG);
+    float* Cf = reinterpret_cast<float*>(C);
+    RS_CUBLAS_CG(cublasSgemm(c.cublas, CUBLAS_OP_T, CUBLAS_OP_N, range, nn, ng, &dV, X, ng, Pf, ng, &zero, Cf, range));
+    k_cggs_mask<float, 1><<<64, 256, 0, c.stream>>>(Cf, range, nn, b0, c.cggs);
+    c.launches++;
+    RS_CUBLAS_CG(cublasSgemm(c.cublas, CUBLAS_OP_N, CUBLAS_OP_N, ng, nn, range, &one, X, ng, Cf, range, &one, Pf, ng));
+  } else if (std::is_same<T, double>::value) {
+    const cuDoubleComplex dV = make_cuDoubleComplex(c.p.dv, 0.0), zero = make_cuDoubleComplex(0.0, 0.0),
+                          one = make_cuDoubleComplex(1.0, 0.0);
+    const cuDoubleComplex* X = reinterpret_cast<const cuDoubleComplex*>(psi);
+    cuDoubleComplex* Pz = reinterpret_cast<cuDoubleComplex*>(PG);
+    cuDoubleComplex* Cz = reinterpret_cast<cuDoubleComplex*>(C);
+    RS_CUBLAS_CG(cublasZgemm(c.cublas, CUBLAS_OP_C, CUBLAS_OP_N, range, nn, ng, &dV, X, ng, Pz, ng, &zero, Cz, range));
+    k_cggs_mask<double, 2><<<64, 256, 0, c.stream>>>(reinterpret_cast<double*>(C), range, nn, b0, c.cggs);
+    c.launches++;
+    RS_CUBLAS_CG(cublasZgemm(c.cublas, CUBLAS_OP_N, CUBLAS_OP_N, ng, nn, range, &one, X, ng, Cz, range, &one, Pz, ng));
+  } else {
+    const cuComplex dV = make_cuComplex((float)c.p.dv, 0.f), zero = make_cuComplex(0.f, 0.f), one = make_cuComplex(1.f, 0.f);
+    const cuComplex* X = reinterpret_cast<const cuComplex*>(psi);
+    cuComplex* Pc = reinterpret_cast<cuComplex*>(PG);
+    cuComplex* Cc = reinterpret_cast<cuComplex*>(C);
+    RS_CUBLAS_CG(cublasCgemm(c.cublas, CUBLAS_OP_C, CUBLAS_OP_N, range, nn, ng, &dV, X, ng, Pc, ng, &zero, Cc, range));
+    k_cggs_mask<float, 2><<<64, 256, 0, c.stream>>>(reinterpret_cast<float*>(C), range, nn, b0, c.cggs);
+    c.launches++;
+    RS_CUBLAS_CG(cublasCgemm(c.cublas, CUBLAS_OP_N, CUBLAS_OP_N, ng, nn, range, &one, X, ng, Cc, range, &one, Pc, ng));
+  }
+  return check_launch("cggs");
+}
+
 template <typename T>
 static int hpsi_any(Ctx& c, int kk, int s, const T* x, T* hx, size_t ld, int nb) {
   if (c.cplx) return hpsi_cplx<T>(c, kk, s, x, hx, ld, nb);
@@ -949,6 +1026,12 @@ static int cg_block_run(Ctx& c, int kk, int s, double* h_esp, double* h_res) {
         RS_TRY(lpc_apply(c, reinterpret_cast<const float*>(G), reinterpret_cast<float*>(PG), nn));
       } else {
         RS_TRY(pc_block<T>(c, k, G, PG, R, Q, Q2, F, &pg_dot));
+      }
+      if (c.cggs) {
+        // inactive bands' gradients are left alone: their CG has stopped (the reference leaves
+        // its icg loop before the preconditioner for them)
+        RS_TRY((cggs_block<T, NC>(c, psi, nb, b0, nn, PG)));
+        pg_dot = false;
       }
       {
         ProfScope ps(c, "cg");

@@ -115,6 +115,7 @@ struct Ctx {
   int rot_update = 0;              // mixed rotation in update form X + X (C - I)
   int nl_fused = 0;                // nonlocal term inside the stencil (1) or by the scatter kernel after it (0)
   int wait_polls = -1;             // hpsi stencil's bounded waits: polls before giving up (-1: the default)
+  int cggs = 0;                    // SWGS: 0 off, 1 cggs_1 (lower bands), 2 cggs_2 (all other bands)
 
   // profiling: 0 off, 1 every kernel family, 2 the hpsi stencil only (light enough for a timed run)
   int profiling = 0;

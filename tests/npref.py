@@ -83,8 +83,10 @@ def np_precond(prob, g, mloop=3):
     return pg
 
 
-def np_cg_band(prob, x, k=0, ncg=3, mloop=3):
-    """One band of d/z_conjugate_gradient_1 (src/conjugate_gradient/cg_module.f90:112-754)."""
+def np_cg_band(prob, x, k=0, ncg=3, mloop=3, others=()):
+    """One band of d/z_conjugate_gradient_1 (src/conjugate_gradient/cg_module.f90:112-754).
+    others: bands the preconditioned gradient is orthogonalised against after every
+    preconditioner call (cggs, src/conjugate_gradient/cggs_module.f90), classical Gram-Schmidt."""
     dV = prob.dV
     cpx = prob.is_complex
     gfac, c1sq = (-1.0, 1.0) if cpx else (-2.0, 4.0)
@@ -102,6 +104,9 @@ def np_cg_band(prob, x, k=0, ncg=3, mloop=3):
         if rb < 0 or abs(E - E1) < 1e-15 or icg == ncg + 1:
             break
         pg = np_precond(prob, g, mloop)
+        if len(others):
+            xs = np.asarray(others)
+            pg = pg - xs.T @ (xs.conj() @ pg * dV)
         rb = float(np.vdot(pg, g).real) * dV
         p = pg.copy() if icg == 1 else pg + (rb / gkgk) * p
         gkgk = rb
@@ -151,3 +156,17 @@ def principal_angles(A, B):
     s = np.linalg.svd(qa.conj().T @ qb, compute_uv=False)
     s = np.clip(s, -1.0, 1.0)
     return float(np.arccos(s.min()))
+
+
+def np_cg_cggs(prob, psi, iswitch, k=0):
+    """All bands of conjugate_gradient with MB_d = 1 and SWGS = iswitch, in band order: band n is
+    orthogonalised against the (updated) bands m < n (1) or all other current bands (2)."""
+    u = psi.copy()
+    es, rs = [], []
+    for n in range(u.shape[0]):
+        idx = range(n) if iswitch == 1 else [m for m in range(u.shape[0]) if m != n]
+        x, e, r = np_cg_band(prob, u[n], k, others=[u[m] for m in idx])
+        u[n] = x
+        es.append(e)
+        rs.append(r)
+    return u, np.array(es), np.array(rs)

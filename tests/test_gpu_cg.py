@@ -115,3 +115,38 @@ def test_converged_eigenvalues_and_subspace(oracle_mod):
     assert res.max() <= 1e-15
     assert np.max(np.abs(np.sort(esp[0, 0]) - np.sort(e_ref))) < 1e-8
     assert npref.principal_angles(u, u_ref) < 1e-6
+
+
+@pytest.mark.parametrize("iswitch", [1, 2])
+@pytest.mark.parametrize("name,k", [("c0", 0), ("tk", 5)])
+def test_cg_with_cggs_matches_oracle(oracle_mod, name, k, iswitch):
+    """SWGS = 1 / 2: the preconditioned gradients orthogonalised against the lower / all other
+    bands inside conjugate_gradient (cggs, src/conjugate_gradient/cggs_module.f90), one band per
+    CG block (MB_d = 1, the oracle's band order)."""
+    prob = synth.make_problem(name)
+    o = oracle_mod.Oracle(prob, k=k, cggs=iswitch)
+    nb = int(prob.nband_k[k])
+    psi = synth.random_wavefunctions(38, nb, prob.ng, is_complex=prob.is_complex, kindex=k)
+    psi = oracle_mod.Oracle(prob, k=k).gram_schmidt(psi)
+    u_ref, e_ref, r_ref = o.cg(psi)
+    with api.BandUpdate(prob, cg_block=1) as g:
+        g.cggs(iswitch)
+        g.set_wf(psi, k=k + 1)
+        esp, res = g.conjugate_gradient(k=k + 1)
+        u = g.get_wf(k=k + 1)
+    assert np.max(np.abs(esp - e_ref)) < 1e-10
+    assert np.all(np.abs(res - r_ref) <= 1e-7 * np.abs(r_ref) + 1e-14)
+    assert np.max(np.abs(u - u_ref)) < 1e-8 * np.max(np.abs(u_ref))
+
+
+def test_cg_with_cggs_mixed_tracks_oracle(oracle_mod):
+    """The same on FP32 bands (mixed precision): energies within 1e-5 Ha of the FP64 oracle."""
+    prob = synth.make_problem("c0")
+    o = oracle_mod.Oracle(prob, cggs=1)
+    psi = oracle_mod.Oracle(prob).gram_schmidt(synth.random_wavefunctions(39, prob.nband, prob.ng))
+    _, e_ref, _ = o.cg(psi)
+    with api.BandUpdate(prob, precision=api.PREC_MIXED, cg_block=1) as g:
+        g.cggs(1)
+        g.set_wf(psi)
+        esp, res = g.conjugate_gradient()
+    assert np.max(np.abs(esp - e_ref)) < 1e-5

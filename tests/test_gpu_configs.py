@@ -135,3 +135,30 @@ def test_c4_grid_two_kpoints_sweeps_track_oracle(oracle_mod):
         assert np.max(np.abs(esp[0, k, :nb] - e_ref)) < 1e-8, k
         m = _gap_index(e_ref, nb - 8, nb - 1)
         assert npref.principal_angles(us[k][:m], u_ref[:m]) < 1e-6, k
+
+
+def test_c4_grid_mixed_solve_matches_fp64_solve():
+    """C4 grid (64^3, complex16, 8 Bloch k-points, uneven band counts, reduced): the mixed
+    precision solve (FP32 bands, complex split-BF16 tensor-core contractions) and the plain FP64
+    solve of the same input, both to max res <= 1e-8 over bands 1..nb_k - nb_k/8 of every
+    k-point: eigenvalues within 1e-8 Ha."""
+    cfg = synth.get_config("c4", nband=48, nband_range=(32, 48))
+    prob = synth.make_problem(cfg)
+    nbk = [int(x) for x in prob.nband_k]
+    conv = [n - n // 8 for n in nbk]
+    out = {}
+    for prec in (api.PREC_FP64, api.PREC_MIXED):
+        with api.BandUpdate(prob, precision=prec) as g:
+            g.init_sweep(-1)
+            for k in range(prob.nk):
+                g.random_wf(75, k=k + 1)
+                g.gram_schmidt(k=k + 1)
+            it, esp, res = g.calc_sweep(400, tol=1e-8)
+            for k in range(prob.nk):
+                assert res[0, k, :conv[k]].max() <= 1e-8, (prec, k, it)
+            out[prec] = (esp.copy(), it)
+    e64, it64 = out[api.PREC_FP64]
+    e32, it32 = out[api.PREC_MIXED]
+    err = max(np.max(np.abs(e32[0, k, :conv[k]] - e64[0, k, :conv[k]])) for k in range(prob.nk))
+    print(f"c4 grid, {nbk} bands: sweeps fp64 {it64}, mixed {it32}; eigenvalue error {err:.2e} Ha")
+    assert err < 1e-8

@@ -220,3 +220,18 @@ def test_golden_fixtures(oracle_mod):
     ot = oracle_mod.Oracle(pt)
     assert np.allclose(np.linalg.eigvalsh(0.5 * (lambda H: H + H.T)(npref.np_hpsi(pt, np.eye(pt.ng))))[:pt.nband],
                        g["t0_eigs"], atol=1e-10)
+
+
+@pytest.mark.parametrize("iswitch", [1, 2])
+@pytest.mark.parametrize("name,k", [("t0", 0), ("tk", 3)])
+def test_oracle_cg_with_cggs_matches_numpy(oracle_mod, name, k, iswitch):
+    """cggs (SWGS = 1, 2) inside the oracle's CG against the numpy restatement, bands in order."""
+    prob = synth.make_problem(name)
+    o = oracle_mod.Oracle(prob, k=k, cggs=iswitch)
+    nb = int(prob.nband_k[k])
+    psi = synth.random_wavefunctions(17, nb, prob.ng, is_complex=prob.is_complex, kindex=k)
+    psi = oracle_mod.Oracle(prob, k=k).gram_schmidt(psi)
+    u, e, r = o.cg(psi)
+    u_np, e_np, r_np = npref.np_cg_cggs(prob, psi, iswitch, k)
+    assert np.max(np.abs(e - e_np)) < 1e-10
+    assert np.max(np.abs(u - u_np)) < 1e-8 * np.max(np.abs(u_np))
