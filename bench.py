@@ -25,7 +25,7 @@ JSON line keys beyond the driver contract:
   clocks               nvidia-smi samples during the timed steps
 
 --impl reference times the same CPU oracle alone (bounded sample per step) for the same config.
---kernel hpsi|gemm|pc|lpc runs one kernel family on its own (timing and ncu captures).
+--kernel hpsi|gemm|pc|cg|lpc runs one kernel family on its own (timing and ncu captures).
 Multi-GPU runs are independent replicas (one problem per GPU): every rank solves its own copy
 and the time is the max over ranks.
 """
@@ -317,6 +317,10 @@ def run_ours(args, dist, rank, ws):
 
     g = api.BandUpdate(prob, precision=prec, pc_mode=pc_mode)
     g.gemm_terms(*terms)
+    sched = tuple(float(x) for x in args.gemm_schedule.split(","))
+    if prec == api.PREC_MIXED:
+        g.gemm_schedule(*sched)
+    g.pc_form(args.pc_form)
     if pc == "learned":
         g.lpc_set_weights(np.load(wpath))
     g.init_sweep(sweep_ref)
@@ -463,6 +467,8 @@ def run_ours(args, dist, rank, ws):
                        "projectors": prob.nzlma, "precision": args.precision, "pc": pc,
                        "lpc_fallbacks": lpc_state[2] if pc == "learned" else None,
                        "gemm_terms": list(terms) if prec == api.PREC_MIXED else None,
+                       "gemm_schedule": list(sched) if prec == api.PREC_MIXED else None,
+                       "pc_form": args.pc_form,
                        "mb_ref": conv if nk > 1 else mb_ref, "tol": TOL, "sweeps_to_tol": iters,
                        "final_res_max": res_max,
                        "l2": "inputs larger than L2 (psi >= 0.5 GB)", "parallelism": f"replicas x{ws}"},
@@ -532,6 +538,28 @@ def run_kernel(args):
                 g.profile(0)
                 del a, b
         return
+    if what == "cg":
+        # one conjugate_gradient call (Ncg = 3) on nb bands, mixed precision with precond_hprsdft
+        cfg = synth.get_config(args.config, nband=nb)
+        if prob.is_complex:
+            cfg = synth.get_config(args.config, nband=nb, nband_range=(nb, nb))
+        pb = synth.make_problem(cfg)
+        with api.BandUpdate(pb, precision=api.PREC_MIXED) as g:
+            g.pc_form(args.pc_form)
+            g.random_wf(5)
+            g.gram_schmidt()
+            g.conjugate_gradient()  # untimed first call
+            g.profile(1)
+            for _ in range(reps):
+                g.random_wf(5)
+                g.gram_schmidt()
+                g.conjugate_gradient()
+            g.synchronize()
+            shares = {n: g.profile_get(n)[0] / reps for n in ("pc", "cg", "hpsi_stencil", "nl_gather", "nl_scatter")}
+            g.profile(0)
+        print(f"cg {args.config} bands={nb} pc_form={args.pc_form}: per call " +
+              ", ".join(f"{k} {v:.3f} ms" for k, v in shares.items()), flush=True)
+        return
     rng = np.random.default_rng(3)
     g_in = rng.standard_normal((nb, prob.ng))
     if what == "pc":
@@ -582,7 +610,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--gemm-terms", default="3,3",
                     help="BF16 terms of the mixed overlap/Hsub and rotation contractions (2 or 3 each)")
-    ap.add_argument("--kernel", default="solve", choices=["solve", "hpsi", "gemm", "pc", "lpc"],
+    ap.add_argument("--pc-form", type=int, default=1, help="FP32 preconditioner form inside CG (1 s-step passes, 2 fused, 0)")
+    ap.add_argument("--gemm-schedule", default="0,0",
+                    help="mixed precision: two BF16 terms in overlap/Hsub, rotation while CG's residual > these")
+    ap.add_argument("--kernel", default="solve", choices=["solve", "hpsi", "gemm", "pc", "cg", "lpc"],
                     help="solve (the benchmark) or one kernel family on its own")
     ap.add_argument("--bands", type=int, default=0, help="--kernel: bands (default all / 256 for gemm)")
     ap.add_argument("--points", type=int, default=0, help="--kernel gemm: K points")

@@ -45,6 +45,7 @@ extern "C" {
 #define RSDFT_ERR_STATE       -7   /* call order (init/set_* missing) */
 #define RSDFT_ERR_UNSUPPORTED -8   /* configuration not built in */
 #define RSDFT_ERR_NUMERIC     -9   /* NaN/Inf detected in inputs or results */
+#define RSDFT_ERR_IO          -10  /* file open / read / write error or malformed file */
 
 /* ---- precision modes ---- */
 #define RSDFT_PREC_FP64   0  /* all FP64 (the plain GPU drop-in) */
@@ -115,6 +116,23 @@ int rsdft_gpu_get_wf_z(int k, int s, double* unk, int ld, int nb);
  * src/wf_module.f90:161-191): element e = ((k0*2^20 + band0)*ML0 + j)*2 + reim holds
  * sum_{t<12} u(e,t) - 6, u = (splitmix64(seed*2^40 + 12e + t) >> 11) * 2^-53. */
 int rsdft_gpu_random_wf(int k, int s, uint64_t seed);
+/* Wavefunction restart files in the reference's format: write_wf_simple
+ * (src/io_write_wf_simple_module.f90:21-276, IO_ctrl = 0, OC < 10) via write_data
+ * (src/io_module.f90:59-259).  Writes bands 1..MB of every (k, s) of the resident unk as a Fortran
+ * sequential unformatted file (4-byte record markers): header (-1, ML.., MB.., MK MS MMBZ,
+ * IO_ctrl OC TYPE_WF), LL2 grid map, occ(MB,MK,MS), aa, bb, kbb(3,MK), one-process parallel
+ * info, then one record per band (s, k, n order) in FP64 (oc 1, 3) or FP32 (oc 4, 5).  occ, aa,
+ * bb, kbb are host arrays of the caller (NULL writes zeros); MB is the largest band count over
+ * the k-points, bands past a k-point's own count are written as zeros. */
+int rsdft_gpu_write_wf(const char* path, int oc, const double* occ, const double* aa, const double* bb,
+                       const double* kbb);
+/* read_wf_simple (src/io_read_wf_simple_module.f90:21-560, IO_ctrl = 0): reads a file of either
+ * layout (new, or the old one without the leading -1), FP64 or FP32, real or complex records,
+ * into the resident unk of every (k, s), placing each point by the file's LL2 grid map.  The grid
+ * and the k-point / spin counts must match the context; occ (MB x MK x MS, may be NULL) receives
+ * the file's occupations.  A complex file read by a real context keeps the real part; a real file
+ * read by a complex context gets zero imaginary parts (as the reference does). */
+int rsdft_gpu_read_wf(const char* path, double* occ);
 
 /* ---- the four module procedures ---- */
 /* hamiltonian: htpsi(:,1:nb) = H tpsi(:,1:nb) (overwrites htpsi).  mem selects host or device
@@ -152,7 +170,11 @@ int rsdft_gpu_precond_d(int k, const double* gk, double* pgk, int ld, int nb, in
 /* The same on FP32 bands, as mixed-precision CG runs it: the mloop CG steps evaluated in the
  * s-step (Krylov-basis) form, 3 mloop + 3 passes over the bands (mloop <= 4). */
 int rsdft_gpu_precond_f(int k, const float* gk, float* pgk, int ld, int nb, int mem);
-/* FP32 precond_hprsdft form: 1 (default) s-step, 0 the recurrence form of the FP64 path. */
+/* FP32 precond_hprsdft form inside conjugate_gradient: 1 (default) the s-step form in 3 mloop + 3
+ * passes, 2 the s-step form fused into two z-streamed passes together with <Pg|g> and the
+ * direction update p = Pg + beta p (src/conjugate_gradient/cg_module.f90:254-283; mloop 1..3,
+ * SWGS off), 0 the recurrence form of the FP64 path.  rsdft_gpu_precond_f uses form 1 for 1
+ * and 2. */
 int rsdft_gpu_set_pc_form(int sstep);
 /* Orthogonalisation of the preconditioned gradient inside conjugate_gradient, the reference's
  * SWGS keyword (src/conjugate_gradient/cg_module.f90:47, cggs at :249-251 and :576-578):
@@ -179,6 +201,12 @@ int rsdft_gpu_set_precision(int precision);
  * (src/sweep_module.f90:46-60,267-278; src/band_module.f90:207; src/dos_module.f90:64-75).
  * mb_ref = -1: per k-point, bands 1..nband_k - nband_k/8 (k-points with uneven band counts). */
 int rsdft_gpu_init_sweep(int mb_ref);
+/* Convergence test of rsdft_gpu_sweep: 0 (default) max over bands 1..mb_ref of the FP64 residual
+ * res(n) <= tol; 2 the reference's conv_check_2 (src/sweep_module.f90:277-288), used by its band
+ * driver (init_sweep(2, mb2_band, esp_conv_tol), src/band_module.f90:207): no eigenvalue of bands
+ * 1..mb_ref moved by tol or more in the last sweep.  esp/res returned are the FP64 residual
+ * check's values of the last sweep. */
+int rsdft_gpu_set_sweep_check(int iconv_check);
 
 /* ---- learned preconditioner (no counterpart in the reference) ----
  * A 4-layer 3-D convolutional network, channels 1-16-16-16-1, 3x3x3 kernels, no biases, tanh
@@ -253,6 +281,12 @@ int rsdft_gpu_selftest_gemm(int m, int n, long long k, int op, double* err);
  * residual of the 128^3 / 2048-band problem wandering between 1e-7 and 1e-4; two-term rotations
  * stall the residual near 5e-9.  No counterpart in the reference. */
 int rsdft_gpu_set_gemm_terms(int overlap_terms, int rotation_terms);
+/* Precision schedule of rsdft_gpu_sweep (mixed precision): the Gram-Schmidt / subspace overlap and
+ * Hsub contractions use two BF16 terms while CG's largest residual of the (k, s) in that sweep
+ * is above res_sm, the band rotation while it is above res_rot; below, the terms set by
+ * rsdft_gpu_set_gemm_terms.  0 switches a threshold off (the default).  No counterpart in the
+ * reference (one precision per build). */
+int rsdft_gpu_set_gemm_schedule(double res_sm, double res_rot);
 /* Tiling of the three-term tensor-core contractions, flags (default 7): bit 0 set, 128 x 256
  * output tiles over K blocks of 32 (else 128 x 128 over 64); bit 1 set, the overlap S of the
  * fused overlap/Hsub contraction is formed by the tiles reaching its upper triangle only (its

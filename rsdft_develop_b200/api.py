@@ -47,11 +47,12 @@ EXPORTS = [
     "rsdft_gpu_init", "rsdft_gpu_finalize", "rsdft_gpu_last_error", "rsdft_gpu_get_stream",
     "rsdft_gpu_synchronize", "rsdft_gpu_set_kpoint", "rsdft_gpu_set_vloc", "rsdft_gpu_set_projectors",
     "rsdft_gpu_set_uvk_d", "rsdft_gpu_set_uvk_z", "rsdft_gpu_set_wf_d", "rsdft_gpu_get_wf_d",
-    "rsdft_gpu_set_wf_z", "rsdft_gpu_get_wf_z", "rsdft_gpu_random_wf", "rsdft_gpu_hamiltonian_d",
+    "rsdft_gpu_set_wf_z", "rsdft_gpu_get_wf_z", "rsdft_gpu_random_wf", "rsdft_gpu_write_wf", "rsdft_gpu_read_wf",
+    "rsdft_gpu_hamiltonian_d",
     "rsdft_gpu_hamiltonian_z", "rsdft_gpu_hamiltonian_f", "rsdft_gpu_hamiltonian_c",
     "rsdft_gpu_conjugate_gradient", "rsdft_gpu_gram_schmidt", "rsdft_gpu_subspace_diag",
     "rsdft_gpu_residual", "rsdft_gpu_precond_d", "rsdft_gpu_precond_f", "rsdft_gpu_set_pc_form", "rsdft_gpu_sweep", "rsdft_gpu_profile",
-    "rsdft_gpu_profile_get", "rsdft_gpu_kernel_launches", "rsdft_gpu_selftest_gemm", "rsdft_gpu_set_gemm_terms", "rsdft_gpu_set_gemm_tile", "rsdft_gpu_set_nl_form", "rsdft_gpu_init_sweep", "rsdft_gpu_set_wait_polls", "rsdft_gpu_set_precision", "rsdft_gpu_set_cggs",
+    "rsdft_gpu_profile_get", "rsdft_gpu_kernel_launches", "rsdft_gpu_selftest_gemm", "rsdft_gpu_set_gemm_terms", "rsdft_gpu_set_gemm_tile", "rsdft_gpu_set_nl_form", "rsdft_gpu_init_sweep", "rsdft_gpu_set_wait_polls", "rsdft_gpu_set_precision", "rsdft_gpu_set_cggs", "rsdft_gpu_set_sweep_check", "rsdft_gpu_set_gemm_schedule",
     "rsdft_gpu_hamiltonian_noalloc_d",
     "rsdft_gpu_lpc_init", "rsdft_gpu_lpc_set_weights", "rsdft_gpu_lpc_get_weights", "rsdft_gpu_lpc_forward",
     "rsdft_gpu_lpc_loss_grad", "rsdft_gpu_lpc_dataset", "rsdft_gpu_lpc_harvest", "rsdft_gpu_lpc_dataset_get",
@@ -101,6 +102,7 @@ def load_library(path: str = LIB_PATH):
         "rsdft_gpu_set_wf_d": [i, i, vp, i, i], "rsdft_gpu_get_wf_d": [i, i, vp, i, i],
         "rsdft_gpu_set_wf_z": [i, i, vp, i, i], "rsdft_gpu_get_wf_z": [i, i, vp, i, i],
         "rsdft_gpu_random_wf": [i, i, C.c_uint64],
+        "rsdft_gpu_write_wf": [C.c_char_p, i, vp, vp, vp, vp], "rsdft_gpu_read_wf": [C.c_char_p, vp],
         "rsdft_gpu_hamiltonian_d": [i, i, vp, vp, i, i, i], "rsdft_gpu_hamiltonian_z": [i, i, vp, vp, i, i, i],
         "rsdft_gpu_hamiltonian_f": [i, i, vp, vp, i, i, i], "rsdft_gpu_hamiltonian_c": [i, i, vp, vp, i, i, i],
         "rsdft_gpu_conjugate_gradient": [i, i, vp, vp], "rsdft_gpu_gram_schmidt": [i, i],
@@ -112,6 +114,7 @@ def load_library(path: str = LIB_PATH):
         "rsdft_gpu_selftest_gemm": [i, i, C.c_longlong, i, C.POINTER(C.c_double)],
         "rsdft_gpu_set_gemm_terms": [i, i], "rsdft_gpu_set_gemm_tile": [i], "rsdft_gpu_set_nl_form": [i],
         "rsdft_gpu_set_wait_polls": [i], "rsdft_gpu_set_precision": [i], "rsdft_gpu_set_cggs": [i],
+        "rsdft_gpu_set_sweep_check": [i], "rsdft_gpu_set_gemm_schedule": [d, d],
         "rsdft_gpu_init_sweep": [i],
         "rsdft_gpu_hamiltonian_noalloc_d": [i, i, vp, vp, i, i],
         "rsdft_gpu_lpc_init": [C.c_ulonglong], "rsdft_gpu_lpc_set_weights": [vp, i],
@@ -193,6 +196,16 @@ class BandUpdate:
         else:
             _call(self.lib.rsdft_gpu_set_projectors, 0, 0, None, None, None, 0, None, None)
 
+    def set_kpoint_operator(self, prob: "synth.Problem", ik: int, k: int = 1, nonlocal_on: bool = True):
+        """Point k-point slot k of this context at k-point ik of prob (same grid, atoms and Dij):
+        its kinetic coefficients (coef_nabk, const_k2) and projector phases uVk."""
+        nabk = np.zeros((3, MDMAX))
+        nabk[:, :prob.md] = prob.kin["coef_nabk"][ik]
+        _call(self.lib.rsdft_gpu_set_kpoint, k, _ptr(nabk), float(prob.kin["const_k2"][ik]), self.nband(k))
+        if nonlocal_on and prob.nzlma > 0:
+            u = np.ascontiguousarray(prob.uvk[ik], np.complex128)
+            _call(self.lib.rsdft_gpu_set_uvk_z, k, _ptr(u))
+
     def _set_projectors(self):
         pr = self.prob
         mjj = np.ascontiguousarray(pr.mjj, np.int32)
@@ -267,6 +280,38 @@ class BandUpdate:
         _call(self.lib.rsdft_gpu_random_wf, k, s, C.c_uint64(seed))
 
     # ---- the four module procedures ----
+    def write_wf(self, path: str, oc: int = 1, occ=None, aa=None, bb=None, kbb=None):
+        """write_wf_simple: the resident bands of every (k, s) in the reference's wf file format
+        (oc 1/3: FP64 records, 4/5: FP32 records)."""
+        def opt(x, shape):
+            if x is None:
+                return None
+            return np.asfortranarray(np.asarray(x, dtype=np.float64).reshape(shape, order="F"))
+        nk = int(self.prob.nk)
+        mb = int(max(self.prob.nband_k))
+        ns = int(self.params.nspin)
+        o, a_, b_, k_ = opt(occ, (mb, nk, ns)), opt(aa, (3, 3)), opt(bb, (3, 3)), opt(kbb, (3, nk))
+        _call(self.lib.rsdft_gpu_write_wf, path.encode(), int(oc), *(None if x is None else x.ctypes.data_as(C.c_void_p)
+                                                                    for x in (o, a_, b_, k_)))
+
+    def read_wf(self, path: str) -> np.ndarray:
+        """read_wf_simple: a wf file (this library's or the reference's) into the resident bands;
+        returns the file's occupations occ(MB, MK, MS) (Fortran order)."""
+        nk = int(self.prob.nk)
+        # the band count of the file is read from its header record (third record)
+        with open(path, "rb") as f:
+            import struct
+            recs = []
+            for _ in range(3):
+                (m,) = struct.unpack("<i", f.read(4))
+                recs.append(f.read(m))
+                f.read(4)
+        newfmt = struct.unpack("<i", recs[0][:4])[0] < 0
+        mb = struct.unpack("<i", (recs[2] if newfmt else recs[1])[:4])[0]
+        occ = np.zeros((mb, nk, int(self.params.nspin)), order="F")
+        _call(self.lib.rsdft_gpu_read_wf, path.encode(), occ.ctypes.data_as(C.c_void_p))
+        return occ
+
     def hamiltonian(self, tpsi: np.ndarray, k: int = 1, s: int = 1, fp32: bool = False) -> np.ndarray:
         """htpsi = H tpsi for a host block tpsi[nb][ML0] (hamiltonian(tpsi,htpsi,n,k,s))."""
         tpsi = np.atleast_2d(tpsi)
@@ -341,6 +386,11 @@ class BandUpdate:
         FP64 final polish of a mixed-precision solve is set_precision(PREC_FP64) + calc_sweep)."""
         _call(self.lib.rsdft_gpu_set_precision, int(precision))
         self.precision = precision
+
+    def sweep_check(self, iconv_check: int):
+        """Convergence test of calc_sweep: 0 FP64 residual <= tol, 2 eigenvalue change < tol
+        (the reference's conv_check_2)."""
+        _call(self.lib.rsdft_gpu_set_sweep_check, int(iconv_check))
 
     def init_sweep(self, mb_ref: int = 0):
         """Check convergence on bands 1..mb_ref (0: all), as init_sweep(..., mb_ref, ...)."""
@@ -454,9 +504,10 @@ class BandUpdate:
         _call(self.lib.rsdft_gpu_selftest_gemm, m, n, k, op, C.byref(e))
         return e.value
 
-    def pc_form(self, sstep: bool) -> None:
-        """FP32 precond_hprsdft evaluation: s-step (default) or the recurrence form."""
-        _call(self.lib.rsdft_gpu_set_pc_form, 1 if sstep else 0)
+    def pc_form(self, form) -> None:
+        """FP32 precond_hprsdft evaluation inside CG: 1 (or True, the default) the s-step form in
+        separate passes, 2 the fused z-streamed s-step form, 0 (or False) the recurrence form."""
+        _call(self.lib.rsdft_gpu_set_pc_form, int(form))
 
     def nl_form(self, fused: bool) -> None:
         """Nonlocal term of the real hpsi: inside the stencil (fused) or by a scatter after it."""
@@ -479,6 +530,11 @@ class BandUpdate:
         if tri:
             flags |= 2 | (8 if tri == 2 else 0)
         _call(self.lib.rsdft_gpu_set_gemm_tile, flags)
+
+    def gemm_schedule(self, res_sm: float, res_rot: float) -> None:
+        """Two BF16 terms in the overlap/Hsub (rotation) contractions of a sweep while CG's
+        largest residual is above res_sm (res_rot); 0 switches a threshold off."""
+        _call(self.lib.rsdft_gpu_set_gemm_schedule, float(res_sm), float(res_rot))
 
     def gemm_terms(self, overlap: int, rotation: int) -> None:
         """BF16 terms (2 or 3) of the mixed-precision overlap/Hsub and rotation contractions."""

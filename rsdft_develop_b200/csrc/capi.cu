@@ -682,6 +682,13 @@ int rsdft_gpu_init_sweep(int mb_ref) {
   return 0;
 }
 
+int rsdft_gpu_set_sweep_check(int iconv_check) {
+  REQUIRE_CTX();
+  RS_CHECK(iconv_check == 0 || iconv_check == 2, RSDFT_ERR_ARG, "sweep check must be 0 or 2");
+  g_ctx->sweep_check = iconv_check;
+  return 0;
+}
+
 }  // extern "C"
 
 // Bands 1..n of k-point k checked for convergence by rsdft_gpu_sweep
@@ -706,16 +713,56 @@ int rsdft_gpu_sweep(int nsweep, double tol, int* iters, double* esp, double* res
   int stall = 0;
   int it = 0;
   std::vector<double> cg_res((size_t)nbmax);
+  // sweep_check 2 (conv_check_2, src/sweep_module.f90:277-288): converged when no eigenvalue of
+  // bands 1..mb_ref moved by tol or more in the sweep; esp0 holds the previous sweep's values
+  const bool by_esp = c.sweep_check == 2;
+  const size_t nall = (size_t)c.p.nspin * c.p.nk * nbmax;
+  std::vector<double> esp_cur(by_esp ? nall : 0, 0.0), esp_old(by_esp ? nall : 0, 0.0);
+  // esp0 of the first sweep: the Ritz values of the context's last sweep (the reference's esp
+  // array keeps them across calc_sweep calls, e.g. from the previous k of the band trajectory)
+  if (by_esp && c.esp_last.size() == nall) esp_old = c.esp_last;
   for (it = 1; it <= nsweep; ++it) {
-    double rmax = 0.0, cg_rmax = 0.0;
+    double rmax = 0.0, cg_rmax = 0.0, dmax = 0.0;
     for (int s = 0; s < c.p.nspin; ++s)
       for (int k = 0; k < c.p.nk; ++k) {
         RS_CHECK(c.wfn(k, s).valid, RSDFT_ERR_STATE, "no wavefunctions resident for (k,s)=(%d,%d)", k + 1, s + 1);
         RS_TRY(cg_run(c, k, s, nullptr, cg_res.data()));
         const int nconv = conv_bands(c, k);
         for (int n = 0; n < nconv; ++n) cg_rmax = std::max(cg_rmax, cg_res[n]);
-        RS_TRY(gssd_run(c, k, s, nullptr, true));
+        const size_t off = ((size_t)s * c.p.nk + k) * nbmax;
+        // precision schedule (mixed precision): two BF16 terms in the contractions while CG's
+        // residual of this (k, s) is above the threshold, then the configured terms
+        const int t_sm = c.gemm_terms_sm, t_rot = c.gemm_terms_rot;
+        double kmax = 0.0;
+        for (int n = 0; n < nconv; ++n) kmax = std::max(kmax, cg_res[n]);
+        if (c.sched_res_sm > 0.0 && kmax > c.sched_res_sm) c.gemm_terms_sm = 2;
+        if (c.sched_res_rot > 0.0 && kmax > c.sched_res_rot) c.gemm_terms_rot = 2;
+        if (c.gemm_terms_sm != t_sm || c.gemm_terms_rot != t_rot) c.sched_sweeps++;
+        const int rc_g = gssd_run(c, k, s, by_esp ? esp_cur.data() + off : nullptr, true);
+        c.gemm_terms_sm = t_sm;
+        c.gemm_terms_rot = t_rot;
+        RS_TRY(rc_g);
+        if (by_esp) {
+          for (int n = 0; n < nconv; ++n) dmax = std::max(dmax, std::fabs(esp_cur[off + n] - esp_old[off + n]));
+        }
       }
+    if (by_esp) {
+      const bool done = tol > 0.0 && dmax < tol;
+      if (done || it == nsweep) {
+        for (int s = 0; s < c.p.nspin; ++s)
+          for (int k = 0; k < c.p.nk; ++k) {
+            const int nb = c.kp[k].nband;
+            const size_t off = ((size_t)s * c.p.nk + k) * nbmax;
+            RS_TRY(rsdft_gpu_residual(k + 1, s + 1, e.data(), r.data()));
+            if (esp) std::memcpy(esp + off, e.data(), sizeof(double) * nb);
+            if (res) std::memcpy(res + off, r.data(), sizeof(double) * nb);
+          }
+      }
+      c.esp_last = esp_cur;
+      if (done) break;
+      esp_old.swap(esp_cur);
+      continue;
+    }
     // The FP64 check (an FP64 H x of every band) runs once CG's own residual of the bands it
     // returned is within kResGate x tol: before that the check cannot pass.  The learned-PC
     // guard checks every sweep.
@@ -799,7 +846,7 @@ int rsdft_gpu_selftest_gemm(int m, int n, long long k, int op, double* err) {
 
 int rsdft_gpu_set_pc_form(int sstep) {
   REQUIRE_CTX();
-  RS_CHECK(sstep == 0 || sstep == 1, RSDFT_ERR_ARG, "sstep must be 0 or 1");
+  RS_CHECK(sstep >= 0 && sstep <= 2, RSDFT_ERR_ARG, "preconditioner form must be 0, 1 or 2");
   g_ctx->pc_sstep = sstep;
   return 0;
 }
@@ -840,6 +887,14 @@ int rsdft_gpu_set_gemm_terms(int overlap_terms, int rotation_terms) {
            "split terms must be 2 or 3");
   g_ctx->gemm_terms_sm = overlap_terms;
   g_ctx->gemm_terms_rot = rotation_terms;
+  return 0;
+}
+
+int rsdft_gpu_set_gemm_schedule(double res_sm, double res_rot) {
+  REQUIRE_CTX();
+  RS_CHECK(res_sm >= 0.0 && res_rot >= 0.0, RSDFT_ERR_ARG, "schedule thresholds must be >= 0");
+  g_ctx->sched_res_sm = res_sm;
+  g_ctx->sched_res_rot = res_rot;
   return 0;
 }
 

@@ -22,57 +22,9 @@
 // can take it instead of recomputing it.
 #include <cstring>
 
-#include "ctx.cuh"
+#include "cgk.cuh"
 
 namespace rsdft {
-
-constexpr int kThreads = 256;
-constexpr int kMaxChunks = 128;
-constexpr int kPS = 8;  // partial slots per (band, chunk)
-
-enum Scal {
-  S_E = 0, S_E1, S_RB, S_GKGK, S_RES, S_W, S_U1, S_U1I, S_U2, S_U2I, S_ACT, S_BETA, S_ACC,
-  S_RR0, S_RR1, S_PCA, S_PCB, S_PCACT,
-  S_MU0, S_MU7 = S_MU0 + 7,  // s-step preconditioner: moments <v0 | B^i v0>, i < 2 mloop
-  S_XI0, S_XI3 = S_XI0 + 3,  // s-step preconditioner: PG = G + sum_i xi_i B^i v0
-  S_COUNT
-};
-
-struct Blk {
-  int nbb;        // bands in the block
-  int nch;        // CTAs (chunks) per band for elementwise/reduction kernels
-  size_t ng;      // reals per band (grid points x components)
-  double* sc;     // scalars [S_COUNT][nbb]
-  double* part;   // partials [nbb][nch][kPS]
-};
-
-__device__ __forceinline__ double& SC(const Blk& k, int which, int b) { return k.sc[(size_t)which * k.nbb + b]; }
-
-template <int ND>
-__device__ __forceinline__ void block_partials(double (&v)[ND], const Blk& k, int b) {
-  __shared__ double red[kThreads / 32][ND];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int d = 0; d < ND; ++d) {
-    double x = v[d];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-    if (lane == 0) red[wid][d] = x;
-  }
-  __syncthreads();
-  if (threadIdx.x < ND) {
-    double t = 0.0;
-#pragma unroll
-    for (int w = 0; w < kThreads / 32; ++w) t += red[w][threadIdx.x];
-    k.part[((size_t)b * k.nch + blockIdx.x) * kPS + threadIdx.x] = t;
-  }
-}
-
-__device__ __forceinline__ double sum_part(const Blk& k, int b, int d) {
-  double t = 0.0;
-  for (int c = 0; c < k.nch; ++c) t += k.part[((size_t)b * k.nch + c) * kPS + d];
-  return t;
-}
 
 // NC = 2 loops run over complex points (pairs of reals)
 #define BAND_LOOP(k, NC)                                                    \
@@ -138,7 +90,7 @@ __global__ void __launch_bounds__(kThreads) k_dots6(Blk k, const T* __restrict__
                                                     const T* __restrict__ hx, const T* __restrict__ hp) {
   BAND_LOOP(k, NC);
   if (SC(k, S_ACT, b) == 0.0) return;
-  constexpr int ND = NC == 1 ? 6 : 8;
+  constexpr int ND = NC == 1 ? 10 : 8;
   double v[ND];
 #pragma unroll
   for (int d = 0; d < ND; ++d) v[d] = 0.0;
@@ -151,6 +103,11 @@ __global__ void __launch_bounds__(kThreads) k_dots6(Blk k, const T* __restrict__
       v[3] += xi * hxi;
       v[4] += pi * hxi;
       v[5] += pi * hpi;
+      // for the estimate of |g|^2 after the step (the reject test ahead of the fused x update)
+      v[6 % ND] += hxi * hxi;
+      v[7 % ND] += hxi * hpi;
+      v[8 % ND] += hpi * hpi;
+      v[9 % ND] += xi * hpi;
     } else {
       const size_t j = off + 2 * i;
       const double xr = x[j], xm = x[j + 1], pr = p[j], pm = p[j + 1];
@@ -168,23 +125,27 @@ __global__ void __launch_bounds__(kThreads) k_dots6(Blk k, const T* __restrict__
   block_partials<ND>(v, k, b);
 }
 
-// hx = u1 hx + u2 hp ; g = gfac (hx - W (u1 x + u2 p)) ; partial |g|^2
+// hx = u1 hx + u2 hp ; g = gfac (hx - W (u1 x + u2 p)) ; partial |g|^2.  Real build: also
+// x = u1 x + u2 p in the same pass for bands whose update k_sc_solve2 did not defer (S_DEF = 0).
 template <typename T, int NC>
-__global__ void __launch_bounds__(kThreads) k_update_hg(Blk k, const T* __restrict__ x, const T* __restrict__ p,
+__global__ void __launch_bounds__(kThreads) k_update_hg(Blk k, T* __restrict__ x, const T* __restrict__ p,
                                                         T* __restrict__ hx, const T* __restrict__ hp,
                                                         T* __restrict__ g, double gfac) {
   BAND_LOOP(k, NC);
   if (SC(k, S_ACT, b) == 0.0) return;
   const double u1 = SC(k, S_U1, b), u2 = SC(k, S_U2, b), W = SC(k, S_W, b);
   const double u1i = SC(k, S_U1I, b), u2i = SC(k, S_U2I, b);
+  const bool upx = NC == 1 && SC(k, S_DEF, b) == 0.0;
   double v[1] = {0.0};
   for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) {
     if (NC == 1) {
       const double h = u1 * (double)hx[off + i] + u2 * (double)hp[off + i];
       const T ht = (T)h;
       hx[off + i] = ht;
-      const T gi = (T)(gfac * ((double)ht - W * (u1 * (double)x[off + i] + u2 * (double)p[off + i])));
+      const double xn = u1 * (double)x[off + i] + u2 * (double)p[off + i];
+      const T gi = (T)(gfac * ((double)ht - W * xn));
       g[off + i] = gi;
+      if (upx) x[off + i] = (T)xn;
       v[0] += (double)gi * (double)gi;
     } else {
       const size_t j = off + 2 * i;
@@ -206,13 +167,28 @@ __global__ void __launch_bounds__(kThreads) k_update_hg(Blk k, const T* __restri
   block_partials<1>(v, k, b);
 }
 
-// x = u1 x + u2 p for accepted bands
+// x = u1 x + u2 p for accepted bands (complex build; real build: the bands whose update was
+// deferred).  Real build, a band k_sc_reject turned down although the estimate let the x update
+// go ahead with H x: x = (x - u2 p) / u1 restores the band up to rounding.
 template <typename T, int NC>
 __global__ void __launch_bounds__(kThreads) k_update_x(Blk k, T* __restrict__ x, const T* __restrict__ p) {
   BAND_LOOP(k, NC);
-  if (SC(k, S_ACT, b) == 0.0 || SC(k, S_ACC, b) == 0.0) return;
+  if (SC(k, S_ACT, b) == 0.0) return;
+  const bool acc = SC(k, S_ACC, b) != 0.0;
   const double u1 = SC(k, S_U1, b), u2 = SC(k, S_U2, b);
   const double u1i = SC(k, S_U1I, b), u2i = SC(k, S_U2I, b);
+  if (NC == 1) {
+    const bool def = SC(k, S_DEF, b) != 0.0;
+    if (acc && def) {
+      for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads)
+        x[off + i] = (T)(u1 * (double)x[off + i] + u2 * (double)p[off + i]);
+    } else if (!acc && !def) {
+      for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads)
+        x[off + i] = (T)(((double)x[off + i] - u2 * (double)p[off + i]) / u1);
+    }
+    return;
+  }
+  if (!acc) return;
   for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) {
     if (NC == 1) {
       x[off + i] = (T)(u1 * (double)x[off + i] + u2 * (double)p[off + i]);
@@ -292,6 +268,7 @@ __global__ void k_sc_solve2(Blk k, double dV) {
     SC(k, S_U2I, b) = 0.0;
     SC(k, S_W, b) = E;
     SC(k, S_E1, b) = E;
+    SC(k, S_DEF, b) = 1.0;
     return;
   }
   // L = U^-H: l11 = 1/u11, l21 = -conj(u12)/(u11 u22), l22 = 1/u22 ; C = L A L^H
@@ -350,6 +327,18 @@ __global__ void k_sc_solve2(Blk k, double dV) {
   SC(k, S_W, b) = W;
   SC(k, S_E1, b) = E;
   SC(k, S_E, b) = W;
+  if (NC == 1) {
+    // |g'|^2 dV after the step, g' = -2 (u1 (hx - W x) + u2 (hp - W p)), from the dots: the x
+    // update may go with the H x / g pass unless the reject test (rb / res > 1e8, k_sc_reject) could
+    // turn the step down; within a factor 1e4 of that test it waits for the exact |g'|^2.
+    const double xx = B11 / dV, px = B12r / dV, pp = B22 / dV, xh = A11 / dV, ph = A12r / dV, pq = A22 / dV;
+    const double hh = sum_part(k, b, 6), hq = sum_part(k, b, 7), qq = sum_part(k, b, 8), xq = sum_part(k, b, 9);
+    const double e11 = hh - 2.0 * W * xh + W * W * xx;
+    const double e12 = hq - W * xq - W * ph + W * W * px;
+    const double e22 = qq - 2.0 * W * pq + W * W * pp;
+    const double est = 4.0 * dV * (z1r * z1r * e11 + 2.0 * z1r * z2r * e12 + z2r * z2r * e22);
+    SC(k, S_DEF, b) = (est > 1.0e4 * SC(k, S_RES, b) || !(est == est)) ? 1.0 : 0.0;
+  }
 }
 
 // residual growth guard (cg_module.f90:360-363)
@@ -668,28 +657,9 @@ __global__ void k_pcs_sc(Blk k, int i, int m, double c0) {
     SC(k, S_MU0 + 2 * i, b) = sum_part(k, b, 1);
     return;
   }
-  double mu[8];
+  double mu[8], xi[5];
   for (int j = 0; j < 2 * m; ++j) mu[j] = SC(k, S_MU0 + j, b);
-  double p[5] = {1.0, 0.0, 0.0, 0.0, 0.0}, r[5] = {1.0, 0.0, 0.0, 0.0, 0.0};
-  double xi[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, f[5];
-  double rr1 = mu[0], rr0;
-  for (int it = 1; it <= m; ++it) {
-    // f = A p = c0 (B p + p); p has degree it - 1, f degree it
-    for (int j = 0; j <= it; ++j) f[j] = c0 * ((j > 0 ? p[j - 1] : 0.0) + (j < it ? p[j] : 0.0));
-    double pAp = 0.0;
-    for (int a = 0; a < it; ++a)
-      for (int c = 0; c <= it; ++c) pAp += p[a] * f[c] * mu[a + c];
-    rr0 = rr1;
-    const double al = rr0 / pAp;
-    for (int j = 0; j < it; ++j) xi[j] += al * p[j];
-    if (it == m) break;
-    for (int j = 0; j <= it; ++j) r[j] -= al * f[j];
-    rr1 = 0.0;
-    for (int a = 0; a <= it; ++a)
-      for (int c = 0; c <= it; ++c) rr1 += r[a] * r[c] * mu[a + c];
-    const double be = rr1 / rr0;
-    for (int j = 0; j <= it; ++j) p[j] = r[j] + be * p[j];
-  }
+  pcs_recurrence(mu, m, c0, xi);
   for (int j = 0; j < m; ++j) SC(k, S_XI0 + j, b) = xi[j];
 }
 
@@ -979,7 +949,8 @@ static int cg_block_run(Ctx& c, int kk, int s, double* h_esp, double* h_res) {
   Blk k;
   k.ng = nreal;
   k.nch = pick_nch(nreal, nbb);
-  RS_TRY(c.ws_red.ensure(sizeof(double) * kPS * (size_t)nbb * pick_nch(nreal, 1)));
+  RS_TRY(c.ws_red.ensure(sizeof(double) *
+                         std::max<size_t>(kPS * (size_t)nbb * pick_nch(nreal, 1), pc_fused_part_doubles(c, nbb))));
   k.sc = c.ws_scal.as<double>();
   k.part = c.ws_red.as<double>();
   T* base = c.ws_cg.as<T>();
@@ -1019,7 +990,11 @@ static int cg_block_run(Ctx& c, int kk, int s, double* h_esp, double* h_res) {
       if (icg == c.p.ncg + 1) break;
       const int pcm = pc_effective(c);
       bool pg_dot = false;  // <PG|G> partials already formed by the preconditioner's last pass
-      if (pcm == RSDFT_PC_NONE) {
+      bool p_done = false;  // rb, beta and p already formed by the fused preconditioner
+      if (pcm == RSDFT_PC_HPRSDFT && std::is_same<T, float>::value && pc_fused_applies(c)) {
+        RS_TRY(pc_fused_step(c, k, reinterpret_cast<const float*>(G), reinterpret_cast<float*>(P), icg == 1 ? 1 : 0));
+        p_done = true;
+      } else if (pcm == RSDFT_PC_NONE) {
         ProfScope ps(c, "cg");
         LAUNCH_E(k_copy<T>, G, PG);
       } else if (pcm == RSDFT_PC_LEARNED && std::is_same<T, float>::value && NC == 1) {
@@ -1033,7 +1008,7 @@ static int cg_block_run(Ctx& c, int kk, int s, double* h_esp, double* h_res) {
         RS_TRY((cggs_block<T, NC>(c, psi, nb, b0, nn, PG)));
         pg_dot = false;
       }
-      {
+      if (!p_done) {
         ProfScope ps(c, "cg");
         if (!pg_dot) LAUNCH_E(k_dot<T>, PG, G, (int)S_ACT);
         LAUNCH_S(k_sc_beta, dV, icg == 1 ? 1 : 0);

@@ -75,6 +75,8 @@ struct Ctx {
   unsigned* d_status = nullptr;
   long long launches = 0;
   int mb_ref = 0;  // bands 1..mb_ref checked for convergence (0: all)
+  int sweep_check = 0;  // rsdft_gpu_sweep convergence: 0 FP64 residual <= tol, 2 eigenvalue change < tol
+  std::vector<double> esp_last;  // Ritz values of the last sweep (sweep_check 2), [s][k][band]
   bool eig_jacobi = false;          // subspace eigensolver: Jacobi (syevj) instead of syevd
   syevjInfo_t syevj = nullptr;
 
@@ -109,7 +111,11 @@ struct Ctx {
   int lpc_fp32 = 0;                // learned PC inference: 0 tensor cores (BF16 activations), 1 FP32 CUDA cores
   int gemm_terms_sm = 3;           // BF16 terms of the overlap / Hsub contractions (mixed precision)
   int gemm_terms_rot = 3;          // BF16 terms of the band rotations (mixed precision)
-  int pc_sstep = 1;                // FP32 precond_hprsdft in s-step form (0: the recurrence form)
+  double sched_res_sm = 0.0;       // sweeps: 2 overlap/Hsub terms while CG's max residual > this (0: off)
+  double sched_res_rot = 0.0;      // sweeps: 2 rotation terms while CG's max residual > this (0: off)
+  long long sched_sweeps = 0;      // (k, s) sweep steps run with reduced terms
+  int pc_sstep = 1;                // FP32 precond_hprsdft: 1 s-step passes, 2 fused z-streamed s-step form
+                                   // inside CG, 0 the recurrence form
   int gemm_wide = 1;               // three-term GEMM tiles 128 x 256 (K blocks of 32), else 128 x 128
   int gemm_tri = 1;                // S by upper-triangle tiles (1), S and Hsub (2), neither (0)
   int rot_update = 0;              // mixed rotation in update form X + X (C - I)

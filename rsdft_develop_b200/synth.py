@@ -162,6 +162,7 @@ class Config:
     nband_range: tuple | None = None  # uneven active band counts per k (seeded)
     reference_form: bool = False       # Dij restricted to equal (l,m) pairs
     dij_sigma: float = 0.5
+    kpoints: tuple | None = None       # explicit reduced k-points (complex16), e.g. a band trajectory
 
     @property
     def L(self) -> float:
@@ -169,7 +170,7 @@ class Config:
 
     @property
     def is_complex(self) -> bool:
-        return self.mp > 0
+        return self.mp > 0 or self.kpoints is not None
 
 
 CONFIGS = {
@@ -391,7 +392,9 @@ def make_problem(cfg: Config | str, cache: bool = True) -> Problem:
         return _PROBLEM_CACHE[key]
     rng = np.random.default_rng(cfg.seed + 1000003 * cfg.n)
     vloc = _gaussian_vloc(cfg, rng)
-    if cfg.mp > 0:
+    if cfg.kpoints is not None:
+        kbb = np.array(cfg.kpoints, dtype=np.float64).reshape(-1, 3)
+    elif cfg.mp > 0:
         kbb = monkhorst_pack(cfg.mp)
     else:
         kbb = np.zeros((1, 3))
