@@ -208,6 +208,35 @@ int rsdft_gpu_init_sweep(int mb_ref);
  * check's values of the last sweep. */
 int rsdft_gpu_set_sweep_check(int iconv_check);
 
+/* ---- SCF pieces (the caller of the band update, src/scf_module.f90:85-563) ----
+ * V_ion: the fixed local potential (localpot_module Vion); Vloc(:,s) = Vion + Vh + Vxc(:,s)
+ * (src/localpot_module.f90:209-215) once rsdft_gpu_potential has run. */
+int rsdft_gpu_set_vion(const double* vion, int ml);
+/* The device density rho(ML, nspin) from the host (initial density, restart) / back to the
+ * host with the Hartree and XC potentials of the last rsdft_gpu_potential (any may be NULL). */
+int rsdft_gpu_set_rho(const double* rho, int ml);
+int rsdft_gpu_get_rho(double* rho, double* vh, double* vxc);
+/* calc_density (src/density_module.f90): rho(:,s) = sum_{k,n} occ(n,k,s) |unk(:,n,k,s)|^2 from
+ * the resident bands; occ (MB, MK, MS) host, Fortran order, k-point weights and spin factor
+ * included as calc_fermi leaves them. */
+int rsdft_gpu_density(const double* occ);
+/* normalize_density: scale rho to nelec electrons. */
+int rsdft_gpu_normalize_density(double nelec);
+/* calc_hartree (FFT Poisson: V_H(G) = 4 pi rho(G)/|G|^2, G != 0) + calc_xc (LDA PZ81,
+ * src/xc/xc_ldapz81_module.f90) from the device density, then Vloc(:,s) = Vion + Vh + Vxc(:,s)
+ * on the device.  ene (4, may be NULL): E_H = 1/2 int rho V_H, E_xc, int rho V_xc, charge. */
+int rsdft_gpu_potential(double* ene);
+/* init_mixing (src/mixing/mixing_module.f90:70-142) for IMIX = 10 (Pulay on the density) with
+ * history mmix (1..8) and beta: Xold = (rho, Vloc) of now. */
+int rsdft_gpu_init_mixing(int mmix, double beta);
+/* calc_sqerr (src/mixing/mixing_module.f90:319-341): sqerr(1:MS) of Vloc, sqerr(MS+1:2MS) of rho
+ * against Xold, each sum of squares / ML. */
+int rsdft_gpu_sqerr(double* sqerr);
+/* perform_mixing (src/mixing/mixing_module.f90:145-298) with pulay_mixing
+ * (src/mixing/mixing_pulay_module.f90:29-111): the device density becomes the mixed one
+ * (beta search for beta > 1 as the reference); beta_used (may be NULL) receives the beta taken. */
+int rsdft_gpu_mix_density(double* beta_used);
+
 /* ---- learned preconditioner (no counterpart in the reference) ----
  * A 4-layer 3-D convolutional network, channels 1-16-16-16-1, 3x3x3 kernels, no biases, tanh
  * between layers, BF16 weights with FP32 accumulation.  With pc_mode RSDFT_PC_LEARNED and
@@ -284,8 +313,9 @@ int rsdft_gpu_set_gemm_terms(int overlap_terms, int rotation_terms);
 /* Precision schedule of rsdft_gpu_sweep (mixed precision): the Gram-Schmidt / subspace overlap and
  * Hsub contractions use two BF16 terms while CG's largest residual of the (k, s) in that sweep
  * is above res_sm, the band rotation while it is above res_rot; below, the terms set by
- * rsdft_gpu_set_gemm_terms.  0 switches a threshold off (the default).  No counterpart in the
- * reference (one precision per build). */
+ * rsdft_gpu_set_gemm_terms.  0 switches a threshold off; the defaults are res_sm = 1e-2 and
+ * res_rot = 1e-4 (the two-term noise, about 2^-16 relative per product, stays well below the
+ * residuals of those sweeps).  No counterpart in the reference (one precision per build). */
 int rsdft_gpu_set_gemm_schedule(double res_sm, double res_rot);
 /* Tiling of the three-term tensor-core contractions, flags (default 7): bit 0 set, 128 x 256
  * output tiles over K blocks of 32 (else 128 x 128 over 64); bit 1 set, the overlap S of the

@@ -54,6 +54,8 @@ EXPORTS = [
     "rsdft_gpu_residual", "rsdft_gpu_precond_d", "rsdft_gpu_precond_f", "rsdft_gpu_set_pc_form", "rsdft_gpu_sweep", "rsdft_gpu_profile",
     "rsdft_gpu_profile_get", "rsdft_gpu_kernel_launches", "rsdft_gpu_selftest_gemm", "rsdft_gpu_set_gemm_terms", "rsdft_gpu_set_gemm_tile", "rsdft_gpu_set_nl_form", "rsdft_gpu_init_sweep", "rsdft_gpu_set_wait_polls", "rsdft_gpu_set_precision", "rsdft_gpu_set_cggs", "rsdft_gpu_set_sweep_check", "rsdft_gpu_set_gemm_schedule",
     "rsdft_gpu_hamiltonian_noalloc_d",
+    "rsdft_gpu_set_vion", "rsdft_gpu_set_rho", "rsdft_gpu_get_rho", "rsdft_gpu_density", "rsdft_gpu_normalize_density",
+    "rsdft_gpu_potential", "rsdft_gpu_init_mixing", "rsdft_gpu_sqerr", "rsdft_gpu_mix_density",
     "rsdft_gpu_lpc_init", "rsdft_gpu_lpc_set_weights", "rsdft_gpu_lpc_get_weights", "rsdft_gpu_lpc_forward",
     "rsdft_gpu_lpc_loss_grad", "rsdft_gpu_lpc_dataset", "rsdft_gpu_lpc_harvest", "rsdft_gpu_lpc_dataset_get",
     "rsdft_gpu_lpc_dataset_add", "rsdft_gpu_lpc_train", "rsdft_gpu_lpc_precond_f", "rsdft_gpu_lpc_status",
@@ -103,6 +105,9 @@ def load_library(path: str = LIB_PATH):
         "rsdft_gpu_set_wf_z": [i, i, vp, i, i], "rsdft_gpu_get_wf_z": [i, i, vp, i, i],
         "rsdft_gpu_random_wf": [i, i, C.c_uint64],
         "rsdft_gpu_write_wf": [C.c_char_p, i, vp, vp, vp, vp], "rsdft_gpu_read_wf": [C.c_char_p, vp],
+        "rsdft_gpu_set_vion": [vp, i], "rsdft_gpu_set_rho": [vp, i], "rsdft_gpu_get_rho": [vp, vp, vp],
+        "rsdft_gpu_density": [vp], "rsdft_gpu_normalize_density": [d], "rsdft_gpu_potential": [vp],
+        "rsdft_gpu_init_mixing": [i, d], "rsdft_gpu_sqerr": [vp], "rsdft_gpu_mix_density": [vp],
         "rsdft_gpu_hamiltonian_d": [i, i, vp, vp, i, i, i], "rsdft_gpu_hamiltonian_z": [i, i, vp, vp, i, i, i],
         "rsdft_gpu_hamiltonian_f": [i, i, vp, vp, i, i, i], "rsdft_gpu_hamiltonian_c": [i, i, vp, vp, i, i, i],
         "rsdft_gpu_conjugate_gradient": [i, i, vp, vp], "rsdft_gpu_gram_schmidt": [i, i],
@@ -311,6 +316,51 @@ class BandUpdate:
         occ = np.zeros((mb, nk, int(self.params.nspin)), order="F")
         _call(self.lib.rsdft_gpu_read_wf, path.encode(), occ.ctypes.data_as(C.c_void_p))
         return occ
+
+    # ---- SCF pieces ----
+    def set_vion(self, vion: np.ndarray):
+        v = np.ascontiguousarray(vion, dtype=np.float64)
+        _call(self.lib.rsdft_gpu_set_vion, _ptr(v), self.prob.ng)
+
+    def set_rho(self, rho: np.ndarray):
+        r = np.ascontiguousarray(rho, dtype=np.float64).reshape(-1)
+        assert r.size == self.prob.ng * self.params.nspin
+        _call(self.lib.rsdft_gpu_set_rho, _ptr(r), self.prob.ng)
+
+    def get_rho(self):
+        ns = int(self.params.nspin)
+        rho = np.zeros((ns, self.prob.ng))
+        vh = np.zeros(self.prob.ng)
+        vxc = np.zeros((ns, self.prob.ng))
+        _call(self.lib.rsdft_gpu_get_rho, _ptr(rho), _ptr(vh), _ptr(vxc))
+        return rho, vh, vxc
+
+    def density(self, occ: np.ndarray):
+        """occ: (nspin, nk, mb) occupations (k weights and spin factor included)."""
+        o = np.ascontiguousarray(occ, dtype=np.float64)
+        assert o.shape == (int(self.params.nspin), int(self.prob.nk), int(self.params.mb))
+        _call(self.lib.rsdft_gpu_density, _ptr(o))
+
+    def normalize_density(self, nelec: float):
+        _call(self.lib.rsdft_gpu_normalize_density, float(nelec))
+
+    def potential(self) -> np.ndarray:
+        ene = np.zeros(4)
+        _call(self.lib.rsdft_gpu_potential, _ptr(ene))
+        return ene
+
+    def init_mixing(self, mmix: int = 4, beta: float = 1.1):
+        _call(self.lib.rsdft_gpu_init_mixing, int(mmix), float(beta))
+
+    def sqerr(self) -> np.ndarray:
+        e = np.zeros(2 * int(self.params.nspin))
+        _call(self.lib.rsdft_gpu_sqerr, _ptr(e))
+        return e
+
+    def mix_density(self) -> float:
+        b = np.zeros(1)
+        _call(self.lib.rsdft_gpu_mix_density, _ptr(b))
+        return float(b[0])
 
     def hamiltonian(self, tpsi: np.ndarray, k: int = 1, s: int = 1, fp32: bool = False) -> np.ndarray:
         """htpsi = H tpsi for a host block tpsi[nb][ML0] (hamiltonian(tpsi,htpsi,n,k,s))."""

@@ -76,7 +76,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         lib64 = os.path.join(cuda, "lib64")
         tmp = OUT + ".tmp"  # linked aside, then moved into place in one step
         cmd = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", tmp, *objs,
-               "-L" + lib64, "-lcublas", "-lcusolver", "-Xlinker", "-rpath," + lib64]
+               "-L" + lib64, "-lcublas", "-lcusolver", "-lcufft", "-Xlinker", "-rpath," + lib64]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)

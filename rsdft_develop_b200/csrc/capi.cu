@@ -275,6 +275,7 @@ static void destroy(Ctx* c) {
     pk.gw64.release(); pk.gw32.release(); pk.ru64.release(); pk.ru32.release();
   }
   for (auto& w : c->wf) w.psi.release();
+  scf_release(*c);
   if (c->d_status) cudaFree(c->d_status);
   if (c->cublas) cublasDestroy(c->cublas);
   if (c->syevj) cusolverDnDestroySyevjInfo(c->syevj);

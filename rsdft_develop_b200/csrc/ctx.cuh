@@ -62,6 +62,16 @@ struct ProfEntry {
   double flops = 0.0;   // algorithmic flops of the bracketed launches
 };
 
+// device state of the SCF pieces (scf.cu): density, potentials, Pulay history
+struct ScfState {
+  DBuf vion, rho, vh, vxc, occ, work, part, ones;
+  DBuf xin, xou, xin_bak, xou_bak, xold_f, xold_g, h, f0, w;
+  bool have_rho = false, mixing = false, plans = false;
+  int plan_f = 0, plan_b = 0;   // cuFFT handles (D2Z, Z2D)
+  int mmix = 4, mmix_count = 0;
+  double beta = 1.1, dif0 = 0.0;
+};
+
 struct Ctx {
   rsdft_gpu_params p{};
   size_t ng = 0;
@@ -80,6 +90,7 @@ struct Ctx {
   bool eig_jacobi = false;          // subspace eigensolver: Jacobi (syevj) instead of syevd
   syevjInfo_t syevj = nullptr;
 
+  ScfState scf;
   std::vector<KPoint> kp;
   DBuf vloc64, vloc32;             // [nspin][ng]
   std::vector<bool> vloc_set;
@@ -111,8 +122,8 @@ struct Ctx {
   int lpc_fp32 = 0;                // learned PC inference: 0 tensor cores (BF16 activations), 1 FP32 CUDA cores
   int gemm_terms_sm = 3;           // BF16 terms of the overlap / Hsub contractions (mixed precision)
   int gemm_terms_rot = 3;          // BF16 terms of the band rotations (mixed precision)
-  double sched_res_sm = 0.0;       // sweeps: 2 overlap/Hsub terms while CG's max residual > this (0: off)
-  double sched_res_rot = 0.0;      // sweeps: 2 rotation terms while CG's max residual > this (0: off)
+  double sched_res_sm = 1e-2;      // sweeps: 2 overlap/Hsub terms while CG's max residual > this (0: off)
+  double sched_res_rot = 1e-4;     // sweeps: 2 rotation terms while CG's max residual > this (0: off)
   long long sched_sweeps = 0;      // (k, s) sweep steps run with reduced terms
   int pc_sstep = 1;                // FP32 precond_hprsdft: 1 s-step passes, 2 fused z-streamed s-step form
                                    // inside CG, 0 the recurrence form
@@ -173,6 +184,7 @@ int kinetic_shifted(Ctx& c, const float* x, float* y, size_t ld, int nb, double 
 // ---- learned preconditioner (lpc.cu) ----
 bool lpc_ready();
 void lpc_release();
+void scf_release(Ctx& c);
 int lpc_apply(Ctx& c, const float* g, float* pg, int nb);
 int pc_effective(const Ctx& c);
 

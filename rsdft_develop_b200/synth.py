@@ -135,6 +135,47 @@ def kinetic_coefficients(h: float, md: int, kcart: np.ndarray) -> dict:
                 coef_nabk=coef_nabk, const_k2=const_k2, zcoef_kin=zcoef, ggg=ggg)
 
 
+def generate_bz(mmm, use_inversion: int = 1):
+    """k-points and weights of generate_bz without symmetry operations (src/bz_module.f90:65-189,
+    Monkhorst_Pack :530-557): the MP mesh on the common integer grid of nk points per axis, k and
+    -k merged (weight 2) unless use_inversion < 1, in the reference's loop order.  mmm = (0, 0, 0)
+    is Gamma-point sampling.  Returns (kbb (N, 3) reduced, weights (N,))."""
+    m1 = [int(x) for x in mmm]
+    if all(x == 0 for x in m1):
+        nk, mm1, mm2 = 2, [2, 2, 2], [2, 2, 2]
+    else:
+        lcm12 = m1[0] * m1[1] // math.gcd(m1[0], m1[1])
+        nk = 2 * (lcm12 * m1[2] // math.gcd(lcm12, m1[2]))
+        mm2 = [nk // x for x in m1]
+        mm1 = [mm2[i] * m1[i] if m1[i] % 2 == 1 else (nk // 2) // m1[i] + mm2[i] * m1[i] for i in range(3)]
+    iw0 = -1 if use_inversion >= 1 else 1
+    seen = set()
+    pts, wts = [], []
+    for i1 in range(-mm1[0], mm1[0] + 1, mm2[0]):
+        for i2 in range(-mm1[1], mm1[1] + 1, mm2[1]):
+            for i3 in range(-mm1[2], mm1[2] + 1, mm2[2]):
+                for iw in range(1, iw0 - 1, -2):
+                    p = []
+                    for v in (i1 * iw, i2 * iw, i3 * iw):
+                        q = int(math.fmod(v, nk))
+                        if q > nk // 2:
+                            q -= nk
+                        if q <= -nk // 2:
+                            q += nk
+                        p.append(q)
+                    p = tuple(p)
+                    if p in seen:
+                        break
+                    if iw == 1:
+                        pts.append(p)
+                        wts.append(1)
+                    else:
+                        wts[-1] = 2
+                    seen.add(p)
+    mmbz = len(seen)
+    return np.array(pts, dtype=np.float64) / nk, np.array(wts, dtype=np.float64) / mmbz
+
+
 def monkhorst_pack(n: int) -> np.ndarray:
     """Reduced Monkhorst-Pack points ``(2r - n - 1)/(2n)`` per axis (src/bz_module.f90:530-557)."""
     r = np.arange(1, n + 1)
