@@ -26,6 +26,33 @@
 
 namespace rsdft {
 
+// 16 bytes of T (4 FP32 or 2 FP64 reals): the unit every CG and preconditioner thread loads and
+// stores, so that each memory instruction moves 16 bytes.
+template <typename T>
+struct Vec {
+  static constexpr int W = 16 / (int)sizeof(T);
+  T v[W];
+};
+template <typename T>
+__device__ __forceinline__ Vec<T> ldv(const T* p) {
+  Vec<T> r;
+  if constexpr (sizeof(T) == 4) {
+    const float4 a = *reinterpret_cast<const float4*>(p);
+    r.v[0] = a.x; r.v[1] = a.y; r.v[2] = a.z; r.v[3] = a.w;
+  } else {
+    const double2 a = *reinterpret_cast<const double2*>(p);
+    r.v[0] = a.x; r.v[1] = a.y;
+  }
+  return r;
+}
+template <typename T>
+__device__ __forceinline__ void stv(T* p, const Vec<T>& r) {
+  if constexpr (sizeof(T) == 4)
+    *reinterpret_cast<float4*>(p) = make_float4(r.v[0], r.v[1], r.v[2], r.v[3]);
+  else
+    *reinterpret_cast<double2*>(p) = make_double2(r.v[0], r.v[1]);
+}
+
 // NC = 2 loops run over complex points (pairs of reals)
 #define BAND_LOOP(k, NC)                                                    \
   const int b = blockIdx.y;                                                 \
@@ -34,16 +61,32 @@ namespace rsdft {
   const size_t per = (npt + (k).nch - 1) / (k).nch;                         \
   const size_t i0 = per * blockIdx.x, i1 = min(npt, i0 + per);
 
+// Elementwise walk of a band in 16-byte groups of VW reals (complex bands: VW / 2 points per
+// group); the band's groups are split into k.nch contiguous chunks, one per CTA.  Bands hold a
+// multiple of VW reals (the stencils require N1 to be a multiple of VW).
+#define GROUP_LOOP(k, T)                                                    \
+  constexpr int VW = Vec<T>::W;                                             \
+  const int b = blockIdx.y;                                                 \
+  const size_t off = (size_t)b * (k).ng;                                    \
+  const size_t ngr = (k).ng / VW;                                           \
+  const size_t per = (ngr + (k).nch - 1) / (k).nch;                         \
+  const size_t g0 = per * blockIdx.x, g1 = min(ngr, g0 + per);
+
 // ---------------------------------------------------------------------------
-// elementwise + reduction kernels on the real view
+// elementwise + reduction kernels on the real view, 16-byte accesses
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_dot(Blk k, const T* __restrict__ a, const T* __restrict__ bb,
                                                   int act_idx) {
-  BAND_LOOP(k, 1);
+  GROUP_LOOP(k, T);
   if (act_idx >= 0 && SC(k, act_idx, b) == 0.0) return;
   double v[1] = {0.0};
-  for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) v[0] += (double)a[off + i] * (double)bb[off + i];
+  for (size_t gi = g0 + threadIdx.x; gi < g1; gi += kThreads) {
+    const size_t e = off + gi * VW;
+    const Vec<T> x = ldv(a + e), y = ldv(bb + e);
+#pragma unroll
+    for (int i = 0; i < VW; ++i) v[0] += (double)x.v[i] * (double)y.v[i];
+  }
   block_partials<1>(v, k, b);
 }
 
@@ -51,75 +94,93 @@ __global__ void __launch_bounds__(kThreads) k_dot(Blk k, const T* __restrict__ a
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_make_g(Blk k, const T* __restrict__ x, const T* __restrict__ hx,
                                                      T* __restrict__ g, double gfac) {
-  BAND_LOOP(k, 1);
+  GROUP_LOOP(k, T);
   if (SC(k, S_ACT, b) == 0.0) return;
   const double E = SC(k, S_E, b);
   double v[1] = {0.0};
-  for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) {
-    const T gi = (T)(gfac * ((double)hx[off + i] - E * (double)x[off + i]));
-    g[off + i] = gi;
-    v[0] += (double)gi * (double)gi;
+  for (size_t gi = g0 + threadIdx.x; gi < g1; gi += kThreads) {
+    const size_t e = off + gi * VW;
+    const Vec<T> xv = ldv(x + e), hv = ldv(hx + e);
+    Vec<T> gv;
+#pragma unroll
+    for (int i = 0; i < VW; ++i) {
+      gv.v[i] = (T)(gfac * ((double)hv.v[i] - E * (double)xv.v[i]));
+      v[0] += (double)gv.v[i] * (double)gv.v[i];
+    }
+    stv(g + e, gv);
   }
   block_partials<1>(v, k, b);
 }
 
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_copy(Blk k, const T* __restrict__ src, T* __restrict__ dst) {
-  BAND_LOOP(k, 1);
+  GROUP_LOOP(k, T);
   if (SC(k, S_ACT, b) == 0.0) return;
-  for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) dst[off + i] = src[off + i];
+  for (size_t gi = g0 + threadIdx.x; gi < g1; gi += kThreads) stv(dst + off + gi * VW, ldv(src + off + gi * VW));
 }
 
 // p = Pg + beta p
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_make_p(Blk k, const T* __restrict__ pg, T* __restrict__ p, int first) {
-  BAND_LOOP(k, 1);
+  GROUP_LOOP(k, T);
   if (SC(k, S_ACT, b) == 0.0) return;
   const T beta = (T)SC(k, S_BETA, b);
-  if (first) {
-    for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) p[off + i] = pg[off + i];
-  } else {
-    for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) p[off + i] = pg[off + i] + beta * p[off + i];
+  for (size_t gi = g0 + threadIdx.x; gi < g1; gi += kThreads) {
+    const size_t e = off + gi * VW;
+    Vec<T> pv = ldv(pg + e);
+    if (!first) {
+      const Vec<T> po = ldv(p + e);
+#pragma unroll
+      for (int i = 0; i < VW; ++i) pv.v[i] = pv.v[i] + beta * po.v[i];
+    }
+    stv(p + e, pv);
   }
 }
 
 // the six dot products of the line minimisation (cg_module.f90:288-296, :623-630);
-// NC = 2 adds Im<p|x> and Im<p|hx> in slots 6 and 7
+// NC = 1 adds <hx|hx>, <hx|hp>, <hp|hp>, <x|hp> for the estimate of |g|^2 after the step (the
+// reject test ahead of the fused x update); NC = 2 adds Im<p|x> and Im<p|hx> in slots 6 and 7
 template <typename T, int NC>
 __global__ void __launch_bounds__(kThreads) k_dots6(Blk k, const T* __restrict__ x, const T* __restrict__ p,
                                                     const T* __restrict__ hx, const T* __restrict__ hp) {
-  BAND_LOOP(k, NC);
+  GROUP_LOOP(k, T);
   if (SC(k, S_ACT, b) == 0.0) return;
   constexpr int ND = NC == 1 ? 10 : 8;
   double v[ND];
 #pragma unroll
   for (int d = 0; d < ND; ++d) v[d] = 0.0;
-  for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) {
-    if (NC == 1) {
-      const double xi = x[off + i], pi = p[off + i], hxi = hx[off + i], hpi = hp[off + i];
-      v[0] += xi * xi;
-      v[1] += pi * xi;
-      v[2] += pi * pi;
-      v[3] += xi * hxi;
-      v[4] += pi * hxi;
-      v[5] += pi * hpi;
-      // for the estimate of |g|^2 after the step (the reject test ahead of the fused x update)
-      v[6 % ND] += hxi * hxi;
-      v[7 % ND] += hxi * hpi;
-      v[8 % ND] += hpi * hpi;
-      v[9 % ND] += xi * hpi;
+  for (size_t gi = g0 + threadIdx.x; gi < g1; gi += kThreads) {
+    const size_t e = off + gi * VW;
+    const Vec<T> xv = ldv(x + e), pv = ldv(p + e), hv = ldv(hx + e), qv = ldv(hp + e);
+    if constexpr (NC == 1) {
+#pragma unroll
+      for (int i = 0; i < VW; ++i) {
+        const double xi = xv.v[i], pi = pv.v[i], hxi = hv.v[i], hpi = qv.v[i];
+        v[0] += xi * xi;
+        v[1] += pi * xi;
+        v[2] += pi * pi;
+        v[3] += xi * hxi;
+        v[4] += pi * hxi;
+        v[5] += pi * hpi;
+        v[6 % ND] += hxi * hxi;
+        v[7 % ND] += hxi * hpi;
+        v[8 % ND] += hpi * hpi;
+        v[9 % ND] += xi * hpi;
+      }
     } else {
-      const size_t j = off + 2 * i;
-      const double xr = x[j], xm = x[j + 1], pr = p[j], pm = p[j + 1];
-      const double hr = hx[j], hm = hx[j + 1], qr = hp[j], qm = hp[j + 1];
-      v[0] += xr * xr + xm * xm;
-      v[1] += pr * xr + pm * xm;
-      v[2] += pr * pr + pm * pm;
-      v[3] += xr * hr + xm * hm;
-      v[4] += pr * hr + pm * hm;
-      v[5] += pr * qr + pm * qm;
-      v[ND - 2] += pr * xm - pm * xr;
-      v[ND - 1] += pr * hm - pm * hr;
+#pragma unroll
+      for (int j = 0; j < VW / 2; ++j) {
+        const double xr = xv.v[2 * j], xm = xv.v[2 * j + 1], pr = pv.v[2 * j], pm = pv.v[2 * j + 1];
+        const double hr = hv.v[2 * j], hm = hv.v[2 * j + 1], qr = qv.v[2 * j], qm = qv.v[2 * j + 1];
+        v[0] += xr * xr + xm * xm;
+        v[1] += pr * xr + pm * xm;
+        v[2] += pr * pr + pm * pm;
+        v[3] += xr * hr + xm * hm;
+        v[4] += pr * hr + pm * hm;
+        v[5] += pr * qr + pm * qm;
+        v[ND - 2] += pr * xm - pm * xr;
+        v[ND - 1] += pr * hm - pm * hr;
+      }
     }
   }
   block_partials<ND>(v, k, b);
@@ -131,38 +192,45 @@ template <typename T, int NC>
 __global__ void __launch_bounds__(kThreads) k_update_hg(Blk k, T* __restrict__ x, const T* __restrict__ p,
                                                         T* __restrict__ hx, const T* __restrict__ hp,
                                                         T* __restrict__ g, double gfac) {
-  BAND_LOOP(k, NC);
+  GROUP_LOOP(k, T);
   if (SC(k, S_ACT, b) == 0.0) return;
   const double u1 = SC(k, S_U1, b), u2 = SC(k, S_U2, b), W = SC(k, S_W, b);
   const double u1i = SC(k, S_U1I, b), u2i = SC(k, S_U2I, b);
   const bool upx = NC == 1 && SC(k, S_DEF, b) == 0.0;
   double v[1] = {0.0};
-  for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) {
-    if (NC == 1) {
-      const double h = u1 * (double)hx[off + i] + u2 * (double)hp[off + i];
-      const T ht = (T)h;
-      hx[off + i] = ht;
-      const double xn = u1 * (double)x[off + i] + u2 * (double)p[off + i];
-      const T gi = (T)(gfac * ((double)ht - W * xn));
-      g[off + i] = gi;
-      if (upx) x[off + i] = (T)xn;
-      v[0] += (double)gi * (double)gi;
+  for (size_t gi = g0 + threadIdx.x; gi < g1; gi += kThreads) {
+    const size_t e = off + gi * VW;
+    const Vec<T> hv = ldv(hx + e), qv = ldv(hp + e), xv = ldv(x + e), pv = ldv(p + e);
+    Vec<T> nh, gv, xn;
+    if constexpr (NC == 1) {
+#pragma unroll
+      for (int i = 0; i < VW; ++i) {
+        const T ht = (T)(u1 * (double)hv.v[i] + u2 * (double)qv.v[i]);
+        nh.v[i] = ht;
+        const double xnd = u1 * (double)xv.v[i] + u2 * (double)pv.v[i];
+        xn.v[i] = (T)xnd;
+        gv.v[i] = (T)(gfac * ((double)ht - W * xnd));
+        v[0] += (double)gv.v[i] * (double)gv.v[i];
+      }
     } else {
-      const size_t j = off + 2 * i;
-      const double hr = hx[j], hm = hx[j + 1], qr = hp[j], qm = hp[j + 1];
-      const T nr = (T)(u1 * hr - u1i * hm + u2 * qr - u2i * qm);
-      const T nm = (T)(u1 * hm + u1i * hr + u2 * qm + u2i * qr);
-      hx[j] = nr;
-      hx[j + 1] = nm;
-      const double xr = x[j], xm = x[j + 1], pr = p[j], pm = p[j + 1];
-      const double yr = u1 * xr - u1i * xm + u2 * pr - u2i * pm;
-      const double ym = u1 * xm + u1i * xr + u2 * pm + u2i * pr;
-      const T gr = (T)(gfac * ((double)nr - W * yr));
-      const T gm = (T)(gfac * ((double)nm - W * ym));
-      g[j] = gr;
-      g[j + 1] = gm;
-      v[0] += (double)gr * (double)gr + (double)gm * (double)gm;
+#pragma unroll
+      for (int j = 0; j < VW / 2; ++j) {
+        const double hr = hv.v[2 * j], hm = hv.v[2 * j + 1], qr = qv.v[2 * j], qm = qv.v[2 * j + 1];
+        const T nr = (T)(u1 * hr - u1i * hm + u2 * qr - u2i * qm);
+        const T nm = (T)(u1 * hm + u1i * hr + u2 * qm + u2i * qr);
+        nh.v[2 * j] = nr;
+        nh.v[2 * j + 1] = nm;
+        const double xr = xv.v[2 * j], xm = xv.v[2 * j + 1], pr = pv.v[2 * j], pm = pv.v[2 * j + 1];
+        const double yr = u1 * xr - u1i * xm + u2 * pr - u2i * pm;
+        const double ym = u1 * xm + u1i * xr + u2 * pm + u2i * pr;
+        gv.v[2 * j] = (T)(gfac * ((double)nr - W * yr));
+        gv.v[2 * j + 1] = (T)(gfac * ((double)nm - W * ym));
+        v[0] += (double)gv.v[2 * j] * (double)gv.v[2 * j] + (double)gv.v[2 * j + 1] * (double)gv.v[2 * j + 1];
+      }
     }
+    stv(hx + e, nh);
+    stv(g + e, gv);
+    if (upx) stv(x + e, xn);
   }
   block_partials<1>(v, k, b);
 }
@@ -172,32 +240,39 @@ __global__ void __launch_bounds__(kThreads) k_update_hg(Blk k, T* __restrict__ x
 // go ahead with H x: x = (x - u2 p) / u1 restores the band up to rounding.
 template <typename T, int NC>
 __global__ void __launch_bounds__(kThreads) k_update_x(Blk k, T* __restrict__ x, const T* __restrict__ p) {
-  BAND_LOOP(k, NC);
+  GROUP_LOOP(k, T);
   if (SC(k, S_ACT, b) == 0.0) return;
   const bool acc = SC(k, S_ACC, b) != 0.0;
   const double u1 = SC(k, S_U1, b), u2 = SC(k, S_U2, b);
   const double u1i = SC(k, S_U1I, b), u2i = SC(k, S_U2I, b);
-  if (NC == 1) {
+  if constexpr (NC == 1) {
     const bool def = SC(k, S_DEF, b) != 0.0;
-    if (acc && def) {
-      for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads)
-        x[off + i] = (T)(u1 * (double)x[off + i] + u2 * (double)p[off + i]);
-    } else if (!acc && !def) {
-      for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads)
-        x[off + i] = (T)(((double)x[off + i] - u2 * (double)p[off + i]) / u1);
+    const bool undo = !acc && !def;
+    if (!(acc && def) && !undo) return;
+    for (size_t gi = g0 + threadIdx.x; gi < g1; gi += kThreads) {
+      const size_t e = off + gi * VW;
+      Vec<T> xv = ldv(x + e);
+      const Vec<T> pv = ldv(p + e);
+#pragma unroll
+      for (int i = 0; i < VW; ++i)
+        xv.v[i] = undo ? (T)(((double)xv.v[i] - u2 * (double)pv.v[i]) / u1)
+                       : (T)(u1 * (double)xv.v[i] + u2 * (double)pv.v[i]);
+      stv(x + e, xv);
     }
     return;
   }
   if (!acc) return;
-  for (size_t i = i0 + threadIdx.x; i < i1; i += kThreads) {
-    if (NC == 1) {
-      x[off + i] = (T)(u1 * (double)x[off + i] + u2 * (double)p[off + i]);
-    } else {
-      const size_t j = off + 2 * i;
-      const double xr = x[j], xm = x[j + 1], pr = p[j], pm = p[j + 1];
-      x[j] = (T)(u1 * xr - u1i * xm + u2 * pr - u2i * pm);
-      x[j + 1] = (T)(u1 * xm + u1i * xr + u2 * pm + u2i * pr);
+  for (size_t gi = g0 + threadIdx.x; gi < g1; gi += kThreads) {
+    const size_t e = off + gi * VW;
+    Vec<T> xv = ldv(x + e);
+    const Vec<T> pv = ldv(p + e);
+#pragma unroll
+    for (int j = 0; j < VW / 2; ++j) {
+      const double xr = xv.v[2 * j], xm = xv.v[2 * j + 1], pr = pv.v[2 * j], pm = pv.v[2 * j + 1];
+      xv.v[2 * j] = (T)(u1 * xr - u1i * xm + u2 * pr - u2i * pm);
+      xv.v[2 * j + 1] = (T)(u1 * xm + u1i * xr + u2 * pm + u2i * pr);
     }
+    stv(x + e, xv);
   }
 }
 
@@ -365,33 +440,6 @@ struct PcCoef {
   int n1, n2, n3, nc;
 };
 
-// 16 bytes of T (4 FP32 or 2 FP64 reals): the unit every preconditioner thread loads and
-// stores, so that each memory instruction moves 16 bytes.
-template <typename T>
-struct Vec {
-  static constexpr int W = 16 / (int)sizeof(T);
-  T v[W];
-};
-template <typename T>
-__device__ __forceinline__ Vec<T> ldv(const T* p) {
-  Vec<T> r;
-  if constexpr (sizeof(T) == 4) {
-    const float4 a = *reinterpret_cast<const float4*>(p);
-    r.v[0] = a.x; r.v[1] = a.y; r.v[2] = a.z; r.v[3] = a.w;
-  } else {
-    const double2 a = *reinterpret_cast<const double2*>(p);
-    r.v[0] = a.x; r.v[1] = a.y;
-  }
-  return r;
-}
-template <typename T>
-__device__ __forceinline__ void stv(T* p, const Vec<T>& r) {
-  if constexpr (sizeof(T) == 4)
-    *reinterpret_cast<float4*>(p) = make_float4(r.v[0], r.v[1], r.v[2], r.v[3]);
-  else
-    *reinterpret_cast<double2*>(p) = make_double2(r.v[0], r.v[1]);
-}
-
 // Walk of the CTA's chunk of x-rows (rows of n1 * NCP reals) in groups of W consecutive reals,
 // consecutive threads on consecutive groups; per group the periodic neighbour offsets of its
 // row (y, z) and the offsets xl / xr, from the group start, of the reals just left and right
@@ -406,9 +454,13 @@ __device__ __forceinline__ void stv(T* p, const Vec<T>& r) {
   const int per = (nrow + (k).nch - 1) / (k).nch;                                                \
   const int r0 = per * blockIdx.x, r1 = min(nrow, r0 + per);                                     \
   const long long pln = (long long)(q).n2 * L;                                                   \
-  for (int t = r0 * NGR + (int)threadIdx.x; t < r1 * NGR; t += kThreads) {                         \
-    const int row = t / NGR, gq = t - row * NGR;                                                     \
-    const int i2 = row % (q).n2, i3 = row / (q).n2;                                              \
+  /* (row, group) of the thread's first item, then advanced by kThreads items per step without \
+     division: the step is srow rows and sg groups */                                            \
+  const int srow = kThreads / NGR, sg = kThreads - srow * NGR;                                  \
+  int row = r0 + (int)threadIdx.x / NGR, gq = (int)threadIdx.x - ((int)threadIdx.x / NGR) * NGR;  \
+  const int pc_n2 = (q).n2;                                                                      \
+  int i2 = row % pc_n2, i3 = row / pc_n2;                                                        \
+  for (; row < r1; ) {                                                                           \
     const long long ym = i2 == 0 ? (long long)((q).n2 - 1) * L : -(long long)L;                  \
     const long long yp = i2 == (q).n2 - 1 ? -(long long)((q).n2 - 1) * L : (long long)L;         \
     const long long zm = i3 == 0 ? (long long)((q).n3 - 1) * pln : -pln;                         \
@@ -416,7 +468,20 @@ __device__ __forceinline__ void stv(T* p, const Vec<T>& r) {
     const long long j = (long long)row * L + (long long)gq * VW;                                  \
     const int xl = gq == 0 ? L - NCP : -NCP;                                                     \
     const int xr = gq == NGR - 1 ? VW - L : VW;
-#define PC_GROUPS_END }
+#define PC_GROUPS_END                                                                            \
+    gq += sg;                                                                                    \
+    int dr = srow;                                                                               \
+    if (gq >= NGR) {                                                                             \
+      gq -= NGR;                                                                                 \
+      ++dr;                                                                                      \
+    }                                                                                            \
+    row += dr;                                                                                   \
+    i2 += dr;                                                                                    \
+    while (i2 >= pc_n2) {                                                                        \
+      i2 -= pc_n2;                                                                               \
+      ++i3;                                                                                      \
+    }                                                                                            \
+  }
 
 // 7-point operator on the group at j, in the storage type's arithmetic (FP32 bands: FP32 math,
 // no per-element conversions); c receives the group's own values.  Same expression per real as
@@ -514,14 +579,6 @@ __global__ void __launch_bounds__(kThreads) k_pc_apply(Blk k, PcCoef q, const T*
   block_partials<1>(v, k, blockIdx.y);
 }
 
-// Elementwise walk of a band in 16-byte groups (the chunking of BAND_LOOP, in groups)
-#define GROUP_LOOP(k, T)                                                    \
-  constexpr int VW = Vec<T>::W;                                             \
-  const int b = blockIdx.y;                                                 \
-  const size_t off = (size_t)b * (k).ng;                                    \
-  const size_t ngr = (k).ng / VW;                                           \
-  const size_t per = (ngr + (k).nch - 1) / (k).nch;                         \
-  const size_t g0 = per * blockIdx.x, g1 = min(ngr, g0 + per);
 
 // first step: PG = G + a Q (starting guess G); (if !last) Rn = Q - a F (Q = R0); partial |Rn|^2
 template <typename T>
@@ -927,6 +984,7 @@ template <typename T, int NC>
 static int cg_block_run(Ctx& c, int kk, int s, double* h_esp, double* h_res) {
   const int nb = c.kp[kk].nband;
   const size_t nreal = c.ng * NC;
+  RS_CHECK(nreal % Vec<T>::W == 0, RSDFT_ERR_UNSUPPORTED, "CG needs bands of a multiple of %d reals", Vec<T>::W);
   int nbb = c.p.cg_block > 0 ? std::min(c.p.cg_block, nb) : nb;
   // real build: H x of all bands lives in ws_hpsi, where the fused GS/SD step that follows in
   // the sweep finds it; the other eight vectors per band are block workspace
