@@ -28,8 +28,9 @@
 // per step.  Every lane owns 4 consecutive reals (16-byte shared loads at 32-bit shared
 // addresses, packed FP32x2 arithmetic); the x neighbours come by warp shuffle when a row is 16
 // or 32 groups wide, else from shared memory.
-// Moments accumulate per thread in FP64.  All waits are bounded: a thread that gives up sets the
-// device status word; the CTA then waits (bounded) for its own copies in flight and leaves.
+// Moments accumulate per thread in packed FP32 pairs, across threads in FP64.  All waits are
+// bounded: a thread that gives up sets the device status word; the CTA then waits (bounded) for
+// its own copies in flight and leaves.
 #include "cgk.cuh"
 #include "ptx.cuh"
 #include "stencil.cuh"
@@ -94,10 +95,10 @@ __device__ __forceinline__ Q4 qfma(float2 c, const Q4& a, const Q4& b) {
   return {__ffma2_rn(c, a.lo, b.lo), __ffma2_rn(c, a.hi, b.hi)};
 }
 __device__ __forceinline__ Q4 qmul(float2 c, const Q4& a) { return {__fmul2_rn(c, a.lo), __fmul2_rn(c, a.hi)}; }
-// <x|y> of a group, FP32 products, then one FP64 add into the accumulator
-__device__ __forceinline__ void qdot(double& acc, const Q4& x, const Q4& y) {
-  const float2 p = __ffma2_rn(x.hi, y.hi, __fmul2_rn(x.lo, y.lo));
-  acc += (double)(p.x + p.y);
+// <x|y> of a group accumulated into a packed FP32 pair (the pass adds the pairs of all threads
+// in FP64 at the end of each item, as the multi-pass kernels add their per-thread FP32 sums)
+__device__ __forceinline__ void qdot(float2& acc, const Q4& x, const Q4& y) {
+  acc = __ffma2_rn(x.hi, y.hi, __ffma2_rn(x.lo, y.lo, acc));
 }
 
 // x neighbours (x - 1, x + 1 in component units) of the group c at group g of a staged row
@@ -169,7 +170,7 @@ __host__ __device__ constexpr int pz_depth(int j) {
 template <int M, int NCP, int NGS, bool MOM, int J>
 __device__ __forceinline__ void pz_task(const PzArgs& a, const PzLayout<(MOM ? M + 1 : M)>& ly, int unit, int r,
                                         uint32_t gslot_r, uint32_t gslot_m, uint32_t gslot_p, int tyv, int y0,
-                                        float* Pb, double (&acc)[(MOM ? 3 * M + 1 : 1)], const float2 (&xi)[M],
+                                        float* Pb, float2 (&acc)[(MOM ? 3 * M + 1 : 1)], const float2 (&xi)[M],
                                         float2 beta2, int lane) {
   constexpr int NLEV = MOM ? M + 1 : M;
   constexpr int NST = NLEV - 1;
@@ -325,9 +326,9 @@ __global__ void __launch_bounds__(kPzMaxThreads, 1) k_pcz(PzArgs a) {
     };
     if (threadIdx.x == 0)
       for (int r = 0; r <= D && r < T; ++r) issue(r);
-    double acc[NV];
+    float2 acc[NV];
 #pragma unroll
-    for (int d = 0; d < NV; ++d) acc[d] = 0.0;
+    for (int d = 0; d < NV; ++d) acc[d] = make_float2(0.f, 0.f);
     float2 xi[M];
     float2 beta2 = make_float2(0.f, 0.f);
     if constexpr (!MOM) {
@@ -396,7 +397,7 @@ __global__ void __launch_bounds__(kPzMaxThreads, 1) k_pcz(PzArgs a) {
     if constexpr (MOM) {
 #pragma unroll
       for (int d = 0; d < NV; ++d) {
-        double x = acc[d];
+        double x = (double)acc[d].x + (double)acc[d].y;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
         if (lane == 0) red[warp][d] = x;
