@@ -4,8 +4,10 @@
 // loop for loop so the CUDA library can be checked against it; nothing in the
 // product (rsdft_develop_b200/) links, imports or calls it.  Parity is pinned
 // by exact known answers (FD rationals, plane-wave dispersion, dense-matrix
-// eigenvalues) in tests/, because the reference ships no golden vectors for
-// this path.
+// eigenvalues) in tests/, and by the reference's own outputs: on the operator of
+// the reference's O2 sample (PSV pseudopotential, PBE, two spins, 48^3 grid) the
+// converged band energies of these sweeps equal the eigenvalues printed in the
+// reference's eight O2 sample logs (tests/test_pseudo_cpu.py).
 //
 // Restated reference routines (paths relative to the RSDFT_DEVELOP tree):
 //   kinetic stencil + V_loc   src/kinetic/d_kinetic_sol_module.f90:29-292 (and the

@@ -201,6 +201,12 @@ class BandUpdate:
         else:
             _call(self.lib.rsdft_gpu_set_projectors, 0, 0, None, None, None, 0, None, None)
 
+    def set_vloc(self, vloc: np.ndarray, s: int = 1):
+        """Local potential of spin s (Vloc(:, s) of the reference, src/localpot_module.f90)."""
+        v = np.ascontiguousarray(vloc, dtype=np.float64)
+        assert v.size == self.prob.ng
+        _call(self.lib.rsdft_gpu_set_vloc, _ptr(v), self.prob.ng, s)
+
     def set_kpoint_operator(self, prob: "synth.Problem", ik: int, k: int = 1, nonlocal_on: bool = True):
         """Point k-point slot k of this context at k-point ik of prob (same grid, atoms and Dij):
         its kinetic coefficients (coef_nabk, const_k2) and projector phases uVk."""

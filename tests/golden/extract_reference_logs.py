@@ -5,8 +5,12 @@ It reads the O2 sample runs of RSDFT (cubic cell, AX = 18.89726878 bohr, 48^3 gr
 under samples_for_supercomputers/*/02_O2-molecule_optimize/real8/result/a.log and the Si band
 runs (*/01_Si_band/result/a.log) and writes reference_logs.json beside this script: the cell,
 the grid and the init_kinetic table the reference printed (lap(m), coef_lap(1:3, m), nab(m),
-coef_nab(1:3, m), ggg), and generate_bz's k-point list (MMM divisions, kbb, weight_bz).  The tests use the
-JSON file only, so they run where the reference tree is absent.
+coef_nab(1:3, m), ggg), and generate_bz's k-point list (MMM divisions, kbb, weight_bz).  From
+every O2 log (real8 and complex16 builds) it also takes what read_PSV printed for the oxygen
+pseudopotential, the G sphere of Init_Ggrid (Ecut, Gcut, NGgrid, NMGL), construct_ps_initrho's
+density sums, and the band energies of scf_iter 1 (both spins: they belong to the operator built
+from the initial density, the same one the preceding sweeps converged).  The tests use the JSON
+file only, so they run where the reference tree is absent.
 """
 import glob
 import json
@@ -67,14 +71,92 @@ def parse_bz(path):
     return out
 
 
+def parse_o2(path):
+    """O2 set-up prints and the scf_iter 1 eigenvalue table of one log."""
+    txt = open(path).read().splitlines()
+    out = {"source": os.path.relpath(path, os.path.dirname(REF))}
+    psv = {}
+    num = r"[-+0-9.Ee]+"
+    for i, line in enumerate(txt):
+        m = re.match(r"\s*Ecut,Gcut=\s*(%s)\s+(%s)" % (num, num), line)
+        if m:
+            out["ecut"], out["gcut"] = float(m.group(1)), float(m.group(2))
+        m = re.match(r"\s*NGgrid=\s*(\d+)", line)
+        if m:
+            out["nggrid"] = int(m.group(1))
+        m = re.match(r"\s*NMGL=\s*(\d+)", line)
+        if m:
+            out["nmgl"] = int(m.group(1))
+        if "*** PSV format ***" in line and not psv:
+            for j in range(i + 1, i + 40):
+                key, _, val = txt[j].partition("=")
+                key = key.strip()
+                vals = val.split()
+                if key == "zatom":
+                    psv["zatom"] = float(vals[0])
+                elif key == "# of radial mesh points":
+                    psv["mr"] = int(vals[0])
+                elif key.startswith("r(1)"):
+                    psv["r_end"] = float(vals[1])
+                elif key == "NRps":
+                    psv["nrps"] = [int(v) for v in vals]
+                elif key == "# of orbitals":
+                    psv["norb"] = int(vals[0])
+                elif key == "angular momentum":
+                    psv["lo"] = [int(v) for v in vals]
+                elif key == "cut off radius":
+                    psv["rps"] = [float(v) for v in vals]
+                elif key == "Zps":
+                    psv["zps"] = float(vals[0])
+                elif key == "xc_pot":
+                    psv["xc_pot"] = vals[0]
+                elif key == "a1,a2,a3,a4":
+                    psv["parloc"] = [float(v) for v in vals] + [float(v) for v in txt[j + 1].split()]
+                elif key == "Reference":
+                    psv["nrf"] = [int(v) for v in vals]
+                elif key == "anorm":
+                    psv["anorm"] = [float(v) for v in vals]
+                elif key == "inorm":
+                    psv["inorm"] = [float(v) for v in vals]
+                elif key == "sum(cdd)":
+                    psv["sum_cdd"] = float(vals[0])
+                elif key == "sum(cdc)":
+                    psv["sum_cdc"] = float(vals[0])
+                    break
+            out["psv"] = psv
+        if "construct_ps_initrho(start)" in line:
+            rows = []
+            for j in range(i + 1, i + 20):
+                if "construct_ps_initrho(end)" in txt[j]:
+                    break
+                f = txt[j].split()
+                if len(f) == 4 and all(re.match(r"^%s$" % num, x) for x in f):
+                    rows.append([float(x) for x in f])
+            out["initrho"] = rows
+        if re.match(r"-+\s*scf_iter=\s*1$", line) and "esp_scf1" not in out:
+            for j in range(i + 1, i + 40):
+                if "esp(n,k,s)" in txt[j]:
+                    rows = []
+                    for jj in range(j + 1, j + 40):
+                        f = txt[jj].split()
+                        if len(f) != 8:
+                            break
+                        rows.append([int(f[0]), int(f[1])] + [float(x) for x in f[2:]])
+                    out["esp_scf1"] = rows
+                    break
+    return out
+
+
 def main():
     logs = sorted(glob.glob(os.path.join(REF, "*", "02_O2-molecule_optimize", "real8", "result", "a.log")))
     data = [parse(p) for p in logs]
     data = [d for d in data if "lap_table" in d and "ax" in d]
     bz = [parse_bz(p) for p in sorted(glob.glob(os.path.join(REF, "*", "01_Si_band", "result", "a.log")))]
     bz = [b for b in bz if "mmm" in b and b.get("kpoints")]
-    json.dump({"kinetic": data, "bz": bz}, open(os.path.join(HERE, "reference_logs.json"), "w"), indent=1)
-    print(f"{len(data)} kinetic tables, {len(bz)} k-point lists -> reference_logs.json")
+    o2 = [parse_o2(p) for p in sorted(glob.glob(os.path.join(REF, "*", "02_O2-molecule_optimize", "*", "result", "a.log")))]
+    o2 = [d for d in o2 if d.get("psv") and d.get("esp_scf1") and d.get("initrho")]
+    json.dump({"kinetic": data, "bz": bz, "o2": o2}, open(os.path.join(HERE, "reference_logs.json"), "w"), indent=1)
+    print(f"{len(data)} kinetic tables, {len(bz)} k-point lists, {len(o2)} O2 set-up/eigenvalue records -> reference_logs.json")
 
 
 if __name__ == "__main__":
