@@ -170,12 +170,14 @@ int rsdft_gpu_precond_d(int k, const double* gk, double* pgk, int ld, int nb, in
 /* The same on FP32 bands, as mixed-precision CG runs it: the mloop CG steps evaluated in the
  * s-step (Krylov-basis) form, 3 mloop + 3 passes over the bands (mloop <= 4). */
 int rsdft_gpu_precond_f(int k, const float* gk, float* pgk, int ld, int nb, int mem);
-/* FP32 precond_hprsdft form inside conjugate_gradient: 1 (default) the s-step form in 3 mloop + 3
- * passes, 2 the s-step form fused into two z-streamed passes together with <Pg|g> and the
- * direction update p = Pg + beta p (src/conjugate_gradient/cg_module.f90:254-283; mloop 1..3,
- * SWGS off), 0 the recurrence form of the FP64 path.  rsdft_gpu_precond_f uses form 1 for 1
- * and 2. */
-int rsdft_gpu_set_pc_form(int sstep);
+/* FP32 precond_hprsdft form inside conjugate_gradient: 3 (default) the s-step form in 3 mloop + 3
+ * passes, the last one forming the CG direction p = Pg + beta p itself (<Pg|g> from the Krylov
+ * moments, src/conjugate_gradient/cg_module.f90:254-283; with SWGS on it runs as form 1),
+ * 1 the same passes leaving Pg for separate <Pg|g> and direction passes,
+ * 2 the s-step form fused into two z-streamed passes together with <Pg|g> and the direction
+ * update (mloop 1..3, SWGS off), 0 the recurrence form of the FP64 path.
+ * rsdft_gpu_precond_f uses form 1 for 1, 2 and 3. */
+int rsdft_gpu_set_pc_form(int form);
 /* Orthogonalisation of the preconditioned gradient inside conjugate_gradient, the reference's
  * SWGS keyword (src/conjugate_gradient/cg_module.f90:47, cggs at :249-251 and :576-578):
  * 0 off (the default), 1 cggs_1 (against the bands below, src/conjugate_gradient/

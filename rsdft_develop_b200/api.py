@@ -561,8 +561,10 @@ class BandUpdate:
         return e.value
 
     def pc_form(self, form) -> None:
-        """FP32 precond_hprsdft evaluation inside CG: 1 (or True, the default) the s-step form in
-        separate passes, 2 the fused z-streamed s-step form, 0 (or False) the recurrence form."""
+        """FP32 precond_hprsdft evaluation inside CG: 3 (the default) the s-step form in separate
+        passes with the CG direction formed by its last pass, 1 (or True) the same leaving Pg for
+        separate direction passes, 2 the fused z-streamed s-step form, 0 (or False) the
+        recurrence form."""
         _call(self.lib.rsdft_gpu_set_pc_form, int(form))
 
     def nl_form(self, fused: bool) -> None:

@@ -268,7 +268,7 @@ static void destroy(Ctx* c) {
   }
   for (auto e : c->event_pool) cudaEventDestroy(e);
   DBuf* bufs[] = {&c->vloc64, &c->vloc32, &c->ws_coef, &c->ws_io_a, &c->ws_io_b, &c->ws_cg, &c->ws_red,
-                  &c->ws_scal, &c->ws_dense, &c->ws_hpsi, &c->ws_flag, &c->ws_rot, &c->ws_solver, &c->ws_info, &c->ws_gemm, &c->ws_out, &c->ws_f64,
+                  &c->ws_scal, &c->ws_dense, &c->ws_gram, &c->ws_hpsi, &c->ws_flag, &c->ws_rot, &c->ws_solver, &c->ws_info, &c->ws_gemm, &c->ws_out, &c->ws_f64,
                   &c->nl.gofs, &c->nl.gjj, &c->nl.gplist, &c->nl.gD, &c->nl.rec_rowptr, &c->nl.rec_pt, &c->nl.rec_g, &c->nl.cov};
   for (DBuf* b : bufs) b->release();
   for (auto& pk : c->nl.perk) {
@@ -845,10 +845,11 @@ int rsdft_gpu_selftest_gemm(int m, int n, long long k, int op, double* err) {
   return check_status(*g_ctx);
 }
 
-int rsdft_gpu_set_pc_form(int sstep) {
+int rsdft_gpu_set_pc_form(int form) {
   REQUIRE_CTX();
-  RS_CHECK(sstep >= 0 && sstep <= 2, RSDFT_ERR_ARG, "preconditioner form must be 0, 1 or 2");
-  g_ctx->pc_sstep = sstep;
+  RS_CHECK(form >= 0 && form <= 3, RSDFT_ERR_ARG, "preconditioner form must be 0, 1, 2 or 3");
+  g_ctx->pc_sstep = form == 3 ? 1 : form;
+  g_ctx->pc_direct = form == 3 ? 1 : 0;
   return 0;
 }
 

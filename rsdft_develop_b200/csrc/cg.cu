@@ -509,12 +509,14 @@ __device__ __forceinline__ Vec<T> apply7v(const T* __restrict__ g, long long j, 
 }
 
 // R = G - A G (the initial residual for the starting guess PG = G, also the first direction);
-// partial |R|^2
-template <typename T, int NCP>
+// partial |R|^2.  NU (s-step form): also <R|G> and <R|B G>, B G = (A G - c0 G) / c0, the first
+// two of nu_i = <B^i R|G> (the later ones follow from the moments, see k_pcs_beta)
+template <typename T, int NCP, bool NU = false>
 __global__ void __launch_bounds__(kThreads) k_pc_first(Blk k, PcCoef q, const T* __restrict__ G,
                                                        T* __restrict__ R) {
   if (SC(k, S_ACT, blockIdx.y) == 0.0) return;
-  T vt = T(0);  // per-thread partial in the storage type, added in FP64 across threads
+  T vt = T(0), n0 = T(0), n1 = T(0);  // per-thread partials in the storage type, added in FP64 across threads
+  const T c0 = (T)q.c0, ic0 = (T)(1.0 / q.c0);
   {
     PC_GROUPS_BEGIN(k, q, T)
     Vec<T> c;
@@ -524,12 +526,21 @@ __global__ void __launch_bounds__(kThreads) k_pc_first(Blk k, PcCoef q, const T*
     for (int i = 0; i < VW; ++i) {
       r.v[i] = c.v[i] - ag.v[i];
       vt += r.v[i] * r.v[i];
+      if (NU) {
+        n0 += r.v[i] * c.v[i];
+        n1 += r.v[i] * ((ag.v[i] - c0 * c.v[i]) * ic0);
+      }
     }
     stv(R + off + j, r);
     PC_GROUPS_END
   }
-  double v[1] = {(double)vt};
-  block_partials<1>(v, k, blockIdx.y);
+  if (NU) {
+    double v[3] = {(double)vt, (double)n0, (double)n1};
+    block_partials<3>(v, k, blockIdx.y);
+  } else {
+    double v[1] = {(double)vt};
+    block_partials<1>(v, k, blockIdx.y);
+  }
 }
 
 // Qn = R + b Q and F = A Qn = A R + b A Q in one pass (Qn written to a third buffer, since
@@ -644,7 +655,7 @@ __global__ void __launch_bounds__(kThreads) k_pc_update(Blk k, const T* __restri
   if (!last) block_partials<1>(v, k, b);
 }
 
-__global__ void k_pc_sc_first(Blk k) {
+__global__ void k_pc_sc_first(Blk k, int nu = 0) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= k.nbb) return;
   if (SC(k, S_ACT, b) == 0.0) {
@@ -654,6 +665,10 @@ __global__ void k_pc_sc_first(Blk k) {
   const double rr1 = sum_part(k, b, 0);
   SC(k, S_RR1, b) = rr1;
   SC(k, S_PCACT, b) = rr1 < 1.0e-24 ? 0.0 : 1.0;  // cgpc_hprsdft_module.f90:181
+  if (nu) {
+    SC(k, S_NU0, b) = sum_part(k, b, 1);
+    SC(k, S_NU1, b) = sum_part(k, b, 2);
+  }
 }
 __global__ void k_pc_sc_alpha(Blk k) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -765,6 +780,73 @@ __global__ void __launch_bounds__(kThreads) k_pcs_combine(Blk k, const T* __rest
   block_partials<1>(d, k, b);
 }
 
+// CG's rb = <PG|G> dV and beta = rb / gkgk (k_sc_beta) without a pass over PG:
+// <PG|G> = <G|G> + sum_i xi_i nu_i with nu_i = <B^i v0|G>.  nu_0 and nu_1 come from k_pc_first;
+// since v0 = G - A G = (1 - c0) G - c0 B G, nu_{i+1} = ((1 - c0) nu_i - mu_i) / c0 for the
+// rest.  <G|G> dV is the rb CG left in S_RB (k_sc_rb, k_sc_reject).
+__global__ void k_pcs_beta(Blk k, int m, double c0, double dV, int first) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= k.nbb || SC(k, S_ACT, b) == 0.0) return;
+  double pgg = SC(k, S_RB, b) / dV;
+  if (SC(k, S_PCACT, b) != 0.0) {
+    double nu[4];
+    nu[0] = SC(k, S_NU0, b);
+    nu[1] = SC(k, S_NU1, b);
+    for (int i = 2; i < m; ++i) nu[i] = ((1.0 - c0) * nu[i - 1] - SC(k, S_MU0 + i - 1, b)) / c0;
+    for (int i = 0; i < m; ++i) pgg += SC(k, S_XI0 + i, b) * nu[i];
+  }
+  const double rb = pgg * dV;
+  SC(k, S_RB, b) = rb;
+  SC(k, S_BETA, b) = first ? 0.0 : rb / SC(k, S_GKGK, b);
+  SC(k, S_GKGK, b) = rb;
+}
+
+// P = PG + beta P with PG = G + sum_{i < M} xi_i v_i (P = PG at the first CG step; PG = G where
+// the preconditioner is inactive), i.e. k_pcs_combine and k_make_p in one pass; bands whose CG
+// has stopped keep P
+template <typename T, int M>
+__global__ void __launch_bounds__(kThreads) k_pcs_combine_p(Blk k, const T* __restrict__ G, const T* __restrict__ V0,
+                                                            const T* __restrict__ V1, const T* __restrict__ V2,
+                                                            const T* __restrict__ V3, T* __restrict__ P, int first) {
+  GROUP_LOOP(k, T);
+  if (SC(k, S_ACT, b) == 0.0) return;
+  const bool on = SC(k, S_PCACT, b) != 0.0;
+  T x[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) x[j] = (on && j < M) ? (T)SC(k, S_XI0 + j, b) : T(0);
+  const T beta = (T)SC(k, S_BETA, b);
+  for (size_t gi = g0 + threadIdx.x; gi < g1; gi += kThreads) {
+    const size_t e = off + gi * VW;
+    Vec<T> pv = ldv(G + e);
+    if (on) {
+      const Vec<T> a0 = ldv(V0 + e);
+#pragma unroll
+      for (int i = 0; i < VW; ++i) pv.v[i] += x[0] * a0.v[i];
+      if (M > 1) {
+        const Vec<T> a1 = ldv(V1 + e);
+#pragma unroll
+        for (int i = 0; i < VW; ++i) pv.v[i] += x[1] * a1.v[i];
+      }
+      if (M > 2) {
+        const Vec<T> a2 = ldv(V2 + e);
+#pragma unroll
+        for (int i = 0; i < VW; ++i) pv.v[i] += x[2] * a2.v[i];
+      }
+      if (M > 3) {
+        const Vec<T> a3 = ldv(V3 + e);
+#pragma unroll
+        for (int i = 0; i < VW; ++i) pv.v[i] += x[3] * a3.v[i];
+      }
+    }
+    if (!first) {
+      const Vec<T> po = ldv(P + e);
+#pragma unroll
+      for (int i = 0; i < VW; ++i) pv.v[i] += beta * po.v[i];
+    }
+    stv(P + e, pv);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // host drivers
 // ---------------------------------------------------------------------------
@@ -795,10 +877,14 @@ static int pick_nch(size_t ng, int nbb, int plane_reals = 0, int n3 = 0) {
 // for mloop CG steps on A x = G from x = G.  Buffers: X0 holds R0 = Q1, then X0/X1/X2 rotate
 // between the residual and the current/next directions; F = A Q.
 // *pg_dot: set when the partials of <PG|G> (bands with S_ACT set) were left in the partial
-// buffer by the last pass
+// buffer by the last pass.  P (s-step form only; p_done is set when it was used): the CG
+// direction P = PG + beta P (first: P = PG) is formed by the last pass instead of PG, with rb
+// and beta set as k_sc_beta sets them.
 template <typename T>
-static int pc_block(Ctx& c, Blk& k, const T* G, T* PG, T* X0, T* X1, T* X2, T* F, bool* pg_dot = nullptr) {
+static int pc_block(Ctx& c, Blk& k, const T* G, T* PG, T* X0, T* X1, T* X2, T* F, bool* pg_dot = nullptr,
+                    T* P = nullptr, int first = 0, bool* p_done = nullptr) {
   if (pg_dot) *pg_dot = false;
+  if (p_done) *p_done = false;
   PcCoef q;
   const double* H = c.p.hgrid;
   q.c0 = c.p.ggg[0] / (H[0] * H[0]) + c.p.ggg[1] / (H[1] * H[1]) + c.p.ggg[2] / (H[2] * H[2]);
@@ -829,8 +915,14 @@ static int pc_block(Ctx& c, Blk& k, const T* G, T* PG, T* X0, T* X1, T* X2, T* F
     qb.c3 = q.c3 / q.c0;
     qb.c0 = 0.0;
     T* v[4] = {X0, X1, X2, F};
-    LAUNCH_PC(k_pc_first, q, G, X0);
-    LAUNCH_S(k_pc_sc_first);
+    const bool direct = P != nullptr && p_done != nullptr;
+    if (direct) {
+      if (q.nc == 1) LAUNCH_E((k_pc_first<T, 1, true>), q, G, X0);
+      else LAUNCH_E((k_pc_first<T, 2, true>), q, G, X0);
+    } else {
+      LAUNCH_PC(k_pc_first, q, G, X0);
+    }
+    LAUNCH_S(k_pc_sc_first, direct ? 1 : 0);
     LAUNCH_S(k_pcs_sc, 0, m, q.c0);
     for (int i = 1; i < m; ++i) {
       if (q.nc == 1) LAUNCH_E((k_pcs_shift<T, 1, true>), qb, v[i - 1], v[i]);
@@ -840,6 +932,17 @@ static int pc_block(Ctx& c, Blk& k, const T* G, T* PG, T* X0, T* X1, T* X2, T* F
     if (q.nc == 1) LAUNCH_E((k_pcs_shift<T, 1, false>), qb, v[m - 1], (T*)nullptr);
     else LAUNCH_E((k_pcs_shift<T, 2, false>), qb, v[m - 1], (T*)nullptr);
     LAUNCH_S(k_pcs_sc, m, m, q.c0);
+    if (direct) {
+      LAUNCH_S(k_pcs_beta, m, q.c0, c.p.dv, first);
+      switch (m) {
+        case 1: LAUNCH_E((k_pcs_combine_p<T, 1>), G, v[0], v[1], v[2], v[3], P, first); break;
+        case 2: LAUNCH_E((k_pcs_combine_p<T, 2>), G, v[0], v[1], v[2], v[3], P, first); break;
+        case 3: LAUNCH_E((k_pcs_combine_p<T, 3>), G, v[0], v[1], v[2], v[3], P, first); break;
+        default: LAUNCH_E((k_pcs_combine_p<T, 4>), G, v[0], v[1], v[2], v[3], P, first); break;
+      }
+      *p_done = true;
+      return check_launch("pc");
+    }
     switch (m) {
       case 1: LAUNCH_E((k_pcs_combine<T, 1>), G, v[0], v[1], v[2], v[3], PG); break;
       case 2: LAUNCH_E((k_pcs_combine<T, 2>), G, v[0], v[1], v[2], v[3], PG); break;
@@ -1063,6 +1166,9 @@ static int cg_block_run(Ctx& c, int kk, int s, double* h_esp, double* h_res) {
         LAUNCH_E(k_copy<T>, G, PG);
       } else if (pcm == RSDFT_PC_LEARNED && std::is_same<T, float>::value && NC == 1) {
         RS_TRY(lpc_apply(c, reinterpret_cast<const float*>(G), reinterpret_cast<float*>(PG), nn));
+      } else if (c.pc_direct && !c.cggs) {
+        // the s-step form writes P itself (its direction pass replaces k_make_p)
+        RS_TRY(pc_block<T>(c, k, G, PG, R, Q, Q2, F, &pg_dot, P, icg == 1 ? 1 : 0, &p_done));
       } else {
         RS_TRY(pc_block<T>(c, k, G, PG, R, Q, Q2, F, &pg_dot));
       }

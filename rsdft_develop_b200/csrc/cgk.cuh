@@ -19,6 +19,7 @@ enum Scal {
   S_DEF,                     // real build: x update deferred until the exact reject test (1) or done with H x (0)
   S_MU0, S_MU7 = S_MU0 + 7,  // s-step preconditioner: moments <v0 | B^i v0>, i < 2 mloop
   S_XI0, S_XI3 = S_XI0 + 3,  // s-step preconditioner: PG = G + sum_i xi_i B^i v0
+  S_NU0, S_NU1,              // s-step preconditioner: <v0 | G>, <B v0 | G> (for <PG | G> without a pass)
   S_COUNT
 };
 

@@ -104,6 +104,7 @@ struct Ctx {
   DBuf ws_red;                     // reduction partials
   DBuf ws_scal;                    // per-band scalars (double)
   DBuf ws_dense;                   // M x M matrices
+  DBuf ws_gram;                    // per-CTA partials of the small-band FP64 Gram matrices
   DBuf ws_hpsi;                    // H psi of all bands (nb x ng): CG's running H x, subspace diag
   DBuf ws_flag;                    // device counters (CG line-search rejections)
   bool cg_hx_ready = false;        // ws_hpsi holds H x of every band of (cg_hx_k, cg_hx_s) after CG
@@ -126,6 +127,7 @@ struct Ctx {
   double sched_res_rot = 1e-4;     // sweeps: 2 rotation terms while CG's max residual > this (0: off)
   long long sched_sweeps = 0;      // (k, s) sweep steps run with reduced terms
   int pc_sstep = 1;                // FP32 precond_hprsdft: 1 s-step passes, 2 fused z-streamed s-step form
+  int pc_direct = 1;               // s-step passes: the last one forms the CG direction P (no PG, no k_make_p)
                                    // inside CG, 0 the recurrence form
   int gemm_wide = 1;               // three-term GEMM tiles 128 x 256 (K blocks of 32), else 128 x 128
   int gemm_tri = 1;                // S by upper-triangle tiles (1), S and Hsub (2), neither (0)

@@ -68,6 +68,106 @@ static int read_info(Ctx& c, int* d_info, int* h_info) {
 }
 
 // ---------------------------------------------------------------------------
+// FP64 Gram matrices of a few bands (nb <= 44): cuBLAS syrk/syrkx/syr2k pick slow kernels for
+// an nb x nb result over a long grid (O2 sample: 3.4 ms per call at nb = 18, ng = 48^3), so the
+// real build forms them here.  Upper triangles (i <= j, column-major) of
+//   S = dV X^T X,  M = dV X^T (H X)  or  M = dV/2 (X^T (H X) + (H X)^T X),
+// each CTA summing a contiguous range of grid points into per-CTA partials, then a fixed-order
+// reduction (deterministic).
+// ---------------------------------------------------------------------------
+constexpr int kGramTK = 64;     // grid points per shared-memory tile
+constexpr int kGramPmax = 4;    // pairs per thread (256 threads: npair <= 1024, nb <= 44)
+constexpr int kGramNbMax = 44;
+
+__global__ void __launch_bounds__(256) k_gram_small(const double* __restrict__ X, const double* __restrict__ HX,
+                                                    int ng, int nb, int npair, int mode, int kper,
+                                                    double* __restrict__ part) {
+  extern __shared__ double gsm[];
+  double* sx = gsm;                       // [kGramTK][nb]
+  double* sh = gsm + kGramTK * nb;        // [kGramTK][nb]
+  const bool wantS = mode & 1, wantM = mode & 2, sym = mode & 4;
+  int pi[kGramPmax], pj[kGramPmax];
+  double aS[kGramPmax], aM[kGramPmax];
+#pragma unroll
+  for (int q = 0; q < kGramPmax; ++q) {
+    const int p = threadIdx.x + q * 256;
+    int j = 0;
+    while ((j + 1) * (j + 2) / 2 <= p) ++j;   // p = j (j + 1) / 2 + i, i <= j
+    pj[q] = j;
+    pi[q] = p - j * (j + 1) / 2;
+    aS[q] = 0.0;
+    aM[q] = 0.0;
+  }
+  const int k0 = blockIdx.x * kper, k1 = min(ng, k0 + kper);
+  for (int kk = k0; kk < k1; kk += kGramTK) {
+    const int tk = min(kGramTK, k1 - kk);
+    for (int idx = threadIdx.x; idx < tk * nb; idx += 256) {
+      const int b = idx / tk, t = idx - b * tk;
+      sx[t * nb + b] = X[(size_t)b * ng + kk + t];
+      if (wantM) sh[t * nb + b] = HX[(size_t)b * ng + kk + t];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < kGramPmax; ++q) {
+      if (threadIdx.x + q * 256 >= npair) break;
+      const int i = pi[q], j = pj[q];
+      double s0 = 0.0, m0 = 0.0;
+      for (int t = 0; t < tk; ++t) {
+        const double xi = sx[t * nb + i], xj = sx[t * nb + j];
+        if (wantS) s0 += xi * xj;
+        if (wantM) m0 += sym ? xi * sh[t * nb + j] + sh[t * nb + i] * xj : xi * sh[t * nb + j];
+      }
+      aS[q] += s0;
+      aM[q] += m0;
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < kGramPmax; ++q) {
+    const int p = threadIdx.x + q * 256;
+    if (p >= npair) break;
+    part[((size_t)blockIdx.x * 2 + 0) * npair + p] = aS[q];
+    part[((size_t)blockIdx.x * 2 + 1) * npair + p] = aM[q];
+  }
+}
+
+__global__ void k_gram_small_reduce(const double* __restrict__ part, int nblk, int npair, int nb, int mode,
+                                    double sS, double sM, double* __restrict__ S, double* __restrict__ M) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npair) return;
+  int j = 0;
+  while ((j + 1) * (j + 2) / 2 <= p) ++j;
+  const int i = p - j * (j + 1) / 2;
+  double ts = 0.0, tm = 0.0;
+  for (int b = 0; b < nblk; ++b) {
+    ts += part[((size_t)b * 2 + 0) * npair + p];
+    tm += part[((size_t)b * 2 + 1) * npair + p];
+  }
+  if (mode & 1) S[i + (size_t)j * nb] = sS * ts;
+  if (mode & 2) M[i + (size_t)j * nb] = sM * tm;
+}
+
+// S (if non-null) = dV X^T X, M (if non-null) = dV X^T HX or, sym, dV/2 (X^T HX + HX^T X):
+// upper triangles; the lower triangles are left as they were
+static int gram_small_f64(Ctx& c, const double* X, const double* HX, int ng, int nb, double dV, double* S, double* M,
+                          bool sym) {
+  const int npair = nb * (nb + 1) / 2;
+  const int mode = (S ? 1 : 0) | (M ? 2 : 0) | (sym ? 4 : 0);
+  int nblk = std::min(2 * 148, std::max(1, (ng + kGramTK - 1) / kGramTK));
+  int kper = (ng + nblk - 1) / nblk;
+  kper = (kper + kGramTK - 1) / kGramTK * kGramTK;
+  nblk = (ng + kper - 1) / kper;
+  RS_TRY(c.ws_gram.ensure(sizeof(double) * 2 * (size_t)npair * nblk));
+  const size_t smem = sizeof(double) * 2 * kGramTK * nb;
+  k_gram_small<<<nblk, 256, smem, c.stream>>>(X, HX, ng, nb, npair, mode, kper, c.ws_gram.as<double>());
+  k_gram_small_reduce<<<(npair + 127) / 128, 128, 0, c.stream>>>(c.ws_gram.as<double>(), nblk, npair, nb, mode, dV,
+                                                                  sym ? 0.5 * dV : dV, S, M);
+  c.launches += 2;
+  RS_CUDA(cudaGetLastError());
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
 // mixed precision (real8): psi stays FP32; S, Hsub and the rotations run as split-BF16
 // tensor-core GEMMs with FP64 results; Cholesky, R^-1 and the eigensolve stay FP64.
 // ---------------------------------------------------------------------------
@@ -382,7 +482,10 @@ int gs_run(Ctx& c, int k, int s, int passes) {
                             nb, &zone, S, nb, X, ng));
     } else {
       double* S = c.ws_dense.as<double>();
-      RS_CUBLAS(cublasDsyrk(c.cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, nb, ng, &dV, v.x, ng, &zero, S, nb));
+      if (nb <= kGramNbMax)
+        RS_TRY(gram_small_f64(c, v.x, nullptr, ng, nb, dV, S, nullptr, false));
+      else
+        RS_CUBLAS(cublasDsyrk(c.cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, nb, ng, &dV, v.x, ng, &zero, S, nb));
       RS_CUSOLVER(cusolverDnDpotrf(c.cusolver, CUBLAS_FILL_MODE_UPPER, nb, S, nb, c.ws_solver.as<double>(), lwork,
                                    c.ws_info.as<int>()));
       RS_TRY(read_info(c, c.ws_info.as<int>(), &info));
@@ -420,6 +523,8 @@ int sd_run(Ctx& c, int k, int s, double* h_esp) {
       RS_CUBLAS(cublasZher2k(c.cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C, nb, ng, &zhdV,
                              reinterpret_cast<cuDoubleComplex*>(v.x), ng, reinterpret_cast<cuDoubleComplex*>(HX), ng,
                              &zero, c.ws_dense.as<cuDoubleComplex>(), nb));
+    else if (nb <= kGramNbMax)
+      RS_TRY(gram_small_f64(c, v.x, HX, ng, nb, c.p.dv, nullptr, c.ws_dense.as<double>(), true));
     else
       RS_CUBLAS(cublasDsyr2k(c.cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, nb, ng, &hdV, v.x, ng, HX, ng, &zero,
                              c.ws_dense.as<double>(), nb));
@@ -499,9 +604,13 @@ int gssd_run(Ctx& c, int k, int s, double* h_esp, bool use_cg_hx) {
     if (!reuse) RS_TRY(hpsi_real<double>(c, k, s, v.x, HX, c.ng, nb));
     ProfScope ps(c, "sd_gemm", 0.0, 2.0 * 2.0 * c.ng * (double)nb * nb);
     // S and M = dV X^T (H X) are symmetric (H is): their upper triangles only
-    RS_CUBLAS(cublasDsyrk(c.cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, nb, ng, &dV, v.x, ng, &zero, S, nb));
-    RS_CUBLAS(cublasDsyrkx(c.cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, nb, ng, &dV, v.x, ng, HX, ng, &zero, M,
-                           nb));
+    if (nb <= kGramNbMax) {
+      RS_TRY(gram_small_f64(c, v.x, HX, ng, nb, dV, S, M, false));
+    } else {
+      RS_CUBLAS(cublasDsyrk(c.cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, nb, ng, &dV, v.x, ng, &zero, S, nb));
+      RS_CUBLAS(cublasDsyrkx(c.cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, nb, ng, &dV, v.x, ng, HX, ng, &zero, M,
+                             nb));
+    }
   }
   {
     ProfScope ps(c, "gs");

@@ -3,18 +3,17 @@
 The set-up the reference runs before its first sweep (src/rsdft.f90 initialisation order:
 read_pseudopot, Init_Ggrid, init_ps_local + construct_ps_local, construct_ps_initrho,
 ps_nloc_initiate -> prep_ps_nloc2, init_hartree + calc_hartree, calc_xc, init_localpot),
-for orthorhombic cells and a Gamma-point (real8) band update:
+for orthorhombic cells and a Gamma-point band update (real8, or complex16 at Gamma):
 
   V_loc(s) = V_ion + V_H[rho] + V_xc[rho_up, rho_down](s)     (src/localpot_module.f90:209-215)
 
 with rho the analytic Gaussian initial density split over spins (Nelectron_spin =
-(Nelectron +- Ndspin) / 2), V_H by the cut-off-sphere FFT solve and V_xc by PBE or LDA PZ81;
+(Nelectron +- Ndspin) / 2), V_H by the cut-off-sphere FFT solve and V_xc by PBE;
 the nonlocal part is the filtered KB projector set with D = sign(D_ii) on the diagonal.
 """
 from __future__ import annotations
 
 import dataclasses
-import math
 
 import numpy as np
 
@@ -62,7 +61,11 @@ class Setup:
         return dataclasses.replace(self.problem, vloc=np.ascontiguousarray(self.vloc[s - 1]))
 
 
-def setup(st: Structure, rcfac: float = 1.5, qcfac: float = 1.0, etafac: float = 8.0) -> Setup:
+def setup(st: Structure, rcfac: float = 1.5, qcfac: float = 1.0, etafac: float = 8.0,
+          complex16: bool = False) -> Setup:
+    """The band update's inputs for st.  complex16: the operator for the complex16 build at the
+    Gamma point (complex wavefunctions, projectors with unit phases), as the reference's
+    complex16 sample runs use it."""
     n = tuple(st.n)
     L = st.lengths
     h = tuple(L[d] / n[d] for d in range(3))
@@ -96,13 +99,15 @@ def setup(st: Structure, rcfac: float = 1.5, qcfac: float = 1.0, etafac: float =
     natom = sum(len(pos) for _, pos in species)
     lmax = max(int(pp.lo.max()) for pp, _ in species)
     cfg = synth.Config(name="structure", n=n[0], h=h[0], nband=st.nband, n_gauss=0, natom=natom,
-                       lmax=lmax, rc=float(max(f.rps.max() for f in filtered)), md=st.md)
+                       lmax=lmax, rc=float(max(f.rps.max() for f in filtered)), md=st.md,
+                       kpoints=((0.0, 0.0, 0.0),) if complex16 else None)
     kbb = np.zeros((1, 3))
     kin = synth.kinetic_coefficients(h[0], st.md, kbb * 0.0)
     pairs = np.stack([np.arange(1, ps.nzlma + 1), np.arange(1, ps.nzlma + 1)], axis=1).astype(np.int32)
     prob = synth.Problem(cfg=cfg, n=n, h=h[0], dV=dV, md=st.md, kin=kin,
                          vloc=np.ascontiguousarray(vloc[0]), nzlma=ps.nzlma, mjj=ps.mjj, jjp=ps.jjp,
-                         uvk=ps.uv[None, :, :].copy(), amap=ps.amap, lmap=ps.lmap, mmap=ps.mmap,
+                         uvk=ps.uv[None, :, :].astype(np.complex128 if complex16 else np.float64),
+                         amap=ps.amap, lmap=ps.lmap, mmap=ps.mmap,
                          pairs=pairs, dij=ps.iuv.astype(np.float64), kbb=kbb, kcart=kbb.copy(),
                          nband_k=np.array([st.nband], np.int32))
     return Setup(structure=st, ggrid=gr, vion=vion, rho=rho, vh=vh, vxc=vxc, vloc=vloc, e_hartree=eh,

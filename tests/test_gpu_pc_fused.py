@@ -1,11 +1,13 @@
-"""The fused z-streamed FP32 preconditioner inside CG against its multi-pass s-step form.
+"""The fused FP32 preconditioner forms inside CG against the multi-pass s-step form.
 
 precond_hprsdft (src/conjugate_gradient/cgpc_hprsdft_module.f90:133-270) followed by the CG
 dot <Pg|g> and the direction update p = Pg + beta p (src/conjugate_gradient/cg_module.f90:
 254-283).  Form 2 evaluates the preconditioner's s-step chain on the fly in two
 z-streamed passes and takes <Pg|g> from the moments; form 1 runs the same s-step arithmetic in
 3 mloop + 3 separate passes (itself held to the FP64 recurrence of the oracle by
-test_gpu_mixed.py).  Form 1 is the default; form 2 is selectable.  One CG call (Ncg = 3)
+test_gpu_mixed.py); form 3 runs form 1's passes but lets the last one write the CG direction
+p = Pg + beta p, with <Pg|g> from the Krylov moments.  Form 3 is the default; 1 and 2 are
+selectable.  One CG call (Ncg = 3)
 from the same start must give the same Ritz values, residuals and bands up to FP32 rounding.  The cases cover every code path of the fused kernel:
 rows read from shared memory (t0, c0, tk: rows of 16, 24 and 32 reals) and by warp shuffle
 (c1 grid: 64 reals, c3 / c4 grids: 128 reals), real and complex (interleaved) bands, halos that
@@ -47,8 +49,9 @@ CASES = [
 ]
 
 
+@pytest.mark.parametrize("form", [2, 3])
 @pytest.mark.parametrize("name,nband,nk,mloop", CASES)
-def test_fused_preconditioner_cg_matches_multipass(name, nband, nk, mloop):
+def test_fused_preconditioner_cg_matches_multipass(name, nband, nk, mloop, form):
     over = {}
     if nband:
         over["nband"] = nband
@@ -59,7 +62,7 @@ def test_fused_preconditioner_cg_matches_multipass(name, nband, nk, mloop):
     nb = int(prob.nband_k[0])
     psis = _start(prob, nb, 81, nk)
     ref = _cg_once(prob, psis, 1, mloop)
-    fus = _cg_once(prob, psis, 2, mloop)
+    fus = _cg_once(prob, psis, form, mloop)
     for k in range(nk):
         (e1, r1, u1), (e2, r2, u2) = ref[k], fus[k]
         assert np.all(np.isfinite(e2)) and np.all(np.isfinite(r2)) and np.all(np.isfinite(u2))
@@ -71,11 +74,11 @@ def test_fused_preconditioner_cg_matches_multipass(name, nband, nk, mloop):
 
 
 def test_fused_preconditioner_mixed_sweeps_converge():
-    """Mixed sweeps with the fused form reach the tolerance in about the sweeps of form 1."""
+    """Mixed sweeps with the fused forms reach the tolerance in about the sweeps of form 1."""
     prob = synth.make_problem("c0")
     mb = prob.nband - prob.nband // 8
     its = {}
-    for form in (1, 2):
+    for form in (1, 2, 3):
         with api.BandUpdate(prob, precision=api.PREC_MIXED) as g:
             g.pc_form(form)
             g.init_sweep(mb)
@@ -84,5 +87,6 @@ def test_fused_preconditioner_mixed_sweeps_converge():
             it, esp, res = g.calc_sweep(400, tol=1e-8)
             assert res[0, 0, :mb].max() <= 1e-8, (form, it)
             its[form] = (it, esp[0, 0].copy())
-    assert abs(its[2][0] - its[1][0]) <= max(3, its[1][0] // 10), its
-    assert np.max(np.abs(its[2][1][:mb] - its[1][1][:mb])) < 1e-8
+    for form in (2, 3):
+        assert abs(its[form][0] - its[1][0]) <= max(3, its[1][0] // 10), its
+        assert np.max(np.abs(its[form][1][:mb] - its[1][1][:mb])) < 1e-8
