@@ -8,8 +8,10 @@ the grid and the init_kinetic table the reference printed (lap(m), coef_lap(1:3,
 coef_nab(1:3, m), ggg), and generate_bz's k-point list (MMM divisions, kbb, weight_bz).  From
 every O2 log (real8 and complex16 builds) it also takes what read_PSV printed for the oxygen
 pseudopotential, the G sphere of Init_Ggrid (Ecut, Gcut, NGgrid, NMGL), construct_ps_initrho's
-density sums, and the band energies of scf_iter 1 (both spins: they belong to the operator built
-from the initial density, the same one the preceding sweeps converged).  The tests use the JSON
+density sums, the band energies of scf_iter 1 (both spins: they belong to the operator built
+from the initial density, the same one the preceding sweeps converged), and what scf_iter 1
+prints about the density of those bands (charges, sum |rho_up - rho_down| dV, and the squared
+changes of V_loc and rho from the initial ones).  The tests use the JSON
 file only, so they run where the reference tree is absent.
 """
 import glob
@@ -134,6 +136,18 @@ def parse_o2(path):
                     rows.append([float(x) for x in f])
             out["initrho"] = rows
         if re.match(r"-+\s*scf_iter=\s*1$", line) and "esp_scf1" not in out:
+            for j in range(i + 1, i + 40):
+                t = txt[j].strip()
+                if "scf_iter=" in t:
+                    break
+                if t.startswith("Charge:"):
+                    out["charge_scf1"] = [float(x) for x in t.split(":")[1].split()]
+                elif t.startswith("sum|rho_up-rho_down|"):
+                    out["sum_abs_spin_scf1"] = float(t.split(":")[1])
+                elif t.startswith("|Vloc-Vloc0|^2/tol"):
+                    out["sqerr_v_scf1"] = [float(x) for x in t.split("=")[1].split("/")[0].split()]
+                elif t.startswith("|rho -rho0 |^2/tol"):
+                    out["sqerr_rho_scf1"] = [float(x) for x in t.split("=")[1].split("/")[0].split()]
             for j in range(i + 1, i + 40):
                 if "esp(n,k,s)" in txt[j]:
                     rows = []

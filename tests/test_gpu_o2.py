@@ -6,7 +6,9 @@ tests/golden/o_pbe_rc15_psv.npz; both spins run in one context (nspin = 2, Vloc 
 converged band energies must match the values the reference printed at scf_iter 1 in all eight
 O2 logs (tests/golden/reference_logs.json): bands 1-5 to 1e-10 Ha, the pi* pair (bands 6-7,
 logged before it had fully converged) to 3e-8 Ha.  FP64 directly; mixed precision after its FP64
-polish, and within 1e-6 Ha before it.
+polish, and within 1e-6 Ha before it; the complex16 build at Gamma in FP64.  The device density of
+the FP64 bands with scf_iter 1's occupations matches that iteration's printed charges, spin
+density sum and squared density change.
 """
 import json
 import os
@@ -14,7 +16,7 @@ import os
 import numpy as np
 import pytest
 
-from rsdft_develop_b200 import api, pseudo, structure
+from rsdft_develop_b200 import api, gga, pseudo, structure
 
 pytestmark = pytest.mark.gpu
 
@@ -41,6 +43,27 @@ def _check(esp, tol15=1e-10, tol67=3e-8):
             assert np.max(np.abs(got[5:7] - ref[5:7])) < tol67, (s, log["source"], got[5:7] - ref[5:7])
 
 
+def _check_density(g, o2):
+    """The device density of the converged bands with scf_iter 1's occupations (7 up, 5 down)
+    against what that iteration prints (tolerances as in test_pseudo_cpu.py)."""
+    occ = np.zeros((2, 1, o2.problem.nband))
+    occ[0, 0, :7] = 1.0
+    occ[1, 0, :5] = 1.0
+    g.density(occ)
+    rho = g.get_rho()[0]
+    dV = o2.problem.dV
+    vh, _ = gga.hartree_sphere(rho.sum(axis=0), o2.ggrid, dV)
+    vxc, _, _ = gga.pbe(rho, o2.problem.n, (o2.problem.h,) * 3, dV)
+    sq_v = np.sum((o2.vion[None, :] + vh[None, :] + vxc - o2.vloc) ** 2, axis=1) / rho.shape[1]
+    sq_rho = np.sum((rho - o2.rho) ** 2, axis=1) / rho.shape[1]
+    spin = float(np.sum(np.abs(rho[0] - rho[1]))) * dV
+    for log in _logs():
+        assert np.allclose(rho.sum(axis=1) * dV, log["charge_scf1"], atol=1e-11)
+        assert abs(spin - log["sum_abs_spin_scf1"]) < 1e-7, (spin, log["sum_abs_spin_scf1"])
+        assert np.allclose(sq_rho, log["sqerr_rho_scf1"], rtol=1e-5, atol=0), (sq_rho, log["sqerr_rho_scf1"])
+        assert np.allclose(sq_v, log["sqerr_v_scf1"], rtol=1e-2, atol=0), (sq_v, log["sqerr_v_scf1"])
+
+
 def _start(g, o2):
     g.set_vloc(o2.vloc[1], s=2)
     g.init_sweep(7)
@@ -55,6 +78,7 @@ def test_o2_fp64_band_energies_match_reference_logs(o2):
         it, esp, res = g.calc_sweep(80, tol=1e-18)
         assert np.max(res[:, 0, :7]) <= 1e-18, (it, res[:, 0, :7])
         _check(esp)
+        _check_density(g, o2)
 
 
 def test_o2_complex16_build_band_energies_match_reference_logs():
