@@ -166,46 +166,6 @@ __global__ void __launch_bounds__(256) k_nl_scatter(const int* __restrict__ cov,
   }
 }
 
-// FP32 bands, four projectors per atom (s + p): the record's four uV values and each band's
-// four coefficients as one 16-byte load each (uV rows and coefficient rows are 16-byte aligned:
-// 4 floats per record, ldc = 4 x atoms), the same multiply-add order as k_nl_scatter.
-__global__ void __launch_bounds__(256) k_nl_scatter4f(const int* __restrict__ cov, int ncov,
-                                                      const int* __restrict__ rowptr, const int* __restrict__ rg,
-                                                      const float4* __restrict__ ru4, const float* __restrict__ coef,
-                                                      int ldc, float* __restrict__ out, long long ld, int nb,
-                                                      int bchunk) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= ncov) return;
-  const int pt = __ldg(cov + i);
-  const int r0 = __ldg(rowptr + pt), r1 = __ldg(rowptr + pt + 1);
-  const int b0 = blockIdx.y * bchunk, b1 = min(nb, b0 + bchunk);
-  constexpr int BU = 4;
-  for (int b = b0; b < b1; b += BU) {
-    float acc[BU], cur[BU];
-#pragma unroll
-    for (int u = 0; u < BU; ++u) {
-      acc[u] = 0.0f;
-      cur[u] = b + u < b1 ? out[(size_t)(b + u) * ld + pt] : 0.0f;
-    }
-    for (int r = r0; r < r1; ++r) {
-      const float4 w = __ldg(ru4 + r);
-      const size_t go = (size_t)__ldg(rg + r) * 4;
-#pragma unroll
-      for (int u = 0; u < BU; ++u) {
-        if (b + u >= b1) break;
-        const float4 cc = __ldg(reinterpret_cast<const float4*>(coef + (size_t)(b + u) * ldc + go));
-        acc[u] = ::fmaf(w.x, cc.x, acc[u]);
-        acc[u] = ::fmaf(w.y, cc.y, acc[u]);
-        acc[u] = ::fmaf(w.z, cc.z, acc[u]);
-        acc[u] = ::fmaf(w.w, cc.w, acc[u]);
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < BU; ++u)
-      if (b + u < b1) out[(size_t)(b + u) * ld + pt] = cur[u] + acc[u];
-  }
-}
-
 template <typename T>
 static int nl_scatter(Ctx& c, int k, const T* coef, T* out, size_t ld, int nb) {
   const NonlocalTables& nl = c.nl;
@@ -216,11 +176,7 @@ static int nl_scatter(Ctx& c, int k, const T* coef, T* out, size_t ld, int nb) {
   const int bchunk = 16;
   const dim3 grid((nl.ncov + 255) / 256, (nb + bchunk - 1) / bchunk);
   ProfScope ps(c, "nl_scatter", (double)nb * nl.ncov * 2.0 * sizeof(T) + (double)nl.nrec * (4 + nl.pg * sizeof(T)));
-  if (nl.pg == 4 && std::is_same<T, float>::value)
-    k_nl_scatter4f<<<grid, 256, 0, c.stream>>>(nl.cov.as<int>(), nl.ncov, nl.rec_rowptr.as<int>(), nl.rec_g.as<int>(),
-                                               reinterpret_cast<const float4*>(ru), reinterpret_cast<const float*>(coef),
-                                               ldc, reinterpret_cast<float*>(out), (long long)ld, nb, bchunk);
-  else if (nl.pg == 4)
+  if (nl.pg == 4)
     k_nl_scatter<T, 4><<<grid, 256, 0, c.stream>>>(nl.cov.as<int>(), nl.ncov, nl.rec_rowptr.as<int>(),
                                                     nl.rec_g.as<int>(), ru, nl.pg, coef, ldc, out, (long long)ld, nb,
                                                     bchunk);
