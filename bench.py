@@ -325,6 +325,7 @@ def run_ours(args, dist, rank, ws):
     if prec == api.PREC_MIXED:
         g.gemm_schedule(*sched)
     g.pc_form(args.pc_form)
+    g.stencil_form(args.stencil_form)
     if pc == "learned":
         g.lpc_set_weights(np.load(wpath))
     g.init_sweep(sweep_ref)
@@ -656,6 +657,7 @@ def run_kernel(args):
     if what == "hpsi":
         precs = {"both": ("fp64", "fp32"), "fp64": ("fp64",), "fp32": ("fp32",)}[args.hpsi_prec]
         with api.BandUpdate(prob, nonlocal_on=not args.no_nonlocal) as g:
+            g.stencil_form(args.stencil_form)
             # complex bands are interleaved (re, im): 2 ng reals each
             ncomp = 2 if prob.is_complex else 1
             x = torch.empty((nb, ncomp * prob.ng), dtype=torch.float64, device="cuda")
@@ -755,6 +757,8 @@ def main():
     ap.add_argument("--gemm-terms", default="3,3",
                     help="BF16 terms of the mixed overlap/Hsub and rotation contractions (2 or 3 each)")
     ap.add_argument("--pc-form", type=int, default=3, help="FP32 preconditioner form inside CG (3 s-step passes with the direction pass, 1 s-step passes, 2 fused, 0)")
+    ap.add_argument("--stencil-form", type=int, default=0,
+                    help="real-build hpsi stencil: 0 V_loc staged with the planes, 1 V_loc read from L2")
     ap.add_argument("--gemm-schedule", default="1e-2,1e-4",
                     help="mixed precision: two BF16 terms in overlap/Hsub, rotation while CG's residual > these")
     ap.add_argument("--kernel", default="solve", choices=["solve", "hpsi", "gemm", "pc", "cg", "lpc"],

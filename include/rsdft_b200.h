@@ -336,6 +336,11 @@ int rsdft_gpu_set_wait_polls(int polls);
  * stencil (one read-modify-write per covered point and band), 1 inside the streaming stencil
  * (records staged per plane).  Measurement knob; no counterpart in the reference. */
 int rsdft_gpu_set_nl_form(int fused);
+/* Real build's hpsi stencil: 0 (default) stages each plane's V_loc rows in shared memory with
+ * the psi rows, 1 the consumer threads read them from global memory (L2-resident), which leaves
+ * shared memory to more psi planes in flight.  Measurement knob; no counterpart in the
+ * reference. */
+int rsdft_gpu_set_stencil_form(int vloc_global);
 
 #ifdef __cplusplus
 }

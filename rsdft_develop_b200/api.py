@@ -52,7 +52,7 @@ EXPORTS = [
     "rsdft_gpu_hamiltonian_z", "rsdft_gpu_hamiltonian_f", "rsdft_gpu_hamiltonian_c",
     "rsdft_gpu_conjugate_gradient", "rsdft_gpu_gram_schmidt", "rsdft_gpu_subspace_diag",
     "rsdft_gpu_residual", "rsdft_gpu_precond_d", "rsdft_gpu_precond_f", "rsdft_gpu_set_pc_form", "rsdft_gpu_sweep", "rsdft_gpu_profile",
-    "rsdft_gpu_profile_get", "rsdft_gpu_kernel_launches", "rsdft_gpu_selftest_gemm", "rsdft_gpu_set_gemm_terms", "rsdft_gpu_set_gemm_tile", "rsdft_gpu_set_nl_form", "rsdft_gpu_init_sweep", "rsdft_gpu_set_wait_polls", "rsdft_gpu_set_precision", "rsdft_gpu_set_cggs", "rsdft_gpu_set_sweep_check", "rsdft_gpu_set_gemm_schedule",
+    "rsdft_gpu_profile_get", "rsdft_gpu_kernel_launches", "rsdft_gpu_selftest_gemm", "rsdft_gpu_set_gemm_terms", "rsdft_gpu_set_gemm_tile", "rsdft_gpu_set_nl_form", "rsdft_gpu_set_stencil_form", "rsdft_gpu_init_sweep", "rsdft_gpu_set_wait_polls", "rsdft_gpu_set_precision", "rsdft_gpu_set_cggs", "rsdft_gpu_set_sweep_check", "rsdft_gpu_set_gemm_schedule",
     "rsdft_gpu_hamiltonian_noalloc_d",
     "rsdft_gpu_set_vion", "rsdft_gpu_set_rho", "rsdft_gpu_get_rho", "rsdft_gpu_density", "rsdft_gpu_normalize_density",
     "rsdft_gpu_potential", "rsdft_gpu_init_mixing", "rsdft_gpu_sqerr", "rsdft_gpu_mix_density",
@@ -118,6 +118,7 @@ def load_library(path: str = LIB_PATH):
         "rsdft_gpu_sweep": [i, d, C.POINTER(C.c_int), vp, vp],
         "rsdft_gpu_selftest_gemm": [i, i, C.c_longlong, i, C.POINTER(C.c_double)],
         "rsdft_gpu_set_gemm_terms": [i, i], "rsdft_gpu_set_gemm_tile": [i], "rsdft_gpu_set_nl_form": [i],
+        "rsdft_gpu_set_stencil_form": [i],
         "rsdft_gpu_set_wait_polls": [i], "rsdft_gpu_set_precision": [i], "rsdft_gpu_set_cggs": [i],
         "rsdft_gpu_set_sweep_check": [i], "rsdft_gpu_set_gemm_schedule": [d, d],
         "rsdft_gpu_init_sweep": [i],
@@ -566,6 +567,11 @@ class BandUpdate:
         separate direction passes, 2 the fused z-streamed s-step form, 0 (or False) the
         recurrence form."""
         _call(self.lib.rsdft_gpu_set_pc_form, int(form))
+
+    def stencil_form(self, vloc_global: bool) -> None:
+        """Real build's hpsi stencil: V_loc rows staged in shared memory (False, the default) or
+        read from L2 by the consumer threads (True)."""
+        _call(self.lib.rsdft_gpu_set_stencil_form, int(bool(vloc_global)))
 
     def nl_form(self, fused: bool) -> None:
         """Nonlocal term of the real hpsi: inside the stencil (fused) or by a scatter after it."""

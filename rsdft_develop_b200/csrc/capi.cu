@@ -853,6 +853,13 @@ int rsdft_gpu_set_pc_form(int form) {
   return 0;
 }
 
+int rsdft_gpu_set_stencil_form(int vloc_global) {
+  REQUIRE_CTX();
+  RS_CHECK(vloc_global == 0 || vloc_global == 1, RSDFT_ERR_ARG, "vloc_global must be 0 or 1");
+  g_ctx->stencil_vloc_global = vloc_global;
+  return 0;
+}
+
 int rsdft_gpu_set_nl_form(int fused) {
   REQUIRE_CTX();
   RS_CHECK(fused == 0 || fused == 1, RSDFT_ERR_ARG, "fused must be 0 or 1");

@@ -127,6 +127,7 @@ struct Ctx {
   double sched_res_rot = 1e-4;     // sweeps: 2 rotation terms while CG's max residual > this (0: off)
   long long sched_sweeps = 0;      // (k, s) sweep steps run with reduced terms
   int pc_sstep = 1;                // FP32 precond_hprsdft: 1 s-step passes, 2 fused z-streamed s-step form
+  int stencil_vloc_global = 0;     // real-build stencil: V_loc rows read from L2 instead of staged
   int pc_direct = 1;               // s-step passes: the last one forms the CG direction P (no PG, no k_make_p)
                                    // inside CG, 0 the recurrence form
   int gemm_wide = 1;               // three-term GEMM tiles 128 x 256 (K blocks of 32), else 128 x 128

@@ -43,6 +43,7 @@ struct WsArgs {
   int vl_elems;         // tile_y rows of n1, rounded to 128 bytes
   int nst;              // stages in the ring
   int bar_off;          // byte offset of the barriers
+  int vlg;              // real build: 1 = V_loc rows read from global memory (L2), not staged
   T c0;
   T cx[MD], cy[MD], cz[MD];
   T cs[3][MD];          // complex build: coef_nabk(d, m); zcoef_kin(d, +m) = c_d(m) - i cs[d][m]
@@ -227,7 +228,7 @@ __global__ void __launch_bounds__(384, 1) k_stencil_ws(const WsArgs<T, MD> a) {
         const bool inch = q >= MD && p < it.zend;
         T* st = stages + (size_t)slot * sstride;
         const uint32_t bytes = (uint32_t)((size_t)rows * n1 * sizeof(T)) +
-                               (inch ? (uint32_t)((size_t)it.ty_valid * n1 * sizeof(T)) : 0u);
+                               (inch && !a.vlg ? (uint32_t)((size_t)it.ty_valid * n1 * sizeof(T)) : 0u);
         mbar_arrive_expect_tx(&full[slot], bytes);
         int r = 0;
         while (r < rows) {
@@ -237,7 +238,7 @@ __global__ void __launch_bounds__(384, 1) k_stencil_ws(const WsArgs<T, MD> a) {
                    &full[slot]);
           r += len;
         }
-        if (inch)
+        if (inch && !a.vlg)
           bulk_g2s(st + a.stage_elems, a.vloc + ((size_t)p * n2 + it.y0) * n1,
                    (uint32_t)((size_t)it.ty_valid * n1 * sizeof(T)), &full[slot]);
         ++issued;
@@ -314,6 +315,19 @@ __global__ void __launch_bounds__(384, 1) k_stencil_ws(const WsArgs<T, MD> a) {
         for (int j = 0; j < P; ++j) acc[q][r][j] = L::dup(T(0));
 
     for (int q = 0; q < it.nplanes; ++q) {
+      const int p = it.z0 - MD + q;
+      const bool inch = q >= MD && p < it.zend;
+      // V_loc rows from global memory (L2-resident), issued before the wait so that their
+      // latency overlaps it; rows past the tile are not read
+      typename L::U vlr[R];
+      if (a.vlg && inch) {
+        const T* vrow = a.vloc + ((size_t)p * n2 + it.y0 + yl) * n1 + x0;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          if (rowok[r]) vlr[r] = __ldg(reinterpret_cast<const typename L::U*>(vrow + (size_t)r * n1));
+          else vlr[r] = typename L::U{};
+        }
+      }
       if (!ws_wait(&full[slot], (uint32_t)(round & 1), abort_flag, a.polls)) {
         if (!*abort_flag) {
           *abort_flag = 1;
@@ -323,8 +337,6 @@ __global__ void __launch_bounds__(384, 1) k_stencil_ws(const WsArgs<T, MD> a) {
       }
       const uint32_t sb = sbase0 + (uint32_t)slot * sstride_b;
       const uint32_t a0 = sb + off0;
-      const int p = it.z0 - MD + q;
-      const bool inch = q >= MD && p < it.zend;
       P2 v[R][P], t[R][P];
       sfor<0, R>([&](auto rc) {
         constexpr int r = decltype(rc)::value;
@@ -337,7 +349,7 @@ __global__ void __launch_bounds__(384, 1) k_stencil_ws(const WsArgs<T, MD> a) {
         const uint32_t av = sb + offv;
         sfor<0, R>([&](auto rc) {
           constexpr int r = decltype(rc)::value;
-          const auto vl = ldrow(av, rc);
+          const auto vl = a.vlg ? vlr[r] : ldrow(av, rc);
 #pragma unroll
           for (int j = 0; j < P; ++j) t[r][j] = L::mul(L::add(c0, L::pair(vl, j)), v[r][j]);
         });
@@ -462,10 +474,13 @@ int launch_stencil_ws(Ctx& c, int k, int s, const T* psi, T* out, size_t ld, int
   const int rows = tile_y + 2 * MD;
   constexpr int AL = 128 / (int)sizeof(T);
   auto rnd = [&](int e) { return ((e + AL - 1) / AL) * AL; };
-  const int stage_elems = rnd(rows * n1), vl_elems = rnd(tile_y * n1);
+  // V_loc rows staged with the plane, or (vlg) read by the consumers from L2, which leaves the
+  // shared memory to more psi planes in flight
+  const int vlg = c.stencil_vloc_global && !vloc_override ? 1 : 0;
+  const int stage_elems = rnd(rows * n1), vl_elems = vlg ? 0 : rnd(tile_y * n1);
   const size_t stage_bytes = sizeof(T) * (size_t)(stage_elems + vl_elems);
   const size_t budget = 227 * 1024 - 256;
-  int S = (int)std::min<size_t>(8, budget / stage_bytes);
+  int S = (int)std::min<size_t>(vlg ? 12 : 8, budget / stage_bytes);
   RS_CHECK(S >= 2, RSDFT_ERR_UNSUPPORTED, "stencil stage (%zu B) does not fit shared memory twice", stage_bytes);
   const int bar_off = (int)(stage_bytes * S);
   const size_t smem = (size_t)bar_off + 16 * (size_t)S + 16;
@@ -510,6 +525,7 @@ int launch_stencil_ws(Ctx& c, int k, int s, const T* psi, T* out, size_t ld, int
   a.vl_elems = vl_elems;
   a.nst = S;
   a.bar_off = bar_off;
+  a.vlg = vlg;
   a.c0 = (T)(c.p.coef_lap0 + c.kp[k].const_k2 + c0_shift);
   for (int m = 0; m < MD; ++m) {
     a.cx[m] = (T)c.p.coef_lap[0][m];

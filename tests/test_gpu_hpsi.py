@@ -44,6 +44,23 @@ def test_hpsi_fp32_matches_oracle(oracle_mod, name):
 
 
 @pytest.mark.parametrize("fp32", [False, True])
+@pytest.mark.parametrize("name", ["t0", "t1", "c0", "c1", "c3"])
+def test_hpsi_vloc_from_l2_matches_oracle(oracle_mod, name, fp32):
+    """Stencil form 1: V_loc rows read from L2 by the consumer threads instead of staged with the
+    plane (generic and compile-time row lengths, ragged last y-tiles)."""
+    prob = synth.make_problem(name)
+    o = oracle_mod.Oracle(prob)
+    psi = synth.random_wavefunctions(25, 5, prob.ng)
+    if fp32:
+        psi = psi.astype(np.float32).astype(np.float64)
+    ref = o.hpsi(psi)
+    with api.BandUpdate(prob) as g:
+        g.stencil_form(True)
+        out = g.hamiltonian(psi, fp32=fp32)
+    assert _rel(out.astype(np.float64), ref) < (TOL32 if fp32 else TOL64)
+
+
+@pytest.mark.parametrize("fp32", [False, True])
 @pytest.mark.parametrize("name", ["t1", "c0", "c2"])
 def test_hpsi_nonlocal_forms_agree(oracle_mod, name, fp32):
     """The nonlocal term added inside the streaming stencil and by the scatter kernel after it
