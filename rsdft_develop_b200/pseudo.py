@@ -138,6 +138,7 @@ def read_psv(path: str, uspp: bool = False) -> PseudoPotential:
         verpot = 1
         znuc, zatom = 0.0, 0.0
         xc_pot = "LDAPZ81"                     # the reader assumes LDA PZ81 for version 1
+        rec.line()                             # one comment record follows the first
     xc_pot = str(xc_pot).strip("'\"")
     zatom = _f(str(zatom))
     nl = int(rec.values(1)[0])
