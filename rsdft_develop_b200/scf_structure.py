@@ -1,0 +1,230 @@
+"""SCF loop for structures read from pseudopotential files (PBE, one or two spins).
+
+The reference's calc_scf (src/scf_module.f90:85-563) around the band update, for the operators
+rsdft_develop_b200.structure builds: per iteration one sweep of every spin on the current
+V_loc, occupations, the density of the new bands, V_out = V_ion + V_H + V_xc^PBE of that
+density, calc_sqerr of (V_out, rho_out) against the previous iteration's pair
+(src/sqerr_module.f90:38-103) as the convergence test, then Pulay mixing of the spin densities,
+renormalisation per spin, and V_loc of the mixed density for the next iteration.  Occupations
+are the fixed-moment filling of the reference's first NFIXED iterations (src/fermi_module.f90):
+the lowest N_s bands of spin s, N_s = (Nelectron +- Ndspin) / 2 (the reference's O2 sample keeps
+that filling to convergence: its occupations print 1 / 0).  Energies follow calc_total_energy
+(src/total_energy_module.f90): Etot = E_kin + E_ion + E_nl + E_H + E_xc + E_ewald, with
+E_kin + E_nl = sum occ e - E_loc.
+
+The band update runs behind a small interface (set_vloc, sweep, density, bands): GpuBands drives
+the library's CUDA path through the C ABI; the tests drive the CPU oracle through the same loop.
+The potential, the mixing and the energies are host work, as in the reference.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+from . import api, gga, structure
+
+
+# ----------------------------------------------------------------------------
+# ion-ion energy
+# ----------------------------------------------------------------------------
+def ewald_energy(st: structure.Structure, eta: float | None = None, tol: float = 1e-14) -> float:
+    """Ewald energy of the ions (point charges Zps at the atoms, neutralising background) in the
+    orthorhombic cell, the quantity calc_ewald returns (src/ewald_module.f90:69-420):
+    1/2 sum'_{i,j,L} Z_i Z_j erfc(sqrt(eta) r) / r + (2 pi / V) sum_{G != 0} |S(G)|^2
+    exp(-G^2 / 4 eta) / G^2 - sqrt(eta / pi) sum Z_i^2 - pi Q^2 / (2 eta V)."""
+    L = np.array(st.lengths, dtype=np.float64)
+    vol = float(np.prod(L))
+    pos, z = [], []
+    for pp, p in st.species:
+        for a in np.asarray(p, np.float64).reshape(-1, 3):
+            pos.append(a * L)
+            z.append(pp.zps)
+    pos = np.array(pos)
+    z = np.array(z)
+    if eta is None:
+        eta = math.pi / vol ** (2.0 / 3.0)
+    se = math.sqrt(eta)
+    # real space: images until erfc(sqrt(eta) r) < tol
+    rcut = 1.0
+    while math.erfc(se * rcut) > tol:
+        rcut += 0.5
+    nimg = [int(math.ceil(rcut / L[d])) + 1 for d in range(3)]
+    er = 0.0
+    rng = [np.arange(-n, n + 1) for n in nimg]
+    sh = np.stack(np.meshgrid(*rng, indexing="ij"), axis=-1).reshape(-1, 3) * L
+    for i in range(len(z)):
+        for j in range(len(z)):
+            d = pos[i] - pos[j] + sh
+            r = np.sqrt(np.sum(d * d, axis=1))
+            keep = (r > 1e-12) & (r < rcut)
+            er += 0.5 * z[i] * z[j] * sum(math.erfc(se * x) / x for x in r[keep])
+    # reciprocal space: until exp(-G^2 / 4 eta) < tol
+    gmax = 2.0 * se * math.sqrt(-math.log(tol))
+    b = 2.0 * math.pi / L
+    ng = [int(math.ceil(gmax / b[d])) + 1 for d in range(3)]
+    m = np.stack(np.meshgrid(*[np.arange(-n, n + 1) for n in ng], indexing="ij"), axis=-1).reshape(-1, 3)
+    g = m * b
+    g2 = np.sum(g * g, axis=1)
+    keep = (g2 > 0) & (g2 <= gmax * gmax)
+    g, g2 = g[keep], g2[keep]
+    ph = g @ pos.T
+    s = (np.cos(ph) * z).sum(axis=1) + 1j * (np.sin(ph) * z).sum(axis=1)
+    eg = 2.0 * math.pi / vol * float(np.sum(np.abs(s) ** 2 * np.exp(-g2 / (4.0 * eta)) / g2))
+    q = float(z.sum())
+    return er + eg - se / math.sqrt(math.pi) * float(np.sum(z * z)) - math.pi * q * q / (2.0 * eta * vol)
+
+
+# ----------------------------------------------------------------------------
+# host pieces
+# ----------------------------------------------------------------------------
+def potential(su: structure.Setup, rho: np.ndarray):
+    """V_loc(s) = V_ion + V_H + V_xc^PBE(s) of rho (nspin, ng), and the energy pieces."""
+    st = su.structure
+    dV = su.problem.dV
+    h = (su.problem.h,) * 3
+    vh, eh = gga.hartree_sphere(rho.sum(axis=0), su.ggrid, dV)
+    vxc, ex, ec = gga.pbe(rho, su.problem.n, h, dV, st.md)
+    v = su.vion[None, :] + vh[None, :] + vxc
+    return v, {"hartree": eh, "xc": ex + ec, "exchange": ex, "correlation": ec,
+               "ion_local": float(np.sum(rho.sum(axis=0) * su.vion)) * dV,
+               "local": float(np.sum(rho * v)) * dV}
+
+
+class Pulay:
+    """Pulay (DIIS) mixing of the density vector (both spins together), history mmix, step beta:
+    rho_in' = sum_i c_i (rho_in,i + beta (rho_out,i - rho_in,i)) with sum c_i = 1 minimising
+    |sum_i c_i (rho_out,i - rho_in,i)|."""
+
+    def __init__(self, mmix: int = 4, beta: float = 0.5):
+        self.mmix, self.beta = mmix, beta
+        self.xin, self.res = [], []
+
+    def mix(self, rin: np.ndarray, rout: np.ndarray) -> np.ndarray:
+        self.xin.append(rin.ravel().copy())
+        self.res.append((rout - rin).ravel().copy())
+        self.xin, self.res = self.xin[-self.mmix:], self.res[-self.mmix:]
+        n = len(self.res)
+        A = np.array([[float(np.dot(a, b)) for b in self.res] for a in self.res])
+        A += 1e-14 * np.trace(A) * np.eye(n)
+        c = np.linalg.solve(A, np.ones(n))
+        c /= c.sum()
+        x = sum(ci * xi for ci, xi in zip(c, self.xin))
+        r = sum(ci * ri for ci, ri in zip(c, self.res))
+        return (x + self.beta * r).reshape(rin.shape)
+
+
+def nonlocal_energy(su: structure.Setup, psi: np.ndarray, occ: np.ndarray) -> float:
+    """sum_n occ_n sum_lma iuV(lma) (dV sum_j uV(j, lma) psi_n(JJP(j, lma)))^2 for one spin."""
+    ps = su.projectors
+    dV = su.problem.dV
+    e = 0.0
+    for p in range(ps.nzlma):
+        m = int(ps.mjj[p])
+        idx = ps.jjp[p, :m] - 1
+        c = dV * (psi[:, idx] @ ps.uv[p, :m])
+        e += float(ps.iuv[p]) * float(np.sum(occ * c * c))
+    return e
+
+
+# ----------------------------------------------------------------------------
+# the band update behind the loop
+# ----------------------------------------------------------------------------
+class GpuBands:
+    """The library's CUDA band update (all spins in one context) for the SCF loop."""
+
+    def __init__(self, su: structure.Setup, precision: int = api.PREC_FP64, seed: int = 1):
+        self.su = su
+        self.ns = su.structure.nspin
+        self.g = api.BandUpdate(su.problem_for_spin(1), precision=precision, nspin=self.ns)
+        for s in range(2, self.ns + 1):
+            self.g.set_vloc(su.vloc[s - 1], s=s)
+        for s in range(1, self.ns + 1):
+            self.g.random_wf(seed + s - 1, s=s)
+            self.g.gram_schmidt(s=s)
+
+    def set_vloc(self, v: np.ndarray):
+        for s in range(self.ns):
+            self.g.set_vloc(v[s], s=s + 1)
+
+    def sweep(self, n: int) -> np.ndarray:
+        _, esp, _ = self.g.calc_sweep(n)
+        return esp[:, 0, :].copy()
+
+    def density(self, occ: np.ndarray) -> np.ndarray:
+        self.g.density(occ[:, None, :])
+        return self.g.get_rho()[0]
+
+    def bands(self, s: int) -> np.ndarray:
+        return self.g.get_wf(s=s + 1)
+
+    def close(self):
+        self.g.close()
+
+
+@dataclasses.dataclass
+class StructureScf:
+    iterations: int
+    converged: bool
+    esp: np.ndarray               # (nspin, nband) of the last sweep
+    occ: np.ndarray
+    rho: np.ndarray               # output density of the last iteration
+    sqerr: list                   # per iteration: sqerr of V_out (per spin) + of rho_out (per spin)
+    energies: dict
+
+
+def run_scf_structure(su: structure.Setup, bands, nsweep: int = 10, diter: int = 100, scf_conv: float = 1e-11,
+                      mmix: int = 1, beta: float = 0.5) -> StructureScf:
+    """calc_scf for su with the band update `bands` (GpuBands or a test adapter): nsweep sweeps on
+    the potential of the initial density, then up to diter iterations until the squared change
+    of V_out (mean over the grid, every spin) is <= scf_conv.  Mixing: linear with step beta by
+    default (mmix = 1); mmix > 1 is Pulay over that many iterations.  With PBE, V_out near the
+    vacuum reacts to density tails around the reference's 1e-10 density cut, so the squared
+    change of V levels off near 1e-12 while energies and eigenvalues are converged to 1e-8."""
+    st = su.structure
+    ns, nb = st.nspin, st.nband
+    dV = su.problem.dV
+    nel = np.asarray(su.nelectron_spin)
+    if np.any(np.abs(nel - np.round(nel)) > 1e-12):
+        raise NotImplementedError("fixed-moment filling needs integer electrons per spin")
+    nocc = [int(round(x)) for x in (nel if ns == 2 else nel / 2.0)]
+    occ = np.zeros((ns, nb))
+    for s in range(ns):
+        occ[s, :nocc[s]] = 1.0 if ns == 2 else 2.0
+    bands.set_vloc(su.vloc)
+    if nsweep > 0:
+        bands.sweep(nsweep)
+    rho_in = su.rho.copy()
+    prev = (su.vloc.copy(), su.rho.copy())
+    mixer = Pulay(mmix, beta)
+    hist = []
+    conv = False
+    esp = rho_out = ene = None
+    it = 0
+    for it in range(1, diter + 1):
+        esp = bands.sweep(1)
+        rho_out = bands.density(occ)
+        v_out, ene = potential(su, rho_out)
+        sq = [float(np.mean((v_out[s] - prev[0][s]) ** 2)) for s in range(ns)] + \
+             [float(np.mean((rho_out[s] - prev[1][s]) ** 2)) for s in range(ns)]
+        hist.append(sq)
+        prev = (v_out, rho_out)
+        if max(sq[:ns]) <= scf_conv:
+            conv = True
+            break
+        rho_in = mixer.mix(rho_in, rho_out)
+        for s in range(ns):
+            rho_in[s] *= (occ[s].sum()) / (float(rho_in[s].sum()) * dV)
+        v_in, _ = potential(su, rho_in)
+        bands.set_vloc(v_in)
+    e_sum = float(np.sum(occ * esp))
+    e_nl = sum(nonlocal_energy(su, bands.bands(s), occ[s]) for s in range(ns))
+    ene = dict(ene)
+    ene["sum_eigen"] = e_sum
+    ene["nonlocal"] = e_nl
+    ene["kinetic"] = e_sum - ene["local"] - e_nl
+    ene["ewald"] = ewald_energy(st)
+    ene["total"] = (ene["kinetic"] + ene["ion_local"] + e_nl + ene["hartree"] + ene["xc"] + ene["ewald"])
+    ene["spin_abs"] = float(np.sum(np.abs(rho_out[0] - rho_out[-1]))) * dV if ns == 2 else 0.0
+    return StructureScf(iterations=it, converged=conv, esp=esp, occ=occ, rho=rho_out, sqerr=hist, energies=ene)

@@ -11,7 +11,8 @@ pseudopotential, the G sphere of Init_Ggrid (Ecut, Gcut, NGgrid, NMGL), construc
 density sums, the band energies of scf_iter 1 (both spins: they belong to the operator built
 from the initial density, the same one the preceding sweeps converged), and what scf_iter 1
 prints about the density of those bands (charges, sum |rho_up - rho_down| dV, and the squared
-changes of V_loc and rho from the initial ones).  The tests use the JSON
+changes of V_loc and rho from the initial ones); and the first SCF cycle's converged state (the
+energy terms printed after its SCF END, its last eigenvalues and spin-density sum).  The tests use the JSON
 file only, so they run where the reference tree is absent.
 """
 import glob
@@ -161,6 +162,50 @@ def parse_o2(path):
     return out
 
 
+ENERGY_KEYS = {
+    "Total Energy": "total", "Ion-Ion": "ewald", "Local Potential": "local",
+    "Ion Local Potential": "ion_local", "Ion Nonlocal Potential": "nonlocal", "Kinetic Energy": "kinetic",
+    "Hartree Energy": "hartree", "Exchange-Correlation Energy": "xc", "Exchange Energy": "exchange",
+    "Correlation Energy": "correlation", "Sum of eigenvalues": "sum_eigen", "Fermi energy": "fermi",
+}
+
+
+def parse_o2_scf(path):
+    """The first SCF cycle's converged state (before the atoms move): the energy block printed
+    after its SCF END, and the eigenvalue table and sum |rho_up - rho_down| of its last
+    iteration."""
+    txt = open(path).read().splitlines()
+    end = next(i for i, l in enumerate(txt) if "SCF END" in l)
+    out = {"source": os.path.relpath(path, os.path.dirname(REF))}
+    m = re.search(r"total # of iteration =\s*(\d+)", "\n".join(txt[end:end + 3]))
+    out["iterations"] = int(m.group(1)) if m else None
+    ene = {}
+    start = next(i for i in range(end, len(txt)) if txt[i].strip().endswith("total energy"))
+    for line in txt[start + 1:start + 40]:
+        if line.startswith("----"):
+            break
+        for label, key in ENERGY_KEYS.items():
+            mm = re.match(re.escape(label) + r"\s+([-+0-9.Ee]+)", line.strip())
+            if mm and key not in ene:
+                ene[key] = float(mm.group(1))
+                break
+    out["energies"] = ene
+    last = max(i for i in range(end) if "scf_iter=" in txt[i])
+    for j in range(last, end):
+        t = txt[j].strip()
+        if t.startswith("sum|rho_up-rho_down|"):
+            out["sum_abs_spin"] = float(t.split(":")[1])
+        if "esp(n,k,s)" in t:
+            rows = []
+            for jj in range(j + 1, j + 40):
+                f = txt[jj].split()
+                if len(f) != 8:
+                    break
+                rows.append([int(f[0]), int(f[1])] + [float(x) for x in f[2:]])
+            out["esp"] = rows
+    return out
+
+
 def main():
     logs = sorted(glob.glob(os.path.join(REF, "*", "02_O2-molecule_optimize", "real8", "result", "a.log")))
     data = [parse(p) for p in logs]
@@ -169,8 +214,12 @@ def main():
     bz = [b for b in bz if "mmm" in b and b.get("kpoints")]
     o2 = [parse_o2(p) for p in sorted(glob.glob(os.path.join(REF, "*", "02_O2-molecule_optimize", "*", "result", "a.log")))]
     o2 = [d for d in o2 if d.get("psv") and d.get("esp_scf1") and d.get("initrho")]
-    json.dump({"kinetic": data, "bz": bz, "o2": o2}, open(os.path.join(HERE, "reference_logs.json"), "w"), indent=1)
-    print(f"{len(data)} kinetic tables, {len(bz)} k-point lists, {len(o2)} O2 set-up/eigenvalue records -> reference_logs.json")
+    o2_scf = [parse_o2_scf(p) for p in sorted(glob.glob(os.path.join(REF, "*", "02_O2-molecule_optimize", "*", "result", "a.log")))]
+    o2_scf = [d for d in o2_scf if d.get("esp") and d["energies"].get("total") is not None]
+    json.dump({"kinetic": data, "bz": bz, "o2": o2, "o2_scf": o2_scf}, open(os.path.join(HERE, "reference_logs.json"), "w"),
+              indent=1)
+    print(f"{len(data)} kinetic tables, {len(bz)} k-point lists, {len(o2)} O2 set-up/eigenvalue records, "
+          f"{len(o2_scf)} converged O2 SCF records -> reference_logs.json")
 
 
 if __name__ == "__main__":

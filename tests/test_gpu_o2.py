@@ -104,3 +104,17 @@ def test_o2_mixed_precision_then_fp64_polish(o2):
         it2, esp, res = g.calc_sweep(40, tol=1e-18)
         assert np.max(res[:, 0, :7]) <= 1e-18, (it2, res[:, 0, :7])
         _check(esp)
+
+
+def test_o2_scf_on_the_gpu_reaches_the_reference_state(o2):
+    """The SCF loop for PSV structures (rsdft_develop_b200.scf_structure) with the CUDA band
+    update, FP64: the converged energy terms, eigenvalues and spin-density sum of the reference's
+    first O2 SCF cycle (tolerances of tests/test_scf_structure_cpu.py)."""
+    from rsdft_develop_b200 import scf_structure
+    from tests.test_scf_structure_cpu import check_against_logs
+    bands = scf_structure.GpuBands(o2, precision=api.PREC_FP64)
+    try:
+        res = scf_structure.run_scf_structure(o2, bands, nsweep=10, diter=60)
+    finally:
+        bands.close()
+    check_against_logs(res)
