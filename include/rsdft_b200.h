@@ -238,6 +238,12 @@ int rsdft_gpu_sqerr(double* sqerr);
  * (src/mixing/mixing_pulay_module.f90:29-111): the device density becomes the mixed one
  * (beta search for beta > 1 as the reference); beta_used (may be NULL) receives the beta taken. */
 int rsdft_gpu_mix_density(double* beta_used);
+/* GGA-PBE exchange-correlation potential of the host density rho (nspin x ML0, Fortran order
+ * rho(ML0, nspin)), as calc_GGAPBE96_2 forms it (src/xc/xc_ggapbe96_2_module.f90:26-370: FD
+ * gradient of the total density of order Md, densities <= 1e-10 skipped): vxc (nspin x ML0,
+ * host) and, if exc is not NULL, exc[0] = E_x, exc[1] = E_c.  Uses the context's grid, H and
+ * Md (<= 6). */
+int rsdft_gpu_xc_pbe(const double* rho, double* vxc, double* exc);
 
 /* ---- learned preconditioner (no counterpart in the reference) ----
  * A 4-layer 3-D convolutional network, channels 1-16-16-16-1, 3x3x3 kernels, no biases, tanh

@@ -55,7 +55,7 @@ EXPORTS = [
     "rsdft_gpu_profile_get", "rsdft_gpu_kernel_launches", "rsdft_gpu_selftest_gemm", "rsdft_gpu_set_gemm_terms", "rsdft_gpu_set_gemm_tile", "rsdft_gpu_set_nl_form", "rsdft_gpu_set_stencil_form", "rsdft_gpu_init_sweep", "rsdft_gpu_set_wait_polls", "rsdft_gpu_set_precision", "rsdft_gpu_set_cggs", "rsdft_gpu_set_sweep_check", "rsdft_gpu_set_gemm_schedule",
     "rsdft_gpu_hamiltonian_noalloc_d",
     "rsdft_gpu_set_vion", "rsdft_gpu_set_rho", "rsdft_gpu_get_rho", "rsdft_gpu_density", "rsdft_gpu_normalize_density",
-    "rsdft_gpu_potential", "rsdft_gpu_init_mixing", "rsdft_gpu_sqerr", "rsdft_gpu_mix_density",
+    "rsdft_gpu_potential", "rsdft_gpu_init_mixing", "rsdft_gpu_sqerr", "rsdft_gpu_mix_density", "rsdft_gpu_xc_pbe",
     "rsdft_gpu_lpc_init", "rsdft_gpu_lpc_set_weights", "rsdft_gpu_lpc_get_weights", "rsdft_gpu_lpc_forward",
     "rsdft_gpu_lpc_loss_grad", "rsdft_gpu_lpc_dataset", "rsdft_gpu_lpc_harvest", "rsdft_gpu_lpc_dataset_get",
     "rsdft_gpu_lpc_dataset_add", "rsdft_gpu_lpc_train", "rsdft_gpu_lpc_precond_f", "rsdft_gpu_lpc_status",
@@ -108,6 +108,7 @@ def load_library(path: str = LIB_PATH):
         "rsdft_gpu_set_vion": [vp, i], "rsdft_gpu_set_rho": [vp, i], "rsdft_gpu_get_rho": [vp, vp, vp],
         "rsdft_gpu_density": [vp], "rsdft_gpu_normalize_density": [d], "rsdft_gpu_potential": [vp],
         "rsdft_gpu_init_mixing": [i, d], "rsdft_gpu_sqerr": [vp], "rsdft_gpu_mix_density": [vp],
+        "rsdft_gpu_xc_pbe": [vp, vp, vp],
         "rsdft_gpu_hamiltonian_d": [i, i, vp, vp, i, i, i], "rsdft_gpu_hamiltonian_z": [i, i, vp, vp, i, i, i],
         "rsdft_gpu_hamiltonian_f": [i, i, vp, vp, i, i, i], "rsdft_gpu_hamiltonian_c": [i, i, vp, vp, i, i, i],
         "rsdft_gpu_conjugate_gradient": [i, i, vp, vp], "rsdft_gpu_gram_schmidt": [i, i],
@@ -363,6 +364,15 @@ class BandUpdate:
         e = np.zeros(2 * int(self.params.nspin))
         _call(self.lib.rsdft_gpu_sqerr, _ptr(e))
         return e
+
+    def xc_pbe(self, rho: np.ndarray):
+        """GGA-PBE V_xc (nspin, ng) and (E_x, E_c) of the host density rho (nspin, ng) on the device."""
+        ns = int(self.params.nspin)
+        r = np.ascontiguousarray(rho, dtype=np.float64).reshape(ns, self.prob.ng)
+        v = np.zeros((ns, self.prob.ng))
+        e = np.zeros(2)
+        _call(self.lib.rsdft_gpu_xc_pbe, _ptr(r), _ptr(v), _ptr(e))
+        return v, float(e[0]), float(e[1])
 
     def mix_density(self) -> float:
         b = np.zeros(1)

@@ -66,6 +66,7 @@ struct ProfEntry {
 struct ScfState {
   DBuf vion, rho, vh, vxc, occ, work, part, ones;
   DBuf xin, xou, xin_bak, xou_bak, xold_f, xold_g, h, f0, w;
+  DBuf gga;                     // rsdft_gpu_xc_pbe: density, gradient, fluxes, potentials, partials
   bool have_rho = false, mixing = false, plans = false;
   int plan_f = 0, plan_b = 0;   // cuFFT handles (D2Z, Z2D)
   int mmix = 4, mmix_count = 0;

@@ -578,7 +578,7 @@ void scf_release(Ctx& c) {
     m.plans = false;
   }
   DBuf* bufs[] = {&m.vion, &m.rho, &m.vh, &m.vxc, &m.occ, &m.work, &m.part, &m.ones, &m.xin, &m.xou,
-                  &m.xin_bak, &m.xou_bak, &m.xold_f, &m.xold_g, &m.h, &m.f0, &m.w};
+                  &m.xin_bak, &m.xou_bak, &m.xold_f, &m.xold_g, &m.h, &m.f0, &m.w, &m.gga};
   for (DBuf* b : bufs) b->release();
   m.have_rho = m.mixing = false;
 }

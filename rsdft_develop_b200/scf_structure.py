@@ -12,9 +12,11 @@ that filling to convergence: its occupations print 1 / 0).  Energies follow calc
 (src/total_energy_module.f90): Etot = E_kin + E_ion + E_nl + E_H + E_xc + E_ewald, with
 E_kin + E_nl = sum occ e - E_loc.
 
-The band update runs behind a small interface (set_vloc, sweep, density, bands): GpuBands drives
-the library's CUDA path through the C ABI; the tests drive the CPU oracle through the same loop.
-The potential, the mixing and the energies are host work, as in the reference.
+The band update runs behind a small interface (set_vloc, sweep, density, bands, and optionally
+xc): GpuBands drives the library's CUDA path through the C ABI (band update, density and the
+PBE potential on the device); the tests drive the CPU oracle through the same loop.  The
+Hartree solve on the cut-off sphere, the mixing and the energies are host work, as in the
+reference.
 """
 from __future__ import annotations
 
@@ -79,13 +81,17 @@ def ewald_energy(st: structure.Structure, eta: float | None = None, tol: float =
 # ----------------------------------------------------------------------------
 # host pieces
 # ----------------------------------------------------------------------------
-def potential(su: structure.Setup, rho: np.ndarray):
-    """V_loc(s) = V_ion + V_H + V_xc^PBE(s) of rho (nspin, ng), and the energy pieces."""
+def potential(su: structure.Setup, rho: np.ndarray, xc=None):
+    """V_loc(s) = V_ion + V_H + V_xc^PBE(s) of rho (nspin, ng), and the energy pieces.  xc: a
+    callable rho -> (V_xc, E_x, E_c) (the device PBE of GpuBands); the host PBE otherwise."""
     st = su.structure
     dV = su.problem.dV
     h = (su.problem.h,) * 3
     vh, eh = gga.hartree_sphere(rho.sum(axis=0), su.ggrid, dV)
-    vxc, ex, ec = gga.pbe(rho, su.problem.n, h, dV, st.md)
+    if xc is not None:
+        vxc, ex, ec = xc(rho)
+    else:
+        vxc, ex, ec = gga.pbe(rho, su.problem.n, h, dV, st.md)
     v = su.vion[None, :] + vh[None, :] + vxc
     return v, {"hartree": eh, "xc": ex + ec, "exchange": ex, "correlation": ec,
                "ion_local": float(np.sum(rho.sum(axis=0) * su.vion)) * dV,
@@ -156,6 +162,10 @@ class GpuBands:
         self.g.density(occ[:, None, :])
         return self.g.get_rho()[0]
 
+    def xc(self, rho: np.ndarray):
+        """PBE V_xc and (E_x, E_c) of rho on the device (rsdft_gpu_xc_pbe)."""
+        return self.g.xc_pbe(rho)
+
     def bands(self, s: int) -> np.ndarray:
         return self.g.get_wf(s=s + 1)
 
@@ -192,6 +202,7 @@ def run_scf_structure(su: structure.Setup, bands, nsweep: int = 10, diter: int =
     occ = np.zeros((ns, nb))
     for s in range(ns):
         occ[s, :nocc[s]] = 1.0 if ns == 2 else 2.0
+    xc = getattr(bands, "xc", None)
     bands.set_vloc(su.vloc)
     if nsweep > 0:
         bands.sweep(nsweep)
@@ -205,7 +216,7 @@ def run_scf_structure(su: structure.Setup, bands, nsweep: int = 10, diter: int =
     for it in range(1, diter + 1):
         esp = bands.sweep(1)
         rho_out = bands.density(occ)
-        v_out, ene = potential(su, rho_out)
+        v_out, ene = potential(su, rho_out, xc)
         sq = [float(np.mean((v_out[s] - prev[0][s]) ** 2)) for s in range(ns)] + \
              [float(np.mean((rho_out[s] - prev[1][s]) ** 2)) for s in range(ns)]
         hist.append(sq)
@@ -216,7 +227,7 @@ def run_scf_structure(su: structure.Setup, bands, nsweep: int = 10, diter: int =
         rho_in = mixer.mix(rho_in, rho_out)
         for s in range(ns):
             rho_in[s] *= (occ[s].sum()) / (float(rho_in[s].sum()) * dV)
-        v_in, _ = potential(su, rho_in)
+        v_in, _ = potential(su, rho_in, xc)
         bands.set_vloc(v_in)
     e_sum = float(np.sum(occ * esp))
     e_nl = sum(nonlocal_energy(su, bands.bands(s), occ[s]) for s in range(ns))
