@@ -37,6 +37,8 @@ class OrcProb(C.Structure):
         ("ncg", C.c_int), ("mloop", C.c_int),
         ("is_complex", C.c_int),
         ("cggs", C.c_int),
+        ("ggg_x", C.c_double * 3),
+        ("coef_nab", (C.c_double * MDMAX) * 3),
     ]
 
 
@@ -95,6 +97,13 @@ class Oracle:
                 p.zc_im[d][m] = kin["zcoef_kin"][k, d, m].imag
         p.coef_lap0 = kin["coef_lap0"]
         p.const_k2 = kin["const_k2"][k]
+        ggg = np.asarray(kin.get("ggg", np.ones(3)), np.float64)
+        if ggg.size >= 6 and np.any(ggg[3:6] != 0.0):
+            for q in range(3):
+                p.ggg_x[q] = float(ggg[3 + q])
+            for d in range(3):
+                for m in range(prob.md):
+                    p.coef_nab[d][m] = kin["coef_nab"][d, m]
         h = prob.h
         p.pc_c0 = 3.0 / h ** 2
         for d in range(3):

@@ -83,6 +83,8 @@ struct OrcProb {
   int ncg, mloop;
   int is_complex;
   int cggs;                        // SWGS: 0 off, 1 cggs_1, 2 cggs_2 (bands then run in order)
+  double ggg_x[3];                 // ggg(4:6): metric of the grid-axis pairs (1,2), (2,3), (3,1)
+  double coef_nab[3][ORC_MDMAX];   // coef_nab(d, m) = nab(m) / H_d, m = 1..md
 };
 
 static inline double conj_(double x) { return x; }
@@ -137,6 +139,46 @@ static void kinetic_band(const OrcProb* P, const T* tpsi, T* htpsi, std::vector<
         }
         htpsi[j] = acc;
       }
+  // non-orthogonal cells: -ggg(4) D_1 D_2 - ggg(5) D_2 D_3 - ggg(6) D_3 D_1 with the FD first
+  // derivatives D_d, applied in the reference's factored form (t = D_a psi, then D_b t;
+  // flag_n12/n23/n31 of src/kinetic/z_kinetic_sol_module.f90:351-530); real coefficients, the
+  // same for every k
+  if (P->ggg_x[0] != 0.0 || P->ggg_x[1] != 0.0 || P->ggg_x[2] != 0.0) {
+    static const int ax[3][2] = {{0, 1}, {1, 2}, {2, 0}};
+    const size_t ng = (size_t)n1 * n2 * n3;
+    thread_local std::vector<T> t;
+    t.resize(ng);
+    const int nn[3] = {n1, n2, n3};
+    for (int q = 0; q < 3; ++q) {
+      if (P->ggg_x[q] == 0.0) continue;
+      const int a = ax[q][0], b = ax[q][1];
+      for (int i3 = 0; i3 < n3; ++i3)
+        for (int i2 = 0; i2 < n2; ++i2)
+          for (int i1 = 0; i1 < n1; ++i1) {
+            T d = T(0);
+            for (int m = 1; m <= md; ++m) {
+              int e[3] = {0, 0, 0};
+              e[a] = m;
+              d += P->coef_nab[a][m - 1] * (W(i1 + e[0], i2 + e[1], i3 + e[2]) - W(i1 - e[0], i2 - e[1], i3 - e[2]));
+            }
+            t[i1 + (size_t)n1 * (i2 + (size_t)n2 * i3)] = d;
+          }
+      for (int i3 = 0; i3 < n3; ++i3)
+        for (int i2 = 0; i2 < n2; ++i2)
+          for (int i1 = 0; i1 < n1; ++i1) {
+            const int i[3] = {i1, i2, i3};
+            T d = T(0);
+            for (int m = 1; m <= md; ++m) {
+              int ip[3] = {i1, i2, i3}, im[3] = {i1, i2, i3};
+              ip[b] = (i[b] + m) % nn[b];
+              im[b] = (i[b] - m + nn[b]) % nn[b];
+              d += P->coef_nab[b][m - 1] * (t[ip[0] + (size_t)n1 * (ip[1] + (size_t)n2 * ip[2])] -
+                                            t[im[0] + (size_t)n1 * (im[1] + (size_t)n2 * im[2])]);
+            }
+            htpsi[i1 + (size_t)n1 * (i2 + (size_t)n2 * i3)] -= P->ggg_x[q] * d;
+          }
+    }
+  }
 }
 
 template <typename T> static T uv_at(const OrcProb* P, size_t idx);

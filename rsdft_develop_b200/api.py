@@ -167,6 +167,10 @@ class BandUpdate:
     def __init__(self, prob: "synth.Problem", precision: int = PREC_FP64, pc_mode: int = PC_HPRSDFT,
                  ncg: int = 3, mloop: int = 3, cg_block: int = 0, nonlocal_on: bool = True,
                  nspin: int = 1):
+        ggg = np.asarray(prob.kin["ggg"], np.float64)
+        if ggg.size > 3 and np.any(ggg[3:] != 0.0):
+            raise NotImplementedError("non-orthogonal cell: the device stencil has no cross-derivative "
+                                      "terms (ggg(4:6) of init_kinetic)")
         self.lib = load_library()
         self.prob = prob
         self.cplx = prob.is_complex

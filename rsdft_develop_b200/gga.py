@@ -29,33 +29,58 @@ def _fd_derivative(f3: np.ndarray, axis: int, nab: np.ndarray, md: int) -> np.nd
     return g
 
 
-def gradient(f: np.ndarray, n: tuple, h: tuple, md: int = 6):
-    """(gx, gy, gz) of a grid function (x fastest) by the reference's FD nabla."""
+def grid_metric(cell, n: tuple) -> np.ndarray:
+    """b(:, j) = |a_j| b_j / (2 pi H_j) of calc_GGAPBE96_2 (src/xc/xc_ggapbe96_2_module.f90:70-73)
+    as the columns of a 3 x 3 array: the Cartesian gradient is sum_j b(:, j) D_j f with D_j the
+    unscaled FD derivative along grid axis j.  cell: three lattice vectors (rows, bohr)."""
+    A = np.asarray(cell, np.float64)
+    vol = float(np.dot(A[0], np.cross(A[1], A[2])))
+    B = 2.0 * math.pi / vol * np.array([np.cross(A[1], A[2]), np.cross(A[2], A[0]), np.cross(A[0], A[1])])
+    out = np.zeros((3, 3))
+    for j in range(3):
+        aj = float(np.sqrt(np.sum(A[j] ** 2)))
+        out[:, j] = aj * B[j] / (2.0 * math.pi * (aj / n[j]))
+    return out
+
+
+def gradient(f: np.ndarray, n: tuple, h: tuple, md: int = 6, bmat: np.ndarray | None = None):
+    """(gx, gy, gz) of a grid function (x fastest) by the reference's FD nabla; bmat (grid_metric)
+    for a non-orthogonal cell, else the grid spacings h of an orthorhombic one."""
     nab = fd_nab_coef(md)
     f3 = f.reshape(n[2], n[1], n[0])
+    if bmat is not None:
+        d = [_fd_derivative(f3, 2 - j, nab, md).reshape(-1) for j in range(3)]
+        return tuple(bmat[c, 0] * d[0] + bmat[c, 1] * d[1] + bmat[c, 2] * d[2] for c in range(3))
     gx = _fd_derivative(f3, 2, nab, md) / h[0]
     gy = _fd_derivative(f3, 1, nab, md) / h[1]
     gz = _fd_derivative(f3, 0, nab, md) / h[2]
     return gx.reshape(-1), gy.reshape(-1), gz.reshape(-1)
 
 
-def _divergence_term(rx, ry, rz, n, h, md):
-    """sum_j d/dx_j (r_j) with the FD nabla, as calc_PBE_x/c apply it (f scaled by 1/h_j,
-    unscaled FD derivative)."""
+def _divergence_term(rx, ry, rz, n, h, md, bmat=None):
+    """sum_j D_j (f_j) with the FD nabla, as calc_PBE_x/c apply it: f_j = sum_c r_c b(c, j)
+    (r_j / h_j in an orthorhombic cell), unscaled FD derivative."""
     nab = fd_nab_coef(md)
     out = np.zeros(rx.size)
+    if bmat is not None:
+        for j in range(3):
+            f3 = (rx * bmat[0, j] + ry * bmat[1, j] + rz * bmat[2, j]).reshape(n[2], n[1], n[0])
+            out += _fd_derivative(f3, 2 - j, nab, md).reshape(-1)
+        return out
     for axis3, r, hj in ((2, rx, h[0]), (1, ry, h[1]), (0, rz, h[2])):
         f3 = (r / hj).reshape(n[2], n[1], n[0])
         out += _fd_derivative(f3, axis3, nab, md).reshape(-1)
     return out
 
 
-def pbe(rho: np.ndarray, n: tuple, h: tuple, dV: float, md: int = 6, mu: float = 0.21951, kp: float = 0.804):
-    """calc_GGAPBE96_2 for rho of shape (nspin, ng): returns (vxc (nspin, ng), Ex, Ec)."""
+def pbe(rho: np.ndarray, n: tuple, h: tuple, dV: float, md: int = 6, mu: float = 0.21951, kp: float = 0.804,
+        bmat: np.ndarray | None = None):
+    """calc_GGAPBE96_2 for rho of shape (nspin, ng): returns (vxc (nspin, ng), Ex, Ec).  bmat:
+    grid_metric of a non-orthogonal cell (h is then unused)."""
     rho = np.atleast_2d(np.asarray(rho, np.float64))
     ns = rho.shape[0]
     beta = mu * 3.0 / math.pi ** 2
-    gx, gy, gz = gradient(rho.sum(axis=0), n, h, md)
+    gx, gy, gz = gradient(rho.sum(axis=0), n, h, md, bmat)
     gg = gx * gx + gy * gy + gz * gz
     pi = math.pi
     # exchange, per spin with trho = 2 rho_s (spin scaling), the gradient of the total density
@@ -75,7 +100,7 @@ def pbe(rho: np.ndarray, n: tuple, h: tuple, dV: float, md: int = 6, mu: float =
         ex_sum += float(np.sum(np.where(ok, t * ex_lda * Fx, 0.0)))
         v = Fx * vx_lda + 24.0 * pi * kp * kp * mu * t ** 3 * gg / den ** 2
         rt = np.where(ok, -18.0 * pi * kp * kp * mu * t ** 4 / den ** 2, rt)
-        vx[s] = np.where(ok, v, 0.0) - _divergence_term(rt * gx, rt * gy, rt * gz, n, h, md)
+        vx[s] = np.where(ok, v, 0.0) - _divergence_term(rt * gx, rt * gy, rt * gz, n, h, md, bmat)
     Ex = ex_sum / factor * dV
     # correlation (PW92 local part + PBE H)
     A00, A01, A02 = 0.031091, 0.015545, 0.016887
@@ -142,7 +167,7 @@ def pbe(rho: np.ndarray, n: tuple, h: tuple, dV: float, md: int = 6, mu: float =
              + dH_dT * (-7.0 / 3.0 * T - trho * 2.0 * T / phi * dphi_dz * dz) + trho * dH_dphi * dphi_dz * dz)
         vc[s] = np.where(ok, v, 0.0)
     rt = np.where(ok, dH_dT * pi / (8.0 * kf * trho * phi ** 2), 0.0)
-    div = _divergence_term(rt * gx, rt * gy, rt * gz, n, h, md)
+    div = _divergence_term(rt * gx, rt * gy, rt * gz, n, h, md, bmat)
     vc -= div[None, :]
     return vx + vc, Ex, Ec
 

@@ -19,8 +19,10 @@ Host-side set-up that feeds the band update: it runs once per structure, as in t
                            folding of prep_uvk_ps_nloc2 :1070-1167
   construct_ps_initrho     src/ps_initrho_module.f90:58-134, 461-560 (analytic Gaussian charge)
 
-Cells are orthorhombic (the band update's grid is rectangular); positions are reduced
-coordinates as in the reference's atom input.
+Cells are given either by three orthorhombic edge lengths or by three lattice vectors (rows,
+bohr; the reference's aa(:, i)), e.g. the FCC cell of its Si sample; positions are reduced
+coordinates as in the reference's atom input.  Orthorhombic cells take the arithmetic of the
+edge-length form unchanged.
 """
 from __future__ import annotations
 
@@ -616,16 +618,52 @@ class GGrid:
         return self.gg.size
 
 
-def make_ggrid(n: tuple, lengths: tuple) -> GGrid:
+def lattice(cell) -> tuple:
+    """(A, orthogonal): the lattice vectors as rows of A (bohr) from three orthorhombic edge
+    lengths or from a 3 x 3 array of vectors, and whether the cell is orthorhombic (the
+    off-diagonal entries of A are exactly zero)."""
+    c = np.asarray(cell, np.float64)
+    if c.ndim == 1:
+        return np.diag(c), True
+    if c.shape != (3, 3):
+        raise ValueError("cell: three edge lengths or three lattice vectors")
+    return c.copy(), bool(np.all(c[~np.eye(3, dtype=bool)] == 0.0))
+
+
+def reciprocal(A: np.ndarray) -> np.ndarray:
+    """Reciprocal vectors b_i (rows) with a_i . b_j = 2 pi delta_ij (get_reciprocal_lattice)."""
+    vol = float(np.dot(A[0], np.cross(A[1], A[2])))
+    return 2.0 * math.pi / vol * np.array([np.cross(A[1], A[2]), np.cross(A[2], A[0]), np.cross(A[0], A[1])])
+
+
+def make_ggrid(n: tuple, cell) -> GGrid:
+    """Init_Ggrid for the FFT box n of the cell (edge lengths or lattice vectors): Gcut is half
+    the smallest distance between opposite faces of the box's reciprocal parallelepiped
+    (CalcCutoff_Ggrid, src/ggrid_module.f90:55-90), the sphere |G|^2 < Gcut^2 - 1e-14 and its
+    shells (construct_NMGL_Ggrid :93-151)."""
+    A, ortho = lattice(cell)
     ng = [(k - 1) // 2 for k in n]
-    b = [2.0 * math.pi / L for L in lengths]
-    r = [b[d] * (2 * ng[d] + 1) for d in range(3)]
-    gcut = min(r) * 0.5
+    if ortho:
+        b = [2.0 * math.pi / A[d, d] for d in range(3)]
+        r = [b[d] * (2 * ng[d] + 1) for d in range(3)]
+        gcut = min(r) * 0.5
+    else:
+        B = reciprocal(A)
+        bl = [float(np.sqrt(np.sum(B[d] ** 2))) * (2 * ng[d] + 1) for d in range(3)]
+        c = float(np.dot(B[0], B[1])) / (bl[0] * bl[1]) * (2 * ng[0] + 1) * (2 * ng[1] + 1)
+        sn = math.sqrt(1.0 - c * c)
+        b0 = np.cross(B[0], B[1])
+        r3 = abs(float(np.dot(B[2], b0)) * (2 * ng[2] + 1) / math.sqrt(float(np.sum(b0 ** 2))))
+        gcut = min(sn * bl[0], sn * bl[1], r3) * 0.5
     ecut = gcut * gcut
     i3, i2, i1 = np.meshgrid(np.arange(-ng[2], ng[2] + 1), np.arange(-ng[1], ng[1] + 1),
                              np.arange(-ng[0], ng[0] + 1), indexing="ij")
     i1, i2, i3 = i1.ravel(), i2.ravel(), i3.ravel()
-    s = (b[0] * i1) ** 2 + (b[1] * i2) ** 2 + (b[2] * i3) ** 2
+    if ortho:
+        s = (b[0] * i1) ** 2 + (b[1] * i2) ** 2 + (b[2] * i3) ** 2
+    else:
+        gx = [B[0, c] * i1 + B[1, c] * i2 + B[2, c] * i3 for c in range(3)]
+        s = gx[0] ** 2 + gx[1] ** 2 + gx[2] ** 2
     keep = s < ecut - 1e-14
     llg = np.stack([i1[keep], i2[keep], i3[keep]], axis=1)
     g2 = s[keep]
@@ -710,10 +748,12 @@ def ionic_potential(species: list, gr: GGrid, vcell: float, parlocs: list | None
 # ----------------------------------------------------------------------------
 # initial density
 # ----------------------------------------------------------------------------
-def initial_density(species: list, n: tuple, lengths: tuple) -> np.ndarray:
+def initial_density(species: list, n: tuple, cell) -> np.ndarray:
     """construct_ps_initrho_r_spin (src/ps_initrho_module.f90:461-547), analytic form: the sum
     over atoms and the 27 nearest cell images of sum_g (a + b r^2) exp(-c r^2); the caller
-    splits it over spins and normalises (normalize_initrho :550-560)."""
+    splits it over spins and normalises (normalize_initrho :550-560).  cell: edge lengths or
+    lattice vectors."""
+    A, ortho = lattice(cell)
     n1, n2, n3 = n
     i3, i2, i1 = np.meshgrid(np.arange(n3), np.arange(n2), np.arange(n1), indexing="ij")
     f1, f2, f3 = (i1 / n1).ravel(), (i2 / n2).ravel(), (i3 / n3).ravel()
@@ -723,9 +763,11 @@ def initial_density(species: list, n: tuple, lengths: tuple) -> np.ndarray:
             for j3 in (-1, 0, 1):
                 for j2 in (-1, 0, 1):
                     for j1 in (-1, 0, 1):
-                        x = lengths[0] * (f1 - a[0] - j1)
-                        y = lengths[1] * (f2 - a[1] - j2)
-                        z = lengths[2] * (f3 - a[2] - j3)
+                        d1, d2, d3 = f1 - a[0] - j1, f2 - a[1] - j2, f3 - a[2] - j3
+                        if ortho:
+                            x, y, z = A[0, 0] * d1, A[1, 1] * d2, A[2, 2] * d3
+                        else:
+                            x, y, z = (A[0, c] * d1 + A[1, c] * d2 + A[2, c] * d3 for c in range(3))
                         rr = x * x + y * y + z * z
                         for g in range(pp.cdd_coef.shape[1]):
                             ca, cb, cc = pp.cdd_coef[:, g]
@@ -800,31 +842,49 @@ class ProjectorSet:
     amap: np.ndarray
     lmap: np.ndarray
     mmap: np.ndarray
+    uvk: np.ndarray | None = None   # (nk, nzlma, maxmjj) with the k phases, when k-points are given
 
 
-def grid_projectors(species: list, filtered: list, n: tuple, lengths: tuple) -> ProjectorSet:
+def grid_projectors(species: list, filtered: list, n: tuple, cell, kbb: np.ndarray | None = None) -> ProjectorSet:
     """prep_ps_nloc2 (src/ps_nloc2_module.f90:42-1067): for each atom and projector, the grid
     points (periodic images included) within the filtered cut-off, the spline-interpolated
     radial value (0 at the atom itself for l > 0) times Ylm; then prep_uvk_ps_nloc2's folding
-    (:1070-1167): repeated grid points summed, |u| <= 1e-14 dropped, in first-seen order."""
+    (:1070-1167): repeated grid points summed, |u| <= 1e-14 dropped, in first-seen order.
+    cell: edge lengths or lattice vectors.  kbb (nk, 3) reduced k: the folded values carry the
+    phase exp(-i 2 pi k . (i / N + m)) of the unfolded point (in-cell index i, image m), as the
+    complex16 build folds them; ProjectorSet.uvk then holds (nk, nzlma, maxmjj) complex values."""
+    A, ortho = lattice(cell)
+    B = reciprocal(A)
     n1, n2, n3 = n
     jj_all, uv_all, iuv, amap, lmap, mmap = [], [], [], [], [], []
+    uvk_all = []
     atom_id = 0
     for (pp, pos), fp in zip(species, filtered):
         for a in pos:
             atom_id += 1
-            R = np.array([a[0] * lengths[0], a[1] * lengths[1], a[2] * lengths[2]])
+            if ortho:
+                R = np.array([a[0] * A[0, 0], a[1] * A[1, 1], a[2] * A[2, 2]])
+            else:
+                R = np.array([a[0] * A[0, c] + a[1] * A[1, c] + a[2] * A[2, c] for c in range(3)])
             ic = [int(round(a[d] * n[d])) for d in range(3)]
             for k in range(pp.norb):
                 l = int(pp.lo[k])
                 rps2 = fp.rps[k] ** 2
-                hw = [int(math.ceil(fp.rps[k] / (lengths[d] / n[d]))) + 2 for d in range(3)]
+                if ortho:
+                    hw = [int(math.ceil(fp.rps[k] / (A[d, d] / n[d]))) + 2 for d in range(3)]
+                else:
+                    hw = [int(math.ceil(fp.rps[k] * float(np.linalg.norm(B[d])) * n[d] / (2.0 * math.pi))) + 2
+                          for d in range(3)]
                 o3, o2, o1 = np.meshgrid(np.arange(-hw[2], hw[2] + 1), np.arange(-hw[1], hw[1] + 1),
                                          np.arange(-hw[0], hw[0] + 1), indexing="ij")
                 id1, id2, id3 = (ic[0] + o1).ravel(), (ic[1] + o2).ravel(), (ic[2] + o3).ravel()
-                x = lengths[0] * (id1 / n1) - R[0]
-                y = lengths[1] * (id2 / n2) - R[1]
-                z = lengths[2] * (id3 / n3) - R[2]
+                if ortho:
+                    x = A[0, 0] * (id1 / n1) - R[0]
+                    y = A[1, 1] * (id2 / n2) - R[1]
+                    z = A[2, 2] * (id3 / n3) - R[2]
+                else:
+                    x, y, z = (A[0, c] * (id1 / n1) + A[1, c] * (id2 / n2) + A[2, c] * (id3 / n3) - R[c]
+                               for c in range(3))
                 r2 = x * x + y * y + z * z
                 keep = r2 <= rps2 + 1e-10
                 id1, id2, id3, x, y, z, r2 = (q[keep] for q in (id1, id2, id3, x, y, z, r2))
@@ -845,6 +905,15 @@ def grid_projectors(species: list, filtered: list, n: tuple, lengths: tuple) -> 
                     slot = rank[inv]
                     jj_all.append(uniq[np.argsort(first, kind="stable")])
                     uv_all.append(np.bincount(slot, weights=u[big], minlength=first.size))
+                    if kbb is not None:
+                        ub = u[big]
+                        t = np.stack([id1[big] / n1, id2[big] / n2, id3[big] / n3], axis=1)
+                        ph = 2.0 * math.pi * (t @ np.asarray(kbb, np.float64).T)      # (npts, nk)
+                        zk = (np.cos(ph) - 1j * np.sin(ph)) * ub[:, None]
+                        uvk_all.append(np.stack([np.bincount(slot, weights=zk[:, q].real, minlength=first.size)
+                                                 + 1j * np.bincount(slot, weights=zk[:, q].imag,
+                                                                    minlength=first.size)
+                                                 for q in range(zk.shape[1])]))
                     iuv.append(pp.inorm[k])
                     amap.append(atom_id)
                     lmap.append(l)
@@ -854,8 +923,11 @@ def grid_projectors(species: list, filtered: list, n: tuple, lengths: tuple) -> 
     mjj = np.array([len(j) for j in jj_all], np.int32)
     jjp = np.zeros((nzlma, maxmjj), np.int32)
     uv = np.zeros((nzlma, maxmjj))
+    uvk = None if kbb is None else np.zeros((len(kbb), nzlma, maxmjj), np.complex128)
     for p in range(nzlma):
         jjp[p, :mjj[p]] = jj_all[p] + 1
         uv[p, :mjj[p]] = uv_all[p]
+        if uvk is not None:
+            uvk[:, p, :mjj[p]] = uvk_all[p]
     return ProjectorSet(nzlma=nzlma, mjj=mjj, jjp=jjp, uv=uv, iuv=np.array(iuv), amap=np.array(amap, np.int32),
-                        lmap=np.array(lmap, np.int32), mmap=np.array(mmap, np.int32))
+                        lmap=np.array(lmap, np.int32), mmap=np.array(mmap, np.int32), uvk=uvk)

@@ -9,8 +9,13 @@ renormalisation per spin, and V_loc of the mixed density for the next iteration.
 are the fixed-moment filling of the reference's first NFIXED iterations (src/fermi_module.f90):
 the lowest N_s bands of spin s, N_s = (Nelectron +- Ndspin) / 2 (the reference's O2 sample keeps
 that filling to convergence: its occupations print 1 / 0).  Energies follow calc_total_energy
-(src/total_energy_module.f90): Etot = E_kin + E_ion + E_nl + E_H + E_xc + E_ewald, with
-E_kin + E_nl = sum occ e - E_loc.
+(src/total_energy_module.f90:60-340): Etot = E_kin + E_ion + E_nl + E_H + E_xc + E_ewald, with
+E_kin + E_nl = sum occ e - E_loc and E_loc = int rho_out V_loc of the potential the last sweep
+used (the reference evaluates it after calc_density, before the potential is updated).
+
+run_scf_kpoints is the same loop for crystals sampled on k-points (the reference's Si sample):
+Methfessel-Paxton occupations (calc_fermi_mp, EKBT 1e-5, KINTEG 5 by default) on the k weights,
+the density summed over k, the nonlocal energy with the k phases of the projectors.
 
 The band update runs behind a small interface (set_vloc, sweep, density, bands, and optionally
 xc): GpuBands drives the library's CUDA path through the C ABI (band update, density and the
@@ -25,7 +30,7 @@ import math
 
 import numpy as np
 
-from . import api, gga, structure
+from . import api, gga, scf, structure
 
 
 # ----------------------------------------------------------------------------
@@ -33,9 +38,11 @@ from . import api, gga, structure
 # ----------------------------------------------------------------------------
 def ewald_energy(st: structure.Structure, eta: float | None = None, tol: float = 1e-14) -> float:
     """Ewald energy of the ions (point charges Zps at the atoms, neutralising background) in the
-    orthorhombic cell, the quantity calc_ewald returns (src/ewald_module.f90:69-420):
+    cell, the quantity calc_ewald returns (src/ewald_module.f90:69-420):
     1/2 sum'_{i,j,L} Z_i Z_j erfc(sqrt(eta) r) / r + (2 pi / V) sum_{G != 0} |S(G)|^2
     exp(-G^2 / 4 eta) / G^2 - sqrt(eta / pi) sum Z_i^2 - pi Q^2 / (2 eta V)."""
+    if not st.orthorhombic:
+        return _ewald_lattice(st, eta, tol)
     L = np.array(st.lengths, dtype=np.float64)
     vol = float(np.prod(L))
     pos, z = [], []
@@ -78,6 +85,52 @@ def ewald_energy(st: structure.Structure, eta: float | None = None, tol: float =
     return er + eg - se / math.sqrt(math.pi) * float(np.sum(z * z)) - math.pi * q * q / (2.0 * eta * vol)
 
 
+def _ewald_lattice(st: structure.Structure, eta: float | None, tol: float) -> float:
+    """ewald_energy for lattice vectors (rows of st.avec): lattice translations and reciprocal
+    vectors as integer combinations, each range wide enough for the real- and reciprocal-space
+    cut-offs along the normal of every pair of cell faces."""
+    A = st.avec
+    vol = st.volume
+    B = 2.0 * math.pi / float(np.dot(A[0], np.cross(A[1], A[2]))) * np.array(
+        [np.cross(A[1], A[2]), np.cross(A[2], A[0]), np.cross(A[0], A[1])])
+    pos, z = [], []
+    for pp, p in st.species:
+        for a in np.asarray(p, np.float64).reshape(-1, 3):
+            pos.append(a @ A)
+            z.append(pp.zps)
+    pos = np.array(pos)
+    z = np.array(z)
+    if eta is None:
+        eta = math.pi / vol ** (2.0 / 3.0)
+    se = math.sqrt(eta)
+    rcut = 1.0
+    while math.erfc(se * rcut) > tol:
+        rcut += 0.5
+    # |n_d| <= rcut |b_d| / (2 pi) + 1 covers every translation shorter than rcut (+ the atoms' spread)
+    nimg = [int(math.ceil(rcut * float(np.linalg.norm(B[d])) / (2.0 * math.pi))) + 2 for d in range(3)]
+    m = np.stack(np.meshgrid(*[np.arange(-x, x + 1) for x in nimg], indexing="ij"), axis=-1).reshape(-1, 3)
+    sh = m @ A
+    er = 0.0
+    for i in range(len(z)):
+        for j in range(len(z)):
+            d = pos[i] - pos[j] + sh
+            r = np.sqrt(np.sum(d * d, axis=1))
+            keep = (r > 1e-12) & (r < rcut)
+            er += 0.5 * z[i] * z[j] * sum(math.erfc(se * x) / x for x in r[keep])
+    gmax = 2.0 * se * math.sqrt(-math.log(tol))
+    ng = [int(math.ceil(gmax * float(np.linalg.norm(A[d])) / (2.0 * math.pi))) + 1 for d in range(3)]
+    m = np.stack(np.meshgrid(*[np.arange(-x, x + 1) for x in ng], indexing="ij"), axis=-1).reshape(-1, 3)
+    g = m @ B
+    g2 = np.sum(g * g, axis=1)
+    keep = (g2 > 0) & (g2 <= gmax * gmax)
+    g, g2 = g[keep], g2[keep]
+    ph = g @ pos.T
+    sg = (np.cos(ph) * z).sum(axis=1) + 1j * (np.sin(ph) * z).sum(axis=1)
+    eg = 2.0 * math.pi / vol * float(np.sum(np.abs(sg) ** 2 * np.exp(-g2 / (4.0 * eta)) / g2))
+    q = float(z.sum())
+    return er + eg - se / math.sqrt(math.pi) * float(np.sum(z * z)) - math.pi * q * q / (2.0 * eta * vol)
+
+
 # ----------------------------------------------------------------------------
 # host pieces
 # ----------------------------------------------------------------------------
@@ -91,7 +144,7 @@ def potential(su: structure.Setup, rho: np.ndarray, xc=None):
     if xc is not None:
         vxc, ex, ec = xc(rho)
     else:
-        vxc, ex, ec = gga.pbe(rho, su.problem.n, h, dV, st.md)
+        vxc, ex, ec = gga.pbe(rho, su.problem.n, h, dV, st.md, bmat=su.bmat)
     v = su.vion[None, :] + vh[None, :] + vxc
     return v, {"hartree": eh, "xc": ex + ec, "exchange": ex, "correlation": ec,
                "ion_local": float(np.sum(rho.sum(axis=0) * su.vion)) * dV,
@@ -204,6 +257,7 @@ def run_scf_structure(su: structure.Setup, bands, nsweep: int = 10, diter: int =
         occ[s, :nocc[s]] = 1.0 if ns == 2 else 2.0
     xc = getattr(bands, "xc", None)
     bands.set_vloc(su.vloc)
+    v_cur = su.vloc
     if nsweep > 0:
         bands.sweep(nsweep)
     rho_in = su.rho.copy()
@@ -229,13 +283,90 @@ def run_scf_structure(su: structure.Setup, bands, nsweep: int = 10, diter: int =
             rho_in[s] *= (occ[s].sum()) / (float(rho_in[s].sum()) * dV)
         v_in, _ = potential(su, rho_in, xc)
         bands.set_vloc(v_in)
+        v_cur = v_in
     e_sum = float(np.sum(occ * esp))
     e_nl = sum(nonlocal_energy(su, bands.bands(s), occ[s]) for s in range(ns))
     ene = dict(ene)
+    ene["local"] = float(np.sum(rho_out * v_cur)) * dV
     ene["sum_eigen"] = e_sum
     ene["nonlocal"] = e_nl
     ene["kinetic"] = e_sum - ene["local"] - e_nl
     ene["ewald"] = ewald_energy(st)
     ene["total"] = (ene["kinetic"] + ene["ion_local"] + e_nl + ene["hartree"] + ene["xc"] + ene["ewald"])
     ene["spin_abs"] = float(np.sum(np.abs(rho_out[0] - rho_out[-1]))) * dV if ns == 2 else 0.0
+    return StructureScf(iterations=it, converged=conv, esp=esp, occ=occ, rho=rho_out, sqerr=hist, energies=ene)
+
+
+# ----------------------------------------------------------------------------
+# crystals on k-points
+# ----------------------------------------------------------------------------
+def nonlocal_energy_k(su: structure.Setup, psi: np.ndarray, occ: np.ndarray, k: int) -> float:
+    """sum_n occ_n sum_lma iuV(lma) |dV sum_j conj(uVk(j, lma, k)) psi_n(JJP(j, lma))|^2 for the
+    bands psi (nb, ng) of k-point k (0-based) of one spin."""
+    prob = su.problem
+    dV = prob.dV
+    e = 0.0
+    for p in range(prob.nzlma):
+        m = int(prob.mjj[p])
+        idx = prob.jjp[p, :m] - 1
+        c = dV * (psi[:, idx] @ np.conj(prob.uvk[k, p, :m]))
+        e += float(prob.dij[p]) * float(np.sum(occ * np.abs(c) ** 2))
+    return e
+
+
+def run_scf_kpoints(su: structure.Setup, bands, nsweep: int = 10, diter: int = 100, scf_conv: float = 1e-15,
+                    mmix: int = 4, beta: float = 0.5, ekbt: float = 1e-5, kinteg: int = 5) -> StructureScf:
+    """calc_scf for a structure set up on k-points (su.structure.kbb / wbz) with the band update
+    `bands`: set_vloc(v (nspin, ng)), sweep(n) -> esp (nspin, nk, nband), density(occ (nspin, nk,
+    nband), weights included) -> rho (nspin, ng), bands(s, k) -> (nband, ng).  nsweep sweeps on
+    the potential of the initial density, then per iteration one sweep of every (k, s),
+    Methfessel-Paxton occupations, the output density and potential, calc_sqerr's test of
+    V_out against the previous iteration (mean over the grid <= scf_conv), Pulay mixing of the
+    density over mmix iterations (linear for mmix = 1), renormalisation per spin."""
+    st = su.structure
+    ns = st.nspin
+    dV = su.problem.dV
+    wbz = np.asarray(st.wbz, np.float64)
+    nel = st.nelectron
+    bands.set_vloc(su.vloc)
+    v_cur = su.vloc
+    if nsweep > 0:
+        bands.sweep(nsweep)
+    rho_in = su.rho.copy()
+    prev = (su.vloc.copy(), su.rho.copy())
+    mixer = Pulay(mmix, beta)
+    hist = []
+    conv = False
+    esp = occ = rho_out = ene = None
+    ef = 0.0
+    it = 0
+    for it in range(1, diter + 1):
+        esp = bands.sweep(1)
+        occ, ef = scf.calc_fermi_mp(esp, wbz, nel, ekbt, kinteg)
+        rho_out = bands.density(occ)
+        v_out, ene = potential(su, rho_out)
+        sq = [float(np.mean((v_out[s] - prev[0][s]) ** 2)) for s in range(ns)] + \
+             [float(np.mean((rho_out[s] - prev[1][s]) ** 2)) for s in range(ns)]
+        hist.append(sq)
+        prev = (v_out, rho_out)
+        if max(sq[:ns]) <= scf_conv:
+            conv = True
+            break
+        rho_in = mixer.mix(rho_in, rho_out)
+        for s in range(ns):
+            rho_in[s] *= float(occ[s].sum()) / (float(rho_in[s].sum()) * dV)
+        v_in, _ = potential(su, rho_in)
+        bands.set_vloc(v_in)
+        v_cur = v_in
+    e_sum = float(np.sum(occ * esp))
+    e_nl = sum(nonlocal_energy_k(su, bands.bands(s, k), occ[s, k], k)
+               for s in range(ns) for k in range(esp.shape[1]))
+    ene = dict(ene)
+    ene["local"] = float(np.sum(rho_out * v_cur)) * dV
+    ene["sum_eigen"] = e_sum
+    ene["nonlocal"] = e_nl
+    ene["kinetic"] = e_sum - ene["local"] - e_nl
+    ene["ewald"] = ewald_energy(st)
+    ene["total"] = (ene["kinetic"] + ene["ion_local"] + e_nl + ene["hartree"] + ene["xc"] + ene["ewald"])
+    ene["fermi"] = float(ef)
     return StructureScf(iterations=it, converged=conv, esp=esp, occ=occ, rho=rho_out, sqerr=hist, energies=ene)

@@ -135,6 +135,46 @@ def kinetic_coefficients(h: float, md: int, kcart: np.ndarray) -> dict:
                 coef_nabk=coef_nabk, const_k2=const_k2, zcoef_kin=zcoef, ggg=ggg)
 
 
+def kinetic_coefficients_lattice(avec: np.ndarray, n: tuple, md: int, kbb: np.ndarray) -> dict:
+    """``init_kinetic`` for any cell (src/kinetic/kinetic_module.f90:28-162, get_ggg_kinetic
+    :196-211).  ``avec`` holds the lattice vectors a_i as rows (bohr), ``n`` the grid, ``kbb``
+    ``(nk, 3)`` reduced k.  ggg(1:6) = |a_i||a_j| b_i . b_j / (4 pi^2) for the axis pairs
+    (1,1), (2,2), (3,3), (1,2), (2,3), (3,1); coef_lap(d, m) = -ggg(d) lap(m) / (2 H_d^2),
+    coef_nab(d, m) = nab(m) / H_d, and the k term c_d = |a_d| b_d . k / (2 pi) in coef_nabk.
+    The off-diagonal ggg enter the stencil as -ggg(4) D_1 D_2 - ggg(5) D_2 D_3 - ggg(6) D_3 D_1.
+    Same keys as :func:`kinetic_coefficients` plus ``hgrid``; ``ggg`` has six entries."""
+    A = np.asarray(avec, dtype=np.float64)
+    vol = float(np.dot(A[0], np.cross(A[1], A[2])))
+    B = 2.0 * math.pi / vol * np.array([np.cross(A[1], A[2]), np.cross(A[2], A[0]), np.cross(A[0], A[1])])
+    alen = np.sqrt(np.sum(A * A, axis=1))
+    hgrid = alen / np.asarray(n, dtype=np.float64)
+    const = 1.0 / (4.0 * math.pi ** 2)
+    pair = ((0, 0), (1, 1), (2, 2), (0, 1), (1, 2), (2, 0))
+    ggg = np.array([alen[i] * alen[j] * float(np.dot(B[i], B[j])) * const for i, j in pair])
+    lap = fd_lap_coef(md)
+    nab = fd_nab_coef(md)
+    c = -0.5 * ggg[:3] / hgrid ** 2
+    coef_lap0 = lap[md] * (c[0] + c[1] + c[2])
+    coef_lap = np.array([[lap[md + m] * c[d] for m in range(1, md + 1)] for d in range(3)])
+    coef_nab = np.array([[nab[md + m] / hgrid[d] for m in range(1, md + 1)] for d in range(3)])
+    kbb = np.atleast_2d(np.asarray(kbb, dtype=np.float64))
+    nk = kbb.shape[0]
+    kcart = kbb @ B
+    coef_nabk = np.zeros((nk, 3, md))
+    const_k2 = np.zeros(nk)
+    zcoef = np.zeros((nk, 3, 2 * md + 1), dtype=np.complex128)
+    for k in range(nk):
+        ck = alen / (2.0 * math.pi) * (B @ kcart[k])
+        for d in range(3):
+            coef_nabk[k, d, :] = coef_nab[d, :] * ck[d]
+        const_k2[k] = 0.5 * float(np.dot(kcart[k], kcart[k]))
+        for m in range(1, md + 1):
+            zcoef[k, :, md - m] = coef_lap[:, m - 1] + 1j * coef_nabk[k, :, m - 1]
+            zcoef[k, :, md + m] = coef_lap[:, m - 1] - 1j * coef_nabk[k, :, m - 1]
+    return dict(coef_lap=coef_lap, coef_lap0=coef_lap0, coef_nab=coef_nab, coef_nabk=coef_nabk,
+                const_k2=const_k2, zcoef_kin=zcoef, ggg=ggg, hgrid=hgrid, kcart=kcart)
+
+
 def generate_bz(mmm, use_inversion: int = 1):
     """k-points and weights of generate_bz without symmetry operations (src/bz_module.f90:65-189,
     Monkhorst_Pack :530-557): the MP mesh on the common integer grid of nk points per axis, k and

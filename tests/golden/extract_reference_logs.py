@@ -12,8 +12,11 @@ density sums, the band energies of scf_iter 1 (both spins: they belong to the op
 from the initial density, the same one the preceding sweeps converged), and what scf_iter 1
 prints about the density of those bands (charges, sum |rho_up - rho_down| dV, and the squared
 changes of V_loc and rho from the initial ones); and the first SCF cycle's converged state (the
-energy terms printed after its SCF END, its last eigenvalues and spin-density sum).  The tests use the JSON
-file only, so they run where the reference tree is absent.
+energy terms printed after its SCF END, its last eigenvalues and spin-density sum).  From the Si
+band runs (FCC cell, 12^3 grid, 63 k-points) it takes the same set-up prints, the Ewald energy,
+the scf_iter 1 eigenvalues of every k-point, the converged SCF energies and last eigenvalues,
+and the band energies along the k trajectory (band_eigv).  The tests use the JSON file only, so
+they run where the reference tree is absent.
 """
 import glob
 import json
@@ -206,6 +209,62 @@ def parse_o2_scf(path):
     return out
 
 
+def _esp_rows(txt, j, ncol):
+    """The eigenvalue table that starts after line j: rows (k, n, values...) of ncol fields."""
+    rows = []
+    for jj in range(j + 1, len(txt)):
+        f = txt[jj].split()
+        if len(f) != ncol or not f[0].isdigit():
+            break
+        rows.append([int(f[0]), int(f[1])] + [float(x) for x in f[2:]])
+    return rows
+
+
+def parse_band_eigv(path):
+    """band_eigv of the band-structure run: per trajectory k-point (in trajectory order; the file
+    lists them grouped by process) its reduced k and the band energies (mb bands)."""
+    txt = open(path).read().splitlines()
+    blocks = []
+    i = 0
+    while i < len(txt):
+        f = txt[i].split()
+        if len(f) == 6 and f[0].isdigit() and f[1].isdigit() and f[5].isdigit():
+            nb = int(f[1])
+            blocks.append((int(f[0]), [float(x) for x in f[2:5]],
+                           [float(txt[i + 1 + n].split()[1]) for n in range(nb)]))
+            i += nb + 1
+        else:
+            i += 1
+    blocks.sort(key=lambda b: b[0])
+    return {"source": os.path.relpath(path, os.path.dirname(REF)), "index": [b[0] for b in blocks],
+            "kpoints": [b[1] for b in blocks], "esp": [b[2] for b in blocks]}
+
+
+def parse_si(path):
+    """The Si sample's prints (FCC cell, 63 k-points, one spin): the set-up items parse_o2 reads,
+    the Ewald energy, the scf_iter 1 eigenvalue table of every k-point (bands 1-9 as printed),
+    the converged energy block and iteration count, and the last SCF iteration's table."""
+    txt = open(path).read().splitlines()
+    out = {k: v for k, v in parse_o2(path).items() if k != "esp_scf1"}
+    out.update({k: v for k, v in parse(path).items() if k != "source"})
+    for line in txt:
+        m = re.match(r"\s*Eewald\(SYSTYPE=0\)=\s*([-+0-9.Ee]+)", line)
+        if m:
+            out["ewald"] = float(m.group(1))
+            break
+    i1 = next(i for i, l in enumerate(txt) if re.match(r"-+\s*scf_iter=\s*1$", l))
+    j = next(j for j in range(i1, len(txt)) if "esp(n,k,s)" in txt[j])
+    out["esp_scf1"] = _esp_rows(txt, j, 5)
+    scf = parse_o2_scf(path)
+    out["iterations"] = scf["iterations"]
+    out["energies"] = scf["energies"]
+    end = next(i for i, l in enumerate(txt) if "SCF END" in l)
+    last = max(i for i in range(end) if "scf_iter=" in txt[i])
+    j = next(j for j in range(last, end) if "esp(n,k,s)" in txt[j])
+    out["esp_last"] = _esp_rows(txt, j, 5)
+    return out
+
+
 def main():
     logs = sorted(glob.glob(os.path.join(REF, "*", "02_O2-molecule_optimize", "real8", "result", "a.log")))
     data = [parse(p) for p in logs]
@@ -216,10 +275,15 @@ def main():
     o2 = [d for d in o2 if d.get("psv") and d.get("esp_scf1") and d.get("initrho")]
     o2_scf = [parse_o2_scf(p) for p in sorted(glob.glob(os.path.join(REF, "*", "02_O2-molecule_optimize", "*", "result", "a.log")))]
     o2_scf = [d for d in o2_scf if d.get("esp") and d["energies"].get("total") is not None]
-    json.dump({"kinetic": data, "bz": bz, "o2": o2, "o2_scf": o2_scf}, open(os.path.join(HERE, "reference_logs.json"), "w"),
-              indent=1)
+    si = [parse_si(p) for p in sorted(glob.glob(os.path.join(REF, "*", "01_Si_band", "result", "a.log")))]
+    si = [d for d in si if d.get("esp_scf1") and d["energies"].get("total") is not None]
+    si_band = [parse_band_eigv(p) for p in sorted(glob.glob(os.path.join(REF, "*", "01_Si_band", "result", "band_eigv")))]
+    si_band = [d for d in si_band if d["esp"]]
+    json.dump({"kinetic": data, "bz": bz, "o2": o2, "o2_scf": o2_scf, "si": si, "si_band": si_band},
+              open(os.path.join(HERE, "reference_logs.json"), "w"), indent=1)
     print(f"{len(data)} kinetic tables, {len(bz)} k-point lists, {len(o2)} O2 set-up/eigenvalue records, "
-          f"{len(o2_scf)} converged O2 SCF records -> reference_logs.json")
+          f"{len(o2_scf)} converged O2 SCF records, {len(si)} Si records, {len(si_band)} Si band tables "
+          f"-> reference_logs.json")
 
 
 if __name__ == "__main__":

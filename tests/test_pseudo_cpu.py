@@ -51,11 +51,16 @@ def o2(pp):
     return structure.setup(structure.o2_molecule(pp))
 
 
-def test_psv_fixture_matches_a_fresh_read():
-    if not os.path.exists(PSV_FILE):
+SI_NPZ = os.path.join(HERE, "golden", "si_pbe_tm_psv.npz")
+SI_FILE = "/root/reference/samples_for_supercomputers/pseudopotential/Si-PBE-TM.psv"
+
+
+@pytest.mark.parametrize("src,npz", [(PSV_FILE, PSV_NPZ), (SI_FILE, SI_NPZ)])
+def test_psv_fixture_matches_a_fresh_read(src, npz):
+    if not os.path.exists(src):
         pytest.skip("reference tree not present")
-    a = pseudo.read_psv(PSV_FILE)
-    b = pseudo.load_npz(PSV_NPZ)
+    a = pseudo.read_psv(src)
+    b = pseudo.load_npz(npz)
     for f in dataclasses.fields(a):
         x, y = getattr(a, f.name), getattr(b, f.name)
         if isinstance(x, np.ndarray):
