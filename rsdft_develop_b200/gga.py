@@ -17,6 +17,7 @@ from __future__ import annotations
 import math
 
 import numpy as np
+import scipy.fft
 
 from .synth import fd_nab_coef
 
@@ -172,14 +173,26 @@ def pbe(rho: np.ndarray, n: tuple, h: tuple, dV: float, md: int = 6, mu: float =
     return vx + vc, Ex, Ec
 
 
+def _hartree_kernel(gr) -> np.ndarray:
+    """4 pi / |G|^2 on the sphere's points of the half spectrum (x axis 0..N1/2), G = 0 and the
+    points outside the sphere 0; cached on gr.  The sphere is symmetric under G -> -G, so the
+    half spectrum carries the whole filter of a real density."""
+    ker = getattr(gr, "_vh_kernel", None)
+    if ker is None:
+        n1, n2, n3 = gr.n
+        ker = np.zeros((n3, n2, n1 // 2 + 1))
+        i1 = np.mod(gr.llg[:, 0], n1)
+        keep = np.any(gr.llg != 0, axis=1) & (i1 <= n1 // 2)
+        ker[np.mod(gr.llg[keep, 2], n3), np.mod(gr.llg[keep, 1], n2), i1[keep]] = 4.0 * math.pi / gr.g2[keep]
+        gr._vh_kernel = ker
+    return ker
+
+
 def hartree_sphere(rho_total: np.ndarray, gr, dV: float):
     """calc_hartree_sol_fftw: V_H(G) = 4 pi rho(G) / |G|^2 on the cut-off sphere of gr (a
-    pseudo.GGrid), G = 0 excluded; returns (V_H, E_H = dV/2 sum rho V_H)."""
+    pseudo.GGrid), G = 0 excluded; returns (V_H, E_H = dV/2 sum rho V_H).  Real-to-complex
+    transforms on all host threads."""
     n1, n2, n3 = gr.n
-    f = np.fft.fftn(rho_total.reshape(n3, n2, n1))
-    keep = np.any(gr.llg != 0, axis=1)
-    idx = (np.mod(gr.llg[keep, 2], n3), np.mod(gr.llg[keep, 1], n2), np.mod(gr.llg[keep, 0], n1))
-    z = np.zeros_like(f)
-    z[idx] = f[idx] * (4.0 * math.pi / gr.g2[keep])
-    vh = np.fft.ifftn(z).real.reshape(-1)
+    f = scipy.fft.rfftn(rho_total.reshape(n3, n2, n1), workers=-1)
+    vh = scipy.fft.irfftn(f * _hartree_kernel(gr), s=(n3, n2, n1), workers=-1).reshape(-1)
     return vh, 0.5 * dV * float(np.dot(rho_total, vh))

@@ -227,7 +227,7 @@ def test_hartree_sphere_solves_poisson_for_a_plane_wave():
     assert np.allclose(vh, 4 * math.pi / g2 * rho, atol=1e-12)
 
 
-O2_SWEEPS = 20
+O2_SWEEPS = 24
 
 
 def _reference_bands(log, s):
