@@ -174,6 +174,81 @@ class Pulay:
         return (x + self.beta * r).reshape(rin.shape)
 
 
+class ReferenceMixer:
+    """perform_mixing with the reference's default IMIX = 10, MMIX = 4, BETA = 1.1: Pulay mixing
+    of the density (src/mixing/mixing_module.f90:145-290, pulay_mixing
+    src/mixing/mixing_pulay_module.f90:29-111).  The history holds (input, output) density
+    pairs; while fewer than mmix pairs exist a step is linear, x_in + beta (x_out - x_in); then
+    x = sum_i c_i x_in,i + beta sum_i c_i (x_out,i - x_in,i) with sum_i c_i = 1 minimising
+    |sum_i c_i (x_out,i - x_in,i)|.  BETA > 1 asks for a search: the first call takes beta =
+    0.05; later calls try beta = 1, 1/2, 1/4, ... (at most 11 tries, the last with the beta of
+    the smallest change) while the squared change of the mixed density from the previous mixed
+    one exceeds half of the previous change.  The result is made non-negative (chk_chrg)."""
+
+    def __init__(self, rho0: np.ndarray, mmix: int = 4, beta: float = 1.1):
+        self.mmix, self.beta = int(mmix), float(beta)
+        self.xin = np.zeros((self.mmix,) + rho0.shape)
+        self.xou = np.zeros((self.mmix,) + rho0.shape)
+        self.xin[-1] = rho0
+        self.count = 0
+        self.xold = rho0.copy()
+        self.dif0 = np.zeros(rho0.shape[0])
+        self.betas = []
+
+    def _pulay(self, f: np.ndarray, beta: float) -> np.ndarray:
+        m = self.mmix
+        self.xou[-1] = f
+        self.count += 1
+        m0 = min(self.count, m)
+        if m == 1 or m0 < m:
+            self.xin[:-1] = self.xin[1:].copy()
+            self.xou[:-1] = self.xou[1:].copy()
+            self.xin[-1] = self.xin[-1] + beta * (self.xou[-1] - self.xin[-1])
+            return self.xin[-1].copy()
+        r = (self.xou[m - m0:] - self.xin[m - m0:]).reshape(m0, -1)
+        c = np.linalg.solve(r @ r.T, np.ones(m0))
+        c /= c.sum()
+        x = np.tensordot(c, self.xin[m - m0:], axes=1)
+        y = np.tensordot(c, self.xou[m - m0:], axes=1)
+        self.xin[:-1] = self.xin[1:].copy()
+        self.xou[:-1] = self.xou[1:].copy()
+        self.xin[-1] = x + beta * (y - x)
+        return self.xin[-1].copy()
+
+    def mix(self, rho_out: np.ndarray) -> np.ndarray:
+        ng = rho_out.shape[1]
+        bak = (self.xin.copy(), self.xou.copy(), self.count)
+        beta = beta_min = self.beta
+        dif_min = np.full(rho_out.shape[0], 1e10)
+        max_loop = 1
+        if beta > 1.0:
+            if np.all(self.dif0 == 0.0):
+                beta = 0.05
+            else:
+                max_loop, beta = 11, 1.0
+        h = dif1 = None
+        for loop in range(1, max_loop + 1):
+            h = self._pulay(rho_out.copy(), beta)
+            dif1 = np.sum((h - self.xold) ** 2, axis=1) / ng
+            safe = np.where(self.dif0 != 0.0, self.dif0, 1.0)
+            diff = np.where(self.dif0 != 0.0, dif1 / safe, 0.0)
+            if np.all(dif1 < dif_min):
+                beta_min, dif_min = beta, dif1
+            if loop < max_loop:
+                if np.any(diff > 0.5):
+                    self.xin, self.xou, self.count = bak[0].copy(), bak[1].copy(), bak[2]
+                    beta *= 0.5
+                else:
+                    break
+                if loop == max_loop - 1:
+                    beta = beta_min
+        self.betas.append(beta)
+        self.dif0 = dif1
+        h = np.abs(h)
+        self.xold = h.copy()
+        return h
+
+
 def nonlocal_energy(su: structure.Setup, psi: np.ndarray, occ: np.ndarray) -> float:
     """sum_n occ_n sum_lma iuV(lma) (dV sum_j uV(j, lma) psi_n(JJP(j, lma)))^2 for one spin."""
     ps = su.projectors
@@ -315,17 +390,18 @@ def nonlocal_energy_k(su: structure.Setup, psi: np.ndarray, occ: np.ndarray, k: 
 
 
 def run_scf_kpoints(su: structure.Setup, bands, nsweep: int = 10, diter: int = 100, scf_conv: float = 1e-15,
-                    mmix: int = 1, beta: float = 0.5, ekbt: float = 1e-5, kinteg: int = 5) -> StructureScf:
+                    mixing: str = "reference", mmix: int = 4, beta: float = 1.1, ekbt: float = 1e-5,
+                    kinteg: int = 5, diag_first: bool = True) -> StructureScf:
     """calc_scf for a structure set up on k-points (su.structure.kbb / wbz) with the band update
-    `bands`: set_vloc(v (nspin, ng)), sweep(n) -> esp (nspin, nk, nband), density(occ (nspin, nk,
-    nband), weights included) -> rho (nspin, ng), bands(s, k) -> (nband, ng).  nsweep sweeps on
-    the potential of the initial density, then per iteration one sweep of every (k, s),
-    Methfessel-Paxton occupations, the output density and potential, calc_sqerr's test of
-    V_out against the previous iteration (mean over the grid <= scf_conv), mixing of the density
-    (linear with step beta for mmix = 1, the default: it takes the reference's Si sample to
-    mean |dV|^2 <= 1e-16 in 20 iterations; mmix > 1 is the plain Pulay class, which on that
-    sample stalls once the one-sweep band update dominates the residual), renormalisation per
-    spin."""
+    `bands`: set_vloc(v (nspin, ng)), sweep(n, diag_first) -> esp (nspin, nk, nband),
+    density(occ (nspin, nk, nband), weights included) -> rho (nspin, ng), bands(s, k) ->
+    (nband, ng).  nsweep sweeps on the potential of the initial density, then per iteration, in
+    the reference's order (src/scf_module.f90:200-460): a Rayleigh-Ritz step of every (k, s) on
+    the new potential (subspace_diag, unless diag_first is False) and one sweep,
+    Methfessel-Paxton occupations, the output density and potential, calc_sqerr's test of V_out
+    against the previous iteration (mean over the grid <= scf_conv), mixing of the density and
+    renormalisation per spin.  mixing "reference": ReferenceMixer (MMIX = mmix, BETA = beta, the
+    reference's defaults 4 and 1.1); "linear": x_in + beta (x_out - x_in)."""
     st = su.structure
     ns = st.nspin
     dV = su.problem.dV
@@ -334,17 +410,22 @@ def run_scf_kpoints(su: structure.Setup, bands, nsweep: int = 10, diter: int = 1
     bands.set_vloc(su.vloc)
     v_cur = su.vloc
     if nsweep > 0:
-        bands.sweep(nsweep)
+        bands.sweep(nsweep, False)
     rho_in = su.rho.copy()
     prev = (su.vloc.copy(), su.rho.copy())
-    mixer = Pulay(mmix, beta)
+    if mixing == "reference":
+        mixer = ReferenceMixer(su.rho, mmix, beta)
+    elif mixing == "linear":
+        mixer = None
+    else:
+        raise ValueError(f"mixing {mixing!r}: 'reference' or 'linear'")
     hist = []
     conv = False
     esp = occ = rho_out = ene = None
     ef = 0.0
     it = 0
     for it in range(1, diter + 1):
-        esp = bands.sweep(1)
+        esp = bands.sweep(1, diag_first)
         occ, ef = scf.calc_fermi_mp(esp, wbz, nel, ekbt, kinteg)
         rho_out = bands.density(occ)
         v_out, ene = potential(su, rho_out)
@@ -355,7 +436,7 @@ def run_scf_kpoints(su: structure.Setup, bands, nsweep: int = 10, diter: int = 1
         if max(sq[:ns]) <= scf_conv:
             conv = True
             break
-        rho_in = mixer.mix(rho_in, rho_out)
+        rho_in = mixer.mix(rho_out) if mixer is not None else rho_in + beta * (rho_out - rho_in)
         for s in range(ns):
             rho_in[s] *= float(occ[s].sum()) / (float(rho_in[s].sum()) * dV)
         v_in, _ = potential(su, rho_in)

@@ -243,7 +243,8 @@ def parse_band_eigv(path):
 def parse_si(path):
     """The Si sample's prints (FCC cell, 63 k-points, one spin): the set-up items parse_o2 reads,
     the Ewald energy, the scf_iter 1 eigenvalue table of every k-point (bands 1-9 as printed),
-    the converged energy block and iteration count, and the last SCF iteration's table."""
+    the converged energy block and iteration count, the last SCF iteration's table, and the
+    squared changes of V_loc and rho printed at every SCF iteration."""
     txt = open(path).read().splitlines()
     out = {k: v for k, v in parse_o2(path).items() if k != "esp_scf1"}
     out.update({k: v for k, v in parse(path).items() if k != "source"})
@@ -262,6 +263,8 @@ def parse_si(path):
     last = max(i for i in range(end) if "scf_iter=" in txt[i])
     j = next(j for j in range(last, end) if "esp(n,k,s)" in txt[j])
     out["esp_last"] = _esp_rows(txt, j, 5)
+    out["sqerr_v"] = [float(l.split("=")[1].split("/")[0]) for l in txt[:end] if l.strip().startswith("|Vloc-Vloc0|^2/tol")]
+    out["sqerr_rho"] = [float(l.split("=")[1].split("/")[0]) for l in txt[:end] if l.strip().startswith("|rho -rho0 |^2/tol")]
     return out
 
 
