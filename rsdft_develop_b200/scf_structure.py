@@ -206,7 +206,14 @@ class ReferenceMixer:
             self.xin[-1] = self.xin[-1] + beta * (self.xou[-1] - self.xin[-1])
             return self.xin[-1].copy()
         r = (self.xou[m - m0:] - self.xin[m - m0:]).reshape(m0, -1)
-        c = np.linalg.solve(r @ r.T, np.ones(m0))
+        a = r @ r.T
+        try:
+            c = np.linalg.solve(a, np.ones(m0))
+        except np.linalg.LinAlgError:            # residuals linearly dependent (e.g. converged)
+            c = np.linalg.lstsq(a, np.ones(m0), rcond=None)[0]
+        if not np.isfinite(c.sum()) or c.sum() == 0.0:
+            c = np.zeros(m0)
+            c[-1] = 1.0
         c /= c.sum()
         x = np.tensordot(c, self.xin[m - m0:], axes=1)
         y = np.tensordot(c, self.xou[m - m0:], axes=1)
@@ -282,7 +289,10 @@ class GpuBands:
         for s in range(self.ns):
             self.g.set_vloc(v[s], s=s + 1)
 
-    def sweep(self, n: int) -> np.ndarray:
+    def sweep(self, n: int, diag_first: bool = False) -> np.ndarray:
+        if diag_first:
+            for s in range(1, self.ns + 1):
+                self.g.subspace_diag(s=s)
         _, esp, _ = self.g.calc_sweep(n)
         return esp[:, 0, :].copy()
 
@@ -313,11 +323,14 @@ class StructureScf:
 
 
 def run_scf_structure(su: structure.Setup, bands, nsweep: int = 10, diter: int = 100, scf_conv: float = 1e-11,
-                      mmix: int = 1, beta: float = 0.5) -> StructureScf:
+                      mmix: int = 1, beta: float = 0.5, mixing: str = "pulay", diag_first: bool = False) -> StructureScf:
     """calc_scf for su with the band update `bands` (GpuBands or a test adapter): nsweep sweeps on
     the potential of the initial density, then up to diter iterations until the squared change
-    of V_out (mean over the grid, every spin) is <= scf_conv.  Mixing: linear with step beta by
-    default (mmix = 1); mmix > 1 is Pulay over that many iterations.  With PBE, V_out near the
+    of V_out (mean over the grid, every spin) is <= scf_conv.  Mixing "pulay": the Pulay class,
+    linear with step beta for mmix = 1 (the default); "reference": ReferenceMixer with MMIX =
+    mmix, BETA = beta (the reference's defaults are 4 and 1.1).  diag_first: a Rayleigh-Ritz step
+    of every spin on the new potential before each iteration's sweep, the reference's order
+    (bands.sweep(n, True)).  With PBE, V_out near the
     vacuum reacts to density tails around the reference's 1e-10 density cut, so the squared
     change of V levels off near 1e-12 while energies and eigenvalues are converged to 1e-8."""
     st = su.structure
@@ -337,13 +350,18 @@ def run_scf_structure(su: structure.Setup, bands, nsweep: int = 10, diter: int =
         bands.sweep(nsweep)
     rho_in = su.rho.copy()
     prev = (su.vloc.copy(), su.rho.copy())
-    mixer = Pulay(mmix, beta)
+    if mixing == "pulay":
+        mixer = Pulay(mmix, beta)
+    elif mixing == "reference":
+        mixer = ReferenceMixer(su.rho, mmix, beta)
+    else:
+        raise ValueError(f"mixing {mixing!r}: 'pulay' or 'reference'")
     hist = []
     conv = False
     esp = rho_out = ene = None
     it = 0
     for it in range(1, diter + 1):
-        esp = bands.sweep(1)
+        esp = bands.sweep(1, True) if diag_first else bands.sweep(1)
         rho_out = bands.density(occ)
         v_out, ene = potential(su, rho_out, xc)
         sq = [float(np.mean((v_out[s] - prev[0][s]) ** 2)) for s in range(ns)] + \
@@ -353,7 +371,7 @@ def run_scf_structure(su: structure.Setup, bands, nsweep: int = 10, diter: int =
         if max(sq[:ns]) <= scf_conv:
             conv = True
             break
-        rho_in = mixer.mix(rho_in, rho_out)
+        rho_in = mixer.mix(rho_in, rho_out) if mixing == "pulay" else mixer.mix(rho_out)
         for s in range(ns):
             rho_in[s] *= (occ[s].sum()) / (float(rho_in[s].sum()) * dV)
         v_in, _ = potential(su, rho_in, xc)

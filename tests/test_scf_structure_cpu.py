@@ -51,10 +51,12 @@ class OracleBands:
     def set_vloc(self, v):
         self.v = v.copy()
 
-    def sweep(self, n):
+    def sweep(self, n, diag_first=False):
         esp = []
         for s in range(self.ns):
             o = self.orc.Oracle(dataclasses.replace(self.su.problem, vloc=np.ascontiguousarray(self.v[s])))
+            if diag_first:
+                self.psi[s], _ = o.subspace_diag(self.psi[s])
             self.psi[s], _, _ = o.sweep(self.psi[s], n)
             e, _ = o.residual(self.psi[s])
             esp.append(e)
@@ -107,6 +109,28 @@ def test_pulay_mixing_reaches_the_linear_fixed_point():
         assert np.max(np.abs(x - x_star)) < 1e-10, mmix
 
 
+def test_reference_mixer_solves_a_linear_fixed_point():
+    """ReferenceMixer (IMIX = 10 Pulay with the BETA = 1.1 search) on x = A x + b: its first step
+    is the 0.05 linear step, then it converges to the fixed point."""
+    rng = np.random.default_rng(4)
+    A = rng.normal(scale=0.2, size=(6, 6))
+    b = rng.normal(size=6)
+    x_star = np.linalg.solve(np.eye(6) - A, b)
+    x0 = np.zeros((1, 6))
+    m = scf_structure.ReferenceMixer(x0, mmix=4, beta=1.1)
+    x = m.mix((A @ x0[0] + b)[None, :])
+    assert np.allclose(x, np.abs(0.05 * b[None, :]))
+    m = scf_structure.ReferenceMixer(np.full((1, 6), 1.0), mmix=4, beta=1.1)
+    x = np.full((1, 6), 1.0)
+    bp = np.abs(b) + 2.0                     # keep the fixed point positive (the mixer takes |x|)
+    x_star = np.linalg.solve(np.eye(6) - A, bp)
+    for _ in range(60):
+        x = m.mix((A @ x[0] + bp)[None, :])
+    assert np.max(np.abs(x[0] - x_star)) < 1e-10
+
+
 def test_o2_scf_with_oracle_bands_reaches_the_reference_state(o2):
-    res = scf_structure.run_scf_structure(o2, OracleBands(o2), nsweep=10, diter=60)
+    """The reference's loop order (Rayleigh-Ritz before each sweep) and its default mixing."""
+    res = scf_structure.run_scf_structure(o2, OracleBands(o2), nsweep=10, diter=60, mixing="reference",
+                                          mmix=4, beta=1.1, diag_first=True)
     check_against_logs(res)
