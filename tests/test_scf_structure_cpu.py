@@ -3,7 +3,9 @@
 The reference's O2 runs (eight logs: four machines, real8 and complex16) converge their first
 SCF cycle (before the atoms move) to the same state; tests/golden/reference_logs.json holds the
 energy terms printed after that cycle's SCF END, its last eigenvalues and its spin-density sum
-(extracted by tests/golden/extract_reference_logs.py).  rsdft_develop_b200.scf_structure runs
+(extracted by tests/golden/extract_reference_logs.py).  In the reference's loop order and mixing
+the oracle run converges to SCFCONV 1e-15 as the reference does and lands on that state to
+~1e-12 Ha in the total energy.  rsdft_develop_b200.scf_structure runs
 the reference's loop order (one sweep per spin per iteration, density of the fixed-moment
 filling, V_ion + V_H + V_xc^PBE, mixing) with the oracle's FP64 band update behind its band
 interface here (the library's CUDA path in tests/test_gpu_o2.py) and must land on that state:
@@ -130,7 +132,12 @@ def test_reference_mixer_solves_a_linear_fixed_point():
 
 
 def test_o2_scf_with_oracle_bands_reaches_the_reference_state(o2):
-    """The reference's loop order (Rayleigh-Ritz before each sweep) and its default mixing."""
-    res = scf_structure.run_scf_structure(o2, OracleBands(o2), nsweep=10, diter=60, mixing="reference",
-                                          mmix=4, beta=1.1, diag_first=True)
-    check_against_logs(res)
+    """The reference's loop order (Rayleigh-Ritz before each sweep), its default mixing and its
+    stop (SCFCONV 1e-15 on the mean squared change of V_loc): the converged state of all eight
+    logs, the total energy to 1e-11 Ha (it lands within ~2e-12), every term to 2e-9 Ha (~8e-10),
+    bands 1-7 of both spins to 2e-10 Ha (~5e-11), sum |rho_up - rho_down| dV to 1e-10."""
+    res = scf_structure.run_scf_structure(o2, OracleBands(o2), nsweep=10, diter=60, scf_conv=1e-15,
+                                          mixing="reference", mmix=4, beta=1.1, diag_first=True)
+    check_against_logs(res, e_tol=2e-9, esp_tol=2e-10, spin_tol=1e-10)
+    for log in _logs():
+        assert abs(res.energies["total"] - log["energies"]["total"]) < 1e-11
