@@ -23,10 +23,13 @@ import numpy as np
 from . import api, synth
 
 
-def k_trajectory(ak: np.ndarray, nfki) -> np.ndarray:
-    """(nktrj, 6): reduced k of every trajectory point and, in columns 3:6, the step
-    bb @ dak of its segment (zero for the closing vertex), as band_module builds ktrj."""
+def k_trajectory(ak: np.ndarray, nfki, bb: np.ndarray | None = None) -> np.ndarray:
+    """(nktrj, 6): reduced k of every trajectory point and, in columns 3:6, the Cartesian step
+    bb @ dak of its segment (zero for the closing vertex), as band_module builds ktrj
+    (src/band_module.f90:124-139).  bb: reciprocal vectors as columns (the identity when None,
+    which leaves the reduced step dak)."""
     ak = np.asarray(ak, dtype=np.float64).reshape(-1, 3)
+    bmat = np.eye(3) if bb is None else np.asarray(bb, dtype=np.float64)
     nbk = ak.shape[0] - 1
     nfki = [int(x) for x in nfki]
     assert len(nfki) == nbk and all(x >= 1 for x in nfki)
@@ -34,7 +37,7 @@ def k_trajectory(ak: np.ndarray, nfki) -> np.ndarray:
     for i in range(nbk):
         dak = (ak[i + 1] - ak[i]) / nfki[i]
         for j in range(nfki[i]):
-            rows.append(np.concatenate([ak[i] + j * dak, dak]))
+            rows.append(np.concatenate([ak[i] + j * dak, bmat @ dak]))
     nk = len(rows)
     if nk > 0:  # nktrj > 1 in the reference always holds for a trajectory of one or more segments
         rows.append(np.concatenate([ak[nbk], np.zeros(3)]))
@@ -64,7 +67,7 @@ def band_structure(cfg: synth.Config, ak, nfki, mb2: int, esp_conv_tol: float = 
     """Run the band driver for the synthetic operator of cfg (its V_loc, atoms and Dij; vloc
     replaces V_loc when given) along the trajectory (ak, nfki); cfg.nband bands are carried,
     bands 1..mb2 are converged."""
-    ktrj = k_trajectory(ak, nfki)
+    ktrj = k_trajectory(ak, nfki, np.eye(3) * (2.0 * np.pi / cfg.L))
     nkt = ktrj.shape[0]
     prob = trajectory_problem(cfg, ak, nfki)
     if vloc is not None:
@@ -99,19 +102,27 @@ def band_structure(cfg: synth.Config, ak, nfki, mb2: int, esp_conv_tol: float = 
     return out
 
 
-def write_band_eigv(path: str, r: BandResult, prob: synth.Problem, efermi: float = 0.0):
-    """Text in the layout of the reference's band_eigv (src/band_module.f90:201-206, :316-337):
-    header, then per trajectory point a line (index, mb2, k, MBV = 1) and one line per band."""
-    bb = np.eye(3) * (2.0 * np.pi / prob.cfg.L)
+def write_band_eigv(path: str, r: BandResult, prob: synth.Problem | None = None, efermi: float = 0.0,
+                    mbv: int = 1, bb: np.ndarray | None = None):
+    """The reference's band_eigv file (src/band_module.f90:191-198, :316-337), as its plotting
+    tool utility/band2gp.f90 reads it: the format tag "version2.1" and the noncollinear flag, the
+    Fermi energy, the reciprocal vectors (bb, columns; 2 pi / L of prob's cubic cell when None),
+    then per trajectory point a line (index, mb2, reduced k, MBV) and one line per band (index,
+    energy, and a second column the reference fills with |esp - esp0| of two copies of the same
+    gathered eigenvalues, i.e. 0).  MBV, the number of valence bands, falls back to 1 outside
+    1..mb2 as the reference's band() does."""
+    if bb is None:
+        bb = np.eye(3) * (2.0 * np.pi / prob.cfg.L)
     mb2 = r.esp.shape[1]
+    if mbv < 1 or mbv > mb2:
+        mbv = 1
     with open(path, "w") as f:
-        f.write(" rsdft-b200 band_eigv F\n")
+        f.write(" version2.1 F\n")
         f.write(f" Fermi_energy(hartree):{efermi:20.15f}\n")
         f.write(" Reciprocal_Lattice_Vectors:\n")
         for d in range(3):
             f.write(" " + "".join(f"{x:20.15f}" for x in bb[:, d]) + "\n")
         for ik in range(r.esp.shape[0]):
-            f.write(f" {ik + 1:6d}{mb2:6d}" + "".join(f"{x:20.12f}" for x in r.ktrj[ik, :3]) + f"{1:8d}\n")
+            f.write(f" {ik + 1:6d}{mb2:6d}" + "".join(f"{x:20.12f}" for x in r.ktrj[ik, :3]) + f"{mbv:8d}\n")
             for n in range(mb2):
-                d = r.desp[ik, n] if np.isfinite(r.desp[ik, n]) else 0.0
-                f.write(f" {n + 1:5d}  {r.esp[ik, n]:22.12G} {d:15.5G}\n")
+                f.write(f" {n + 1:5d}  {r.esp[ik, n]:22.12G} {0.0:15.5G}\n")

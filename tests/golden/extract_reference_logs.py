@@ -243,8 +243,9 @@ def parse_band_eigv(path):
 def parse_si(path):
     """The Si sample's prints (FCC cell, 63 k-points, one spin): the set-up items parse_o2 reads,
     the Ewald energy, the scf_iter 1 eigenvalue table of every k-point (bands 1-9 as printed),
-    the converged energy block and iteration count, the last SCF iteration's table, and the
-    squared changes of V_loc and rho printed at every SCF iteration."""
+    the converged energy block and iteration count, the last SCF iteration's table, the
+    squared changes of V_loc and rho printed at every SCF iteration, and the band run's k
+    trajectory (reduced k and the Cartesian step bb dak per point)."""
     txt = open(path).read().splitlines()
     out = {k: v for k, v in parse_o2(path).items() if k != "esp_scf1"}
     out.update({k: v for k, v in parse(path).items() if k != "source"})
@@ -263,6 +264,8 @@ def parse_si(path):
     last = max(i for i in range(end) if "scf_iter=" in txt[i])
     j = next(j for j in range(last, end) if "esp(n,k,s)" in txt[j])
     out["esp_last"] = _esp_rows(txt, j, 5)
+    i0 = next(i for i, l in enumerate(txt) if l.strip().startswith("nktrj="))
+    out["ktrj"] = [[float(x) for x in txt[i].split()[1:7]] for i in range(i0 + 1, i0 + 1 + int(txt[i0].split("=")[1]))]
     out["sqerr_v"] = [float(l.split("=")[1].split("/")[0]) for l in txt[:end] if l.strip().startswith("|Vloc-Vloc0|^2/tol")]
     out["sqerr_rho"] = [float(l.split("=")[1].split("/")[0]) for l in txt[:end] if l.strip().startswith("|rho -rho0 |^2/tol")]
     return out
