@@ -30,7 +30,7 @@ import math
 
 import numpy as np
 
-from . import api, gga, scf, structure
+from . import api, gga, scf, structure, vrho
 
 
 # ----------------------------------------------------------------------------
@@ -320,6 +320,32 @@ class StructureScf:
     rho: np.ndarray               # output density of the last iteration
     sqerr: list                   # per iteration: sqerr of V_out (per spin) + of rho_out (per spin)
     energies: dict
+    vloc: np.ndarray | None = None  # (nspin, ng) the potential of the last sweep
+
+
+def to_vrho(su: structure.Setup, res: StructureScf) -> vrho.Vrho:
+    """What write_data (OC = 2, 3, ...) saves at the end of an SCF: the output density, the
+    potential of the last sweep, and V_H, V_xc of the output density (src/scf_module.f90 leaves
+    Vloc un-updated on exit and recomputes V_H, V_xc at the top of each iteration)."""
+    st = su.structure
+    vh, _ = gga.hartree_sphere(res.rho.sum(axis=0), su.ggrid, su.problem.dV)
+    vxc, _, _ = gga.pbe(res.rho, su.problem.n, (su.problem.h,) * 3, su.problem.dV, st.md, bmat=su.bmat)
+    atoms = np.concatenate([np.asarray(p, np.float64).reshape(-1, 3) for _, p in st.species])
+    ki = np.concatenate([np.full(len(np.asarray(p).reshape(-1, 3)), e + 1, np.int32)
+                         for e, (_, p) in enumerate(st.species)])
+    zn = np.array([int(round(pp.zelement)) for pp, _ in st.species], np.int32)
+    return vrho.Vrho(n=tuple(su.problem.n), rho=res.rho.copy(), vloc=np.asarray(res.vloc).copy(), vh=vh,
+                     vxc=vxc, efermi=float(res.energies.get("fermi", 0.0)), aa=st.avec, atoms=atoms,
+                     ki_atom=ki, zn_atom=zn)
+
+
+def restart_setup(su: structure.Setup, v: vrho.Vrho) -> structure.Setup:
+    """su with the density and potential of a vrho file (read_data with IC = 2, 3, ...): the SCF
+    starts from them instead of the initial density."""
+    if tuple(v.n) != tuple(su.problem.n) or v.rho.shape != su.rho.shape:
+        raise ValueError("vrho: grid or spin count differs from the structure's")
+    return dataclasses.replace(su, rho=v.rho.copy(), vloc=v.vloc.copy(),
+                               problem=dataclasses.replace(su.problem, vloc=np.ascontiguousarray(v.vloc[0])))
 
 
 def run_scf_structure(su: structure.Setup, bands, nsweep: int = 10, diter: int = 100, scf_conv: float = 1e-11,
@@ -388,7 +414,8 @@ def run_scf_structure(su: structure.Setup, bands, nsweep: int = 10, diter: int =
     ene["ewald"] = ewald_energy(st)
     ene["total"] = (ene["kinetic"] + ene["ion_local"] + e_nl + ene["hartree"] + ene["xc"] + ene["ewald"])
     ene["spin_abs"] = float(np.sum(np.abs(rho_out[0] - rho_out[-1]))) * dV if ns == 2 else 0.0
-    return StructureScf(iterations=it, converged=conv, esp=esp, occ=occ, rho=rho_out, sqerr=hist, energies=ene)
+    return StructureScf(iterations=it, converged=conv, esp=esp, occ=occ, rho=rho_out, sqerr=hist, energies=ene,
+                        vloc=np.array(v_cur))
 
 
 # ----------------------------------------------------------------------------
@@ -472,4 +499,5 @@ def run_scf_kpoints(su: structure.Setup, bands, nsweep: int = 10, diter: int = 1
     ene["ewald"] = ewald_energy(st)
     ene["total"] = (ene["kinetic"] + ene["ion_local"] + e_nl + ene["hartree"] + ene["xc"] + ene["ewald"])
     ene["fermi"] = float(ef)
-    return StructureScf(iterations=it, converged=conv, esp=esp, occ=occ, rho=rho_out, sqerr=hist, energies=ene)
+    return StructureScf(iterations=it, converged=conv, esp=esp, occ=occ, rho=rho_out, sqerr=hist, energies=ene,
+                        vloc=np.array(v_cur))

@@ -131,13 +131,44 @@ def test_reference_mixer_solves_a_linear_fixed_point():
     assert np.max(np.abs(x[0] - x_star)) < 1e-10
 
 
-def test_o2_scf_with_oracle_bands_reaches_the_reference_state(o2):
+@pytest.fixture(scope="module")
+def o2_scf(o2):
+    return scf_structure.run_scf_structure(o2, OracleBands(o2), nsweep=10, diter=60, scf_conv=1e-15,
+                                           mixing="reference", mmix=4, beta=1.1, diag_first=True)
+
+
+def test_o2_scf_with_oracle_bands_reaches_the_reference_state(o2_scf):
     """The reference's loop order (Rayleigh-Ritz before each sweep), its default mixing and its
     stop (SCFCONV 1e-15 on the mean squared change of V_loc): the converged state of all eight
     logs, the total energy to 1e-11 Ha (it lands within ~2e-12), every term to 2e-9 Ha (~8e-10),
     bands 1-7 of both spins to 2e-10 Ha (~5e-11), sum |rho_up - rho_down| dV to 1e-10."""
-    res = scf_structure.run_scf_structure(o2, OracleBands(o2), nsweep=10, diter=60, scf_conv=1e-15,
-                                          mixing="reference", mmix=4, beta=1.1, diag_first=True)
+    res = o2_scf
     check_against_logs(res, e_tol=2e-9, esp_tol=2e-10, spin_tol=1e-10)
     for log in _logs():
         assert abs(res.energies["total"] - log["energies"]["total"]) < 1e-11
+
+
+def test_o2_restart_from_vrho_file(o2, o2_scf, tmp_path):
+    """The converged state saved as the reference's vrho file (write_data, OC = 3), read back with
+    its points in a shuffled order through the file's grid map, restarts the SCF (read_data,
+    IC = 3): the first iteration's squared change of V_loc starts below 1e-8 (4.7e-5 from the
+    initial density) and fresh random bands reach 1e-13 within 10 iterations at the same total
+    energy."""
+    from rsdft_develop_b200 import vrho
+    v = scf_structure.to_vrho(o2, o2_scf)
+    path = str(tmp_path / "vrho.dat1")
+    n = o2.problem.n
+    rng = np.random.default_rng(2)
+    i3, i2, i1 = np.meshgrid(np.arange(n[2]), np.arange(n[1]), np.arange(n[0]), indexing="ij")
+    ll = np.stack([i1.ravel(), i2.ravel(), i3.ravel()], axis=1)[rng.permutation(o2.problem.ng)]
+    vrho.write_vrho(path, v, ll)
+    w = vrho.read_vrho(path, n, 2)
+    for f in ("rho", "vloc", "vh", "vxc"):
+        assert np.array_equal(getattr(w, f), getattr(v, f)), f
+    assert np.array_equal(w.aa, o2.structure.avec) and w.zn_atom.tolist() == [8]
+    su2 = scf_structure.restart_setup(o2, w)
+    res = scf_structure.run_scf_structure(su2, OracleBands(su2, seed=7), nsweep=10, diter=10, scf_conv=1e-13,
+                                          mixing="reference", mmix=4, beta=1.1, diag_first=True)
+    assert max(res.sqerr[0][:2]) < 1e-8, res.sqerr[0]
+    assert res.converged, (res.iterations, res.sqerr[-2:])
+    assert abs(res.energies["total"] - o2_scf.energies["total"]) < 1e-9, res.energies["total"] - o2_scf.energies["total"]
