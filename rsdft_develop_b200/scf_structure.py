@@ -437,7 +437,7 @@ def nonlocal_energy_k(su: structure.Setup, psi: np.ndarray, occ: np.ndarray, k: 
 
 def run_scf_kpoints(su: structure.Setup, bands, nsweep: int = 10, diter: int = 100, scf_conv: float = 1e-15,
                     mixing: str = "reference", mmix: int = 4, beta: float = 1.1, ekbt: float = 1e-5,
-                    kinteg: int = 5, diag_first: bool = True) -> StructureScf:
+                    kinteg: int = 5, diag_first: bool = True, kgroup=None) -> StructureScf:
     """calc_scf for a structure set up on k-points (su.structure.kbb / wbz) with the band update
     `bands`: set_vloc(v (nspin, ng)), sweep(n, diag_first) -> esp (nspin, nk, nband),
     density(occ (nspin, nk, nband), weights included) -> rho (nspin, ng), bands(s, k) ->
@@ -447,8 +447,17 @@ def run_scf_kpoints(su: structure.Setup, bands, nsweep: int = 10, diter: int = 1
     Methfessel-Paxton occupations, the output density and potential, calc_sqerr's test of V_out
     against the previous iteration (mean over the grid <= scf_conv), mixing of the density and
     renormalisation per spin.  mixing "reference": ReferenceMixer (MMIX = mmix, BETA = beta, the
-    reference's defaults 4 and 1.1); "linear": x_in + beta (x_out - x_in)."""
+    reference's defaults 4 and 1.1); "linear": x_in + beta (x_out - x_in).
+
+    kgroup: a kparallel.KpointGroup when the k-points are split over ranks; `bands` then holds
+    the k-points kgroup.klist only (its sweep returns those, its density sums over those, its
+    bands(s, j) takes the local index j), the eigenvalues are gathered for the occupations and
+    the density and band-energy sums are added over the ranks; every rank returns the same
+    result."""
+    from .kparallel import KpointGroup
     st = su.structure
+    kg = kgroup if kgroup is not None else KpointGroup(su.problem.nk, local=True)
+    kl = kg.klist
     ns = st.nspin
     dV = su.problem.dV
     wbz = np.asarray(st.wbz, np.float64)
@@ -471,9 +480,9 @@ def run_scf_kpoints(su: structure.Setup, bands, nsweep: int = 10, diter: int = 1
     ef = 0.0
     it = 0
     for it in range(1, diter + 1):
-        esp = bands.sweep(1, diag_first)
+        esp = kg.gather_esp(bands.sweep(1, diag_first))
         occ, ef = scf.calc_fermi_mp(esp, wbz, nel, ekbt, kinteg)
-        rho_out = bands.density(occ)
+        rho_out = kg.sum(bands.density(occ[:, kl[0]:kl[-1] + 1]))
         v_out, ene = potential(su, rho_out)
         sq = [float(np.mean((v_out[s] - prev[0][s]) ** 2)) for s in range(ns)] + \
              [float(np.mean((rho_out[s] - prev[1][s]) ** 2)) for s in range(ns)]
@@ -489,8 +498,8 @@ def run_scf_kpoints(su: structure.Setup, bands, nsweep: int = 10, diter: int = 1
         bands.set_vloc(v_in)
         v_cur = v_in
     e_sum = float(np.sum(occ * esp))
-    e_nl = sum(nonlocal_energy_k(su, bands.bands(s, k), occ[s, k], k)
-               for s in range(ns) for k in range(esp.shape[1]))
+    e_nl = kg.sum(sum(nonlocal_energy_k(su, bands.bands(s, j), occ[s, k], k)
+                      for s in range(ns) for j, k in enumerate(kl)))
     ene = dict(ene)
     ene["local"] = float(np.sum(rho_out * v_cur)) * dV
     ene["sum_eigen"] = e_sum

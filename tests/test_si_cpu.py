@@ -140,16 +140,17 @@ def test_si_oracle_eigenvalues_match_scf_iter1(si):
 class OracleBandsK:
     """The oracle's FP64 complex16 band update for every (k, s) behind run_scf_kpoints' interface."""
 
-    def __init__(self, su, orc, seed=1):
+    def __init__(self, su, orc, seed=1, klist=None):
         self.su, self.orc = su, orc
         p = su.problem
-        self.ns, self.nk = su.structure.nspin, p.nk
+        self.klist = list(range(p.nk)) if klist is None else list(klist)
+        self.ns, self.nk = su.structure.nspin, len(self.klist)
         self.v = su.vloc.copy()
         self.psi = {}
         for s in range(self.ns):
-            for k in range(self.nk):
+            for j, k in enumerate(self.klist):
                 o = orc.Oracle(p, k=k)
-                self.psi[s, k] = o.gram_schmidt(
+                self.psi[s, j] = o.gram_schmidt(
                     synth.random_wavefunctions(seed + k, su.structure.nband, p.ng).astype(np.complex128))
 
     def set_vloc(self, v):
@@ -159,12 +160,12 @@ class OracleBandsK:
         esp = np.zeros((self.ns, self.nk, self.su.structure.nband))
         for s in range(self.ns):
             pr = dataclasses.replace(self.su.problem, vloc=np.ascontiguousarray(self.v[s]))
-            for k in range(self.nk):
+            for j, k in enumerate(self.klist):
                 o = self.orc.Oracle(pr, k=k)
                 if diag_first:
-                    self.psi[s, k], _ = o.subspace_diag(self.psi[s, k])
-                self.psi[s, k], _, _ = o.sweep(self.psi[s, k], n)
-                esp[s, k], _ = o.residual(self.psi[s, k])
+                    self.psi[s, j], _ = o.subspace_diag(self.psi[s, j])
+                self.psi[s, j], _, _ = o.sweep(self.psi[s, j], n)
+                esp[s, j], _ = o.residual(self.psi[s, j])
         return esp
 
     def bands(self, s, k):
