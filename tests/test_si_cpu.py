@@ -181,7 +181,7 @@ class OracleBandsK:
 def si_scf(si):
     orc = _oracle()
     bands = OracleBandsK(si, orc)
-    res = scf_structure.run_scf_kpoints(si, bands, nsweep=10, diter=40, scf_conv=1e-16)
+    res = scf_structure.run_scf_kpoints(si, bands, nsweep=10, diter=40, scf_conv=1e-15)
     return res, bands
 
 
