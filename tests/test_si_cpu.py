@@ -250,3 +250,42 @@ def test_si_band_structure_of_the_converged_potential(si, si_scf):
             assert np.allclose(t["kpoints"][i], kbb[j], atol=1e-12)
             d = e[:12] - np.array(t["esp"][i])
             assert np.all(d < 1e-7) and np.all(d > -1e-6), (i, d)
+
+
+def test_si_gamma_real8_operator_matches_the_complex16_one(si):
+    """The real8 build at Gamma (real bands, the real stencil path with the cross terms, projectors
+    without phases) gives the Gamma eigenvalues of the complex16 k-point set."""
+    orc = _oracle()
+    pp = pseudo.load_npz(os.path.join(HERE, "golden", "si_pbe_tm_psv.npz"))
+    st = structure.si_crystal(pp)
+    su = structure.setup(st)
+    assert not su.problem.is_complex and abs(su.problem.kin["ggg"][3] + 0.5) < 1e-12
+    prob = dataclasses.replace(su.problem, vloc=np.ascontiguousarray(si.vloc[0]))
+    o = orc.Oracle(prob)
+    psi = o.gram_schmidt(synth.random_wavefunctions(3, 16, prob.ng))
+    psi, _, _ = o.sweep(psi, 30)
+    e_r, res = o.residual(psi)
+    assert np.max(res[:8]) < 1e-16
+    oc, psic = _converge(orc, si.problem, 0, 16, 30)
+    e_c, _ = oc.residual(psic)
+    assert np.max(np.abs(e_r[:8] - e_c[:8])) < 1e-11, e_r[:8] - e_c[:8]
+
+
+def test_si_two_spin_scf_equals_the_one_spin_scf():
+    """nspin = 2 with no initial moment (the initial density split in halves, occupations
+    Methfessel-Paxton over both spins) converges to the spin-unpolarised state: equal spin
+    densities, the one-spin total energy and eigenvalues (2 x 2 x 2 mesh, 8 bands)."""
+    orc = _oracle()
+    pp = pseudo.load_npz(os.path.join(HERE, "golden", "si_pbe_tm_psv.npz"))
+    kbb, w = synth.generate_bz((2, 2, 2))
+    out = []
+    for ns in (1, 2):
+        st = dataclasses.replace(structure.si_crystal(pp, kbb, w, nband=8), nspin=ns)
+        su = structure.setup(st)
+        res = scf_structure.run_scf_kpoints(su, OracleBandsK(su, orc), nsweep=8, diter=30, scf_conv=1e-14)
+        assert res.converged, (ns, res.sqerr[-2:])
+        out.append(res)
+    one, two = out
+    assert np.max(np.abs(two.rho[0] - two.rho[1])) < 1e-9
+    assert abs(two.energies["total"] - one.energies["total"]) < 1e-9
+    assert np.max(np.abs(two.esp[0] - one.esp[0])) < 1e-8 and np.max(np.abs(two.esp[1] - one.esp[0])) < 1e-8
