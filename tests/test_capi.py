@@ -54,6 +54,9 @@ def test_calls_before_init_fail_cleanly():
     assert b"rsdft_gpu_init" in lib.rsdft_gpu_last_error()
     assert lib.rsdft_gpu_init(None) == -1
     assert lib.rsdft_gpu_kernel_launches() == 0
+    e = np.zeros(2)
+    assert lib.rsdft_gpu_xc_pbe(C.c_void_p(x.ctypes.data), C.c_void_p(x.ctypes.data), C.c_void_p(e.ctypes.data)) == -7
+    assert b"rsdft_gpu_init" in lib.rsdft_gpu_last_error()
 
 
 def test_oracle_not_imported_by_product():
