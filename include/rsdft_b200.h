@@ -242,7 +242,7 @@ int rsdft_gpu_mix_density(double* beta_used);
  * rho(ML0, nspin)), as calc_GGAPBE96_2 forms it (src/xc/xc_ggapbe96_2_module.f90:26-370: FD
  * gradient of the total density of order Md, densities <= 1e-10 skipped): vxc (nspin x ML0,
  * host) and, if exc is not NULL, exc[0] = E_x, exc[1] = E_c.  Uses the context's grid, H and
- * Md (<= 6). */
+ * Md (<= 6); the gradient is taken along the grid axes with 1/H per axis (orthorhombic cells). */
 int rsdft_gpu_xc_pbe(const double* rho, double* vxc, double* exc);
 
 /* ---- learned preconditioner (no counterpart in the reference) ----
