@@ -175,18 +175,27 @@ class Pulay:
 
 
 class ReferenceMixer:
-    """perform_mixing with the reference's default IMIX = 10, MMIX = 4, BETA = 1.1: Pulay mixing
-    of the density (src/mixing/mixing_module.f90:145-290, pulay_mixing
-    src/mixing/mixing_pulay_module.f90:29-111).  The history holds (input, output) density
-    pairs; while fewer than mmix pairs exist a step is linear, x_in + beta (x_out - x_in); then
-    x = sum_i c_i x_in,i + beta sum_i c_i (x_out,i - x_in,i) with sum_i c_i = 1 minimising
-    |sum_i c_i (x_out,i - x_in,i)|.  BETA > 1 asks for a search: the first call takes beta =
-    0.05; later calls try beta = 1, 1/2, 1/4, ... (at most 11 tries, the last with the beta of
-    the smallest change) while the squared change of the mixed density from the previous mixed
-    one exceeds half of the previous change.  The result is made non-negative (chk_chrg)."""
+    """perform_mixing (src/mixing/mixing_module.f90:145-290) for the density-mixing choices of
+    IMIX: 0-9 simple mixing (simple_mixing :381-387), 10-19 Pulay (pulay_mixing,
+    src/mixing/mixing_pulay_module.f90:29-111; the reference's default IMIX = 10 with MMIX = 4,
+    BETA = 1.1), 20-29 Broyden (broyden_mixing, src/mixing/mixing_broyden_module.f90:11-188).
 
-    def __init__(self, rho0: np.ndarray, mmix: int = 4, beta: float = 1.1):
-        self.mmix, self.beta = int(mmix), float(beta)
+    Pulay: the history holds (input, output) density pairs; while fewer than mmix pairs exist a
+    step is linear, x_in + beta (x_out - x_in); then x = sum_i c_i x_in,i + beta sum_i c_i
+    (x_out,i - x_in,i) with sum_i c_i = 1 minimising |sum_i c_i (x_out,i - x_in,i)|.  Broyden:
+    Johnson's modified Broyden step over the same history, residual weights 1/|F_k| (at most 1)
+    and w_0 = beta.  Simple: (1 - beta) x_old + beta x_out.  BETA > 1 asks for a search: the
+    first call takes beta = 0.05; later calls try beta = 1, 1/2, 1/4, ... (at most 11 tries, the
+    last with the beta of the smallest change) while the squared change of the mixed density
+    from the previous mixed one exceeds half of the previous change.  The result is made
+    non-negative (chk_chrg).  Odd IMIX (potential mixing) and 30-39 (Pulay in G space) are not
+    built."""
+
+    def __init__(self, rho0: np.ndarray, mmix: int = 4, beta: float = 1.1, imix: int = 10):
+        if imix % 2 == 1 or not 0 <= imix <= 29:
+            raise NotImplementedError(f"IMIX {imix}: density mixing 0-9, 10-19 or 20-29 (even) only")
+        self.scheme = ("simple", "pulay", "broyden")[imix // 10]
+        self.mmix, self.beta = max(1, int(mmix)), float(beta)
         self.xin = np.zeros((self.mmix,) + rho0.shape)
         self.xou = np.zeros((self.mmix,) + rho0.shape)
         self.xin[-1] = rho0
@@ -222,6 +231,50 @@ class ReferenceMixer:
         self.xin[-1] = x + beta * (y - x)
         return self.xin[-1].copy()
 
+    def _broyden(self, f: np.ndarray, alpha: float) -> np.ndarray:
+        m = self.mmix
+        self.xou[-1] = f
+        self.count += 1
+        m0 = min(self.count, m)
+        if m == 1 or m0 == 1:
+            self.xin[:-1] = self.xin[-1]
+            self.xou[:-1] = self.xou[-1]
+            self.xin[-1] = (1.0 - alpha) * self.xin[-1] + alpha * self.xou[-1]
+            return self.xin[-1].copy()
+        if m0 < m:                                # the history moves to the first m0 slots
+            self.xin[:m0 - 1] = self.xin[1:m0].copy()
+            self.xou[:m0 - 1] = self.xou[1:m0].copy()
+            self.xin[m0 - 1] = self.xin[-1]
+            self.xou[m0 - 1] = self.xou[-1]
+        xin, xou = self.xin[:m0].reshape(m0, -1), self.xou[:m0].reshape(m0, -1)
+        F = xou - xin
+        w = np.ones(m0)
+        nf = np.sum(F * F, axis=1)
+        pos = nf > 0.0
+        w[pos] = np.minimum(1.0, 1.0 / np.sqrt(nf[pos]))
+        dF = F[1:] - F[:-1]
+        nrm = 1.0 / np.sqrt(np.sum(dF * dF, axis=1))
+        dF *= nrm[:, None]
+        dX = (xin[1:] - xin[:-1]) * nrm[:, None]
+        u = alpha * dF + dX
+        wk = w[:-1]
+        cm = wk * (dF @ F[-1])
+        a = np.outer(wk, wk) * (dF @ dF.T) + alpha * alpha * np.eye(m0 - 1)
+        gamma = cm @ np.linalg.inv(a)
+        xnew = xin[-1] + alpha * F[-1] - (wk * gamma) @ u
+        if m0 == m:
+            self.xin[:-1] = self.xin[1:].copy()
+            self.xou[:-1] = self.xou[1:].copy()
+        self.xin[-1] = xnew.reshape(f.shape)
+        return self.xin[-1].copy()
+
+    def _step(self, f: np.ndarray, beta: float) -> np.ndarray:
+        if self.scheme == "pulay":
+            return self._pulay(f, beta)
+        if self.scheme == "broyden":
+            return self._broyden(f, beta)
+        return (1.0 - beta) * self.xold + beta * f
+
     def mix(self, rho_out: np.ndarray) -> np.ndarray:
         ng = rho_out.shape[1]
         bak = (self.xin.copy(), self.xou.copy(), self.count)
@@ -235,7 +288,7 @@ class ReferenceMixer:
                 max_loop, beta = 11, 1.0
         h = dif1 = None
         for loop in range(1, max_loop + 1):
-            h = self._pulay(rho_out.copy(), beta)
+            h = self._step(rho_out.copy(), beta)
             dif1 = np.sum((h - self.xold) ** 2, axis=1) / ng
             safe = np.where(self.dif0 != 0.0, self.dif0, 1.0)
             diff = np.where(self.dif0 != 0.0, dif1 / safe, 0.0)
@@ -349,12 +402,13 @@ def restart_setup(su: structure.Setup, v: vrho.Vrho) -> structure.Setup:
 
 
 def run_scf_structure(su: structure.Setup, bands, nsweep: int = 10, diter: int = 100, scf_conv: float = 1e-11,
-                      mmix: int = 1, beta: float = 0.5, mixing: str = "pulay", diag_first: bool = False) -> StructureScf:
+                      mmix: int = 1, beta: float = 0.5, mixing: str = "pulay", diag_first: bool = False,
+                      imix: int = 10) -> StructureScf:
     """calc_scf for su with the band update `bands` (GpuBands or a test adapter): nsweep sweeps on
     the potential of the initial density, then up to diter iterations until the squared change
     of V_out (mean over the grid, every spin) is <= scf_conv.  Mixing "pulay": the Pulay class,
-    linear with step beta for mmix = 1 (the default); "reference": ReferenceMixer with MMIX =
-    mmix, BETA = beta (the reference's defaults are 4 and 1.1).  diag_first: a Rayleigh-Ritz step
+    linear with step beta for mmix = 1 (the default); "reference": ReferenceMixer with IMIX =
+    imix, MMIX = mmix, BETA = beta (the reference's defaults are 10, 4 and 1.1).  diag_first: a Rayleigh-Ritz step
     of every spin on the new potential before each iteration's sweep, the reference's order
     (bands.sweep(n, True)).  On the reference's O2 sample the reference order and mixing reach
     scf_conv = 1e-15 (24 iterations with the oracle band update); linear mixing without the
@@ -380,7 +434,7 @@ def run_scf_structure(su: structure.Setup, bands, nsweep: int = 10, diter: int =
     if mixing == "pulay":
         mixer = Pulay(mmix, beta)
     elif mixing == "reference":
-        mixer = ReferenceMixer(su.rho, mmix, beta)
+        mixer = ReferenceMixer(su.rho, mmix, beta, imix)
     else:
         raise ValueError(f"mixing {mixing!r}: 'pulay' or 'reference'")
     hist = []
@@ -437,7 +491,7 @@ def nonlocal_energy_k(su: structure.Setup, psi: np.ndarray, occ: np.ndarray, k: 
 
 def run_scf_kpoints(su: structure.Setup, bands, nsweep: int = 10, diter: int = 100, scf_conv: float = 1e-15,
                     mixing: str = "reference", mmix: int = 4, beta: float = 1.1, ekbt: float = 1e-5,
-                    kinteg: int = 5, diag_first: bool = True, kgroup=None) -> StructureScf:
+                    kinteg: int = 5, diag_first: bool = True, kgroup=None, imix: int = 10) -> StructureScf:
     """calc_scf for a structure set up on k-points (su.structure.kbb / wbz) with the band update
     `bands`: set_vloc(v (nspin, ng)), sweep(n, diag_first) -> esp (nspin, nk, nband),
     density(occ (nspin, nk, nband), weights included) -> rho (nspin, ng), bands(s, k) ->
@@ -446,8 +500,8 @@ def run_scf_kpoints(su: structure.Setup, bands, nsweep: int = 10, diter: int = 1
     the new potential (subspace_diag, unless diag_first is False) and one sweep,
     Methfessel-Paxton occupations, the output density and potential, calc_sqerr's test of V_out
     against the previous iteration (mean over the grid <= scf_conv), mixing of the density and
-    renormalisation per spin.  mixing "reference": ReferenceMixer (MMIX = mmix, BETA = beta, the
-    reference's defaults 4 and 1.1); "linear": x_in + beta (x_out - x_in).
+    renormalisation per spin.  mixing "reference": ReferenceMixer (IMIX = imix, MMIX = mmix,
+    BETA = beta, the reference's defaults 10, 4 and 1.1); "linear": x_in + beta (x_out - x_in).
 
     kgroup: a kparallel.KpointGroup when the k-points are split over ranks; `bands` then holds
     the k-points kgroup.klist only (its sweep returns those, its density sums over those, its
@@ -469,7 +523,7 @@ def run_scf_kpoints(su: structure.Setup, bands, nsweep: int = 10, diter: int = 1
     rho_in = su.rho.copy()
     prev = (su.vloc.copy(), su.rho.copy())
     if mixing == "reference":
-        mixer = ReferenceMixer(su.rho, mmix, beta)
+        mixer = ReferenceMixer(su.rho, mmix, beta, imix)
     elif mixing == "linear":
         mixer = None
     else:

@@ -111,6 +111,31 @@ def test_pulay_mixing_reaches_the_linear_fixed_point():
         assert np.max(np.abs(x - x_star)) < 1e-10, mmix
 
 
+@pytest.mark.parametrize("imix", [0, 10, 20])
+def test_reference_mixer_schemes_solve_a_linear_fixed_point(imix):
+    """Simple (IMIX 0, BETA 0.5), Pulay (10) and Broyden (20) density mixing (BETA 1.1, with the
+    search) reach the fixed point of x = A x + b; Pulay and Broyden within 40 steps."""
+    rng = np.random.default_rng(4)
+    A = rng.normal(scale=0.2, size=(2, 6, 6))
+    bp = np.abs(rng.normal(size=(2, 6))) + 2.0
+    x_star = np.array([np.linalg.solve(np.eye(6) - A[s], bp[s]) for s in range(2)])
+    m = scf_structure.ReferenceMixer(np.full((2, 6), 1.0), mmix=4, beta=0.5 if imix == 0 else 1.1, imix=imix)
+    x = np.full((2, 6), 1.0)
+    for it in range(400):
+        x = m.mix(np.array([A[s] @ x[s] + bp[s] for s in range(2)]))
+        if np.max(np.abs(x - x_star)) < 1e-10:
+            break
+    assert np.max(np.abs(x - x_star)) < 1e-10, (imix, it)
+    if imix:
+        assert it < 40, (imix, it)
+
+
+def test_reference_mixer_refuses_potential_and_gspace_mixing():
+    for imix in (1, 11, 30):
+        with pytest.raises(NotImplementedError):
+            scf_structure.ReferenceMixer(np.ones((1, 4)), imix=imix)
+
+
 def test_reference_mixer_solves_a_linear_fixed_point():
     """ReferenceMixer (IMIX = 10 Pulay with the BETA = 1.1 search) on x = A x + b: its first step
     is the 0.05 linear step, then it converges to the fixed point."""
