@@ -187,14 +187,15 @@ class ReferenceMixer:
     and w_0 = beta.  Simple: (1 - beta) x_old + beta x_out.  BETA > 1 asks for a search: the
     first call takes beta = 0.05; later calls try beta = 1, 1/2, 1/4, ... (at most 11 tries, the
     last with the beta of the smallest change) while the squared change of the mixed density
-    from the previous mixed one exceeds half of the previous change.  The result is made
-    non-negative (chk_chrg).  Odd IMIX (potential mixing) and 30-39 (Pulay in G space) are not
-    built."""
+    from the previous mixed one exceeds half of the previous change.  Even IMIX mixes the density
+    (the result is made non-negative, chk_chrg), odd IMIX the potential V_loc (the SCF loop then
+    takes the mixed potential as the next input); 30-39 (Pulay in G space) is not built."""
 
     def __init__(self, rho0: np.ndarray, mmix: int = 4, beta: float = 1.1, imix: int = 10):
-        if imix % 2 == 1 or not 0 <= imix <= 29:
-            raise NotImplementedError(f"IMIX {imix}: density mixing 0-9, 10-19 or 20-29 (even) only")
+        if not 0 <= imix <= 29:
+            raise NotImplementedError(f"IMIX {imix}: simple 0-9, Pulay 10-19 or Broyden 20-29 only")
         self.scheme = ("simple", "pulay", "broyden")[imix // 10]
+        self.potential = imix % 2 == 1
         self.mmix, self.beta = max(1, int(mmix)), float(beta)
         self.xin = np.zeros((self.mmix,) + rho0.shape)
         self.xou = np.zeros((self.mmix,) + rho0.shape)
@@ -304,7 +305,8 @@ class ReferenceMixer:
                     beta = beta_min
         self.betas.append(beta)
         self.dif0 = dif1
-        h = np.abs(h)
+        if not self.potential:
+            h = np.abs(h)
         self.xold = h.copy()
         return h
 
@@ -434,9 +436,10 @@ def run_scf_structure(su: structure.Setup, bands, nsweep: int = 10, diter: int =
     if mixing == "pulay":
         mixer = Pulay(mmix, beta)
     elif mixing == "reference":
-        mixer = ReferenceMixer(su.rho, mmix, beta, imix)
+        mixer = ReferenceMixer(su.vloc if imix % 2 else su.rho, mmix, beta, imix)
     else:
         raise ValueError(f"mixing {mixing!r}: 'pulay' or 'reference'")
+    vmix = mixing == "reference" and imix % 2 == 1
     hist = []
     conv = False
     esp = rho_out = ene = None
@@ -452,10 +455,13 @@ def run_scf_structure(su: structure.Setup, bands, nsweep: int = 10, diter: int =
         if max(sq[:ns]) <= scf_conv:
             conv = True
             break
-        rho_in = mixer.mix(rho_in, rho_out) if mixing == "pulay" else mixer.mix(rho_out)
-        for s in range(ns):
-            rho_in[s] *= (occ[s].sum()) / (float(rho_in[s].sum()) * dV)
-        v_in, _ = potential(su, rho_in, xc)
+        if vmix:
+            v_in = mixer.mix(v_out)
+        else:
+            rho_in = mixer.mix(rho_in, rho_out) if mixing == "pulay" else mixer.mix(rho_out)
+            for s in range(ns):
+                rho_in[s] *= (occ[s].sum()) / (float(rho_in[s].sum()) * dV)
+            v_in, _ = potential(su, rho_in, xc)
         bands.set_vloc(v_in)
         v_cur = v_in
     e_sum = float(np.sum(occ * esp))
@@ -523,11 +529,12 @@ def run_scf_kpoints(su: structure.Setup, bands, nsweep: int = 10, diter: int = 1
     rho_in = su.rho.copy()
     prev = (su.vloc.copy(), su.rho.copy())
     if mixing == "reference":
-        mixer = ReferenceMixer(su.rho, mmix, beta, imix)
+        mixer = ReferenceMixer(su.vloc if imix % 2 else su.rho, mmix, beta, imix)
     elif mixing == "linear":
         mixer = None
     else:
         raise ValueError(f"mixing {mixing!r}: 'reference' or 'linear'")
+    vmix = mixing == "reference" and imix % 2 == 1
     hist = []
     conv = False
     esp = occ = rho_out = ene = None
@@ -545,10 +552,13 @@ def run_scf_kpoints(su: structure.Setup, bands, nsweep: int = 10, diter: int = 1
         if max(sq[:ns]) <= scf_conv:
             conv = True
             break
-        rho_in = mixer.mix(rho_out) if mixer is not None else rho_in + beta * (rho_out - rho_in)
-        for s in range(ns):
-            rho_in[s] *= float(occ[s].sum()) / (float(rho_in[s].sum()) * dV)
-        v_in, _ = potential(su, rho_in)
+        if vmix:
+            v_in = mixer.mix(v_out)
+        else:
+            rho_in = mixer.mix(rho_out) if mixer is not None else rho_in + beta * (rho_out - rho_in)
+            for s in range(ns):
+                rho_in[s] *= float(occ[s].sum()) / (float(rho_in[s].sum()) * dV)
+            v_in, _ = potential(su, rho_in)
         bands.set_vloc(v_in)
         v_cur = v_in
     e_sum = float(np.sum(occ * esp))

@@ -130,10 +130,12 @@ def test_reference_mixer_schemes_solve_a_linear_fixed_point(imix):
         assert it < 40, (imix, it)
 
 
-def test_reference_mixer_refuses_potential_and_gspace_mixing():
-    for imix in (1, 11, 30):
+def test_reference_mixer_refuses_gspace_mixing_and_keeps_potential_signs():
+    for imix in (30, 31, 40):
         with pytest.raises(NotImplementedError):
             scf_structure.ReferenceMixer(np.ones((1, 4)), imix=imix)
+    m = scf_structure.ReferenceMixer(-np.ones((1, 4)), mmix=4, beta=0.5, imix=11)
+    assert np.all(m.mix(-2.0 * np.ones((1, 4))) < 0.0)          # potentials keep their sign
 
 
 def test_reference_mixer_solves_a_linear_fixed_point():

@@ -291,19 +291,21 @@ def test_si_two_spin_scf_equals_the_one_spin_scf():
     assert np.max(np.abs(two.esp[0] - one.esp[0])) < 1e-8 and np.max(np.abs(two.esp[1] - one.esp[0])) < 1e-8
 
 
-def test_si_broyden_mixing_reaches_the_pulay_state():
-    """IMIX = 20 (Broyden) and the default IMIX = 10 (Pulay) converge the Si operator on the
-    2 x 2 x 2 mesh to the same total energy and eigenvalues (bands 1-6; the top two of the eight
-    carried bands converge slowest in a one-sweep-per-iteration SCF)."""
+def test_si_other_mixing_schemes_reach_the_pulay_state():
+    """IMIX = 20 (Broyden of the density) and 11 (Pulay of the potential) converge the Si
+    operator on the 2 x 2 x 2 mesh to the state of the default IMIX = 10 (Pulay of the density):
+    the same total energy and eigenvalues (bands 1-6; the top two of the eight carried bands
+    converge slowest in a one-sweep-per-iteration SCF)."""
     orc = _oracle()
     pp = pseudo.load_npz(os.path.join(HERE, "golden", "si_pbe_tm_psv.npz"))
     kbb, w = synth.generate_bz((2, 2, 2))
     su = structure.setup(structure.si_crystal(pp, kbb, w, nband=8))
     out = {}
-    for imix in (10, 20):
+    for imix in (10, 20, 11):
         res = scf_structure.run_scf_kpoints(su, OracleBandsK(su, orc), nsweep=8, diter=40, scf_conv=1e-14,
                                             imix=imix)
         assert res.converged, (imix, res.sqerr[-2:])
         out[imix] = res
-    assert abs(out[20].energies["total"] - out[10].energies["total"]) < 1e-10
-    assert np.max(np.abs(out[20].esp[:, :, :6] - out[10].esp[:, :, :6])) < 1e-7
+    for imix in (20, 11):
+        assert abs(out[imix].energies["total"] - out[10].energies["total"]) < 1e-10, imix
+        assert np.max(np.abs(out[imix].esp[:, :, :6] - out[10].esp[:, :, :6])) < 1e-7, imix
