@@ -30,7 +30,7 @@ import math
 
 import numpy as np
 
-from . import api, gga, scf, structure, vrho
+from . import api, gga, pseudo, scf, structure, vrho
 
 
 # ----------------------------------------------------------------------------
@@ -174,6 +174,28 @@ class Pulay:
         return (x + self.beta * r).reshape(rin.shape)
 
 
+def _kerker_weights(n: tuple, bb: np.ndarray):
+    """(wq, wq2) on the FFT box, shape (n3, n2, n1): the reference's G index of box point i is
+    i - N, or i where that falls below -(N - 1) / 2 (get_Kerker_weights)."""
+    idx = []
+    for N in n:
+        i = np.arange(N)
+        j = i - N
+        idx.append(np.where(j < -((N - 1) // 2), i, j))
+    j1, j2, j3 = idx
+    J3, J2, J1 = np.meshgrid(j3, j2, j1, indexing="ij")
+    g = [J1 * bb[c, 0] + J2 * bb[c, 1] + J3 * bb[c, 2] for c in range(3)]
+    gg = g[0] ** 2 + g[1] ** 2 + g[2] ** 2
+    nz = gg[gg > 0.0]
+    gmin, gmax = float(nz.min()), float(nz.max())
+    b1 = 19.0 * gmin * gmax / (gmax - 20.0 * gmin)
+    b2 = ((1.5 * 0.529177) ** 2) ** 2
+    with np.errstate(divide="ignore", invalid="ignore"):
+        wq = np.where(gg == 0.0, 1.0, (gg + b1) / np.where(gg == 0.0, 1.0, gg))
+        wq2 = np.where(gg == 0.0, 1.0, gg / (gg + b2))
+    return wq, wq2
+
+
 class ReferenceMixer:
     """perform_mixing (src/mixing/mixing_module.f90:145-290) for the density-mixing choices of
     IMIX: 0-9 simple mixing (simple_mixing :381-387), 10-19 Pulay (pulay_mixing,
@@ -189,21 +211,69 @@ class ReferenceMixer:
     last with the beta of the smallest change) while the squared change of the mixed density
     from the previous mixed one exceeds half of the previous change.  Even IMIX mixes the density
     (the result is made non-negative, chk_chrg), odd IMIX the potential V_loc (the SCF loop then
-    takes the mixed potential as the next input); 30-39 (Pulay in G space) is not built."""
+    takes the mixed potential as the next input).  IMIX 30-39 runs the Pulay step on the Fourier
+    coefficients (pulay_g_mixing :124-205, get_Kerker_weights :275-337): residual products
+    weighted by (|G|^2 + q1) / |G|^2 and updates damped by |G|^2 / (|G|^2 + q2), with q1 = 19
+    |G|min^2 |G|max^2 / (|G|max^2 - 20 |G|min^2) over the FFT box and q2 = (1.5 x 0.529177)^4
+    (BMIX squared twice, as the reference does); it needs grid = (n, bb) with bb the reciprocal
+    vectors as columns."""
 
-    def __init__(self, rho0: np.ndarray, mmix: int = 4, beta: float = 1.1, imix: int = 10):
-        if not 0 <= imix <= 29:
-            raise NotImplementedError(f"IMIX {imix}: simple 0-9, Pulay 10-19 or Broyden 20-29 only")
-        self.scheme = ("simple", "pulay", "broyden")[imix // 10]
+    def __init__(self, rho0: np.ndarray, mmix: int = 4, beta: float = 1.1, imix: int = 10, grid=None):
+        if not 0 <= imix <= 39:
+            raise NotImplementedError(f"IMIX {imix}: simple 0-9, Pulay 10-19, Broyden 20-29 or G-space Pulay 30-39")
+        self.scheme = ("simple", "pulay", "broyden", "pulay_g")[imix // 10]
         self.potential = imix % 2 == 1
         self.mmix, self.beta = max(1, int(mmix)), float(beta)
-        self.xin = np.zeros((self.mmix,) + rho0.shape)
-        self.xou = np.zeros((self.mmix,) + rho0.shape)
+        shape = rho0.shape
+        if self.scheme == "pulay_g":
+            if grid is None:
+                raise ValueError("IMIX 30-39 needs grid = (n, bb)")
+            self.n = tuple(grid[0])
+            self.wq, self.wq2 = _kerker_weights(self.n, np.asarray(grid[1], np.float64))
+            rho0 = self._fft(rho0)
+            shape = rho0.shape
+        self.xin = np.zeros((self.mmix,) + shape, rho0.dtype)
+        self.xou = np.zeros((self.mmix,) + shape, rho0.dtype)
         self.xin[-1] = rho0
         self.count = 0
-        self.xold = rho0.copy()
-        self.dif0 = np.zeros(rho0.shape[0])
+        self.xold = (self._ifft(rho0) if self.scheme == "pulay_g" else rho0).copy()
+        self.dif0 = np.zeros(shape[0])
         self.betas = []
+
+    def _fft(self, x: np.ndarray) -> np.ndarray:
+        n1, n2, n3 = self.n
+        return np.fft.fftn(x.reshape(-1, n3, n2, n1), axes=(1, 2, 3))
+
+    def _ifft(self, z: np.ndarray) -> np.ndarray:
+        return np.fft.ifftn(z, axes=(1, 2, 3)).real.reshape(z.shape[0], -1)
+
+    def _pulay_g(self, f: np.ndarray, beta: float) -> np.ndarray:
+        m = self.mmix
+        self.xou[-1] = self._fft(f)
+        self.count += 1
+        m0 = min(self.count, m)
+        if m == 1 or m0 < m:
+            self.xin[:-1] = self.xin[1:].copy()
+            self.xou[:-1] = self.xou[1:].copy()
+            self.xin[-1] = self.xin[-1] + beta * self.wq2 * (self.xou[-1] - self.xin[-1])
+            return self._ifft(self.xin[-1])
+        r = (self.xou[m - m0:] - self.xin[m - m0:]).reshape(m0, -1)
+        w = np.broadcast_to(self.wq, self.xin.shape[1:]).reshape(-1)
+        a = (np.conj(r) * w) @ r.T
+        try:
+            c = np.linalg.solve(a, np.ones(m0, complex))
+        except np.linalg.LinAlgError:
+            c = np.linalg.lstsq(a, np.ones(m0, complex), rcond=None)[0]
+        if not np.isfinite(c.sum()) or c.sum() == 0.0:
+            c = np.zeros(m0, complex)
+            c[-1] = 1.0
+        c /= c.sum()
+        x = np.tensordot(c, self.xin[m - m0:], axes=1)
+        y = np.tensordot(c, self.xou[m - m0:], axes=1)
+        self.xin[:-1] = self.xin[1:].copy()
+        self.xou[:-1] = self.xou[1:].copy()
+        self.xin[-1] = x + beta * self.wq2 * (y - x)
+        return self._ifft(self.xin[-1])
 
     def _pulay(self, f: np.ndarray, beta: float) -> np.ndarray:
         m = self.mmix
@@ -272,6 +342,8 @@ class ReferenceMixer:
     def _step(self, f: np.ndarray, beta: float) -> np.ndarray:
         if self.scheme == "pulay":
             return self._pulay(f, beta)
+        if self.scheme == "pulay_g":
+            return self._pulay_g(f, beta)
         if self.scheme == "broyden":
             return self._broyden(f, beta)
         return (1.0 - beta) * self.xold + beta * f
@@ -436,7 +508,8 @@ def run_scf_structure(su: structure.Setup, bands, nsweep: int = 10, diter: int =
     if mixing == "pulay":
         mixer = Pulay(mmix, beta)
     elif mixing == "reference":
-        mixer = ReferenceMixer(su.vloc if imix % 2 else su.rho, mmix, beta, imix)
+        mixer = ReferenceMixer(su.vloc if imix % 2 else su.rho, mmix, beta, imix,
+                               grid=(su.problem.n, pseudo.reciprocal(su.structure.avec).T))
     else:
         raise ValueError(f"mixing {mixing!r}: 'pulay' or 'reference'")
     vmix = mixing == "reference" and imix % 2 == 1
@@ -529,7 +602,8 @@ def run_scf_kpoints(su: structure.Setup, bands, nsweep: int = 10, diter: int = 1
     rho_in = su.rho.copy()
     prev = (su.vloc.copy(), su.rho.copy())
     if mixing == "reference":
-        mixer = ReferenceMixer(su.vloc if imix % 2 else su.rho, mmix, beta, imix)
+        mixer = ReferenceMixer(su.vloc if imix % 2 else su.rho, mmix, beta, imix,
+                               grid=(su.problem.n, pseudo.reciprocal(su.structure.avec).T))
     elif mixing == "linear":
         mixer = None
     else:

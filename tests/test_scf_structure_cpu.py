@@ -130,8 +130,8 @@ def test_reference_mixer_schemes_solve_a_linear_fixed_point(imix):
         assert it < 40, (imix, it)
 
 
-def test_reference_mixer_refuses_gspace_mixing_and_keeps_potential_signs():
-    for imix in (30, 31, 40):
+def test_reference_mixer_refuses_unknown_imix_and_keeps_potential_signs():
+    for imix in (40, 41, -1):
         with pytest.raises(NotImplementedError):
             scf_structure.ReferenceMixer(np.ones((1, 4)), imix=imix)
     m = scf_structure.ReferenceMixer(-np.ones((1, 4)), mmix=4, beta=0.5, imix=11)

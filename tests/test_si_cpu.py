@@ -292,7 +292,8 @@ def test_si_two_spin_scf_equals_the_one_spin_scf():
 
 
 def test_si_other_mixing_schemes_reach_the_pulay_state():
-    """IMIX = 20 (Broyden of the density) and 11 (Pulay of the potential) converge the Si
+    """IMIX = 20 (Broyden of the density), 11 (Pulay of the potential) and 30 (Pulay of the
+    density's Fourier coefficients with the Kerker weights) converge the Si
     operator on the 2 x 2 x 2 mesh to the state of the default IMIX = 10 (Pulay of the density):
     the same total energy and eigenvalues (bands 1-6; the top two of the eight carried bands
     converge slowest in a one-sweep-per-iteration SCF)."""
@@ -301,11 +302,11 @@ def test_si_other_mixing_schemes_reach_the_pulay_state():
     kbb, w = synth.generate_bz((2, 2, 2))
     su = structure.setup(structure.si_crystal(pp, kbb, w, nband=8))
     out = {}
-    for imix in (10, 20, 11):
+    for imix in (10, 20, 11, 30):
         res = scf_structure.run_scf_kpoints(su, OracleBandsK(su, orc), nsweep=8, diter=40, scf_conv=1e-14,
                                             imix=imix)
         assert res.converged, (imix, res.sqerr[-2:])
         out[imix] = res
-    for imix in (20, 11):
+    for imix in (20, 11, 30):
         assert abs(out[imix].energies["total"] - out[10].energies["total"]) < 1e-10, imix
         assert np.max(np.abs(out[imix].esp[:, :, :6] - out[10].esp[:, :, :6])) < 1e-7, imix
