@@ -103,6 +103,75 @@ def calc_fermi_mp(esp: np.ndarray, wbz: np.ndarray, nelec: float, ekbt: float = 
     return occ, ef
 
 
+def fermi_dirac(esp: np.ndarray, wbz: np.ndarray, nelec: float, ekbt: float):
+    """Fermi-Dirac occupations occ(s, k, n) (weights and 2/nspin included) and the Fermi level:
+    fermi_dirac without the fixed-spin branch (src/fermi_dirac_module.f90:11-250): bisection of
+    the level on the bands mb1.. (100 cycles, tolerance 1e-10 on the electron count, the upper
+    bound raised by min(100 ekbt, 0.1)); if it does not settle, the lowest band is taken as
+    filled and the search repeats on the bands above; f = 1 / (exp(x) + 1) with x = (e - ef) /
+    ekbt cut at |x| > 36.9 (a step function for ekbt < 1e-10); the remaining electron-count
+    error is added to the highest occupied band of every (k, s)."""
+    esp = np.asarray(esp, np.float64)
+    ns, nk, nb = esp.shape
+    w = np.asarray(wbz, np.float64)[None, :, None] * (2.0 / ns)
+    eps, big = 1e-10, 36.9
+
+    def ff(e, ef):
+        if ekbt < eps:
+            return np.where(e - ef > 0.0, 0.0, np.where(e - ef < 0.0, 1.0, 0.5))
+        x = (e - ef) / ekbt
+        with np.errstate(over="ignore"):
+            return np.where(x > big, 0.0, np.where(x < -big, 1.0, 1.0 / (np.exp(np.clip(x, -big, big)) + 1.0)))
+
+    if abs(2 * nb - nelec) < eps:
+        return np.ones_like(esp) * w, float(esp.max())
+    for mb1 in range(nb):
+        sub = esp[:, :, mb1:]
+        ef1, ef2 = float(sub.min()), float(sub.max())
+        if ef1 == ef2:
+            ef1, ef2 = ef1 - 0.01, ef2 + 0.01
+        ef2 += min(ekbt * 1e2, 0.1)
+        zne = nelec - 2.0 * mb1
+        found = False
+        for _ in range(100):
+            ef = 0.5 * (ef1 + ef2)
+            f = ff(sub, ef)
+            n = float(np.sum(f * w))
+            if n - zne > eps:
+                ef2 = ef
+            elif n - zne < -eps:
+                ef1 = ef
+            else:
+                found = True
+                break
+        if found:
+            occ = np.zeros_like(esp)
+            occ[:, :, :mb1] = np.broadcast_to(w, (ns, nk, mb1))
+            occ[:, :, mb1:] = f * w
+            err = nelec - float(occ.sum())
+            if abs(err) > 0.0:
+                for s in range(ns):
+                    for k in range(nk):
+                        pos = np.nonzero(occ[s, k, mb1:] > 0.0)[0]
+                        if pos.size:
+                            occ[s, k, mb1 + pos[-1]] += err / (nk * ns)
+            return occ, ef
+    raise RuntimeError("fermi_dirac: the Fermi level did not settle (the reference stops with FERMI(1))")
+
+
+def entropy_fd(ekbt: float, occ: np.ndarray) -> float:
+    """entropy_fd (src/fermi_dirac_module.f90:330-351) as the reference evaluates it on the
+    weighted occupations: sum over (s, k, n) of (2 / ns) ekbt S(f) with f = occ ns / 2 and
+    S(f) = -f ln f - (1 - f) ln(1 - f)."""
+    ns = occ.shape[0]
+    f = occ * (ns / 2.0)
+    g = 1.0 - f
+    with np.errstate(divide="ignore", invalid="ignore"):
+        sf = -np.where(f > 0.0, f * np.log(np.where(f > 0.0, f, 1.0)), 0.0) \
+             - np.where(g > 0.0, g * np.log(np.where(g > 0.0, g, 1.0)), 0.0)
+    return float(np.sum((2.0 / ns) * ekbt * sf))
+
+
 @dataclasses.dataclass
 class ScfResult:
     iterations: int

@@ -570,7 +570,8 @@ def nonlocal_energy_k(su: structure.Setup, psi: np.ndarray, occ: np.ndarray, k: 
 
 def run_scf_kpoints(su: structure.Setup, bands, nsweep: int = 10, diter: int = 100, scf_conv: float = 1e-15,
                     mixing: str = "reference", mmix: int = 4, beta: float = 1.1, ekbt: float = 1e-5,
-                    kinteg: int = 5, diag_first: bool = True, kgroup=None, imix: int = 10) -> StructureScf:
+                    kinteg: int = 5, diag_first: bool = True, kgroup=None, imix: int = 10,
+                    occupations: str = "mp") -> StructureScf:
     """calc_scf for a structure set up on k-points (su.structure.kbb / wbz) with the band update
     `bands`: set_vloc(v (nspin, ng)), sweep(n, diag_first) -> esp (nspin, nk, nband),
     density(occ (nspin, nk, nband), weights included) -> rho (nspin, ng), bands(s, k) ->
@@ -582,12 +583,18 @@ def run_scf_kpoints(su: structure.Setup, bands, nsweep: int = 10, diter: int = 1
     renormalisation per spin.  mixing "reference": ReferenceMixer (IMIX = imix, MMIX = mmix,
     BETA = beta, the reference's defaults 10, 4 and 1.1); "linear": x_in + beta (x_out - x_in).
 
+    occupations "mp": Methfessel-Paxton of order kinteg (calc_fermi_mp, the reference's
+    default); "fd": Fermi-Dirac (fermi_dirac, MP_VERSION -1) with its entropy term, the free
+    energy E - TS in energies["free"].
+
     kgroup: a kparallel.KpointGroup when the k-points are split over ranks; `bands` then holds
     the k-points kgroup.klist only (its sweep returns those, its density sums over those, its
     bands(s, j) takes the local index j), the eigenvalues are gathered for the occupations and
     the density and band-energy sums are added over the ranks; every rank returns the same
     result."""
     from .kparallel import KpointGroup
+    if occupations not in ("mp", "fd"):
+        raise ValueError(f"occupations {occupations!r}: 'mp' or 'fd'")
     st = su.structure
     kg = kgroup if kgroup is not None else KpointGroup(su.problem.nk, local=True)
     kl = kg.klist
@@ -616,7 +623,10 @@ def run_scf_kpoints(su: structure.Setup, bands, nsweep: int = 10, diter: int = 1
     it = 0
     for it in range(1, diter + 1):
         esp = kg.gather_esp(bands.sweep(1, diag_first))
-        occ, ef = scf.calc_fermi_mp(esp, wbz, nel, ekbt, kinteg)
+        if occupations == "fd":
+            occ, ef = scf.fermi_dirac(esp, wbz, nel, ekbt)
+        else:
+            occ, ef = scf.calc_fermi_mp(esp, wbz, nel, ekbt, kinteg)
         rho_out = kg.sum(bands.density(occ[:, kl[0]:kl[-1] + 1]))
         v_out, ene = potential(su, rho_out)
         sq = [float(np.mean((v_out[s] - prev[0][s]) ** 2)) for s in range(ns)] + \
@@ -646,5 +656,8 @@ def run_scf_kpoints(su: structure.Setup, bands, nsweep: int = 10, diter: int = 1
     ene["ewald"] = ewald_energy(st)
     ene["total"] = (ene["kinetic"] + ene["ion_local"] + e_nl + ene["hartree"] + ene["xc"] + ene["ewald"])
     ene["fermi"] = float(ef)
+    if occupations == "fd":
+        ene["entropy"] = scf.entropy_fd(ekbt, occ)
+        ene["free"] = ene["total"] - ene["entropy"]
     return StructureScf(iterations=it, converged=conv, esp=esp, occ=occ, rho=rho_out, sqerr=hist, energies=ene,
                         vloc=np.array(v_cur))

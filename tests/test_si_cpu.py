@@ -20,7 +20,7 @@ import os
 import numpy as np
 import pytest
 
-from rsdft_develop_b200 import pseudo, scf_structure, structure, synth
+from rsdft_develop_b200 import pseudo, scf, scf_structure, structure, synth
 
 HERE = os.path.dirname(__file__)
 
@@ -206,6 +206,11 @@ def test_si_scf_reaches_the_reference_state(si, si_scf):
             assert abs(res.energies[key] - ref[key]) < 6e-7, (key, res.energies[key], ref[key], log["source"])
         last = np.array([r[2] for r in log["esp_last"]]).reshape(63, 9)[:, :8]
         assert np.max(np.abs(res.esp[0, :, :8] - last)) < 1e-7
+        # the printed entropy is entropy_fd of the weighted occupations at EKBT 1e-5 (nonzero for
+        # an insulator: S is taken of f w_k), and Free Energy = Etot - entropy
+        ent = scf.entropy_fd(1e-5, res.occ)
+        assert abs(ent - ref["entropy"]) < 1e-12, (ent, ref["entropy"])
+        assert abs(res.energies["total"] - ent - ref["free"]) < 1e-9
 
 
 def test_si_scf_follows_the_reference_iterations(si_scf):
