@@ -475,6 +475,14 @@ def restart_setup(su: structure.Setup, v: vrho.Vrho) -> structure.Setup:
                                problem=dataclasses.replace(su.problem, vloc=np.ascontiguousarray(v.vloc[0])))
 
 
+def _harris(e_sum: float, ene_in: dict, st: structure.Structure) -> float:
+    """Harris-Foulkes energy of the last iteration (calc_with_rhoIN_total_energy,
+    src/total_energy_module.f90:345-346): sum occ e - int rho_in V_in + E_H[rho_in] +
+    E_xc[rho_in] + int rho_in V_ion + E_ewald, with rho_in the density V_in was built from."""
+    return (e_sum - ene_in["local"] + ene_in["hartree"] + ene_in["xc"] + ene_in["ion_local"]
+            + ewald_energy(st))
+
+
 def run_scf_structure(su: structure.Setup, bands, nsweep: int = 10, diter: int = 100, scf_conv: float = 1e-11,
                       mmix: int = 1, beta: float = 0.5, mixing: str = "pulay", diag_first: bool = False,
                       imix: int = 10) -> StructureScf:
@@ -513,6 +521,7 @@ def run_scf_structure(su: structure.Setup, bands, nsweep: int = 10, diter: int =
     else:
         raise ValueError(f"mixing {mixing!r}: 'pulay' or 'reference'")
     vmix = mixing == "reference" and imix % 2 == 1
+    ene_in = None if vmix else potential(su, su.rho, xc)[1]
     hist = []
     conv = False
     esp = rho_out = ene = None
@@ -534,13 +543,15 @@ def run_scf_structure(su: structure.Setup, bands, nsweep: int = 10, diter: int =
             rho_in = mixer.mix(rho_in, rho_out) if mixing == "pulay" else mixer.mix(rho_out)
             for s in range(ns):
                 rho_in[s] *= (occ[s].sum()) / (float(rho_in[s].sum()) * dV)
-            v_in, _ = potential(su, rho_in, xc)
+            v_in, ene_in = potential(su, rho_in, xc)
         bands.set_vloc(v_in)
         v_cur = v_in
     e_sum = float(np.sum(occ * esp))
     e_nl = sum(nonlocal_energy(su, bands.bands(s), occ[s]) for s in range(ns))
     ene = dict(ene)
     ene["local"] = float(np.sum(rho_out * v_cur)) * dV
+    if ene_in is not None:
+        ene["harris"] = _harris(e_sum, ene_in, st)
     ene["sum_eigen"] = e_sum
     ene["nonlocal"] = e_nl
     ene["kinetic"] = e_sum - ene["local"] - e_nl
@@ -616,6 +627,7 @@ def run_scf_kpoints(su: structure.Setup, bands, nsweep: int = 10, diter: int = 1
     else:
         raise ValueError(f"mixing {mixing!r}: 'reference' or 'linear'")
     vmix = mixing == "reference" and imix % 2 == 1
+    ene_in = None if vmix else potential(su, su.rho)[1]
     hist = []
     conv = False
     esp = occ = rho_out = ene = None
@@ -642,7 +654,7 @@ def run_scf_kpoints(su: structure.Setup, bands, nsweep: int = 10, diter: int = 1
             rho_in = mixer.mix(rho_out) if mixer is not None else rho_in + beta * (rho_out - rho_in)
             for s in range(ns):
                 rho_in[s] *= float(occ[s].sum()) / (float(rho_in[s].sum()) * dV)
-            v_in, _ = potential(su, rho_in)
+            v_in, ene_in = potential(su, rho_in)
         bands.set_vloc(v_in)
         v_cur = v_in
     e_sum = float(np.sum(occ * esp))
@@ -656,6 +668,8 @@ def run_scf_kpoints(su: structure.Setup, bands, nsweep: int = 10, diter: int = 1
     ene["ewald"] = ewald_energy(st)
     ene["total"] = (ene["kinetic"] + ene["ion_local"] + e_nl + ene["hartree"] + ene["xc"] + ene["ewald"])
     ene["fermi"] = float(ef)
+    if ene_in is not None:
+        ene["harris"] = _harris(e_sum, ene_in, st)
     if occupations == "fd":
         ene["entropy"] = scf.entropy_fd(ekbt, occ)
         ene["free"] = ene["total"] - ene["entropy"]

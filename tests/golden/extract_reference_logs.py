@@ -170,7 +170,7 @@ ENERGY_KEYS = {
     "Ion Local Potential": "ion_local", "Ion Nonlocal Potential": "nonlocal", "Kinetic Energy": "kinetic",
     "Hartree Energy": "hartree", "Exchange-Correlation Energy": "xc", "Exchange Energy": "exchange",
     "Correlation Energy": "correlation", "Sum of eigenvalues": "sum_eigen", "Fermi energy": "fermi",
-    "Entropy": "entropy", "Free Energy": "free",
+    "Entropy": "entropy", "Free Energy": "free", "Harris Energy": "harris",
 }
 
 

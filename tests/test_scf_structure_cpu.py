@@ -167,12 +167,14 @@ def o2_scf(o2):
 def test_o2_scf_with_oracle_bands_reaches_the_reference_state(o2_scf):
     """The reference's loop order (Rayleigh-Ritz before each sweep), its default mixing and its
     stop (SCFCONV 1e-15 on the mean squared change of V_loc): the converged state of all eight
-    logs, the total energy to 1e-11 Ha (it lands within ~2e-12), every term to 2e-9 Ha (~8e-10),
+    logs, the total and Harris-Foulkes energies to 1e-11 Ha (they land within ~2e-12), every term
+    to 2e-9 Ha (~8e-10),
     bands 1-7 of both spins to 2e-10 Ha (~5e-11), sum |rho_up - rho_down| dV to 1e-10."""
     res = o2_scf
     check_against_logs(res, e_tol=2e-9, esp_tol=2e-10, spin_tol=1e-10)
     for log in _logs():
         assert abs(res.energies["total"] - log["energies"]["total"]) < 1e-11
+        assert abs(res.energies["harris"] - log["energies"]["harris"]) < 1e-11
 
 
 def test_o2_restart_from_vrho_file(o2, o2_scf, tmp_path):

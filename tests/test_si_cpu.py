@@ -200,6 +200,7 @@ def test_si_scf_reaches_the_reference_state(si, si_scf):
     for log in _logs():
         ref = log["energies"]
         assert abs(res.energies["total"] - ref["total"]) < 1e-9, (res.energies["total"], ref["total"])
+        assert abs(res.energies["harris"] - ref["harris"]) < 1e-9, (res.energies["harris"], ref["harris"])
         assert abs(res.energies["ewald"] - ref["ewald"]) < 1e-12
         for key in ("kinetic", "hartree", "xc", "exchange", "correlation", "ion_local", "local", "nonlocal",
                     "sum_eigen"):
