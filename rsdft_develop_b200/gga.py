@@ -173,6 +173,55 @@ def pbe(rho: np.ndarray, n: tuple, h: tuple, dV: float, md: int = 6, mu: float =
     return vx + vc, Ex, Ec
 
 
+def lda_pz81(rho: np.ndarray, dV: float):
+    """calc_LDAPZ81 (src/xc/xc_ldapz81_module.f90:17-219) for rho of shape (nspin, ng): Slater
+    exchange per spin (scaled by 2^(1/3) for two spins; non-positive densities skipped) and the
+    Perdew-Zunger 1981 correlation with the von Barth-Hedin interpolation
+    f(zeta) = ((1 + zeta)^(4/3) + (1 - zeta)^(4/3) - 2) / (2^(4/3) - 2) between its unpolarised
+    and polarised fits (|rho_s| used, one spin split in halves).  Returns (vxc (nspin, ng), Ex,
+    Ec) with the energies integrated over the cell."""
+    rho = np.atleast_2d(np.asarray(rho, np.float64))
+    ns = rho.shape[0]
+    cnst = 2.0 ** (1.0 / 3.0) if ns == 2 else 1.0
+    vx = np.zeros_like(rho)
+    ex_sum = 0.0
+    for s in range(ns):
+        pos = rho[s] > 0.0
+        exd = -cnst * 0.75 * np.cbrt(3.0 / math.pi * rho[s][pos])
+        ex_sum += float(np.sum(rho[s][pos] * exd))
+        vx[s][pos] = 4.0 / 3.0 * exd
+    gam, b1, b2 = (-0.1423, -0.0843), (1.0529, 1.3981), (0.3334, 0.2611)
+    A, B, C, D = (0.0311, 0.01555), (-0.048, -0.0269), (0.002, 0.0007), (-0.0116, -0.0048)
+    fac = 0.5 if ns == 1 else 1.0
+    ra, rb = np.abs(rho[0] * fac), np.abs(rho[-1] * fac)
+    tr = ra + rb
+    ok = tr > 0.0
+    t = np.where(ok, tr, 1.0)
+    rs = np.cbrt(3.0 / (4.0 * math.pi) / t)
+    hi = rs >= 1.0
+    sq = np.sqrt(rs)
+    lnr = np.log(rs)
+    ecd, mu = [], []
+    for p in (0, 1):
+        den = 1.0 + b1[p] * sq + b2[p] * rs
+        e_hi = gam[p] / den
+        m_hi = e_hi + e_hi / 3.0 * (0.5 * b1[p] / sq + b2[p]) / (1.0 / rs + b1[p] / sq + b2[p])
+        e_lo = A[p] * lnr + B[p] + C[p] * rs * lnr + D[p] * rs
+        m_lo = e_lo - (A[p] + C[p] * rs * (1.0 + lnr) + rs * D[p]) / 3.0
+        ecd.append(np.where(hi, e_hi, e_lo))
+        mu.append(np.where(hi, m_hi, m_lo))
+    c0 = 1.0 / (2.0 ** (4.0 / 3.0) - 2.0)
+    f = c0 * ((2.0 * ra) ** (4.0 / 3.0) + (2.0 * rb) ** (4.0 / 3.0) - 2.0 * t ** (4.0 / 3.0)) / t ** (4.0 / 3.0)
+    ec_sum = float(np.sum(np.where(ok, t * (ecd[0] + (ecd[1] - ecd[0]) * f), 0.0)))
+    g = c0 * 4.0 / 3.0 * 2.0 * (np.cbrt(2.0 * ra) - np.cbrt(2.0 * rb)) / t ** (4.0 / 3.0)
+    dfa, dfb = g * rb, -g * ra
+    base = mu[0] + (mu[1] - mu[0]) * f
+    vc = np.zeros_like(rho)
+    vc[0] = np.where(ok, base + (ecd[1] - ecd[0]) * dfa, 0.0)
+    vc[-1] = np.where(ok, base + (ecd[1] - ecd[0]) * dfb, 0.0)
+    return vx + vc, ex_sum * dV, ec_sum * dV
+
+
 def _hartree_kernel(gr) -> np.ndarray:
     """4 pi / |G|^2 on the sphere's points of the half spectrum (x axis 0..N1/2), G = 0 and the
     points outside the sphere 0; cached on gr.  The sphere is symmetric under G -> -G, so the

@@ -144,7 +144,7 @@ def potential(su: structure.Setup, rho: np.ndarray, xc=None):
     if xc is not None:
         vxc, ex, ec = xc(rho)
     else:
-        vxc, ex, ec = gga.pbe(rho, su.problem.n, h, dV, st.md, bmat=su.bmat)
+        vxc, ex, ec = structure.host_xc(st.xc, rho, su.problem.n, h, dV, st.md, su.bmat)
     v = su.vion[None, :] + vh[None, :] + vxc
     return v, {"hartree": eh, "xc": ex + ec, "exchange": ex, "correlation": ec,
                "ion_local": float(np.sum(rho.sum(axis=0) * su.vion)) * dV,
@@ -456,7 +456,7 @@ def to_vrho(su: structure.Setup, res: StructureScf) -> vrho.Vrho:
     Vloc un-updated on exit and recomputes V_H, V_xc at the top of each iteration)."""
     st = su.structure
     vh, _ = gga.hartree_sphere(res.rho.sum(axis=0), su.ggrid, su.problem.dV)
-    vxc, _, _ = gga.pbe(res.rho, su.problem.n, (su.problem.h,) * 3, su.problem.dV, st.md, bmat=su.bmat)
+    vxc, _, _ = structure.host_xc(st.xc, res.rho, su.problem.n, (su.problem.h,) * 3, su.problem.dV, st.md, su.bmat)
     atoms = np.concatenate([np.asarray(p, np.float64).reshape(-1, 3) for _, p in st.species])
     ki = np.concatenate([np.full(len(np.asarray(p).reshape(-1, 3)), e + 1, np.int32)
                          for e, (_, p) in enumerate(st.species)])
@@ -506,7 +506,7 @@ def run_scf_structure(su: structure.Setup, bands, nsweep: int = 10, diter: int =
     occ = np.zeros((ns, nb))
     for s in range(ns):
         occ[s, :nocc[s]] = 1.0 if ns == 2 else 2.0
-    xc = getattr(bands, "xc", None)
+    xc = getattr(bands, "xc", None) if structure.is_pbe(st.xc) else None   # the device kernel is PBE
     bands.set_vloc(su.vloc)
     v_cur = su.vloc
     if nsweep > 0:

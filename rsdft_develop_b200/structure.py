@@ -86,6 +86,20 @@ class Setup:
         return dataclasses.replace(self.problem, vloc=np.ascontiguousarray(self.vloc[s - 1]))
 
 
+def is_pbe(xc: str) -> bool:
+    return xc.upper() in ("GGAPBE96", "PBE", "PBE96")
+
+
+def host_xc(xc: str, rho: np.ndarray, n: tuple, h: tuple, dV: float, md: int, bmat=None):
+    """V_xc and (E_x, E_c) of rho for the structure's XCtype: GGAPBE96 (calc_GGAPBE96_2) or
+    LDAPZ81 (calc_LDAPZ81, the reference's default)."""
+    if is_pbe(xc):
+        return gga.pbe(rho, n, h, dV, md, bmat=bmat)
+    if xc.upper() in ("LDAPZ81", "LDA", "PZ81"):
+        return gga.lda_pz81(rho, dV)
+    raise NotImplementedError(f"xc {xc}: GGAPBE96 or LDAPZ81")
+
+
 def setup(st: Structure, rcfac: float = 1.5, qcfac: float = 1.0, etafac: float = 8.0,
           complex16: bool = False) -> Setup:
     """The band update's inputs for st.  complex16: the operator for the complex16 build at the
@@ -120,9 +134,7 @@ def setup(st: Structure, rcfac: float = 1.5, qcfac: float = 1.0, etafac: float =
         r = rho0 / ns
         rho[s] = r * (nes[s] / (float(r.sum()) * dV))
     vh, eh = gga.hartree_sphere(rho.sum(axis=0), gr, dV)
-    if st.xc.upper() not in ("GGAPBE96", "PBE", "PBE96"):
-        raise NotImplementedError(f"xc {st.xc}: structures from PSV files take PBE here")
-    vxc, ex, ec = gga.pbe(rho, n, h, dV, st.md, bmat=bmat)
+    vxc, ex, ec = host_xc(st.xc, rho, n, h, dV, st.md, bmat)
     exc = ex + ec
     vloc = vion[None, :] + vh[None, :] + vxc
     filtered = [pseudo.filter_projectors(pp, gr.gcut, rcfac, qcfac, etafac) for pp, _ in species]

@@ -67,3 +67,43 @@ def test_si_scf_with_fermi_dirac_occupations():
     assert abs(out["fd"].energies["entropy"] - scf.entropy_fd(1e-3, out["fd"].occ)) < 1e-15
     assert abs(out["fd"].energies["free"] - (out["fd"].energies["total"] - out["fd"].energies["entropy"])) < 1e-15
     assert abs(out["fd"].occ.sum() - 8.0) < 1e-9
+
+
+def test_lda_pz81_against_the_oracle_and_its_spin_limits():
+    """gga.lda_pz81 (calc_LDAPZ81 with spin) equals the oracle's unpolarised PZ81, two equal spin
+    halves equal one spin, and V_xc is the derivative of E_xc in the polarised case."""
+    from oracle import scf_oracle
+    from rsdft_develop_b200 import gga
+    rng = np.random.default_rng(0)
+    rho = rng.uniform(0.0, 2.0, 4000) ** 3                 # rs on both sides of 1
+    v, ex, ec = gga.lda_pz81(rho[None, :], 1.0)
+    vo, exc_o, _ = scf_oracle.lda_pz81(rho)
+    assert np.max(np.abs(v[0] - vo)) < 1e-13 and abs(ex + ec - exc_o) < 1e-10
+    v2, ex2, ec2 = gga.lda_pz81(np.stack([rho / 2, rho / 2]), 1.0)
+    assert np.max(np.abs(v2 - v)) < 1e-13 and abs(ex2 + ec2 - ex - ec) < 1e-10
+    r = np.stack([rng.uniform(0.01, 1.0, 50), rng.uniform(0.01, 1.0, 50)])
+    v, _, _ = gga.lda_pz81(r, 1.0)
+    for s in (0, 1):
+        d = np.zeros_like(r)
+        d[s] = 1e-6 * r[s]
+        ep = sum(gga.lda_pz81(r + d, 1.0)[1:])
+        em = sum(gga.lda_pz81(r - d, 1.0)[1:])
+        # E is a sum over points: dE/d(rho_s(i)) at every point at once via a common relative step
+        assert abs((ep - em) / 2.0 - float(np.sum(v[s] * d[s]))) < 1e-9
+
+
+def test_si_scf_with_lda():
+    """XCtype LDAPZ81 (the reference's default) in the structure set-up and the k-point SCF."""
+    from oracle import oracle as orc
+    from tests.test_si_cpu import OracleBandsK
+    import dataclasses
+    orc.set_threads(4)
+    pp = pseudo.load_npz(os.path.join(HERE, "golden", "si_pbe_tm_psv.npz"))
+    kbb, w = synth.generate_bz((2, 2, 2))
+    st = dataclasses.replace(structure.si_crystal(pp, kbb, w, nband=8), xc="LDAPZ81")
+    su = structure.setup(st)
+    res = scf_structure.run_scf_kpoints(su, OracleBandsK(su, orc), nsweep=8, diter=30, scf_conv=1e-14)
+    assert res.converged
+    pbe = structure.setup(structure.si_crystal(pp, kbb, w, nband=8))
+    assert np.max(np.abs(su.vxc - pbe.vxc)) > 1e-3            # a different functional
+    assert -8.0 < res.energies["total"] < -7.7
