@@ -1,11 +1,14 @@
-"""SCF loop for structures read from pseudopotential files (PBE, one or two spins).
+"""SCF loop for structures read from pseudopotential files (PBE or LDA PZ81, one or two spins,
+Gamma or k-points).
 
 The reference's calc_scf (src/scf_module.f90:85-563) around the band update, for the operators
-rsdft_develop_b200.structure builds: per iteration one sweep of every spin on the current
-V_loc, occupations, the density of the new bands, V_out = V_ion + V_H + V_xc^PBE of that
-density, calc_sqerr of (V_out, rho_out) against the previous iteration's pair
-(src/sqerr_module.f90:38-103) as the convergence test, then Pulay mixing of the spin densities,
-renormalisation per spin, and V_loc of the mixed density for the next iteration.  Occupations
+rsdft_develop_b200.structure builds: per iteration (optionally after a Rayleigh-Ritz step on the
+new potential, the reference's order) one sweep of every spin on the current V_loc,
+occupations, the density of the new bands, V_out = V_ion + V_H + V_xc of that density,
+calc_sqerr of (V_out, rho_out) against the previous iteration's pair
+(src/sqerr_module.f90:38-103) as the convergence test, then mixing (ReferenceMixer restates the
+reference's perform_mixing: simple, Pulay, Broyden or G-space Pulay, of the density or the
+potential), renormalisation per spin, and V_loc of the mixed density for the next iteration.  Occupations
 are the fixed-moment filling of the reference's first NFIXED iterations (src/fermi_module.f90):
 the lowest N_s bands of spin s, N_s = (Nelectron +- Ndspin) / 2 (the reference's O2 sample keeps
 that filling to convergence: its occupations print 1 / 0).  Energies follow calc_total_energy
@@ -14,8 +17,10 @@ E_kin + E_nl = sum occ e - E_loc and E_loc = int rho_out V_loc of the potential 
 used (the reference evaluates it after calc_density, before the potential is updated).
 
 run_scf_kpoints is the same loop for crystals sampled on k-points (the reference's Si sample):
-Methfessel-Paxton occupations (calc_fermi_mp, EKBT 1e-5, KINTEG 5 by default) on the k weights,
-the density summed over k, the nonlocal energy with the k phases of the projectors.
+Methfessel-Paxton (calc_fermi_mp, EKBT 1e-5, KINTEG 5 by default) or Fermi-Dirac occupations on
+the k weights, the density summed over k (and over ranks when the k-points are split), the
+nonlocal energy with the k phases of the projectors.  Both loops report the Harris-Foulkes
+energy, and to_vrho / restart_setup write and read the reference's vrho restart file.
 
 The band update runs behind a small interface (set_vloc, sweep, density, bands, and optionally
 xc): GpuBands drives the library's CUDA path through the C ABI (band update, density and the
