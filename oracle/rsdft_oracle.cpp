@@ -7,11 +7,15 @@
 // eigenvalues) in tests/, and by the reference's own outputs: on the operator of
 // the reference's O2 sample (PSV pseudopotential, PBE, two spins, 48^3 grid) the
 // converged band energies of these sweeps equal the eigenvalues printed in the
-// reference's eight O2 sample logs (tests/test_pseudo_cpu.py).
+// reference's eight O2 sample logs (tests/test_pseudo_cpu.py), and on the operator of
+// its Si sample (FCC cell, 63 k-points, complex16) those printed in its three Si logs,
+// with the SCF over these sweeps landing on the logged total energies
+// (tests/test_scf_structure_cpu.py, tests/test_si_cpu.py).
 //
 // Restated reference routines (paths relative to the RSDFT_DEVELOP tree):
 //   kinetic stencil + V_loc   src/kinetic/d_kinetic_sol_module.f90:29-292 (and the
-//                             complex flag_nab branch :144-200, z_kinetic_sol_module.f90)
+//                             complex flag_nab branch :144-200, z_kinetic_sol_module.f90;
+//                             non-orthogonal cross terms flag_n12/n23/n31 :351-530)
 //   periodic halo             src/bc/bcset_3_module.f90:15-151 (one rank: wrap)
 //   nonlocal gather/Dij/scatter src/ps_nloc_mr_module.f90:1159-1359
 //                             (KB form src/d_ps_nloc2_op_module.f90:146-288 is the
