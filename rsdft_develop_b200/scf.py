@@ -103,6 +103,47 @@ def calc_fermi_mp(esp: np.ndarray, wbz: np.ndarray, nelec: float, ekbt: float = 
     return occ, ef
 
 
+def calc_fermi_mp_fixed(esp: np.ndarray, wbz: np.ndarray, nelec: float, dspn: float, ekbt: float = 1e-5,
+                        kinteg: int = 5):
+    """The fixed-moment branch of calc_fermi_mp (src/fermi_module.f90:187-238, iterations up to
+    NFIXED with two spins): each spin s has its own Fermi level for N_s = Nelectron / 2 +- Ndspin
+    / 2 electrons (+ for spin 1), found by the same bracket-and-bisect search; occupations carry
+    the k weights (one electron per state).  Returns (occ (2, nk, nb), (ef_up, ef_down))."""
+    esp = np.asarray(esp, np.float64)
+    if esp.shape[0] != 2:
+        raise ValueError("a fixed moment needs two spins")
+    occ = np.zeros_like(esp)
+    efs = []
+    for s in range(2):
+        zne = 0.5 * nelec + (1.0 if s == 0 else -1.0) * 0.5 * dspn
+        e = esp[s:s + 1]
+        w = np.asarray(wbz, np.float64)[None, :, None]
+
+        def nel(ef):
+            return float(np.sum(ff0(kinteg, (e - ef) / ekbt) * w))
+
+        ef = _get_ef(zne, e, np.asarray(wbz), 2)
+        for loop in range(1, 1000001):
+            ef1, ef2 = ef - loop * 0.0004, ef + loop * 0.0004
+            if (zne - nel(ef1)) * (zne - nel(ef2)) <= 0.0:
+                break
+        for _ in range(1000000):
+            ef = 0.5 * (ef1 + ef2)
+            o = ff0(kinteg, (e - ef) / ekbt) * w
+            d = float(o.sum()) - zne
+            if d > 1e-12:
+                ef2 = ef
+            elif d < -1e-12:
+                ef1 = ef
+            else:
+                break
+            if 0.5 * (ef1 + ef2) in (ef1, ef2):      # the bracket cannot shrink further
+                break
+        occ[s] = o[0]
+        efs.append(ef)
+    return occ, tuple(efs)
+
+
 def fermi_dirac(esp: np.ndarray, wbz: np.ndarray, nelec: float, ekbt: float):
     """Fermi-Dirac occupations occ(s, k, n) (weights and 2/nspin included) and the Fermi level:
     fermi_dirac without the fixed-spin branch (src/fermi_dirac_module.f90:11-250): bisection of

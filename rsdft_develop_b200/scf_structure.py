@@ -587,7 +587,7 @@ def nonlocal_energy_k(su: structure.Setup, psi: np.ndarray, occ: np.ndarray, k: 
 def run_scf_kpoints(su: structure.Setup, bands, nsweep: int = 10, diter: int = 100, scf_conv: float = 1e-15,
                     mixing: str = "reference", mmix: int = 4, beta: float = 1.1, ekbt: float = 1e-5,
                     kinteg: int = 5, diag_first: bool = True, kgroup=None, imix: int = 10,
-                    occupations: str = "mp") -> StructureScf:
+                    occupations: str = "mp", nfixed: int = 0) -> StructureScf:
     """calc_scf for a structure set up on k-points (su.structure.kbb / wbz) with the band update
     `bands`: set_vloc(v (nspin, ng)), sweep(n, diag_first) -> esp (nspin, nk, nband),
     density(occ (nspin, nk, nband), weights included) -> rho (nspin, ng), bands(s, k) ->
@@ -600,7 +600,8 @@ def run_scf_kpoints(su: structure.Setup, bands, nsweep: int = 10, diter: int = 1
     BETA = beta, the reference's defaults 10, 4 and 1.1); "linear": x_in + beta (x_out - x_in).
 
     occupations "mp": Methfessel-Paxton of order kinteg (calc_fermi_mp, the reference's
-    default); "fd": Fermi-Dirac (fermi_dirac, MP_VERSION -1) with its entropy term, the free
+    default; with two spins the first nfixed iterations keep the moment Ndspin of the
+    structure, each spin filled to its own level); "fd": Fermi-Dirac (fermi_dirac, MP_VERSION -1) with its entropy term, the free
     energy E - TS in energies["free"].
 
     kgroup: a kparallel.KpointGroup when the k-points are split over ranks; `bands` then holds
@@ -642,6 +643,9 @@ def run_scf_kpoints(su: structure.Setup, bands, nsweep: int = 10, diter: int = 1
         esp = kg.gather_esp(bands.sweep(1, diag_first))
         if occupations == "fd":
             occ, ef = scf.fermi_dirac(esp, wbz, nel, ekbt)
+        elif ns == 2 and it <= nfixed:
+            occ, efs = scf.calc_fermi_mp_fixed(esp, wbz, nel, st.ndspin, ekbt, kinteg)
+            ef = max(efs)
         else:
             occ, ef = scf.calc_fermi_mp(esp, wbz, nel, ekbt, kinteg)
         rho_out = kg.sum(bands.density(occ[:, kl[0]:kl[-1] + 1]))

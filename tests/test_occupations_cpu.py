@@ -107,3 +107,22 @@ def test_si_scf_with_lda():
     pbe = structure.setup(structure.si_crystal(pp, kbb, w, nband=8))
     assert np.max(np.abs(su.vxc - pbe.vxc)) > 1e-3            # a different functional
     assert -8.0 < res.energies["total"] < -7.7
+
+
+def test_fixed_moment_occupations():
+    """calc_fermi_mp's fixed-moment branch: N/2 + dspn/2 electrons in spin 1 and N/2 - dspn/2 in
+    spin 2, each to its own level; on a spectrum with a gap in each spin channel this is the
+    integer filling the O2 loop uses (7 up, 5 down for 12 electrons and a moment of 2)."""
+    rng = np.random.default_rng(7)
+    e = np.sort(rng.uniform(-1.0, 0.0, size=(2, 1, 18)), axis=2)
+    e[0, :, 7:] += 0.5
+    e[1, :, 5:] += 0.5
+    occ, (ef_up, ef_dn) = scf.calc_fermi_mp_fixed(e, np.array([1.0]), 12.0, 2.0)
+    want = np.zeros((2, 1, 18))
+    want[0, 0, :7] = 1.0
+    want[1, 0, :5] = 1.0
+    assert np.max(np.abs(occ - want)) < 1e-12
+    assert e[0, 0, 6] < ef_up < e[0, 0, 7] and e[1, 0, 4] < ef_dn < e[1, 0, 5]
+    e2, w2 = _bands(ns=2, nk=4)
+    occ, _ = scf.calc_fermi_mp_fixed(e2, w2, 7.0, 1.0, 1e-2)
+    assert abs(occ[0].sum() - 4.0) < 1e-10 and abs(occ[1].sum() - 3.0) < 1e-10
